@@ -1,0 +1,191 @@
+/*
+ * xbg.h -- C ABI of the B200-native XBeach_GPU coupled step.
+ *
+ * This header is the drop-in boundary for the reference's per-timestep path:
+ * the host step functions declared in XBeachGPU.h:348-353
+ *     void wavebnd(XBGPUParam, std::vector<Wavebndparam>);        (Wavestep.cu:512)
+ *     void flowbnd(XBGPUParam, slbnd, wndbnd, wavebnd);           (Wave_gpu.cu:1020)
+ *     void wavestep(XBGPUParam);                                   (Wavestep.cu:755)
+ *     void flowstep(XBGPUParam);                                   (Wave_gpu.cu:1106)
+ *     void sedimentstep(XBGPUParam);                               (Wave_gpu.cu:1405)
+ * plus the dt logic and running means of one mainloopGPU iteration
+ * (Wave_gpu.cu:610-757).  The reference keeps its state in ~120 file-scope
+ * device pointers (Wave_gpu.cu:26-241); here the state lives behind an opaque
+ * handle that owns all device memory.  Plain C types only: pointers, sizes,
+ * ints and doubles.
+ *
+ * Conventions
+ *  - Every call returns an int status (XBG_OK or an XBG_ERR_* code); no call
+ *    exits the process (the reference calls exit() from CUDA_CHECK,
+ *    Wavestep.cu:4-18, and on a NaN dt, Wave_gpu.cu:642-647).
+ *  - Grid layout is the reference's: structure of arrays, cell i = ix + iy*nx
+ *    (x cross-shore, offshore boundary at ix = 0), directional fields stored as
+ *    theta-planes f[i + itheta*nx*ny] (Wave_kernel.cu:264).
+ *  - zb is bed depth, positive down; hh = zb + zs (Wave_gpu.cu:2009-2010).
+ *  - Field values are float for an XBG_FP32 handle and double for an XBG_FP64
+ *    handle, except the wet flags (int32).  Time and dt are always double.
+ *  - All device work of a handle is ordered on one handle-owned CUDA stream.
+ *    Calls that return host data synchronise that stream; the others do not.
+ *    One handle must not be used from two host threads at once.
+ */
+#ifndef XBG_H
+#define XBG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define XBG_OK            0
+#define XBG_ERR_ARG       1  /* bad argument or size                          */
+#define XBG_ERR_CUDA      2  /* a CUDA runtime call failed                    */
+#define XBG_ERR_NAN       3  /* dt became 0, inf or NaN: "Model crashed!"     */
+#define XBG_ERR_DT        4  /* initial dt below 1e-8 (Wave_gpu.cu:2670-2677) */
+#define XBG_ERR_TIMEOUT   5  /* a bounded device wait ran out                 */
+#define XBG_ERR_STATE     6  /* call out of order (e.g. no wave boundary set) */
+#define XBG_ERR_NOMEM     7  /* device allocation failed                      */
+#define XBG_ERR_BOUNDARY  8  /* time ran past the last uploaded boundary data */
+
+#define XBG_FP32 0
+#define XBG_FP64 1
+
+/* ---- parameters (XBGPUParam, XBeachGPU.h:62-154) ------------------------
+ * Angles are in radians (the parameter file gives degrees and read_input.cpp
+ * converts them).  xbg_params_default() fills the reference defaults;
+ * xbg_params_sanity() applies the cross-parameter rules of checkparamsanity
+ * (read_input.cpp:1227-1443) that bear on the step path.                    */
+typedef struct xbg_params {
+    int    nx, ny;          /* grid size                                    */
+    double dx;              /* grid spacing [m]                             */
+    int    swave, flow, sedtrans, morphology;
+    double g, rho, eps;     /* gravity, water density, drying height        */
+    double cf, cfsand, cfreef;       /* bottom friction                     */
+    double nuh, nuhfac;     /* viscosity (nuh = smag when usesmago = 1)     */
+    int    usesmago;
+    double smag;
+    double lat, fc, Cd;     /* latitude [rad], Coriolis, wind drag          */
+    double wci, hwci;       /* wave-current interaction switch, min depth   */
+    int    breakmodel;      /* 1 Roelvink, 2 Baldock                        */
+    double gammaa, n, alpha, gammax, beta;
+    double fw, fwsand, fwreef;
+    int    roller;          /* roller model on/off                          */
+    double thetamin, thetamax, dtheta;   /* directional bins [rad]          */
+    int    ntheta;
+    double D50, D90, rhosed, wws, drydzmax, wetdzmax, maxslpchg, por,
+           morfac, sus, bed, facsk, facas;
+    int    wavebndtype;     /* 1 constant records, >=2 wave-group chunks    */
+    double CFL, sedstart, outputtimestep, endtime;
+    double dtbc, rtlength;  /* wave-group record step and chunk length [s]  */
+    int    means;           /* accumulate running means every step (1)      */
+} xbg_params;
+
+void xbg_params_default(xbg_params* p);
+/* endbnd: time of the last boundary record (min over sea level, wind and
+ * wave series), used to clamp endtime as checkparamsanity does.           */
+int  xbg_params_sanity(xbg_params* p, double endbnd);
+
+/* ---- fields ------------------------------------------------------------- */
+enum xbg_field {
+    XBG_F_ZB = 0, XBG_F_ZS, XBG_F_HH, XBG_F_UU, XBG_F_VV,
+    XBG_F_HU, XBG_F_HV, XBG_F_HUM, XBG_F_HVM, XBG_F_QX, XBG_F_QY,
+    XBG_F_UEU, XBG_F_VEV, XBG_F_VMAGEU, XBG_F_VMAGEV, XBG_F_VU, XBG_F_UV,
+    XBG_F_UUOLD, XBG_F_VVOLD, XBG_F_ZSOLD, XBG_F_DZSDT,
+    XBG_F_H, XBG_F_E, XBG_F_D, XBG_F_DR, XBG_F_R,
+    XBG_F_K, XBG_F_C, XBG_F_CG, XBG_F_FX, XBG_F_FY, XBG_F_URMS, XBG_F_UST,
+    XBG_F_THETAMEAN, XBG_F_CFM, XBG_F_FWM,
+    XBG_F_CC, XBG_F_CEQSG, XBG_F_STDEP, XBG_F_DZB, XBG_F_ROLTHICK, XBG_F_KTURB,
+    XBG_F_HMEAN, XBG_F_UUMEAN, XBG_F_VVMEAN, XBG_F_HHMEAN, XBG_F_ZSMEAN,
+    XBG_F_CMEAN, XBG_F_ZSMAX,
+    XBG_F_WETU, XBG_F_WETV,          /* int32 flags                        */
+    XBG_F_UMEANBND,                  /* ny values (ubnd1D running mean)    */
+    XBG_F_EE, XBG_F_RR,              /* nx*ny*ntheta (theta-planes)        */
+    XBG_F_COUNT
+};
+
+/* ---- lifecycle ---------------------------------------------------------- */
+typedef struct xbg_handle xbg_handle;
+
+/* Allocates all device state for p (after xbg_params_sanity) on the current
+ * CUDA device and sets the reference's initial condition for the constant
+ * parts (theta bins Wavestep.cu:79-86; Wave_gpu.cu:1988-2015, 2187-2510).
+ * Fields are zero until set with xbg_set_field / xbg_init_state.          */
+int  xbg_create(const xbg_params* p, int precision, xbg_handle** out);
+int  xbg_destroy(xbg_handle* h);
+const char* xbg_status_string(int status);
+
+/* Reference initial state from bathymetry zb and the first sea-level record
+ * (Wave_gpu.cu:1988-2015, 2519-2551, 2637-2692): zs, hh, hu/hv/hum/hvm = hh,
+ * stdep = 5 m, cfm/fwm by updatezom, initial dt = 0.5*min(0.5*CFL*dx/sqrt(g h)),
+ * ee column 0 from the first boundary record.  zb: nx*ny host values.      */
+int  xbg_init_state(xbg_handle* h, const void* zb, double zs0, double zs1);
+
+/* ---- state IO ----------------------------------------------------------- */
+int  xbg_field_count(const xbg_handle* h, int field, size_t* count);
+int  xbg_set_field(xbg_handle* h, int field, const void* host, size_t count);
+int  xbg_get_field(xbg_handle* h, int field, void* host, size_t count);
+/* Zero-copy access: the device pointer of a field (owned by the handle). */
+int  xbg_field_device_ptr(xbg_handle* h, int field, void** dptr, size_t* count);
+
+/* ---- boundaries ----------------------------------------------------------
+ * Wave boundary data of one chunk: St[nrec][ntheta][ny] (Stfile layout
+ * Wavestep.cu:703-706) and qbnd[nrec][4][ny] (qfile layout :709-712), with
+ * record times t0 + m*dtbc (wavebndtype >= 2) or times[m] (wavebndtype 1).
+ * Trep: representative period of the chunk.  The per-step interpolation of
+ * wavebnd (Wavestep.cu:684-741) runs on the device.  A second chunk may be
+ * queued while the first is in use (slot = 0 current, 1 next).            */
+int  xbg_set_wave_boundary(xbg_handle* h, int slot, const double* St,
+                           const double* qbnd, int nrec, const double* times,
+                           double t0, double tend, double Trep);
+/* Sea-level records (time, wlev0, wlev1) and wind records (time, U, V),
+ * interpolated on the device each step as flowbnd does
+ * (Wave_gpu.cu:1020-1103).                                                 */
+int  xbg_set_sealevel(xbg_handle* h, const double* time, const double* wlev0,
+                      const double* wlev1, int n);
+int  xbg_set_wind(xbg_handle* h, const double* time, const double* U,
+                  const double* V, int n);
+
+/* ---- stepping ----------------------------------------------------------
+ * The pieces of one mainloopGPU iteration, in the reference's order.  Each
+ * enqueues device work only; dt and time live on the device.             */
+int  xbg_compute_dt(xbg_handle* h);        /* Wave_gpu.cu:620-698          */
+int  xbg_wave_boundary(xbg_handle* h);     /* wavebnd, Wavestep.cu:512     */
+int  xbg_flow_boundary(xbg_handle* h);     /* flowbnd, Wave_gpu.cu:1020    */
+int  xbg_wave_step(xbg_handle* h);         /* wavestep, Wavestep.cu:755    */
+int  xbg_flow_step(xbg_handle* h);         /* flowstep, Wave_gpu.cu:1106   */
+int  xbg_sediment_step(xbg_handle* h);     /* sedimentstep, :1405 (runs only
+                                              when sedtrans=1, t>=sedstart) */
+int  xbg_accumulate_means(xbg_handle* h);  /* Wave_gpu.cu:731-757          */
+/* One whole coupled step (all of the above), replayed from a CUDA graph. */
+int  xbg_step(xbg_handle* h);
+/* Up to nsteps coupled steps; steps after the device reaches endtime, an
+ * output time or an error are skipped on the device.  Does not synchronise. */
+int  xbg_advance(xbg_handle* h, int nsteps);
+/* Synchronise and read time, dt, step count and the device status word.  */
+int  xbg_get_time(xbg_handle* h, double* totaltime, double* dt, int64_t* nstep,
+                  int* flags);
+#define XBG_FLAG_OUTPUT_DUE   1   /* nextoutputtime reached               */
+#define XBG_FLAG_ENDED        2   /* totaltime >= endtime                 */
+#define XBG_FLAG_NEED_BOUNDARY 4  /* next wave-boundary chunk consumed    */
+/* Output bookkeeping of mainloopGPU (Wave_gpu.cu:784-930): divide the means
+ * by the step count, advance nextoutputtime; xbg_reset_means clears them. */
+int  xbg_output_done(xbg_handle* h);
+int  xbg_reset_means(xbg_handle* h);
+/* Set time and dt directly (e.g. to replay a fixed-dt sequence). */
+int  xbg_set_time(xbg_handle* h, double totaltime, double dt, double wdt);
+int  xbg_sync(xbg_handle* h);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* Number of kernel launches this handle has enqueued since creation. */
+int  xbg_launch_count(const xbg_handle* h, int64_t* count);
+/* Device-side water and sediment ledgers (sum zs*dx^2, sum (C*h) dx^2,
+ * sum zb dx^2) in double, computed on the device.                         */
+int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,
+              double* bed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XBG_H */
