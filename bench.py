@@ -1,0 +1,309 @@
+"""Coupled cell-updates/s of the XBeach_GPU coupled step on B200.
+
+Workload: the large single domain (barred beach, nx=2048 x ny=1024, dx=2 m,
+18 directional bins over -90..90 deg, JONSWAP-shaped wave-group forcing,
+sediment with morfac 10), FP32, seeded synthetic inputs.  One step = one
+whole coupled timestep (dt, boundaries, wave action, shallow-water flow,
+sediment and bed, running means) over every cell, replayed from the CUDA
+graph of libxbg_b200.so.  Multi-GPU: independent replicas (the path has no
+exchange step), value = cells * steps * ranks / max-over-ranks time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Prints one JSON line (rank 0).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+B_ALGO = lambda nt: 4 * (77 + 4 * nt)   # algorithmic bytes per coupled cell-update
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--nx", type=int, default=2048)
+    ap.add_argument("--ny", type=int, default=1024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def setup_model(nx, ny, seed=0):
+    from xbeach_gpu_b200.model import Model
+    from xbeach_gpu_b200.scenarios import make_case
+    p, zb, bnd = make_case("barred_beach", seed=seed, nx=nx, ny=ny)
+    m = Model(p)
+    m.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.init_state(zb, 0.0, 0.0)
+    return p, m, bnd
+
+
+def cpu_baseline_port(nx_full, ny_full, seconds=12.0):
+    """The oracle (CPU restatement, serial) on a 256 x 128 crop of the same
+    barred-beach workload, run for a bounded time: cell-updates/s, 1 core."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from xbeach_gpu_b200.scenarios import make_case
+    nx, ny = 256, 128
+    p, zb, bnd = make_case("barred_beach", nx=nx, ny=ny)
+    o = pyoracle.Oracle(p)
+    o.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    o.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    o.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    o.init_state(zb, 0.0, 0.0)
+    o.advance(2)
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < seconds:
+        o.advance(2)
+        n += 2
+    el = time.perf_counter() - t0
+    return {"value": nx * ny * n / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "sample": f"oracle restatement, serial, barred beach crop {nx}x{ny} ntheta={p.ntheta}, "
+                      f"{n} coupled steps in {el:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU code (wave_CPU.cpp and its flow
+    and sediment kernels run on the CPU, oracle/_ref) on the host cores."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from xbeach_gpu_b200.scenarios import make_case
+    if not pyoracle.ref_available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libxbg_ref.so not built (needs the reference checkout at build time)"}
+    nx, ny = 256, 128
+    p, zb, bnd = make_case("barred_beach", nx=nx, ny=ny)
+    o = pyoracle.Oracle(p)   # prepares a physically consistent state
+    o.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    o.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    o.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    o.init_state(zb, 0.0, 0.0)
+    o.advance(3)
+    r = pyoracle.RefEmu(p)
+    from xbeach_gpu_b200.abi import FIELD_NAMES
+    for n in FIELD_NAMES:
+        r.set(n, o.get(n))
+    t, dt, _, _, _ = o.time()
+    nb = int(t // p.dtbc)
+    St = bnd["St"][nb].astype(np.float32)
+    per_step = []
+    steps = args.steps + args.warmup
+    for k in range(steps):
+        r.step_inputs(dt, t + k * dt, np.float32(bnd["Trep"]), St, bnd["q"][nb].astype(np.float32),
+                      bnd["q"][nb + 1].astype(np.float32), 0.5, 1.0, 0.0, 0.0, 0.0, 0.0)
+        t0 = time.perf_counter()
+        for call in ("wave_step", "flow_boundary", "flow_step", "sediment_step"):
+            r.call(call)
+        per_step.append(time.perf_counter() - t0)
+        if sum(per_step) > 60.0:
+            break
+    timed = per_step[min(args.warmup, len(per_step) - 1):]
+    el = float(np.sum(timed))
+    v = nx * ny * len(timed) / el
+    sample = (f"reference wave_CPU.cpp + reference flow/sediment kernels on the CPU (serial), barred beach "
+              f"crop {nx}x{ny} ntheta={p.ntheta}, {len(timed)} timed steps")
+    return {"metric": "coupled cell-updates/s", "value": v, "unit": "cell-updates/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": len(timed), "warmup": args.warmup, "ms_per_step": 1e3 * el / len(timed),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded barred beach)",
+            "config": {"workload": f"barred_beach {args.nx}x{args.ny} ntheta=18 (sample {nx}x{ny})"},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_
+        dist = dist_
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.impl == "reference":
+        out = run_reference(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+    import torch
+    torch.cuda.set_device(local)
+    p, m, bnd = setup_model(args.nx, args.ny, seed=rank)
+    C = p.nx * p.ny
+    stream = torch.cuda.ExternalStream(m.stream())
+    W = max(3, args.warmup)
+    K = args.steps
+    m.advance(W)
+    m.sync()
+    launches0 = m.launches()
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    m.advance(K)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    t_end, dt_end, nstep, flags, rc = m.time()
+    if rc != 0:
+        raise RuntimeError(f"device status {rc} after the timed steps")
+    launches = m.launches() - launches0
+    # per-kernel times of full steps (events between launches), for the roofline
+    prof = {}
+    for _ in range(5):
+        for name, t in m.profile_step():
+            prof.setdefault(name, []).append(t)
+    kern = {k: float(np.mean(v)) for k, v in prof.items()}
+    # end to end through the C ABI with host buffers: every step streams the
+    # boundary records it interpolates from pinned host memory and reads the
+    # step's clock (time, dt, status) back to the host
+    nyt = p.ny * p.ntheta
+    recs = torch.empty((2, nyt), dtype=torch.float32, pin_memory=True)
+    qrec = torch.empty((2, 4 * p.ny), dtype=torch.float32, pin_memory=True)
+    Ke = max(10, K // 4)
+    t0 = time.perf_counter()
+    for k in range(Ke):
+        t_now = m.time()[0]
+        nb = int(t_now // p.dtbc)
+        recs.numpy()[:] = bnd["St"][nb:nb + 2].reshape(2, -1)
+        qrec.numpy()[:] = bnd["q"][nb:nb + 2].reshape(2, -1)
+        m.put_wave_records(0, nb, recs.numpy(), qrec.numpy())
+        m.step()
+    _, _, _, _, rc = m.time()
+    e2e_s = time.perf_counter() - t0
+    h2d = recs.numel() * 4 + qrec.numel() * 4
+    d2h = 232   # the device clock struct read by xbg_get_time
+    # max over ranks
+    if dist:
+        tt = torch.tensor([ms, e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(tt[0]), float(tt[1])
+    value = C * K * world / (ms / 1e3)
+    e2e = C * Ke * world / e2e_s
+    peak, peak_kind = peaks()
+    # dominant kernel: the fused wave-action kernel
+    dom = max(kern, key=kern.get)
+    nt = p.ntheta
+    algo_dom = {"k_wave_main": 4 * (4 * nt + 16)}.get(dom, None)
+    rows = p.ny - 2 if dom == "k_wave_main" else p.ny
+    roof = None
+    if algo_dom:
+        achieved = algo_dom * p.nx * rows / (kern[dom] / 1e3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "algorithmic_bytes_per_cell": algo_dom, "ms_per_launch": kern[dom]}
+    step_gbs = B_ALGO(nt) * C * K / (ms / 1e3) / 1e9
+    out = {
+        "metric": "coupled cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded barred beach, JONSWAP-shaped groups)",
+        "config": {"workload": f"barred_beach {p.nx}x{p.ny} ntheta={nt} (large single domain)",
+                   "nx": p.nx, "ny": p.ny, "ntheta": nt, "cells": C, "parallelism": f"replicas x{world}",
+                   "l2": "state ~2 GB per GPU, larger than the 126 MB L2 (no flush needed)",
+                   "sim_time_s": t_end},
+        "roofline": roof,
+        "roofline_step": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
+                          "frac": step_gbs / peak, "algorithmic_bytes_per_cell_update": B_ALGO(nt),
+                          "peak_kind": peak_kind},
+        "kernels_ms": kern,
+        "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline_port(p.nx, p.ny)
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"unavailable": str(e)}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    m.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -139,6 +139,12 @@ int  xbg_field_device_ptr(xbg_handle* h, int field, void** dptr, size_t* count);
 int  xbg_set_wave_boundary(xbg_handle* h, int slot, const double* St,
                            const double* qbnd, int nrec, const double* times,
                            double t0, double tend, double Trep);
+/* Overwrite records [first, first+n) of a queued or current chunk from host
+ * memory in the handle's element type (float for XBG_FP32), stream-ordered
+ * and without synchronising: boundary records streamed while the model runs.
+ * St: n*ntheta*ny values, q: n*4*ny values.                                */
+int  xbg_put_wave_records(xbg_handle* h, int slot, int first, int n,
+                          const void* St, const void* q);
 /* Sea-level records (time, wlev0, wlev1) and wind records (time, U, V),
  * interpolated on the device each step as flowbnd does
  * (Wave_gpu.cu:1020-1103).                                                 */
@@ -180,6 +186,13 @@ int  xbg_sync(xbg_handle* h);
 /* ---- diagnostics -------------------------------------------------------- */
 /* Number of kernel launches this handle has enqueued since creation. */
 int  xbg_launch_count(const xbg_handle* h, int64_t* count);
+/* The handle's CUDA stream (a cudaStream_t), for callers that time or order
+ * their own work against the model's. */
+int  xbg_get_stream(xbg_handle* h, void** stream);
+/* Run one coupled step without the graph, with a CUDA event after every
+ * kernel; returns each kernel's duration [ms] and name.  *n: in = capacity,
+ * out = kernels run.                                                      */
+int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
 /* Device-side water and sediment ledgers (sum zs*dx^2, sum (C*h) dx^2,
  * sum zb dx^2) in double, computed on the device.                         */
 int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,

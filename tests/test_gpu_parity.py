@@ -1,0 +1,159 @@
+"""CUDA path (through the C ABI) against the oracle and the reference's golden
+vectors.
+
+Tolerance: relative field error max|a-b| / max|b| <= 1e-5 per phase in FP32
+(the FP32 bar of the north star), <= 1e-12 in FP64; integer wet flags exact.
+"""
+import numpy as np
+import pytest
+
+import golden_replay as gr
+import pyoracle
+from helpers import (FLOW_OUT, FLOWBND_OUT, MEANS_OUT, SED_OUT, WAVE_OUT, random_inputs, rel_err,
+                     small_params)
+from xbeach_gpu_b200.abi import XBG_FP32, XBG_FP64, XBG_FLAG_ENDED
+from xbeach_gpu_b200.model import Model
+from xbeach_gpu_b200.scenarios import make_case
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-5
+TOL64 = 1e-12
+
+
+def _cmp(a_handle, b, names, tol, what, prefix=None):
+    bad = []
+    for n in names:
+        a = a_handle.get(n)
+        bb = b[f"{prefix}_{n}"] if prefix else b.get(n)
+        if n in ("wetu", "wetv"):
+            if not np.array_equal(a, bb):
+                bad.append((n, "flags differ"))
+            continue
+        e = rel_err(a, bb)
+        if not e <= tol:
+            bad.append((n, e))
+    assert not bad, f"{what}: {bad}"
+
+
+@pytest.mark.parametrize("name", sorted(gr.CASES))
+def test_golden_phases(name):
+    """Each phase of the CUDA step against the reference's own outputs."""
+    p, m, g = gr.setup(Model, name)
+    gr.start_step(m, p)
+    m.wave_boundary()
+    for tag, call, outs in gr.PHASES:
+        getattr(m, call)()
+        _cmp(m, g, outs, TOL32, f"{name} {tag}", prefix=tag)
+
+
+VARIANTS = {
+    "default": dict(kw={}, steep=False),
+    "baldock": dict(kw=dict(breakmodel=2), steep=False),
+    "wci": dict(kw=dict(wci=1.0, hwci=0.5), steep=False),
+    "noroller": dict(kw=dict(roller=0), steep=False),
+    "nowaves": dict(kw=dict(swave=0), steep=False),
+    "steep": dict(kw=dict(morfac=10.0), steep=True),
+    "nosmago": dict(kw=dict(usesmago=0, nuh=0.7), steep=False),
+}
+
+
+def _pair(variant, seed, precision, nx=45, ny=29, ntheta=7):
+    v = VARIANTS[variant]
+    p, bnd = small_params(nx, ny, ntheta, **v["kw"])
+    f = random_inputs(p, seed, steep=v["steep"])
+    hs = [Model(p, precision), pyoracle.Oracle(p, precision)]
+    for h in hs:
+        for k, val in f.items():
+            h.set(k, val)
+        h.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+        h.set_sealevel([0.0, 1e6], [0.05, 0.05], [0.2, 0.2])
+        h.set_wind([0.0, 1e6], [-3.0, -3.0], [2.0, 2.0])
+        h.set_time(151.7, 0.27, 0.27)
+    return p, hs[0], hs[1]
+
+
+@pytest.mark.parametrize("precision", [XBG_FP32, XBG_FP64])
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
+def test_phases_vs_oracle(variant, precision):
+    tol = TOL32 if precision == XBG_FP32 else TOL64
+    p, m, o = _pair(variant, 5, precision)
+    for h in (m, o):
+        if p.swave == 1:
+            h.call("wave_boundary")
+    if p.swave == 1:
+        m.wave_step(); o.call("wave_step")
+        _cmp(m, o, WAVE_OUT, tol, f"{variant} wave")
+    m.flow_boundary(); o.call("flow_boundary")
+    _cmp(m, o, FLOWBND_OUT, tol, f"{variant} flowbnd")
+    m.flow_step(); o.call("flow_step")
+    _cmp(m, o, FLOW_OUT, tol, f"{variant} flow")
+    m.sediment_step(); o.call("sediment_step")
+    _cmp(m, o, SED_OUT, tol, f"{variant} sediment")
+    m.accumulate_means(); o.call("accumulate_means")
+    _cmp(m, o, MEANS_OUT, tol, f"{variant} means")
+
+
+def _beach(nx, ny, ntheta, precision=XBG_FP32, **kw):
+    p, zb, bnd = make_case("linear_beach", nx=nx, ny=ny, ntheta=ntheta)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    hs = [Model(p, precision), pyoracle.Oracle(p, precision)]
+    for h in hs:
+        h.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+        h.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        h.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        h.init_state(zb, 0.0, 0.0)
+    return p, hs[0], hs[1]
+
+
+def test_multistep_graph_vs_oracle():
+    """Whole coupled steps replayed from the CUDA graph against the oracle's
+    step-by-step run: time and dt agree and fields stay within the FP32 bar."""
+    p, m, o = _beach(64, 32, 10, sedstart=0.0)
+    for chunk in range(4):
+        m.advance(25)
+        o.advance(25)
+        tm, dtm, nm, _, rcm = m.time()
+        to, dto, no, _, rco = o.time()
+        assert rcm == 0 and rco == 0
+        assert nm == no
+        assert abs(tm - to) <= 1e-9 * max(1.0, to) and abs(dtm - dto) <= 1e-6 * dto
+    # after many steps, differences of a few ulps per step (transcendental
+    # functions, the tree-summed ubnd1D column mean) grow; the bar for a
+    # whole run is 1e-3 on H, zs, u, v, zb
+    errs = {n: rel_err(m.get(n), o.get(n)) for n in ["H", "zs", "uu", "vv", "zb", "ee", "rr", "C", "hh"]}
+    bad = {n: e for n, e in errs.items() if not e <= 1e-3}
+    assert not bad, errs
+
+
+def test_full_run_linear_beach():
+    """The reference's CPU-runnable case (200 x 100, 10 bins, 600 s): final
+    H, zs, u, v, zb within 1e-3 of the oracle."""
+    p, m, o = _beach(200, 100, 10, sedstart=0.0, endtime=600.0, outputtimestep=600.0)
+    for _ in range(200):
+        m.advance(50)
+        t, _, _, fl, rc = m.time()
+        assert rc == 0
+        if fl & XBG_FLAG_ENDED:
+            break
+    while True:
+        o.advance(500)
+        t2, _, _, fl2, rc2 = o.time()
+        assert rc2 == 0
+        if fl2 & XBG_FLAG_ENDED:
+            break
+    assert abs(t - 600.0) < 1e-6 and abs(t2 - 600.0) < 1e-6
+    assert m.time()[2] == o.time()[2]
+    for n in ["H", "zs", "uu", "vv", "zb"]:
+        assert rel_err(m.get(n), o.get(n)) <= 1e-3, n
+
+
+def test_deterministic():
+    runs = []
+    for _ in range(2):
+        p, m, o = _beach(64, 32, 10, sedstart=0.0)
+        m.advance(40)
+        runs.append({n: m.get(n).copy() for n in ["ee", "rr", "zs", "uu", "vv", "zb", "C"]})
+    for n in runs[0]:
+        assert np.array_equal(runs[0][n], runs[1][n]), n

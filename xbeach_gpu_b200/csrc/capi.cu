@@ -1,0 +1,607 @@
+// capi.cu -- host side of the C ABI declared in include/xbg.h.
+//
+// One handle owns every device buffer of one model, one CUDA stream and one
+// captured CUDA graph of a whole coupled step.  Nothing here synchronises the
+// stream except the calls that return host data (get_field, get_time, mass)
+// and the boundary upload, which must know which chunk slot is in use.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstring>
+#include <cstdio>
+#include <vector>
+#include <algorithm>
+#include "xbg_common.cuh"
+#include "../../include/xbg.h"
+
+namespace xbg {
+template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int wave_parts(const Konst<R>&);
+template <class R> int wave_prepare(const Konst<R>&);
+template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int step_begin_blocks(const Konst<R>&);
+template <class R> int launch_step_begin(const Dev<R>&, const Konst<R>&, const Series*, int, cudaStream_t, Prof*);
+template <class R> int launch_ubnd(const Dev<R>&, const Konst<R>&, const Series*, cudaStream_t, Prof*);
+template <class R> int launch_wavebnd(const Dev<R>&, const Konst<R>&, const Series*, cudaStream_t, Prof*, int);
+template <class R> int launch_means(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> void launch_output_done(const Dev<R>&, const Konst<R>&, cudaStream_t);
+template <class R> void launch_reset_means(const Dev<R>&, cudaStream_t);
+template <class R> void launch_mass(const Dev<R>&, double, double*, cudaStream_t);
+
+template <class R>
+__global__ void k_set_slot(Clock* c, int logical, int nrec, double t0, double tend, double Trep) {
+    int phys = logical == 0 ? c->cur_slot : (c->cur_slot ^ 1);
+    c->slot_valid[phys] = 1;
+    c->slot_nrec[phys] = nrec;
+    c->slot_t0[phys] = t0;
+    c->slot_tend[phys] = tend;
+    c->slot_Trep[phys] = Trep;
+    if (logical == 1) c->flags &= ~XBG_FLAG_NEED_BOUNDARY;
+}
+}  // namespace xbg
+
+using namespace xbg;
+
+// ------------------------------------------------------------------ params
+extern "C" void xbg_params_default(xbg_params* p) {   // XBeachGPU.h:62-154
+    std::memset(p, 0, sizeof(*p));
+    p->swave = 1; p->flow = 1; p->sedtrans = 0; p->morphology = 0;
+    p->g = 9.81; p->rho = 1025.0; p->eps = 0.01;
+    p->cf = 0.01; p->cfsand = 0.0; p->cfreef = 0.0;
+    p->nuh = 1.0; p->nuhfac = 1.0; p->usesmago = 1; p->smag = 0.3;
+    p->lat = 0.0; p->fc = 0.0; p->Cd = 0.002; p->wci = 0.0; p->hwci = 0.1;
+    p->breakmodel = 1; p->gammaa = 0.6; p->n = 8.0; p->alpha = 1.0; p->gammax = 2.0; p->beta = 0.15;
+    p->fw = 0.001; p->fwsand = 0.0; p->fwreef = 0.0;
+    p->roller = 1;
+    p->thetamin = -90 * 3.14159265 / 180; p->thetamax = 90 * 3.14159265 / 180;
+    p->dtheta = 0.0; p->ntheta = 0;
+    p->D50 = 0.00038; p->D90 = 0.00053; p->rhosed = 2650.0; p->wws = 0.0509;
+    p->drydzmax = 1.0; p->wetdzmax = 0.3; p->maxslpchg = 0.01; p->por = 0.4; p->morfac = 1.0;
+    p->sus = 1.0; p->bed = 1.0; p->facsk = 0.2; p->facas = 0.2;
+    p->wavebndtype = 2;
+    p->CFL = 0.7; p->sedstart = 3600.0; p->outputtimestep = 0.0; p->endtime = 0.0;
+    p->dtbc = 1.0; p->rtlength = 3600.0;
+    p->means = 1;
+}
+
+// checkparamsanity (read_input.cpp:1227-1443, the step-path rules), the
+// theta bins of waveinitGPU (Wavestep.cu:33-45) and the Coriolis parameter
+// (Wave_gpu.cu:2060-2064).
+extern "C" int xbg_params_sanity(xbg_params* p, double endbnd) {
+    const double tiny = 0.0000001;
+    if (p->nx <= 0 || p->ny <= 0 || p->dx < tiny) return XBG_ERR_ARG;
+    if (std::fabs(p->endtime - 0.0) <= tiny) p->endtime = 1.0 / tiny;
+    p->endtime = std::min(p->endtime, endbnd);
+    if (p->swave == 0) { p->ntheta = 1; p->dtheta = p->thetamax - p->thetamin; }
+    if (std::fabs(p->outputtimestep) <= tiny) p->outputtimestep = p->endtime;
+    if (std::fabs(p->cfsand) < tiny) { if (p->cf < tiny) p->cf = tiny; p->cfsand = p->cf; }
+    if (std::fabs(p->cfreef) < tiny) p->cfreef = p->cfsand;
+    if (std::fabs(p->fwsand) < tiny) { if (p->fw < tiny) p->fw = tiny; p->fwsand = p->fw; }
+    if (std::fabs(p->fwreef) < tiny) p->fwreef = p->fwsand;
+    if (p->usesmago == 1) p->nuh = p->smag;
+    if (p->swave == 1) {
+        if (p->dtheta > 0.0) p->ntheta = (int)std::round((p->thetamax - p->thetamin) / p->dtheta);
+        else { if (p->ntheta == 0) p->ntheta = 1; p->dtheta = (p->thetamax - p->thetamin) / p->ntheta; }
+    }
+    double wearth = 3.14159265 * (1.0 / 24.0) / 1800.0;
+    p->fc = 2.0 * wearth * std::sin(p->lat);
+    return XBG_OK;
+}
+
+extern "C" const char* xbg_status_string(int s) {
+    switch (s) {
+        case XBG_OK: return "ok";
+        case XBG_ERR_ARG: return "bad argument";
+        case XBG_ERR_CUDA: return "CUDA error";
+        case XBG_ERR_NAN: return "model crashed: dt is 0, inf or NaN";
+        case XBG_ERR_DT: return "initial time step below 1e-8";
+        case XBG_ERR_TIMEOUT: return "device wait timed out";
+        case XBG_ERR_STATE: return "call out of order";
+        case XBG_ERR_NOMEM: return "out of device memory";
+        case XBG_ERR_BOUNDARY: return "ran past the uploaded wave boundary";
+    }
+    return "unknown status";
+}
+
+// ------------------------------------------------------------------ handle
+struct xbg_handle {
+    virtual ~xbg_handle() {}
+    xbg_params P;
+    int precision = XBG_FP32;
+    int64_t launches = 0;
+    virtual int init_state(const void* zb, double zs0, double zs1) = 0;
+    virtual int field_count(int f, size_t* n) = 0;
+    virtual int set_field(int f, const void* p, size_t n) = 0;
+    virtual int get_field(int f, void* p, size_t n) = 0;
+    virtual int device_ptr(int f, void** p, size_t* n) = 0;
+    virtual int set_wave_boundary(int slot, const double* St, const double* q, int nrec,
+                                  const double* times, double t0, double tend, double Trep) = 0;
+    virtual int set_series(int which, const double* t, const double* a, const double* b, int n) = 0;
+    virtual int piece(int which) = 0;
+    virtual int step(int nsteps) = 0;
+    virtual int get_time(double* t, double* dt, int64_t* n, int* flags) = 0;
+    virtual int set_time(double t, double dt, double wdt) = 0;
+    virtual int output_done() = 0;
+    virtual int reset_means() = 0;
+    virtual int mass(double* w, double* s, double* b) = 0;
+    virtual int sync() = 0;
+    virtual void* stream() = 0;
+    virtual int profile(float* ms, const char** names, int* n) = 0;
+    virtual int put_wave_records(int slot, int first, int n, const void* St, const void* q) = 0;
+};
+
+namespace {
+
+#define CK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { last_err = e_; return e_ == cudaErrorMemoryAllocation ? XBG_ERR_NOMEM : XBG_ERR_CUDA; } } while (0)
+
+template <class R>
+struct Handle : public xbg_handle {
+    Dev<R> S;
+    Konst<R> K;
+    Clock* clk = nullptr;
+    Series* ser = nullptr;
+    R* zsold_buf[2] = {nullptr, nullptr};
+    R* ee_buf[2] = {nullptr, nullptr};
+    R* rr_buf[2] = {nullptr, nullptr};
+    size_t slot_cap = 0;        // elements of St per slot
+    std::vector<void*> allocs;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int per_step_launches = 0;
+    int nwave = 0;
+    cudaError_t last_err = cudaSuccess;
+    double* mass_buf = nullptr;
+
+    template <class T> int alloc(T** p, size_t n) {
+        void* q = nullptr;
+        if (n == 0) n = 1;
+        CK(cudaMalloc(&q, n * sizeof(T)));
+        CK(cudaMemsetAsync(q, 0, n * sizeof(T), st));
+        allocs.push_back(q);
+        *p = (T*)q;
+        return XBG_OK;
+    }
+
+    int setup(const xbg_params* p, int prec) {
+        P = *p;
+        precision = prec;
+        int nx = P.nx, ny = P.ny, nt = P.ntheta;
+        if (nx < 4 || ny < 4 || nt < 1 || nt > XBG_MAX_THETA) return XBG_ERR_ARG;
+        size_t C = (size_t)nx * ny;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        std::memset(&S, 0, sizeof(S));
+        S.nx = nx; S.ny = ny; S.nt = nt; S.C = (int)C;
+        int rc;
+        for (int f = 0; f < NF2D; f++) if ((rc = alloc(&S.f[f], C))) return rc;
+        for (int f = 0; f < NTMP; f++) if ((rc = alloc(&S.tmp[f], C))) return rc;
+        if ((rc = alloc(&S.wetu, C)) || (rc = alloc(&S.wetv, C)) || (rc = alloc(&S.umeanbnd, (size_t)ny))) return rc;
+        for (int k = 0; k < 2; k++) {
+            if ((rc = alloc(&ee_buf[k], C * nt)) || (rc = alloc(&rr_buf[k], C * nt)) || (rc = alloc(&zsold_buf[k], C)))
+                return rc;
+            S.ee[k] = ee_buf[k]; S.rr[k] = rr_buf[k]; S.zsold[k] = zsold_buf[k];
+        }
+        if ((rc = alloc(&S.edge, (size_t)4 * nx * nt)) || (rc = alloc(&S.St, (size_t)ny * nt))) return rc;
+        // K
+        std::memset(&K, 0, sizeof(K));
+        K.nx = nx; K.ny = ny; K.nt = nt;
+        K.swave = P.swave; K.flow = P.flow; K.roller = P.roller; K.breakmodel = P.breakmodel;
+        K.usesmago = P.usesmago; K.wavebndtype = P.wavebndtype; K.means = P.means;
+        K.dx = (R)P.dx; K.eps = (R)P.eps; K.g = (R)P.g; K.rho = (R)P.rho; K.cfl = (R)P.CFL;
+        K.dtheta = (R)P.dtheta; K.gammax = (R)P.gammax; K.gammaa = (R)P.gammaa; K.alpha = (R)P.alpha;
+        K.nexp = (R)P.n; K.beta = (R)P.beta; K.wci = (R)P.wci; K.hwci = (R)P.hwci;
+        K.nuh = (R)P.nuh; K.nuhfac = (R)P.nuhfac; K.fc = (R)P.fc; K.Cd = (R)P.Cd;
+        K.D50 = (R)P.D50; K.D90 = (R)P.D90; K.rhosed = (R)P.rhosed; K.wws = (R)P.wws;
+        K.drydzmax = (R)P.drydzmax; K.wetdzmax = (R)P.wetdzmax; K.maxslpchg = (R)P.maxslpchg;
+        K.por = (R)P.por; K.morfac = (R)P.morfac; K.sus = (R)P.sus; K.facsk = (R)P.facsk;
+        K.facas = (R)P.facas; K.cfsand = (R)P.cfsand; K.cfreef = (R)P.cfreef;
+        K.fwsand = (R)P.fwsand; K.fwreef = (R)P.fwreef;
+        R phi = (R)((1.0f + (R)std::sqrt((R)5.0f)) / 2);
+        K.aphi = 1 / (phi + 1); K.bphi = phi / (phi + 1);
+        K.twopi = 8 * (R)std::atan((R)1.0f);
+        K.endtime = P.endtime; K.outputtimestep = P.outputtimestep; K.sedstart = P.sedstart;
+        K.dtbc = P.dtbc; K.eps_d = P.eps; K.sedtrans = P.sedtrans;
+        for (int i = 0; i < nt; i++) {   // Wavestep.cu:79-86
+            K.theta[i] = (R)(i * (P.dtheta) + P.thetamin + 0.5f * P.dtheta);
+            K.cxsth[i] = (R)std::cos(K.theta[i]);
+            K.sxnth[i] = (R)std::sin(K.theta[i]);
+        }
+        if (wave_prepare(K)) return XBG_ERR_CUDA;
+        // reductions and clock
+        int nflow = step_begin_blocks(K);
+        nwave = wave_parts(K);
+        if ((rc = alloc(&S.part_flow, (size_t)nflow)) || (rc = alloc(&S.part_wave, (size_t)nwave)) ||
+            (rc = alloc(&S.counter, 1)) || (rc = alloc(&clk, 1)) || (rc = alloc(&ser, 1)) ||
+            (rc = alloc(&mass_buf, 3)))
+            return rc;
+        S.clk = clk;
+        std::vector<R> big((size_t)nwave, (R)3.0e38f);
+        CK(cudaMemcpyAsync(S.part_wave, big.data(), nwave * sizeof(R), cudaMemcpyHostToDevice, st));
+        Clock c;
+        std::memset(&c, 0, sizeof(c));
+        c.nextoutputtime = P.outputtimestep;   // Wave_gpu.cu:2959
+        c.WAVstep = 1; c.SLstep = 1; c.WNDstep = 1;
+        c.n_wave_parts = nwave;
+        CK(cudaMemcpyAsync(clk, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return XBG_OK;
+    }
+
+    ~Handle() override {
+        if (st) cudaStreamSynchronize(st);
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        for (void* p : allocs) cudaFree(p);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int host_cur_slot = 0;
+    int read_clock(Clock& c) {
+        CK(cudaStreamSynchronize(st));
+        CK(cudaMemcpy(&c, clk, sizeof(c), cudaMemcpyDeviceToHost));
+        host_cur_slot = c.cur_slot;
+        return XBG_OK;
+    }
+
+    R* field_ptr(int f, size_t* n, int par) {
+        size_t C = (size_t)S.C;
+        *n = C;
+        switch (f) {
+            case XBG_F_EE: *n = C * K.nt; return ee_buf[par];
+            case XBG_F_RR: *n = C * K.nt; return rr_buf[par];
+            case XBG_F_ZSOLD: return zsold_buf[par];
+            case XBG_F_UMEANBND: *n = K.ny; return S.umeanbnd;
+            default: break;
+        }
+        static const int map[] = {ZB, ZS, HH, UU, VV, HU, HV, HUM, HVM, QX, QY, UEU, VEV, VMAGEU, VMAGEV,
+                                  VU, UV, UUOLD, VVOLD, -1, DZSDT, H, E, D, DR, ROL, WK, CC_, CG, FX, FY,
+                                  URMS, UST, THM, CFM, FWM, CSED, CEQSG, STDEP, DZB, ROLTHICK, KTURB,
+                                  HMEAN, UUMEAN, VVMEAN, HHMEAN, ZSMEAN, CMEAN, ZSMAX};
+        if (f < 0 || f >= (int)(sizeof(map) / sizeof(map[0])) || map[f] < 0) return nullptr;
+        return S.f[map[f]];
+    }
+
+    int field_count(int f, size_t* n) override {
+        if (f == XBG_F_WETU || f == XBG_F_WETV) { *n = (size_t)S.C; return XBG_OK; }
+        if (!field_ptr(f, n, 0)) return XBG_ERR_ARG;
+        return XBG_OK;
+    }
+    int set_field(int f, const void* p, size_t n) override {
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        if (f == XBG_F_WETU || f == XBG_F_WETV) {
+            if (n != (size_t)S.C) return XBG_ERR_ARG;
+            CK(cudaMemcpy(f == XBG_F_WETU ? S.wetu : S.wetv, p, n * sizeof(int), cudaMemcpyHostToDevice));
+            return XBG_OK;
+        }
+        size_t m;
+        R* d = field_ptr(f, &m, c.par);
+        if (!d || m != n) return XBG_ERR_ARG;
+        CK(cudaMemcpy(d, p, n * sizeof(R), cudaMemcpyHostToDevice));
+        // double-buffered fields: both sets, so a piece-wise step (without
+        // compute_dt flipping the set) reads what was set
+        R* other = nullptr;
+        if (f == XBG_F_ZSOLD) other = zsold_buf[c.par ^ 1];
+        if (f == XBG_F_EE) other = ee_buf[c.par ^ 1];
+        if (f == XBG_F_RR) other = rr_buf[c.par ^ 1];
+        if (other) CK(cudaMemcpy(other, p, n * sizeof(R), cudaMemcpyHostToDevice));
+        return XBG_OK;
+    }
+    int get_field(int f, void* p, size_t n) override {
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        if (f == XBG_F_WETU || f == XBG_F_WETV) {
+            if (n != (size_t)S.C) return XBG_ERR_ARG;
+            CK(cudaMemcpy(p, f == XBG_F_WETU ? S.wetu : S.wetv, n * sizeof(int), cudaMemcpyDeviceToHost));
+            return XBG_OK;
+        }
+        size_t m;
+        R* d = field_ptr(f, &m, c.par);
+        if (!d || m != n) return XBG_ERR_ARG;
+        CK(cudaMemcpy(p, d, n * sizeof(R), cudaMemcpyDeviceToHost));
+        return XBG_OK;
+    }
+    int device_ptr(int f, void** p, size_t* n) override {
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        if (f == XBG_F_WETU || f == XBG_F_WETV) { *p = f == XBG_F_WETU ? S.wetu : S.wetv; *n = S.C; return XBG_OK; }
+        R* d = field_ptr(f, n, c.par);
+        if (!d) return XBG_ERR_ARG;
+        *p = d;
+        return XBG_OK;
+    }
+
+    // Reference initial condition, computed on the host as main() does
+    // (Wave_gpu.cu:1988-2015, 2040-2052, 2457-2510, 2637-2692).
+    int init_state(const void* zbp, double zs0, double zs1) override {
+        int nx = K.nx, ny = K.ny;
+        size_t C = (size_t)S.C;
+        const R* zbin = (const R*)zbp;
+        std::vector<R> zb(zbin, zbin + C), zs(C), hh(C), stdep(C, (R)5.0f), cfm(C), fwm(C);
+        for (int iy = 0; iy < ny; iy++)
+            for (int ix = 0; ix < nx; ix++) {
+                size_t i = ix + (size_t)iy * nx;
+                double zsbnd = zs0 + (zs1 - zs0) * (iy) / ny;
+                R a = (R)zsbnd, b = (R)(-1 * zb[i]);
+                zs[i] = (a < b) ? b : a;
+                double h = (double)zb[i] + zsbnd;
+                hh[i] = (R)((h < P.eps) ? P.eps : h);
+            }
+        for (size_t i = 0; i < C; i++) {   // updatezom
+            if (stdep[i] < (R)0.05f) { cfm[i] = (R)P.cfreef; fwm[i] = (R)P.fwreef; }
+            else { cfm[i] = (R)P.cfsand; fwm[i] = (R)P.fwsand; }
+        }
+        // initial dt: FLOWDT with 0.5*CFL, minimum, times 0.5 (Wave_gpu.cu:2648-2679)
+        R cfl = (R)(0.5f * P.CFL);
+        double mn = 1e300;
+        for (size_t i = 0; i < C; i++) {
+            R v = cfl * (R)P.dx / (std::sqrt((R)9.81f * hh[i]));
+            mn = std::min(mn, (double)v);
+        }
+        double dt0 = (double)(R)mn * 0.5;
+        if (dt0 < 0.00000001) return XBG_ERR_DT;
+        CK(cudaMemcpy(S.f[ZB], zb.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S.f[ZS], zs.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S.f[HH], hh.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        for (int f : {HU, HV, HUM, HVM}) CK(cudaMemcpy(S.f[f], hh.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S.f[STDEP], stdep.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S.f[CFM], cfm.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S.f[FWM], fwm.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        CK(cudaMemcpy(zsold_buf[c.par], zs.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(zsold_buf[c.par ^ 1], zs.data(), C * sizeof(R), cudaMemcpyHostToDevice));
+        c.dt = dt0;
+        c.wdt = (float)dt0;
+        if (P.swave == 1) {
+            if (!c.slot_valid[c.cur_slot]) return XBG_ERR_STATE;
+            R Trep = (R)c.slot_Trep[c.cur_slot];
+            c.Trep = (double)Trep;
+            c.sigm = (double)(R)(2.0f * 3.14159265 / (double)Trep);
+            // ee column 0 from the first record (Wavestep.cu:355-375)
+            std::vector<R> col((size_t)ny * K.nt);
+            CK(cudaMemcpy(col.data(), S.stfile[c.cur_slot], col.size() * sizeof(R), cudaMemcpyDeviceToHost));
+            for (int t = 0; t < K.nt; t++)
+                CK(cudaMemcpy2D(ee_buf[c.par] + (size_t)t * C, (size_t)nx * sizeof(R), &col[(size_t)t * ny],
+                                sizeof(R), sizeof(R), ny, cudaMemcpyHostToDevice));
+        }
+        CK(cudaMemcpy(clk, &c, sizeof(c), cudaMemcpyHostToDevice));
+        return XBG_OK;
+    }
+
+    int set_wave_boundary(int slot, const double* St, const double* q, int nrec, const double* times,
+                          double t0, double tend, double Trep) override {
+        if (slot < 0 || slot > 1 || nrec < 2 || !St || !q) return XBG_ERR_ARG;
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        int phys = slot == 0 ? c.cur_slot : (c.cur_slot ^ 1);
+        size_t ns = (size_t)nrec * K.nt * K.ny, nq = (size_t)nrec * 4 * K.ny;
+        if (ns > slot_cap) {   // (re)allocate both slots; the step graph is re-captured
+            for (int k = 0; k < 2; k++) {
+                R* a; R* b;
+                if ((rc = alloc(&a, ns)) || (rc = alloc(&b, nq))) return rc;
+                if (S.stfile[k]) {
+                    CK(cudaMemcpy(a, S.stfile[k], slot_cap * sizeof(R), cudaMemcpyDeviceToDevice));
+                    CK(cudaMemcpy(b, S.qfile[k], slot_cap / K.nt * 4 * sizeof(R), cudaMemcpyDeviceToDevice));
+                }
+                S.stfile[k] = a; S.qfile[k] = b;
+            }
+            slot_cap = ns;
+            drop_graph();
+        }
+        std::vector<R> hs(ns), hq(nq);
+        for (size_t j = 0; j < ns; j++) hs[j] = (R)St[j];
+        for (size_t j = 0; j < nq; j++) hq[j] = (R)q[j];
+        CK(cudaMemcpy(S.stfile[phys], hs.data(), ns * sizeof(R), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(S.qfile[phys], hq.data(), nq * sizeof(R), cudaMemcpyHostToDevice));
+        if (times) {
+            if (nrec > XBG_MAX_SERIES) return XBG_ERR_ARG;
+            CK(cudaMemcpy(ser->wavet, times, nrec * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        k_set_slot<R><<<1, 1, 0, st>>>(clk, slot, nrec, t0, tend, Trep);
+        launches++;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        return XBG_OK;
+    }
+
+    int set_series(int which, const double* t, const double* a, const double* b, int n) override {
+        if (n < 2 || n > XBG_MAX_SERIES) return XBG_ERR_ARG;
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        if (which == 0) {
+            CK(cudaMemcpy(ser->slt, t, n * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ser->sla, a, n * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ser->slb, b, n * sizeof(double), cudaMemcpyHostToDevice));
+            c.nsl = n; c.SLstep = 1;
+        } else {
+            CK(cudaMemcpy(ser->wt, t, n * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ser->wa, a, n * sizeof(double), cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(ser->wb, b, n * sizeof(double), cudaMemcpyHostToDevice));
+            c.nwnd = n; c.WNDstep = 1;
+        }
+        CK(cudaMemcpy(clk, &c, sizeof(c), cudaMemcpyHostToDevice));
+        return XBG_OK;
+    }
+
+    void drop_graph() {
+        if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+        if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+    }
+
+    // one coupled step: the body of mainloopGPU (Wave_gpu.cu:620-757)
+    int enqueue_step(Prof* pf = nullptr) {
+        int n = 0;
+        n += launch_step_begin(S, K, ser, nwave, st, pf);
+        if (K.swave == 1) n += launch_wavebnd(S, K, ser, st, pf, 0);
+        if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
+        if (K.swave == 1) n += launch_wave(S, K, st, pf);
+        if (K.flow == 1) n += launch_flow(S, K, st, pf);
+        if (P.sedtrans == 1) n += launch_sed(S, K, st, pf);
+        if (K.means) n += launch_means(S, K, st, pf);
+        return n;
+    }
+
+    int profile_step(float* ms, const char** names, int* n) {
+        Prof pf;
+        pf.st = st;
+        for (int k = 0; k < 65; k++) CK(cudaEventCreate(&pf.ev[k]));
+        CK(cudaEventRecord(pf.ev[0], st));
+        int nl = enqueue_step(&pf);
+        launches += nl;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        int m = std::min(*n, pf.n);
+        for (int k = 0; k < m; k++) {
+            CK(cudaEventElapsedTime(&ms[k], pf.ev[k], pf.ev[k + 1]));
+            if (names) names[k] = pf.name[k];
+        }
+        *n = m;
+        for (int k = 0; k < 65; k++) cudaEventDestroy(pf.ev[k]);
+        return XBG_OK;
+    }
+
+    int put_records(int slot, int first, int n, const void* St, const void* q) {
+        if (slot < 0 || slot > 1 || first < 0 || n < 1 || !St || !q) return XBG_ERR_ARG;
+        size_t nyt = (size_t)K.ny * K.nt;
+        if ((size_t)(first + n) * nyt > slot_cap) return XBG_ERR_ARG;
+        // slot 0 is the chunk in use as of the last call that read the clock
+        int phys = slot == 0 ? host_cur_slot : (host_cur_slot ^ 1);
+        CK(cudaMemcpyAsync(S.stfile[phys] + (size_t)first * nyt, St, (size_t)n * nyt * sizeof(R),
+                           cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(S.qfile[phys] + (size_t)first * 4 * K.ny, q, (size_t)n * 4 * K.ny * sizeof(R),
+                           cudaMemcpyHostToDevice, st));
+        return XBG_OK;
+    }
+
+    int piece(int which) override {
+        int n = 0;
+        switch (which) {
+            case 0: n = launch_step_begin(S, K, ser, nwave, st, nullptr); break;
+            case 1: if (K.swave == 1) n = launch_wavebnd(S, K, ser, st, nullptr, 1); break;
+            case 2: if (K.flow == 1) n = launch_ubnd(S, K, ser, st, nullptr); break;
+            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr); break;
+            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr); break;
+            case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr); break;
+            case 6: n = launch_means(S, K, st, nullptr); break;
+            default: return XBG_ERR_ARG;
+        }
+        launches += n;
+        CK(cudaGetLastError());
+        return XBG_OK;
+    }
+
+    int step(int nsteps) override {
+        if (!gexec) {
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            per_step_launches = enqueue_step();
+            cudaError_t e = cudaStreamEndCapture(st, &graph);
+            if (e != cudaSuccess) { last_err = e; return XBG_ERR_CUDA; }
+            CK(cudaGraphInstantiate(&gexec, graph, 0));
+        }
+        for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(gexec, st));
+        launches += (int64_t)per_step_launches * nsteps;
+        return XBG_OK;
+    }
+
+    int get_time(double* t, double* dt, int64_t* n, int* flags) override {
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        if (t) *t = c.totaltime;
+        if (dt) *dt = c.dt;
+        if (n) *n = c.nstep_total;
+        if (flags) *flags = c.flags;
+        return c.status;
+    }
+    int set_time(double t, double dt, double wdt) override {
+        Clock c;
+        int rc = read_clock(c);
+        if (rc) return rc;
+        c.totaltime = t; c.dt = dt; c.wdt = (float)wdt;
+        c.halt = 0;
+        c.do_sed = (P.sedtrans == 1 && t >= P.sedstart) ? 1 : 0;
+        CK(cudaMemcpy(clk, &c, sizeof(c), cudaMemcpyHostToDevice));
+        return XBG_OK;
+    }
+    int output_done() override { launch_output_done(S, K, st); launches += 2; CK(cudaGetLastError()); return XBG_OK; }
+    int reset_means() override { launch_reset_means(S, st); launches += 2; CK(cudaGetLastError()); return XBG_OK; }
+    int mass(double* w, double* s, double* b) override {
+        CK(cudaMemsetAsync(mass_buf, 0, 3 * sizeof(double), st));
+        launch_mass(S, P.dx * P.dx, mass_buf, st);
+        launches++;
+        double h[3];
+        CK(cudaMemcpyAsync(h, mass_buf, sizeof(h), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        *w = h[0]; *s = h[1]; *b = h[2];
+        return XBG_OK;
+    }
+    int sync() override { CK(cudaStreamSynchronize(st)); return XBG_OK; }
+    void* stream() override { return (void*)st; }
+    int profile(float* ms, const char** names, int* n) override { return profile_step(ms, names, n); }
+    int put_wave_records(int slot, int first, int n, const void* St, const void* q) override {
+        return put_records(slot, first, n, St, q);
+    }
+};
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+int xbg_create(const xbg_params* p, int precision, xbg_handle** out) {
+    if (!p || !out) return XBG_ERR_ARG;
+    *out = nullptr;
+    xbg_handle* h = nullptr;
+    int rc;
+    if (precision == XBG_FP32) { auto* q = new Handle<float>(); rc = q->setup(p, precision); h = q; }
+    else if (precision == XBG_FP64) { auto* q = new Handle<double>(); rc = q->setup(p, precision); h = q; }
+    else return XBG_ERR_ARG;
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return XBG_OK;
+}
+int xbg_destroy(xbg_handle* h) { delete h; return XBG_OK; }
+int xbg_init_state(xbg_handle* h, const void* zb, double zs0, double zs1) { return h ? h->init_state(zb, zs0, zs1) : XBG_ERR_ARG; }
+int xbg_field_count(const xbg_handle* h, int f, size_t* n) { return h ? const_cast<xbg_handle*>(h)->field_count(f, n) : XBG_ERR_ARG; }
+int xbg_set_field(xbg_handle* h, int f, const void* p, size_t n) { return h ? h->set_field(f, p, n) : XBG_ERR_ARG; }
+int xbg_get_field(xbg_handle* h, int f, void* p, size_t n) { return h ? h->get_field(f, p, n) : XBG_ERR_ARG; }
+int xbg_field_device_ptr(xbg_handle* h, int f, void** p, size_t* n) { return h ? h->device_ptr(f, p, n) : XBG_ERR_ARG; }
+int xbg_set_wave_boundary(xbg_handle* h, int slot, const double* St, const double* q, int nrec,
+                          const double* times, double t0, double tend, double Trep) {
+    return h ? h->set_wave_boundary(slot, St, q, nrec, times, t0, tend, Trep) : XBG_ERR_ARG;
+}
+int xbg_set_sealevel(xbg_handle* h, const double* t, const double* a, const double* b, int n) { return h ? h->set_series(0, t, a, b, n) : XBG_ERR_ARG; }
+int xbg_set_wind(xbg_handle* h, const double* t, const double* a, const double* b, int n) { return h ? h->set_series(1, t, a, b, n) : XBG_ERR_ARG; }
+int xbg_compute_dt(xbg_handle* h) { return h ? h->piece(0) : XBG_ERR_ARG; }
+int xbg_wave_boundary(xbg_handle* h) { return h ? h->piece(1) : XBG_ERR_ARG; }
+int xbg_flow_boundary(xbg_handle* h) { return h ? h->piece(2) : XBG_ERR_ARG; }
+int xbg_wave_step(xbg_handle* h) { return h ? h->piece(3) : XBG_ERR_ARG; }
+int xbg_flow_step(xbg_handle* h) { return h ? h->piece(4) : XBG_ERR_ARG; }
+int xbg_sediment_step(xbg_handle* h) { return h ? h->piece(5) : XBG_ERR_ARG; }
+int xbg_accumulate_means(xbg_handle* h) { return h ? h->piece(6) : XBG_ERR_ARG; }
+int xbg_step(xbg_handle* h) { return h ? h->step(1) : XBG_ERR_ARG; }
+int xbg_advance(xbg_handle* h, int n) { return h ? h->step(n) : XBG_ERR_ARG; }
+int xbg_get_time(xbg_handle* h, double* t, double* dt, int64_t* n, int* flags) { return h ? h->get_time(t, dt, n, flags) : XBG_ERR_ARG; }
+int xbg_output_done(xbg_handle* h) { return h ? h->output_done() : XBG_ERR_ARG; }
+int xbg_reset_means(xbg_handle* h) { return h ? h->reset_means() : XBG_ERR_ARG; }
+int xbg_set_time(xbg_handle* h, double t, double dt, double wdt) { return h ? h->set_time(t, dt, wdt) : XBG_ERR_ARG; }
+int xbg_sync(xbg_handle* h) { return h ? h->sync() : XBG_ERR_ARG; }
+int xbg_launch_count(const xbg_handle* h, int64_t* n) { if (!h || !n) return XBG_ERR_ARG; *n = h->launches; return XBG_OK; }
+int xbg_get_stream(xbg_handle* h, void** s) { if (!h || !s) return XBG_ERR_ARG; *s = h->stream(); return XBG_OK; }
+int xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n) {
+    if (!h || !ms || !n) return XBG_ERR_ARG;
+    return h->profile(ms, names, n);
+}
+int xbg_put_wave_records(xbg_handle* h, int slot, int first, int n, const void* St, const void* q) {
+    return h ? h->put_wave_records(slot, first, n, St, q) : XBG_ERR_ARG;
+}
+int xbg_mass(xbg_handle* h, double* w, double* s, double* b) { return h ? h->mass(w, s, b) : XBG_ERR_ARG; }
+
+}  // extern "C"

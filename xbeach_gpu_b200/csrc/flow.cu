@@ -1,0 +1,529 @@
+// flow.cu -- shallow-water step on the staggered grid (flowstep,
+// Wave_gpu.cu:1106-1403; kernels of Flow_kernel.cu) in five fused passes.
+// Each pass cuts where the reference reads a field that an earlier launch of
+// the same step rewrote at a neighbouring cell; inside a pass, neighbour
+// values of per-cell intermediates are recomputed instead of stored.
+//
+//   k_flow_a     udepthmomcont, vdepthmomcont, smago  -> hum hvm wetu wetv nuh
+//   k_flow_u     wlevslopes(x), ududx_adv, vdudy_adv, viscou1+2, eulerustep,
+//                latbnd(uu)                           -> uu*
+//   k_flow_v     wlevslopes(y), vdvdy_adv, udvdx_adv, viscov1+2, eulervstep,
+//                vvlatbnd                             -> vv*
+//   k_flow_corr  wrkuu2Ocorr+uu2Ocorr, wrkvv2Ocorr+vv2Ocorr -> uu, vv
+//   k_flow_cont  depthhu, depthhv, CalcQFlow, continuity -> hu hv qx qy zs* dzsdt
+//   k_flow_final wrkzs2Ocorr+zs2Ocorr, latbnd(zs), hsbnd, calcuvvu, uvlatbnd
+// (* = a per-step buffer).  viscovbnd (Flow_kernel.cu:1461) changes viscv only
+// at rows 0 and ny-2, whose eulervstep results vvlatbnd then overwrites, so it
+// has no effect on the state and is not evaluated.
+#include "xbg_common.cuh"
+
+namespace xbg {
+
+template <class R>
+__device__ __forceinline__ R minmod(R d1, R d2) {   // Flow_kernel.cu:23-41
+    R r = (R)0.0f;
+    if (d1 * d2 > (R)0.0f) {
+        if (d1 > (R)0.0f) r = DM<R>::fmin(d1, d2);
+        if (d1 < (R)0.0f) r = DM<R>::fmax(d1, d2);
+    }
+    return r;
+}
+
+#define IDX(x, y) ((x) + (y) * nx)
+
+// smago (Flow_kernel.cu:1282-1316) at cell (ix, iy)
+template <class R>
+__device__ __forceinline__ R smago_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
+    const int nx = K.nx, ny = K.ny;
+    const R* uu = S.f[UU]; const R* vv = S.f[VV];
+    int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+    R dx = K.dx, nuh = K.nuh, nuhfac = K.nuhfac, rho = K.rho;
+    R b = nuhfac * ld(S.f[HH] + i) * DM<R>::pow(ld(S.f[DR] + i) / rho, (R)(1.0f / 3.0f));
+    if (K.usesmago == 1) {
+        R dudx = (ld(uu + i) - ld(uu + IDX(xm, iy))) / dx;
+        R dudy = (R)0.50f * (ld(uu + IDX(ix, yp)) - ld(uu + IDX(ix, ym)) + ld(uu + IDX(xm, yp)) - ld(uu + IDX(xm, ym))) / dx;
+        R dvdy = (ld(vv + i) - ld(vv + IDX(ix, ym))) / dx;
+        R dvdx = (R)0.50f * (ld(vv + IDX(xp, iy)) - ld(vv + IDX(xm, iy)) + ld(vv + IDX(xp, ym)) - ld(vv + IDX(xm, ym))) / dx;
+        R tau = DM<R>::sqrt((R)2.0f * dudx * dudx + (R)2.0f * dvdy * dvdy + DM<R>::pow(dudy + dvdx, (R)2.0f));
+        return DM<R>::fmax(nuh * nuh * dx * dx * tau, b);
+    }
+    return DM<R>::fmax(nuh, b);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_a(Dev<R> S, Konst<R> K) {
+    if (halted(S.clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    R eps = K.eps;
+    R hh = ld(S.f[HH] + i);
+    R humi = (R)0.5f * (hh + ld(S.f[HH] + IDX(pp(ix, nx), iy)));
+    S.wetu[i] = (ld(S.f[HU] + i) > eps && humi > eps) ? 1 : 0;
+    S.f[HUM][i] = DM<R>::fmax(humi, eps);
+    R hvmi = (R)0.5f * (hh + ld(S.f[HH] + IDX(ix, pp(iy, ny))));
+    S.wetv[i] = (ld(S.f[HV] + i) > eps && hvmi > eps) ? 1 : 0;
+    S.f[HVM][i] = DM<R>::fmax(hvmi, eps);
+    S.tmp[T_NUH][i] = smago_cell(S, K, ix, iy);
+}
+
+// eulerustep (Flow_kernel.cu:1487-1544) at an interior-x cell, with the
+// advection (ududx_adv :752, vdudy_adv :887) and viscosity (viscou1 :1319,
+// viscou2 :1358) terms evaluated in place.
+template <class R>
+__device__ R euler_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R wu) {
+    const int nx = K.nx, ny = K.ny;
+    const R* uu = S.f[UU]; const R* vv = S.f[VV]; const R* hu = S.f[HU]; const R* hv = S.f[HV];
+    const R* hum = S.f[HUM]; const R* hvm = S.f[HVM]; const R* nuhg = S.tmp[T_NUH];
+    const R* hh = S.f[HH];
+    int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+    R dx = K.dx, g = K.g, rho = K.rho;
+    R uui = ld(uu + i);
+    if (ld(S.wetu + i) != 1) return (R)0.0f;
+    R humi = ld(hum + i);
+    // wlevslopes, x
+    R dzsdx = (ld(S.f[ZS] + IDX(xp, iy)) - ld(S.f[ZS] + i)) / dx;
+    // ududx_adv
+    R uur = ld(uu + IDX(xp, iy)), uul = ld(uu + IDX(xm, iy));
+    R ududx = (R)0.0f;
+    R qin = (R)0.5f * (ld(hu + i) * uui + ld(hu + IDX(xm, iy)) * uul);
+    R du = uui - uul;
+    if (qin > (R)0.0f) {
+        if (du > (R)0.5f) ududx = ududx + (R)0.5f * (uul + uui) * (uui - uul) / dx;
+        else ududx = ududx + qin / humi * (uui - uul) / dx;
+    }
+    qin = (R)-0.5f * (ld(hu + i) * uui + ld(hu + IDX(xp, iy)) * uur);
+    du = uur - uui;
+    if (qin > (R)0.0f) {
+        if (du > (R)0.5f) ududx = ududx - (R)0.5f * (uur + uui) * (uui - uur) / dx;
+        else ududx = ududx + qin / humi * (uui - uur) / dx;
+    }
+    // vdudy_adv
+    R uut = ld(uu + IDX(ix, yp)), uub = ld(uu + IDX(ix, ym));
+    R vb = ld(vv + IDX(ix, ym)), vbr = ld(vv + IDX(xp, ym)), vi = ld(vv + i), vr = ld(vv + IDX(xp, iy));
+    R vdudy = (R)0.0f;
+    qin = (R)0.5f * (vb * ld(hv + IDX(ix, ym)) + vbr * ld(hv + IDX(xp, ym)));
+    R dv = vi - vb;
+    if (qin > (R)0.0f) {
+        if (dv > (R)0.5f) vdudy = vdudy + (R)0.5f * (vb + vbr) * (uui - uub) / dx;
+        else vdudy = vdudy + qin / humi * (uui - uub) / dx;
+    }
+    qin = (R)-0.5f * (vi * ld(hv + i) + vr * ld(hv + IDX(xp, iy)));
+    dv = ld(vv + IDX(ix, yp)) - vi;
+    if (qin > (R)0.0f) {
+        if (dv > (R)0.5f) vdudy = vdudy - (R)0.5f * (vi + vr) * (uui - uut) / dx;
+        else vdudy = vdudy + qin / humi * (uui - uut) / dx;
+    }
+    // viscou1 + viscou2
+    R nuh1 = ld(nuhg + IDX(xp, iy)), nuh2 = ld(nuhg + i);
+    R dudx1 = nuh1 * ld(hh + IDX(xp, iy)) * (uur - uui) / dx;
+    R dudx2 = nuh2 * ld(hh + i) * (uui - uul) / dx;
+    R visc = ((R)1.0f / humi) * ((dudx1 - dudx2) / (dx));
+    nuh1 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xp, iy)) + ld(nuhg + IDX(xp, yp)) + ld(nuhg + IDX(ix, yp)));
+    nuh2 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xp, iy)) + ld(nuhg + IDX(xp, ym)) + ld(nuhg + IDX(ix, ym)));
+    R dudy1 = nuh1 * (R)0.5f * (ld(hvm + i) + ld(hvm + IDX(xp, iy))) * (uut - uui) / dx;
+    R dudy2 = nuh2 * (R)0.5f * (ld(hvm + IDX(ix, ym)) + ld(hvm + IDX(xp, ym))) * (uui - uub) / dx;
+    visc = visc + ((R)1.0f / humi) * ((dudy1 - dudy2) / dx * (R)ld(S.wetu + IDX(ix, yp)) * (R)ld(S.wetu + IDX(ix, ym)));
+    // eulerustep
+    R hmin = (R)0.2;
+    int sw = (wu > (R)0.0) - (wu < (R)0.0);
+    R urms = ld(S.f[URMS] + i), vmag = ld(S.f[VMAGEU] + i);
+    R taubx = ld(S.f[CFM] + i) * rho * ld(S.f[UEU] + i) * DM<R>::sqrt((R)1.3456f * urms * urms + vmag * vmag);
+    return uui - dtf * (ududx + vdudy - visc + g * dzsdx + taubx / (rho * ld(hu + i)) -
+                        ld(S.f[FX] + i) / (rho * DM<R>::fmax(humi, hmin)) -
+                        (R)1.25f * K.Cd * (R)sw * wu * wu / (rho * humi) - K.fc * ld(S.f[VU] + i));
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_u(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    R dtf = (R)clk->dt, wu = (R)clk->windu;
+    // latbnd(uu): rows 0 / ny-1 take the updated rows 1 / ny-2
+    int sy = iy;
+    if (iy == 0) sy = 1;
+    if (iy == ny - 1) sy = ny - 2;
+    R v = (ix > 0) ? euler_u(S, K, ix, sy, dtf, wu) : ld(S.f[UU] + IDX(ix, sy));
+    S.tmp[T_UU][IDX(ix, iy)] = v;
+}
+
+// vdvdy_adv (Flow_kernel.cu:1024-1074) at a row that eulervstep updates.
+template <class R>
+__device__ __forceinline__ R vdvdy_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
+    const int nx = K.nx, ny = K.ny;
+    const R* vv = S.f[VV]; const R* hv = S.f[HV];
+    R r = (R)0.0f;
+    if (ix > 0 && iy > 0 && iy < ny - 2) {
+        int i = IDX(ix, iy), ym = mm(iy), yp = pp(iy, ny);
+        R dx = K.dx, hvmi = ld(S.f[HVM] + i);
+        R vi = ld(vv + i), vb = ld(vv + IDX(ix, ym)), vt = ld(vv + IDX(ix, yp));
+        R qin = (R)0.5f * (vi * ld(hv + i) + vb * ld(hv + IDX(ix, ym)));
+        R dv = vi - vb;
+        if (qin > (R)0.0f) {
+            if (dv > (R)0.5f) r = r + (R)0.5f * (vb - vi) * (vi - vb) / (dx);
+            else r = r + qin / hvmi * (vi - vb) / (dx);
+        }
+        qin = (R)-0.5f * (ld(hv + i) * vi + ld(hv + IDX(ix, yp)) * vt);
+        dv = vt - vi;
+        if (qin > (R)0.0f) {
+            if (dv > (R)0.5f) r = r - (R)0.5f * (vt + vi) * (vi - vt) / (dx);
+            else r = r + qin / hvmi * (vi - vt) / (dx);
+        }
+    }
+    return r;
+}
+
+// eulervstep (Flow_kernel.cu:1546-1599) at ix > 0, iy < ny-2, with udvdx_adv
+// (:1159, on the updated uu*), vdvdy_adv and viscov1 + viscov2.
+template <class R>
+__device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R wv) {
+    const int nx = K.nx, ny = K.ny;
+    const R* uu = S.tmp[T_UU]; const R* vv = S.f[VV]; const R* hu = S.f[HU];
+    const R* hum = S.f[HUM]; const R* hvm = S.f[HVM]; const R* nuhg = S.tmp[T_NUH];
+    const R* hh = S.f[HH];
+    int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+    R dx = K.dx, g = K.g, rho = K.rho;
+    R vvi = ld(vv + i);
+    if (ld(S.wetv + i) != 1) return (R)0.0f;
+    R hvmi = ld(hvm + i);
+    R dzsdy = (ld(S.f[ZS] + IDX(ix, yp)) - ld(S.f[ZS] + i)) / dx;
+    R vdvdy = vdvdy_cell(S, K, ix, iy);
+    // udvdx_adv
+    R ul = ld(uu + IDX(xm, iy)), ultl = ld(uu + IDX(xm, yp)), ui = ld(uu + i), ur = ld(uu + IDX(xp, iy));
+    R vl = ld(vv + IDX(xm, iy)), vr = ld(vv + IDX(xp, iy));
+    R udvdx = (R)0.0f;
+    R qin = (R)(0.5 * (double)(ul * ld(hu + IDX(xm, iy)) + ultl * ld(hu + IDX(xm, yp))));
+    R du = ui - ul;
+    if (qin > (R)0.0f) {
+        if (du > (R)0.5f) udvdx = udvdx + (R)0.5f * (ul + ultl) * (vvi - vl) / (dx);
+        else udvdx = udvdx + qin / hvmi * (vvi - vl) / (dx);
+    }
+    qin = (R)(-0.5 * (double)(ui * ld(hu + i) + ld(uu + IDX(ix, yp)) * ld(hu + IDX(ix, yp))));
+    du = ur - ui;
+    if (qin > (R)0.0f) {
+        if (du > (R)0.5f) udvdx = udvdx - (R)0.5f * (ui + ur) * (vvi - vr) / (dx);
+        else udvdx = udvdx + qin / hvmi * (vvi - vr) / (dx);
+    }
+    // viscov1 + viscov2
+    R vt = ld(vv + IDX(ix, yp)), vb = ld(vv + IDX(ix, ym));
+    R nuh1 = ld(nuhg + IDX(ix, yp)), nuh2 = ld(nuhg + i);
+    R dvdy1 = nuh1 * ld(hh + IDX(ix, yp)) * (vt - vvi) / dx;
+    R dvdy2 = nuh2 * ld(hh + i) * (vvi - vb) / dx;
+    R visc = ((R)1.0f / hvmi) * (dvdy1 - dvdy2) / dx * (R)ld(S.wetv + IDX(ix, yp)) * (R)ld(S.wetv + IDX(ix, ym));
+    nuh1 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xp, iy)) + ld(nuhg + IDX(xp, yp)) + ld(nuhg + IDX(ix, yp)));
+    nuh2 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xm, iy)) + ld(nuhg + IDX(xm, yp)) + ld(nuhg + IDX(ix, yp)));
+    R dvdx1 = nuh1 * (R)0.5f * (ld(hum + i) + ld(hum + IDX(ix, yp))) * (vr - vvi) / dx;
+    R dvdx2 = nuh2 * (R)0.5f * (ld(hum + IDX(xm, iy)) + ld(hum + IDX(xm, yp))) * (vvi - vl) / dx;
+    visc = visc + ((R)1.0f / hvmi) * ((dvdx1 - dvdx2) / (dx) * (R)ld(S.wetv + IDX(xp, iy)) * (R)ld(S.wetv + IDX(xm, iy)));
+    R hmin = (R)0.2;
+    int sw = (wv > (R)0.0) - (wv < (R)0.0);
+    R urms = ld(S.f[URMS] + i), vmag = ld(S.f[VMAGEV] + i);
+    R tauby = ld(S.f[CFM] + i) * rho * ld(S.f[VEV] + i) * DM<R>::sqrt((R)1.3456f * urms * urms + vmag * vmag);
+    return vvi - dtf * (udvdx + vdvdy - visc + g * dzsdy + tauby / (rho * ld(S.f[HV] + i)) -
+                        ld(S.f[FY] + i) / (rho * DM<R>::fmax(hvmi, hmin)) + K.fc * ld(S.f[UV] + i) -
+                        (R)1.25f * K.Cd * (R)sw * wv * wv / (rho * hvmi));
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_v(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    R dtf = (R)clk->dt, wv = (R)clk->windv;
+    // vvlatbnd: row 0 <- row 1, row ny-2 <- row ny-3; row ny-1 keeps its value
+    int sy = iy;
+    if (iy == 0) sy = 1;
+    if (iy == ny - 2) sy = ny - 3;
+    R v;
+    if (sy < ny - 2 && ix > 0) v = euler_v(S, K, ix, sy, dtf, wv);
+    else v = ld(S.f[VV] + IDX(ix, sy));
+    S.tmp[T_VV][IDX(ix, iy)] = v;
+}
+
+// wrkuu2Ocorr (Flow_kernel.cu:1960-2044) at cell (ix, iy)
+template <class R>
+__device__ __forceinline__ void wrk_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
+    const int nx = K.nx, ny = K.ny;
+    const R* zs = S.f[ZS]; const R* zb = S.f[ZB]; const R* uu = S.tmp[T_UU]; const R* uo = S.f[UUOLD];
+    const R* qx = S.f[QX]; const R* qy = S.f[QY];
+    int i = IDX(ix, iy);
+    int xm = mm(ix), xm2 = mm2(ix), xp = pp(ix, nx), xp2 = pp2(ix, nx);
+    int ym = mm(iy), yp = pp(iy, ny), yp2 = pp2(iy, ny);
+    R eps2 = K.eps * (R)2.0f;
+    w1 = (R)0.0f; w2 = (R)0.0f;
+    if (ix > 0) {
+        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm2, iy)), ld(zs + IDX(xm, iy))), ld(zs + i)), ld(zs + IDX(xp, iy))), ld(zs + IDX(xp2, iy)));
+        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm2, iy)), ld(zb + IDX(xm, iy))), ld(zb + i)), ld(zb + IDX(xp, iy))), ld(zb + IDX(xp2, iy)));
+        if (minzs + minzb > eps2) {
+            R qs = ld(qx + i) + ld(qx + IDX(xm, iy));
+            if (qs > (R)0.0f) w1 = (R)0.5f * minmod(ld(uu + i) - ld(uo + IDX(xm, iy)), ld(uu + IDX(xm, iy)) - ld(uo + IDX(xm2, iy)));
+            if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(ld(uo + i) - ld(uu + IDX(xm, iy)), ld(uo + IDX(xp, iy)) - ld(uu + i));
+        }
+        if (iy > 0) {
+            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(ix, iy)), ld(zs + IDX(ix, ym))), ld(zs + IDX(ix, yp))), ld(zs + IDX(ix, yp2)));
+            mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xp, iy)), ld(zs + IDX(xp, ym))), ld(zs + IDX(xp, yp))), ld(zs + IDX(xp, yp2))));
+            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(ix, iy)), ld(zb + IDX(ix, ym))), ld(zb + IDX(ix, yp))), ld(zb + IDX(ix, yp2)));
+            mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xp, iy)), ld(zb + IDX(xp, ym))), ld(zb + IDX(xp, yp))), ld(zb + IDX(xp, yp2))));
+            if (mzs + mzb > eps2) {
+                R qs = ld(qy + IDX(xp, iy)) + ld(qy + i);
+                if (qs > (R)0.0f) w2 = (R)0.5f * minmod(ld(uu + IDX(ix, yp)) - ld(uo + i), ld(uu + i) - ld(uo + IDX(ix, ym)));
+                if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(ld(uo + IDX(ix, yp)) - ld(uu + i), ld(uo + IDX(ix, yp2)) - ld(uu + IDX(ix, yp)));
+            }
+        }
+    }
+}
+
+// wrkvv2Ocorr (Flow_kernel.cu:2046-2128) at cell (ix, iy)
+template <class R>
+__device__ __forceinline__ void wrk_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
+    const int nx = K.nx, ny = K.ny;
+    const R* zs = S.f[ZS]; const R* zb = S.f[ZB]; const R* vv = S.tmp[T_VV]; const R* vo = S.f[VVOLD];
+    const R* qx = S.f[QX]; const R* qy = S.f[QY];
+    int i = IDX(ix, iy);
+    int xm = mm(ix), xp = pp(ix, nx), xp2 = pp2(ix, nx);
+    int ym = mm(iy), ym2 = mm2(iy), yp = pp(iy, ny), yp2 = pp2(iy, ny);
+    R eps2 = K.eps * (R)2.0f;
+    w1 = (R)0.0f; w2 = (R)0.0f;
+    if (ix > 0 && iy > 0 && iy < ny - 2) {
+        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(ix, ym2)), ld(zs + IDX(ix, ym))), ld(zs + IDX(ix, iy))), ld(zs + IDX(ix, yp))), ld(zs + IDX(ix, yp2)));
+        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(ix, ym2)), ld(zb + IDX(ix, ym))), ld(zb + IDX(ix, iy))), ld(zb + IDX(ix, yp))), ld(zb + IDX(ix, yp2)));
+        if (minzs + minzb > eps2) {
+            R qs = ld(qy + i) + ld(qy + IDX(ix, ym));
+            if (qs > (R)0.0f) w1 = (R)0.5f * minmod(ld(vv + i) - ld(vo + IDX(ix, ym)), ld(vv + IDX(ix, ym)) - ld(vo + IDX(ix, ym2)));
+            if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(ld(vo + i) - ld(vv + IDX(ix, ym)), ld(vo + IDX(ix, yp)) - ld(vv + i));
+        }
+        R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm, iy)), ld(zs + IDX(ix, iy))), ld(zs + IDX(xp, iy))), ld(zs + IDX(xp2, iy)));
+        mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm, yp)), ld(zs + IDX(ix, yp))), ld(zs + IDX(xp, yp))), ld(zs + IDX(xp2, yp))));
+        R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm, iy)), ld(zb + IDX(ix, iy))), ld(zb + IDX(xp, iy))), ld(zb + IDX(xp2, iy)));
+        mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm, yp)), ld(zb + IDX(ix, yp))), ld(zb + IDX(xp, yp))), ld(zb + IDX(xp2, yp))));
+        if (mzs + mzb > eps2) {
+            R qs = ld(qx + IDX(ix, yp)) + ld(qx + i);
+            if (qs > (R)0.0f) w2 = (R)0.5f * minmod(ld(vv + IDX(xp, iy)) - ld(vo + i), ld(vv + i) - ld(vo + IDX(xm, iy)));
+            if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(ld(vo + IDX(xp, iy)) - ld(vv + i), ld(vo + IDX(xp2, iy)) - ld(vv + IDX(xp, iy)));
+        }
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_corr(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    R dtf = (R)clk->dt, dx = K.dx;
+    const R* qx = S.f[QX]; const R* qy = S.f[QY];
+    R u = ld(S.tmp[T_UU] + i), v = ld(S.tmp[T_VV] + i);
+    if (ix > 0 && iy > 0) {
+        int xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+        // uu2Ocorr (Flow_kernel.cu:2210-2245)
+        R w1i, w2i, w1r, t0, t1, w2b;
+        wrk_u(S, K, ix, iy, w1i, w2i);
+        wrk_u(S, K, xp, iy, w1r, t0);
+        wrk_u(S, K, ix, ym, t1, w2b);
+        R qe = (R)0.5f * (ld(qx + IDX(xp, iy)) + ld(qx + i));
+        R qw = (R)0.5f * (ld(qx + i) + ld(qx + IDX(xm, iy)));
+        R qn = (R)0.5f * (ld(qy + IDX(ix, ym)) + ld(qy + IDX(xp, ym)));
+        R qs = (R)0.5f * (ld(qy + i) + ld(qy + IDX(xm, iy)));
+        u = u - dtf / ld(S.f[HUM] + i) * ((qe * w1r - qw * w1i) / dx + (qs * w2i - qn * w2b) / dx);
+        // vv2Ocorr (Flow_kernel.cu:2247-2282)
+        R v1i, v2i, v2l, v1t, t2, t3;
+        wrk_v(S, K, ix, iy, v1i, v2i);
+        wrk_v(S, K, xm, iy, t2, v2l);
+        wrk_v(S, K, ix, yp, v1t, t3);
+        qe = (R)0.5f * (ld(qx + IDX(ix, yp)) + ld(qx + i));
+        qw = (R)0.5f * (ld(qx + IDX(xm, iy)) + ld(qx + IDX(xm, yp)));
+        qn = (R)0.5f * (ld(qy + i) + ld(qy + IDX(ix, ym)));
+        qs = (R)0.5f * (ld(qy + IDX(ix, yp)) + ld(qy + i));
+        v = v - dtf / ld(S.f[HVM] + i) * ((qe * v2i - qw * v2l) / dx + (qs * v1t - qn * v1i) / dx);
+    }
+    S.f[UU][i] = u;
+    S.f[VV][i] = v;
+}
+
+// depthhu / depthhv (Flow_kernel.cu:653-750)
+template <class R>
+__device__ __forceinline__ R depth_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
+    const int nx = K.nx;
+    int i = IDX(ix, iy), j = IDX(pp(ix, nx), iy);
+    R zsi = ld(S.f[ZS] + i), zsr = ld(S.f[ZS] + j);
+    R b = DM<R>::fmax((R)-1.0f * ld(S.f[ZB] + i), (R)-1.0f * ld(S.f[ZB] + j));
+    R u = ld(S.f[UU] + i), h;
+    const R ummn = (R)0.0f;
+    if (u > ummn) h = zsi - b;
+    else if (u < (R)-1.0f * ummn) h = zsr - b;
+    else h = DM<R>::fmax(DM<R>::fmax(zsi, zsr) - b, K.eps);
+    return DM<R>::fmax(h, (R)0.0f);
+}
+template <class R>
+__device__ __forceinline__ R depth_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
+    const int nx = K.nx, ny = K.ny;
+    int i = IDX(ix, iy), j = IDX(ix, pp(iy, ny));
+    R zsi = ld(S.f[ZS] + i), zst = ld(S.f[ZS] + j);
+    R b = DM<R>::fmax((R)-1.0f * ld(S.f[ZB] + i), (R)-1.0f * ld(S.f[ZB] + j));
+    R v = ld(S.f[VV] + i), h;
+    const R ummn = (R)0.0f;
+    if (v > ummn) h = zsi - b;
+    else if (v < (R)-1 * ummn) h = zst - b;
+    else h = DM<R>::fmax(DM<R>::fmax(zsi, zst) - b, K.eps);
+    return DM<R>::fmax(h, (R)0.0f);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_cont(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    R dtf = (R)clk->dt;
+    R hu = depth_u(S, K, ix, iy), hv = depth_v(S, K, ix, iy);
+    R qxi = ld(S.f[UU] + i) * hu, qyi = ld(S.f[VV] + i) * hv;   // CalcQFlow
+    S.f[HU][i] = hu; S.f[HV][i] = hv;
+    S.f[QX][i] = qxi; S.f[QY][i] = qyi;
+    R zs = ld(S.f[ZS] + i);
+    if (ix > 0) {   // continuity (Flow_kernel.cu:1626-1681)
+        int xm = mm(ix), ym = mm(iy);
+        R qxl = ld(S.f[UU] + IDX(xm, iy)) * depth_u(S, K, xm, iy);
+        R qyb = (ym == iy) ? qyi : ld(S.f[VV] + IDX(ix, ym)) * depth_v(S, K, ix, ym);
+        R dzdt = (qxl - qxi + qyb - qyi) / K.dx;
+        S.f[DZSDT][i] = dzdt;
+        zs = zs + dzdt * dtf;
+    }
+    S.tmp[T_ZS][i] = zs;
+}
+
+// wrkzs2Ocorr (Flow_kernel.cu:2130-2208) at cell (ix, iy); zs is the
+// post-continuity level, zsold the previous step's.
+template <class R>
+__device__ __forceinline__ void wrk_z(const Dev<R>& S, const Konst<R>& K, const R* zso, int ix, int iy, R& w1, R& w2) {
+    const int nx = K.nx, ny = K.ny;
+    const R* zs = S.tmp[T_ZS]; const R* zb = S.f[ZB];
+    int i = IDX(ix, iy);
+    int xm = mm(ix), xp = pp(ix, nx), xp2 = pp2(ix, nx), ym = mm(iy), yp = pp(iy, ny), yp2 = pp2(iy, ny);
+    R eps2 = K.eps * (R)2.0f;
+    w1 = (R)0.0f; w2 = (R)0.0f;
+    if (ix > 0) {
+        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm, iy)), ld(zs + i)), ld(zs + IDX(xp, iy))), ld(zs + IDX(xp2, iy)));
+        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm, iy)), ld(zb + i)), ld(zb + IDX(xp, iy))), ld(zb + IDX(xp2, iy)));
+        if (minzs + minzb > eps2) {
+            R u = ld(S.f[UU] + i);
+            if (u > (R)0.0f) w1 = u * (R)0.5f * minmod(ld(zs + IDX(xp, iy)) - ld(zso + i), ld(zs + i) - ld(zso + IDX(xm, iy)));
+            if (u < (R)0.0f) w1 = (R)-1.0f * u * (R)0.5f * minmod(ld(zso + IDX(xp2, iy)) - ld(zs + IDX(xp, iy)), ld(zso + IDX(xp, iy)) - ld(zs + i));
+        }
+        if (iy > 0) {
+            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(ix, ym)), ld(zs + i)), ld(zs + IDX(ix, yp))), ld(zs + IDX(ix, yp2)));
+            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(ix, ym)), ld(zb + i)), ld(zb + IDX(ix, yp))), ld(zb + IDX(ix, yp2)));
+            if (mzs + mzb > eps2) {
+                R v = ld(S.f[VV] + i);
+                if (v > (R)0.0f) w2 = v * (R)0.5f * minmod(ld(zs + IDX(ix, yp)) - ld(zso + i), ld(zs + i) - ld(zso + IDX(ix, ym)));
+                if (v < (R)0.0f) w2 = v * (R)0.5f * minmod(ld(zso + IDX(ix, yp2)) - ld(zs + IDX(ix, yp)), ld(zso + IDX(ix, yp)) - ld(zs + i));
+            }
+        }
+    }
+}
+
+// zs after zs2Ocorr (Flow_kernel.cu:2284-2317) at (ix, iy); w1, w2: its wrk.
+template <class R>
+__device__ __forceinline__ R zs_corr(const Dev<R>& S, const Konst<R>& K, const R* zso, int ix, int iy, R dtf, R& w1, R& w2) {
+    const int nx = K.nx;
+    wrk_z(S, K, zso, ix, iy, w1, w2);
+    R z = ld(S.tmp[T_ZS] + IDX(ix, iy));
+    if (ix > 0 && iy > 0) {
+        R w1l, t0, t1, w2b;
+        wrk_z(S, K, zso, mm(ix), iy, w1l, t0);
+        wrk_z(S, K, zso, ix, mm(iy), t1, w2b);
+        z = z - dtf * ((w1 - w1l) / K.dx + (w2 - w2b) / K.dx);
+    }
+    return z;
+}
+
+// calcuvvu (Flow_kernel.cu:467-544) at (ix, iy)
+template <class R>
+__device__ __forceinline__ void uvvu_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R* o6) {
+    const int nx = K.nx, ny = K.ny;
+    const R* uu = S.f[UU]; const R* vv = S.f[VV]; const R* ust = S.f[UST]; const R* thm = S.f[THM];
+    int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+    R usti = ld(ust + i), tmi = ld(thm + i);
+    R ustr = ld(ust + IDX(xp, iy)), tmr = ld(thm + IDX(xp, iy));
+    R ustt = ld(ust + IDX(ix, yp)), tmt = ld(thm + IDX(ix, yp));
+    R wu = (R)ld(S.wetu + i), wv = (R)ld(S.wetv + i);
+    R vu = (R)0.25f * (ld(vv + IDX(ix, ym)) + ld(vv + i) + ld(vv + IDX(xp, ym)) + ld(vv + IDX(xp, iy))) * wu;
+    R uv = (R)0.25f * (ld(uu + IDX(xm, iy)) + ld(uu + i) + ld(uu + IDX(xm, yp)) + ld(uu + IDX(ix, yp))) * wv;
+    R vsu = (R)0.5f * (usti * DM<R>::sin(tmi) + ustr * DM<R>::sin(tmr)) * wu;
+    R usu = (R)0.5f * (usti * DM<R>::cos(tmi) + ustr * DM<R>::cos(tmr)) * wu;
+    R ue = ld(uu + i) - usu;
+    R ve = vu - vsu;
+    R usv = (R)0.5f * (usti * DM<R>::cos(tmi) + ustt * DM<R>::cos(tmt)) * wv;
+    R vsv = (R)0.5f * (usti * DM<R>::sin(tmi) + ustt * DM<R>::sin(tmt)) * wv;
+    R vvv = ld(vv + i) - vsv;
+    R uvv = uv - usv;
+    o6[0] = vu; o6[1] = uv; o6[2] = ue; o6[3] = vvv;
+    o6[4] = DM<R>::sqrt(ue * ue + ve * ve);
+    o6[5] = DM<R>::sqrt(uvv * uvv + vvv * vvv);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const R* zsold_in = S.zsold[clk->par ^ 1];
+    R* zsold_out = S.zsold[clk->par];
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    R dtf = (R)clk->dt;
+    int sy = iy;
+    if (iy == 0) sy = 1;
+    if (iy == ny - 1) sy = ny - 2;
+    R w1, w2;
+    R zf = zs_corr(S, K, zsold_in, ix, iy, dtf, w1, w2);
+    if (ix > 0 && iy > 0) {   // zs2Ocorr flux update
+        S.f[QX][i] = ld(S.f[QX] + i) + w1;
+        S.f[QY][i] = ld(S.f[QY] + i) + w2;
+    }
+    if (sy != iy) {           // latbnd(zs)
+        R a, b;
+        zf = zs_corr(S, K, zsold_in, ix, sy, dtf, a, b);
+    }
+    S.f[ZS][i] = zf;
+    S.f[HH][i] = DM<R>::fmax(ld(S.f[ZB] + i) + zf, K.eps);   // hsbnd
+    S.f[UUOLD][i] = ld(S.f[UU] + i);
+    S.f[VVOLD][i] = ld(S.f[VV] + i);
+    zsold_out[i] = zf;
+    R o6[6];
+    uvvu_cell(S, K, ix, sy, o6);   // calcuvvu + uvlatbnd
+    S.f[VU][i] = o6[0]; S.f[UV][i] = o6[1]; S.f[UEU][i] = o6[2]; S.f[VEV][i] = o6[3];
+    S.f[VMAGEU][i] = o6[4]; S.f[VMAGEV][i] = o6[5];
+}
+
+template <class R>
+int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+    dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
+    k_flow_a<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_flow_a");
+    k_flow_u<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_flow_u");
+    k_flow_v<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_flow_v");
+    k_flow_corr<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_flow_corr");
+    k_flow_cont<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_flow_cont");
+    k_flow_final<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_flow_final");
+    return 6;
+}
+template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
+template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
+
+}  // namespace xbg

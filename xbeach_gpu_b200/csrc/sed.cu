@@ -1,0 +1,293 @@
+// sed.cu -- sediment transport and bed update (sedimentstep,
+// Wave_gpu.cu:1405-1635; kernels of Sediment_kernel.cu) in three passes.
+//
+//   k_sed_a  longturb (rolthick; kturb = 0, Sediment_kernel.cu:161), Sbvr,
+//            Rvr, Erosus                      -> rolthick ceqsg Tsg* ua* facero*
+//   k_sed_b  Susp, Conc, CClatbnd, bedupdate  -> C* zb* hh* stdep* dzb
+//   k_sed_c  zblatbnd, avalanching (gathered per cell), updatezb, zblatbnd,
+//            updatezom                        -> zb stdep zs hh dzb cfm fwm C
+// (* = per-step buffer).  hardlayer and zblatbnd(Sout) (:824-879) feed only
+// the bed-load divergence that bedupdate has commented out (:954) and are not
+// evaluated.  All kernels skip the step unless sedtrans = 1 and t >= sedstart
+// (Wave_gpu.cu:724), a flag the device clock sets.
+#include "xbg_common.cuh"
+
+namespace xbg {
+
+#define IDX(x, y) ((x) + (y) * nx)
+
+__device__ __forceinline__ bool sed_skip(const Clock* c) {
+    return halted(c) || *((volatile const int*)&c->do_sed) == 0;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (sed_skip(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy), xm = mm(ix), ym = mm(iy);
+    R dtf = (R)clk->dt, Trep = (R)clk->Trep;
+    R rho = K.rho, g = K.g, eps = K.eps;
+    R c = ld(S.f[CC_] + i);
+    // longturb (Sediment_kernel.cu:27-164)
+    R rolth = ld(S.f[ROLTHICK] + i) + dtf * (DM<R>::fabs(ld(S.f[DZSDT] + i)) - K.beta * c);
+    S.f[ROLTHICK][i] = DM<R>::fmax(rolth, (R)0.0f);
+    S.f[KTURB][i] = (R)0.0f;
+    // Sbvr (:167-326); kturb is 0 after longturb
+    R zo = (R)0.006f, sedcal = (R)1.0f, bulk = (R)1.0f;
+    R D50 = K.D50, D90 = K.D90;
+    R drho = (K.rhosed - rho) / rho;
+    R dester = DM<R>::pow(drho * g, (R)(1.0f / 3.0f)) / (R)0.0001f * D50;
+    R hh = ld(S.f[HH] + i);
+    R hhi = DM<R>::fmax(hh, (R)0.01f);
+    R ue = (R)(0.5 * (double)(ld(S.f[UEU] + IDX(xm, iy)) + ld(S.f[UEU] + i)));
+    R ve = (R)(0.5 * (double)(ld(S.f[VEV] + IDX(ix, ym)) + ld(S.f[VEV] + i)));
+    R vmags = ue * ue + ve * ve;
+    R ML = DM<R>::fmax(DM<R>::fmin(DM<R>::sqrt((R)2.0f * ld(S.f[ROL] + i) * Trep / (rho * c)), hhi), (R)0.01f);
+    R dcfin = DM<R>::exp(DM<R>::fmin(hhi, (R)100.0f) / ML);
+    R dcf = DM<R>::fmin((R)1 / (dcfin - (R)1), (R)1.0f);
+    R kb = K.nuhfac * DM<R>::pow(ld(S.f[DR] + i) / rho, (R)0.66666666667f) * dcf;
+    R urms = ld(S.f[URMS] + i);
+    R Urms2 = urms * urms + (R)1.45f * (kb + (R)0.0f);
+    R Tsg = DM<R>::fmax((R)0.1f * hhi / K.wws, (R)0.5f);
+    R Ucr;
+    if (D50 <= (R)0.0005f) Ucr = (R)0.19f * DM<R>::pow(D50, (R)0.1f) * DM<R>::log10((R)4.0f * hhi / D90);
+    else Ucr = (R)8.50f * DM<R>::pow(D50, (R)0.6f) * DM<R>::log10((R)4.0f * hhi / D90);
+    R hdrag = DM<R>::fmax(hhi, (R)10.0f * zo);
+    R Cd = (R)0.4f / (DM<R>::log(hdrag / zo) - (R)1.0f);
+    Cd = Cd * Cd;
+    R Asb = (R)0.005f * hhi * DM<R>::pow((R)1 / hhi / (drho * g), (R)1.2f);
+    R Ass = (R)0.012f * D50 * DM<R>::pow(dester, (R)-0.6f) / (DM<R>::pow(drho * g * D50, (R)1.2f));
+    R T1 = vmags + (R)0.018f / Cd * Urms2;
+    T1 = DM<R>::fmin(T1, (R)100000.0f * g / ld(S.f[CFM] + i) * D50 * drho);
+    T1 = DM<R>::sqrt(T1);
+    R wetz = hhi > eps ? (R)1 : (R)0;
+    R T2 = (R)0.0f;
+    if (T1 > Ucr && hhi > eps) T2 = DM<R>::pow(T1 - Ucr, (R)2.4f);
+    R ceqb = Asb * T2;
+    ceqb = DM<R>::fmin(ceqb / hhi, (R)0.05f);
+    R ceqbg = ((R)1 - bulk) * ceqb * sedcal * wetz;
+    R ceqs = DM<R>::fmin(Ass * T2 / hhi, (R)0.05f);
+    R ceqsg = (ceqs + bulk * ceqb) * sedcal * wetz;
+    S.f[CEQSG][i] = ceqsg;
+    S.tmp[T_CEQBG][i] = ceqbg;
+    S.tmp[T_TSG][i] = Tsg;
+    // Rvr (:477-509)
+    {
+        R m1 = (R)0.0f, m2 = (R)0.7939f, m3 = (R)-0.6065f, m4 = (R)0.3539f, m5 = (R)0.6373f, m6 = (R)0.5995f;
+        R alpha = (R)-1.0f * DM<R>::log10(DM<R>::exp((R)1.0f)) / m4;
+        R beta = DM<R>::exp(m3 / m4);
+        R k = (R)(2 * XBG_PI / (double)(c * Trep));
+        R Ur = (R)3.0f / (R)8.0f * DM<R>::sqrt((R)2.0f) * ld(S.f[H] + i) * k / DM<R>::pow(k * hh, (R)3.0f);
+        Ur = DM<R>::fmax(Ur, (R)0.00001f);
+        R Bm = m1 + (m2 - m1) / ((R)1.0f + beta * DM<R>::pow(Ur, alpha));
+        R B1 = (R)((double)((R)-90.0f + (R)90.0f * DM<R>::tanh(m5 / DM<R>::pow(Ur, m6))) * XBG_PI / 180.0f);
+        R Sk = Bm * DM<R>::cos(B1);
+        R As = Bm * DM<R>::sin(B1);
+        S.tmp[T_UA][i] = (K.facsk * Sk - K.facas * As) * urms;
+    }
+    // Erosus (:512-531)
+    {
+        R exp_ero = K.morfac * dtf / ((R)1.0f - K.por) * hh * (ceqsg * (R)1.0f / Tsg + ceqbg * (R)1.0f / dtf);
+        S.tmp[T_FACERO][i] = DM<R>::fmin((R)1.0f, ld(S.f[STDEP] + i) * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
+    }
+}
+
+// Susp (Sediment_kernel.cu:534-719): suspended fluxes Sus, Svs at (ix, iy)
+template <class R>
+__device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R& Sus, R& Svs) {
+    const int nx = K.nx, ny = K.ny;
+    int i = IDX(ix, iy), xp = pp(ix, nx), yp = pp(iy, ny);
+    const R* ua = S.tmp[T_UA];
+    R dx = K.dx, eps = K.eps, facsl = (R)1.6f;
+    R hhi = ld(S.f[HH] + i), zbi = ld(S.f[ZB] + i), zbr = ld(S.f[ZB] + IDX(xp, iy)), zbt = ld(S.f[ZB] + IDX(ix, yp));
+    R cci = ld(S.f[CSED] + i), ccr = ld(S.f[CSED] + IDX(xp, iy)), cct = ld(S.f[CSED] + IDX(ix, yp));
+    R uui = ld(S.f[UU] + i), vvi = ld(S.f[VV] + i), tm = ld(S.f[THM] + i);
+    R uai = ld(ua + i), uar = ld(ua + IDX(xp, iy)), uat = ld(ua + IDX(ix, yp));
+    double ctm = (double)DM<R>::cos(tm), stm = (double)DM<R>::sin(tm);
+    R uau = (R)(0.5 * ctm * (double)(uai + uar));
+    R uav = (R)(0.5 * stm * (double)(uar + uai));
+    R uv = ld(S.f[UV] + i), vu = ld(S.f[VU] + i);
+    R urep = ld(S.f[UEU] + i) + uau;
+    R vmagu = DM<R>::sqrt(DM<R>::pow((uui + uau), (R)2.0f) + DM<R>::pow((vu + uav), (R)2.0f));
+    uau = (R)(0.5 * ctm * (double)(uai + uat));
+    uav = (R)(0.5 * stm * (double)(uat + uai));
+    R vrep = ld(S.f[VEV] + i) + uav;
+    R vmagv = DM<R>::sqrt(DM<R>::pow(uv + uau, (R)2.0f) + DM<R>::pow(vvi + uav, (R)2.0f));
+    R dzbdx = (R)-1.0f * (zbr - zbi) / dx;
+    R dzbdy = (R)-1.0f * (zbt - zbi) / dx;
+    R hu = ld(S.f[HU] + i), hv = ld(S.f[HV] + i);
+    R wu = hu > eps ? (R)1.0f : (R)0.0f;
+    R wv = hv > eps ? (R)1.0f : (R)0.0f;
+    R cu, cv;
+    if (urep > (R)0.0f) cu = cci;
+    else if (urep < (R)0.0f) cu = ccr;
+    else cu = (R)0.50f * (cci + ccr);
+    R dcsdx = (ccr - cci) / dx;
+    if (vrep > (R)0.0f) cv = cci;
+    else if (vrep < (R)0.0f) cv = cct;
+    else cv = (R)0.50f * (cci + cct);
+    R dcsdy = (cct - cci) / dx;
+    R Dc = K.nuh + K.nuhfac * hhi * DM<R>::pow(ld(S.f[DR] + i) / K.rho, (R)(1.0f / 3.0f));
+    Sus = K.sus * (cu * urep * hu - Dc * hu * dcsdx - facsl * cu * vmagu * hu * dzbdx) * wu;
+    Svs = K.sus * (cv * vrep * hv - Dc * hv * dcsdy - facsl * cv * vmagv * hv * dzbdy) * wv;
+}
+
+// Conc (Sediment_kernel.cu:721-780) at (ix, iy): new C, ero, depo
+template <class R>
+__device__ __forceinline__ R conc_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R& ero, R& depo) {
+    const int nx = K.nx;
+    int i = IDX(ix, iy);
+    R Susi, Svsi, Susl, t0, t1, Svsb;
+    susp_cell(S, K, ix, iy, Susi, Svsi);
+    int xm = mm(ix), ym = mm(iy);
+    if (xm != ix) susp_cell(S, K, xm, iy, Susl, t0); else Susl = Susi;
+    if (ym != iy) susp_cell(S, K, ix, ym, t1, Svsb); else Svsb = Svsi;
+    R hhi = ld(S.f[HH] + i);
+    R wetz = hhi > K.eps ? (R)1.0f : (R)0.0f;
+    R Tsg = ld(S.tmp[T_TSG] + i);
+    ero = ld(S.tmp[T_FACERO] + i) * hhi * ld(S.f[CEQSG] + i) * (R)1.0f / Tsg;
+    R dsusdx = (Susi - Susl) / K.dx;
+    R dsvsdy = (Svsi - Svsb) / K.dx;
+    R cs = (dtf * Tsg) / (dtf + Tsg) * (hhi * ld(S.f[CSED] + i) / dtf - (dsusdx + dsvsdy - ero)) * wetz;
+    cs = DM<R>::fmax(cs, (R)0.0f);
+    cs = DM<R>::fmin(cs, (R)0.1f * hhi);
+    depo = cs / Tsg;
+    return cs / hhi;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_sed_b(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (sed_skip(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    R dtf = (R)clk->dt;
+    R ero, depo;
+    R cnew = conc_cell(S, K, ix, iy, dtf, ero, depo);
+    // CClatbnd (Sediment_kernel.cu:782-821)
+    if (iy == 0 || iy == ny - 1) {
+        R e2, d2;
+        cnew = conc_cell(S, K, ix, iy == 0 ? pp(0, ny) : mm(ny - 1), dtf, e2, d2);
+    }
+    if (ix == 0) cnew = (R)0.0f;
+    S.tmp[T_UU][i] = cnew;   // per-step buffer reused for the new C
+    if (K.morfac > (R)0.0f) {
+        // bedupdate (:881-968), bed-load divergence commented out there
+        R dzg = K.morfac * dtf / ((R)1.0f - K.por) * (ero - depo);
+        S.tmp[T_ZB][i] = ld(S.f[ZB] + i) + dzg;
+        S.tmp[T_HH][i] = ld(S.f[HH] + i) + dzg;
+        S.f[DZB][i] = (R)-1 * dzg;
+        S.tmp[T_STDEP][i] = ld(S.f[STDEP] + i) - dzg;
+    }
+}
+
+// zblatbnd source cell (Sediment_kernel.cu:970-1018, pre-kernel reads)
+__device__ __forceinline__ int zbl_src(int ix, int iy, int nx, int ny) {
+    int sx = ix, sy = iy;
+    if (iy == 0) sy = pp(iy, ny);
+    if (iy == ny - 1) sy = mm(iy);
+    if (ix == 0) { sx = pp(ix, nx); sy = iy; }
+    return sx + sy * nx;
+}
+
+// avalanching (Sediment_kernel.cu:1020-1137) transfers (dzbx, dzby) of (ix, iy)
+template <class R>
+__device__ __forceinline__ void aval_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R& dzbx, R& dzby) {
+    const int nx = K.nx, ny = K.ny;
+    const R* zb = S.tmp[T_ZB]; const R* sd = S.tmp[T_STDEP];
+    int xp = pp(ix, nx), yp = pp(iy, ny);
+    R Zbi = ld(zb + zbl_src(ix, iy, nx, ny)), Zbt = ld(zb + zbl_src(ix, yp, nx, ny)), Zbr = ld(zb + zbl_src(xp, iy, nx, ny));
+    R sti = ld(sd + zbl_src(ix, iy, nx, ny)), stt = ld(sd + zbl_src(ix, yp, nx, ny)), str = ld(sd + zbl_src(xp, iy, nx, ny));
+    R dx = K.dx, maxchg = K.maxslpchg;
+    R dzmax = ld(S.tmp[T_HH] + IDX(ix, iy)) > K.eps ? K.wetdzmax : K.drydzmax;
+    dzbx = (R)0.0f; dzby = (R)0.0f;
+    R dzbdx = (Zbr - Zbi) / dx;
+    if (DM<R>::fabs(dzbdx) > dzmax) {
+        R s = dzbdx / DM<R>::fabs(dzbdx);
+        dzbx = s * (DM<R>::fabs(dzbdx) - dzmax) * dx;
+        if (s > (R)0) {
+            dzbx = DM<R>::fmin(dzbx, maxchg * dtf / dx);
+            dzbx = DM<R>::fmin(dzbx, sti);
+        } else {
+            dzbx = DM<R>::fmax(dzbx, (R)-1.0f * maxchg * dtf / dx);
+            dzbx = DM<R>::fmax(dzbx, (R)-1.0f * str);
+        }
+    }
+    R dzbdy = (Zbt - Zbi) / dx;
+    if (DM<R>::fabs(dzbdy) > dzmax) {
+        R s = dzbdy / DM<R>::fabs(dzbdy);
+        dzby = s * (DM<R>::fabs(dzbdy) - dzmax) * dx;
+        if (s > (R)0) {
+            dzby = DM<R>::fmin(dzby, maxchg * dtf / dx);
+            dzby = DM<R>::fmin(dzby, sti);
+        } else {
+            dzby = DM<R>::fmax(dzby, (R)-1 * maxchg * dtf / dx);
+            dzby = DM<R>::fmax(dzby, (R)-1 * stt);
+        }
+    }
+}
+
+// bed change of (ix, iy) gathered from its own and its neighbours' transfers,
+// in the order a serial launch adds them: ((-dzby[below] - dzbx[left]) + dzbx) + dzby
+template <class R>
+__device__ __forceinline__ R ddzb_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf) {
+    R a = (R)0.0f, bx, by, t;
+    if (iy > 0) { aval_cell(S, K, ix, iy - 1, dtf, t, by); a = a - by; }
+    if (ix > 0) { aval_cell(S, K, ix - 1, iy, dtf, bx, t); a = a - bx; }
+    aval_cell(S, K, ix, iy, dtf, bx, by);
+    a = a + bx;
+    a = a + by;
+    return a;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_sed_c(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (sed_skip(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    S.f[CSED][i] = ld(S.tmp[T_UU] + i);
+    if (K.morfac > (R)0.0f) {
+        R dtf = (R)clk->dt;
+        R dd = ddzb_cell(S, K, ix, iy, dtf);
+        // updatezb (:1139-1160) at the own cell
+        S.f[DZB][i] = ld(S.f[DZB] + i) - dd;
+        S.f[ZS][i] = ld(S.f[ZS] + i) - dd;
+        S.f[HH][i] = ld(S.tmp[T_HH] + i) - dd;
+        // zb, stdep: updatezb at the zblatbnd source, then the copy
+        int s = zbl_src(ix, iy, nx, ny);
+        int sx = s % nx, sy = s / nx;
+        R ds = (s == i) ? dd : ddzb_cell(S, K, sx, sy, dtf);
+        int s1 = zbl_src(sx, sy, nx, ny);
+        R zbn = ld(S.tmp[T_ZB] + s1) + ds;
+        R sdn = ld(S.tmp[T_STDEP] + s1) - ds;
+        S.f[ZB][i] = zbn;
+        S.f[STDEP][i] = sdn;
+        // updatezom (:1162-1190)
+        if (sdn < (R)0.05f) { S.f[CFM][i] = K.cfreef; S.f[FWM][i] = K.fwreef; }
+        else { S.f[CFM][i] = K.cfsand; S.f[FWM][i] = K.fwsand; }
+    }
+}
+
+template <class R>
+int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+    dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
+    k_sed_a<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_sed_a");
+    k_sed_b<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_sed_b");
+    k_sed_c<R><<<g, b, 0, st>>>(S, K);
+    PMARK(pf, "k_sed_c");
+    return 3;
+}
+template int launch_sed<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
+template int launch_sed<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
+
+}  // namespace xbg

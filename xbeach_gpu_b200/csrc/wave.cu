@@ -1,0 +1,1038 @@
+// wave.cu -- wave action balance of one step (wavestep, Wavestep.cu:755-1167;
+// arithmetic of the reference's CPU judge, wave_CPU.cpp).
+//
+// Kernels (launch order):
+//   k_disp       dispersion (wave_CPU.cpp:154-205) per cell -> k, c, cg
+//   k_wave_main  rows 1..ny-2: offshore boundary + sanity + action, x/y/theta
+//                second-order upwind advection of ee and rr with the Euler
+//                step, energy, energint, roelvink|baldock, dissipation,
+//                meandir, radstress.  All theta bins of a cell live in
+//                registers; ctheta (propagtheta) is evaluated on the fly from
+//                per-cell slopes and never stored.  Emits the per-block
+//                WAVEDT minimum for the next step's dt.
+//   k_wave_edge  rows 0 and ny-1, whose ee/rr are copies of rows 1 / ny-2
+//                (rollerlatbnd, wave_CPU.cpp:830-870) between the passes.
+//   k_wave_force wavforce + twodimbnd(noix) + breakerdelay + twodimbnd(ust).
+#include "xbg_common.cuh"
+
+namespace xbg {
+
+// ---------------------------------------------------------------- helpers
+// (R)(1.5*(double)a - 0.5*(double)b): one rounding of the exact value, as the
+// double literals of xadvecupwind2CPU give (wave_CPU.cpp:426-453).
+template <class R> __device__ __forceinline__ R up2d(R a, R b) {
+    return DM<R>::fma((R)1.5, a, (R)-0.5 * b);
+}
+// 1.5f*a - 0.5f*b with two roundings (thetaadvecuw2hoCPU, wave_CPU.cpp:747-790).
+template <class R> __device__ __forceinline__ R up2f(R a, R b) {
+    R x = (R)1.5f * a;
+    R y = (R)0.5f * b;
+    return x - y;
+}
+
+// dispersion relation, wave_CPU.cpp:154-205 (golden-ratio relaxation)
+template <class R>
+__device__ void disp_cell(const Konst<R>& K, R sg, R h, R& k_, R& c_, R& cg_) {
+    R g = K.g;
+    R L0 = K.twopi * g / (sg * sg);
+    R L1 = L0, L2, errdisp;
+    for (int n = 1; n < 200; n++) {
+        L2 = (R)((double)L0 * ::tanh(2 * XBG_PI * (double)h / (double)L1));
+        errdisp = DM<R>::fabs(L2 - L1);
+        L1 = (L1 * K.aphi + L2 * K.bphi);
+        if (errdisp <= 0.0001f) break;
+        if (n == 199) {
+            L1 = L0 * DM<R>::pow(DM<R>::tanh(DM<R>::pow(sg * sg * h / g, (R)(3.0f / 4.0f))), (R)(2.0f / 3.0f));
+            break;
+        }
+    }
+    R kk = (R)(2 * XBG_PI / (double)L1);
+    k_ = kk;
+    R cc = sg / kk;
+    c_ = cc;
+    R kkhh = cmin(kk * h, (R)10.0f);
+    R s2kh = DM<R>::sinh((R)2.0f * kkhh);
+    cg_ = cc * ((R)0.5f + kkhh / s2kh);
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_disp(Dev<R> S, Konst<R> K) {
+    if (halted(S.clk)) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.C) return;
+    R sg = (R)S.clk->sigm;
+    R k_, c_, cg_;
+    disp_cell(K, sg, ld(S.f[HH] + i), k_, c_, cg_);
+    S.f[WK][i] = k_;
+    S.f[CC_][i] = c_;
+    S.f[CG][i] = cg_;
+}
+
+// Per-cell slope terms of propagtheta (wave_CPU.cpp:226-306).
+template <class R>
+struct CthCoef { R s, dhdx, dhdy, dudx, dudy, dvdx, dvdy, wci, sg; };
+
+template <class R>
+__device__ __forceinline__ CthCoef<R> cth_coef(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R sg) {
+    const int nx = K.nx, ny = K.ny;
+    const R* hh = S.f[HH]; const R* uu = S.f[UU]; const R* vv = S.f[VV];
+    int xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+    R dxf = K.dx;
+    R sx = (R)(xp - xm) * dxf, sy = (R)(yp - ym) * dxf;
+    CthCoef<R> c;
+    c.dhdx = (ld(hh + xp + iy * nx) - ld(hh + xm + iy * nx)) / sx;
+    c.dudx = (ld(uu + xp + iy * nx) - ld(uu + xm + iy * nx)) / sx;
+    c.dvdx = (ld(vv + xp + iy * nx) - ld(vv + xm + iy * nx)) / sx;
+    c.dhdy = (ld(hh + ix + yp * nx) - ld(hh + ix + ym * nx)) / sy;
+    c.dudy = (ld(uu + ix + yp * nx) - ld(uu + ix + ym * nx)) / sy;
+    c.dvdy = (ld(vv + ix + yp * nx) - ld(vv + ix + ym * nx)) / sy;
+    int i = ix + iy * nx;
+    R h = ld(hh + i);
+    R kh = cmin(ld(S.f[WK] + i) * h, (R)10.0f);
+    c.s = sg / DM<R>::sinh((R)2.0f * kh);
+    c.wci = K.wci * cmin(h / K.hwci, (R)1.0f);
+    c.sg = sg;
+    return c;
+}
+template <class R>
+__device__ __forceinline__ R cth_eval(const CthCoef<R>& c, R cx, R sx) {
+    R ctht = (c.s) * (c.dhdx * sx - c.dhdy * cx) +
+             c.wci * (cx * (sx * c.dudx - cx * c.dudy) + sx * (sx * c.dvdx - cx * c.dvdy));
+    return cmin(cmax(ctht, (R)(-0.25f * c.sg)), (R)(0.25f * c.sg));
+}
+
+// x/y second-order upwind fluxes of one theta plane, xadvecupwind2CPU /
+// yadvecupwind2CPU (wave_CPU.cpp:367-560).  q(-2..2) are the plane's values at
+// the clamped neighbours mminus2, mminus, i, pplus, pplus2.
+template <class R>
+__device__ __forceinline__ R adv2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin, R dxplus_i) {
+    R arrin, arrmin;
+    if (cf > (R)0.0f) {
+        arrin = up2d(qi, qm);
+        if (arrin < (R)0.0f) arrin = qi;
+        arrin = arrin * cf;
+    } else {
+        arrin = up2d(qp, qp2);
+        if (arrin < (R)0.0f) arrin = qp;
+        arrin = arrin * cf;
+    }
+    if (cfmin > (R)0.0f) {
+        arrmin = up2d(qm, qm2);
+        if (arrmin < (R)0.0f) arrmin = qm;
+        arrmin = arrmin * cfmin;
+    } else {
+        arrmin = up2d(qi, qp);
+        if (arrmin < (R)0.0f) arrmin = qi;
+        arrmin = arrmin * cfmin;
+    }
+    return (arrin - arrmin) * dxplus_i;
+}
+
+// Advected field of one cell: q_new[t] = q[t] - dt*(xadv + yadv + thetaadv).
+// loadq(ix, iy, t) returns the (transformed) plane value at a grid point.
+template <class R, int NMAX, class LoadQ>
+__device__ __forceinline__ void advect_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy,
+                                            const R* speed, const R* cthv, LoadQ loadq, R dtf,
+                                            R* out) {
+    const int nx = K.nx, ny = K.ny, nt = K.nt;
+    int i = ix + iy * nx;
+    int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
+    int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
+    R dxplus_i = (R)1.0f / K.dx;
+    R wci = K.wci * cmin(ld(S.f[HH] + i) / K.hwci, (R)1.0f);
+    R ccg = ld(speed + i);
+    R ccgxmin = ld(speed + xm + iy * nx), ccgxmax = ld(speed + xp + iy * nx);
+    R ccgymin = ld(speed + ix + ym * nx), ccgymax = ld(speed + ix + yp * nx);
+    const R* uu = S.f[UU]; const R* vv = S.f[VV];
+    R uui = ld(uu + i) * wci;
+    R uuixmin = ld(uu + xm + iy * nx) * wci;
+    R uuixmax = ld(uu + xp + iy * nx) * wci;
+    R vvi = wci * ld(vv + i);
+    R vviymin = wci * ld(vv + ix + ym * nx);
+    R vviymax = wci * ld(vv + ix + yp * nx);
+    R own[NMAX];
+#pragma unroll
+    for (int t = 0; t < NMAX; t++) own[t] = (t < nt) ? loadq(ix, iy, t) : (R)0;
+    R dth = K.dtheta;
+#pragma unroll
+    for (int t = 0; t < NMAX; t++) {
+        if (t < nt) {
+            R ct = K.cxsth[t], st = K.sxnth[t];
+            R cgx = (R)0.5f * (ccg * ct + uui + ccgxmax * ct + uuixmax);
+            R cgxmin = (R)0.5f * (ccg * ct + uui + ccgxmin * ct + uuixmin);
+            R xa = adv2(loadq(xm2, iy, t), loadq(xm, iy, t), own[t], loadq(xp, iy, t), loadq(xp2, iy, t),
+                        cgx, cgxmin, dxplus_i);
+            R cgy = (R)0.5f * (ccg * st + vvi + ccgymax * st + vviymax);
+            R cgymin = (R)0.5f * (ccg * st + vvi + ccgymin * st + vviymin);
+            R ya = adv2(loadq(ix, ym2, t), loadq(ix, ym, t), own[t], loadq(ix, yp, t), loadq(ix, yp2, t),
+                        cgy, cgymin, dxplus_i);
+            // thetaadvecuw2hoCPU (wave_CPU.cpp:706-806) with clamped bins
+            R ta = (R)0.0f;
+            if (nt > 1) {
+                const int tm = t > 0 ? t - 1 : 0;
+                const int tm2 = t > 1 ? t - 2 : 0;
+                const int t1 = (t + 1 < NMAX) ? t + 1 : t;
+                const int t2 = (t + 2 < NMAX) ? t + 2 : t1;
+                R e_p = (t + 1 < nt) ? own[t1] : own[t];
+                R e_p2 = (t + 2 < nt) ? own[t2] : e_p;
+                R c_p = (t + 1 < nt) ? cthv[t1] : cthv[t];
+                R cthetab = (R)0.5f * (cthv[t] + c_p);
+                R eupw;
+                if (cthetab > (R)0.0f) {
+                    eupw = up2f(own[t], own[tm]);
+                    if (eupw < (R)0.0f) eupw = own[t];
+                } else {
+                    eupw = up2f(e_p, e_p2);
+                    if (eupw < (R)0.0f) eupw = e_p;
+                }
+                R arrint = cthetab * eupw;
+                cthetab = (R)0.5f * (cthv[tm] + cthv[t]);
+                if (cthetab > (R)0.0f) {
+                    eupw = up2f(own[tm], own[tm2]);
+                    if (eupw < (R)0.0f) eupw = own[tm];
+                } else {
+                    eupw = up2f(own[t], e_p);
+                    if (eupw < (R)0.0f) eupw = own[t];
+                }
+                R arrmint = cthetab * eupw;
+                ta = (arrint - arrmint) / dth;
+                if (t == nt - 1) ta = ((R)0.0f - arrmint) / dth;
+                if (t == 0) ta = (arrint - (R)0.0f) / dth;
+            }
+            out[t] = own[t] - dtf * (xa + ya + ta);
+        } else {
+            out[t] = (R)0;
+        }
+    }
+}
+
+// Per-cell chain after advection: energy, energint, roelvink|baldock and
+// dissipation (wave_CPU.cpp:873-1092).  e (advected ee with the row copy
+// applied) and r (rr before dissipation) are updated in place.
+template <class R>
+struct CellOut { R E, H, D, R_, DR; };
+
+template <class R, int NMAX>
+__device__ __forceinline__ CellOut<R> chain_cell(const Dev<R>& S, const Konst<R>& K, int i, R sg, R dtf,
+                                                 R Trep, R* e, R* r) {
+    const int nt = K.nt;
+    R rho = K.rho, g = K.g, dth = K.dtheta;
+    R hh = ld(S.f[HH] + i);
+    CellOut<R> o;
+    // energyCPU
+#pragma unroll
+    for (int t = 0; t < NMAX; t++)
+        if (t < nt) e[t] = cmax(e[t] * sg, (R)0.0f);
+    // energintCPU
+    R Etmp = (R)0.0f;
+#pragma unroll
+    for (int t = 0; t < NMAX; t++)
+        if (t < nt) Etmp = Etmp + e[t];
+    Etmp = Etmp * dth;
+    R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
+    R idiv = cmax((R)1.0f, DM<R>::pow(Htmp / (K.gammax * hh), (R)2.0f));
+#pragma unroll
+    for (int t = 0; t < NMAX; t++)
+        if (t < nt) e[t] = e[t] / idiv;
+    Htmp = cmin(Htmp, K.gammax * hh);
+    R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
+    R k = ld(S.f[WK] + i);
+    R fw = ld(S.f[FWM] + i);
+    R Dv;
+    if (K.breakmodel == 1) {
+        // roelvinkCPU (wave_CPU.cpp:927-985): double arithmetic as there
+        R fac = (R)(8.0 / (double)rho / (double)g);
+        R Ht = DM<R>::sqrt(Eint * fac);
+        R Qb = (R)(1.0 - ::exp(cmax(-1.0 * (double)DM<R>::pow((Ht / K.gammaa / hh), K.nexp), -100.0)));
+        Qb = cmin(Qb, (R)1.0f);
+        Dv = (R)((double)Qb * 2.0 * (double)K.alpha / (double)Trep * (double)Eint * (double)Ht / (double)hh);
+        R uorb = (R)(XBG_PI * (double)Ht / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
+        Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
+                                  (double)uorb * (double)uorb);
+    } else {
+        // baldockCPU (wave_CPU.cpp:987-1028)
+        R khh = k * hh;
+        R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
+        R Rr = Hb / cmax(Htmp, (R)0.00001f);
+        R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
+        Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
+        R uorb = (R)(XBG_PI * (double)Htmp / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
+        Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
+                                  (double)uorb * (double)uorb);
+    }
+    // dissipationCPU (wave_CPU.cpp:1030-1092)
+    R wci = K.wci * cmin(hh / K.hwci, (R)1.0f);
+    R cc = ld(S.f[CC_] + i);
+    R uui = ld(S.f[UU] + i) * wci, vvi = ld(S.f[VV] + i) * wci;
+    R RR = (R)0.0f, drr = (R)0.0f;
+    R Emax = cmax(Eint, (R)0.0000001f);
+    bool wet = hh > K.eps;
+#pragma unroll
+    for (int t = 0; t < NMAX; t++) {
+        if (t < nt) {
+            R cx = cc * K.cxsth[t] + uui;
+            R cy = cc * K.sxnth[t] + vvi;
+            R eet = e[t];
+            R dd = eet * Dv / Emax;
+            R rrt;
+            if (wet) {
+                rrt = r[t];
+                R rrd = (R)2.0f * g * K.beta * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+                eet = cmax(eet - dtf * dd, (R)0.0f);
+                rrt = cmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                drr = drr + rrd;
+            } else {
+                eet = (R)0.0f; rrt = (R)0.0f; drr = (R)0.0f;
+            }
+            RR = RR + rrt;
+            e[t] = eet;
+            r[t] = rrt;
+        }
+    }
+    o.E = Eint; o.H = Htmp; o.D = Dv; o.R_ = RR * dth; o.DR = drr * dth;
+    return o;
+}
+
+// meandir + radstress (wave_CPU.cpp:1095-1162) of the final ee (e) and rr (r);
+// writes everything a cell owns at the end of the wave pass.
+template <class R, int NMAX>
+__device__ __forceinline__ void finish_cell(const Dev<R>& S, const Konst<R>& K, int i, const R* e,
+                                            const R* r, const CellOut<R>& o, R* een, R* rrn) {
+    const int nt = K.nt, C = S.C;
+    R rho = K.rho, g = K.g, dth = K.dtheta;
+    R sume = (R)0, sumethet = (R)0;
+    R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0, sum2 = 0;
+#pragma unroll
+    for (int t = 0; t < NMAX; t++) {
+        if (t < nt) {
+            R et = e[t], rt = r[t];
+            R cx = K.cxsth[t], sx = K.sxnth[t];
+            sume = sume + et;
+            sumethet = sumethet + et * K.theta[t];
+            sum2 = sum2 + et;
+            txx = txx + (((R)1.0f + cx * cx) * et);
+            tyy = tyy + (((R)1.0f + sx * sx) * et);
+            txy = txy + (sx * cx * et);
+            rxx = rxx + ((cx * cx) * rt);
+            ryy = ryy + ((sx * sx) * rt);
+            rxy = rxy + (sx * cx * rt);
+            een[i + (size_t)t * C] = et;
+            rrn[i + (size_t)t * C] = rt;
+        }
+    }
+    sume = cmax(sume, (R)0.00001f);
+    S.f[THM][i] = (sumethet / (R)nt) / (sume / (R)nt);
+    S.f[E][i] = sume * dth;
+    S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
+    S.f[D][i] = o.D;
+    S.f[ROL][i] = o.R_;
+    S.f[DR][i] = o.DR;
+    R n = ld(S.f[CG] + i) / ld(S.f[CC_] + i);
+    S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
+    S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
+    S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
+}
+
+template <class R>
+__device__ __forceinline__ void block_min_store(R v, R* dst) {
+    // warp shuffle, then one value per warp through shared memory
+    for (int o = 16; o > 0; o >>= 1) v = DM<R>::fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ R wmin[32];
+    int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    int nw = (blockDim.x * blockDim.y + 31) / 32;
+    if ((tid & 31) == 0) wmin[tid >> 5] = v;
+    __syncthreads();
+    if (tid < 32) {
+        R m = tid < nw ? wmin[tid] : (R)3.0e38f;
+        for (int o = 16; o > 0; o >>= 1) m = DM<R>::fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (tid == 0) *dst = m;
+    }
+}
+
+// ctheta of every bin of a cell and WAVEDT (Wave_kernel.cu:232-249):
+// min over theta of cfl*dtheta/|ctheta|.
+template <class R, int NMAX>
+__device__ __forceinline__ R ctheta_cell(const Konst<R>& K, const CthCoef<R>& cc, R* cthv) {
+    R mindt = (R)9999999.9f;
+#pragma unroll
+    for (int t = 0; t < NMAX; t++) {
+        if (t < K.nt) {
+            cthv[t] = cth_eval(cc, K.cxsth[t], K.sxnth[t]);
+            mindt = DM<R>::fmin(K.cfl * K.dtheta / DM<R>::fabs(cthv[t]), mindt);
+        } else {
+            cthv[t] = (R)0;
+        }
+    }
+    return mindt;
+}
+
+template <class R, int NMAX>
+__global__ void __launch_bounds__(256) k_wave_main(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    R dtw = (R)3.0e38f;
+    if (ix < nx && iy <= ny - 2) {
+        int i = ix + iy * nx;
+        int par = clk->par;
+        const R* eeo = S.ee[par ^ 1];
+        const R* rro = S.rr[par ^ 1];
+        R* een = S.ee[par];
+        R* rrn = S.rr[par];
+        R sg = (R)clk->sigm;
+        R dtf = (R)clk->dt;
+        R Trep = (R)clk->Trep;
+        R tt = (R)clk->totaltime;
+        R taper = (R)cmin((double)tt / 100.0, 1.0);
+        const R* St = S.St;
+        CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
+        R cthv[NMAX];
+        dtw = ctheta_cell<R, NMAX>(K, cc, cthv);
+        // ee after offshorebndWav, sanity and action (wave_CPU.cpp:24-70, 308-326)
+        auto qe = [&](int x, int y, int t) -> R {
+            R v = (x == 0) ? St[y + t * ny] * taper : ld(eeo + x + y * nx + (size_t)t * C);
+            v = cmax(v, (R)0.000f);
+            return v / sg;
+        };
+        auto qr = [&](int x, int y, int t) -> R { return ld(rro + x + y * nx + (size_t)t * C); };
+        R e[NMAX], r[NMAX];
+        advect_cell<R, NMAX>(S, K, ix, iy, S.f[CG], cthv, qe, dtf, e);
+        if (K.roller == 1) {
+            advect_cell<R, NMAX>(S, K, ix, iy, S.f[CC_], cthv, qr, dtf, r);
+        } else {
+#pragma unroll
+            for (int t = 0; t < NMAX; t++) r[t] = (t < nt) ? qr(ix, iy, t) : (R)0;
+        }
+        if (iy == 1 || iy == ny - 2) {   // advected rows 1 / ny-2 for the edge rows
+            int slot = (iy == 1) ? 0 : 1;
+#pragma unroll
+            for (int t = 0; t < NMAX; t++) {
+                if (t < nt) {
+                    S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = e[t];
+                    S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = r[t];
+                }
+            }
+        }
+        CellOut<R> o = chain_cell<R, NMAX>(S, K, i, sg, dtf, Trep, e, r);
+        finish_cell<R, NMAX>(S, K, i, e, r, o, een, rrn);
+    }
+    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
+}
+
+// thetaadvecuw2hoCPU (wave_CPU.cpp:706-806) at bin t from the clamped bin
+// window e(t-2..t+2) and ctheta window c(t-1..t+1).
+template <class R>
+__device__ __forceinline__ R theta_adv(R em2, R em, R e0, R ep, R ep2, R cm, R c0, R cp, int t, int nt, R dth) {
+    if (nt <= 1) return (R)0.0f;
+    R cthetab = (R)0.5f * (c0 + cp);
+    R eupw;
+    if (cthetab > (R)0.0f) {
+        eupw = up2f(e0, em);
+        if (eupw < (R)0.0f) eupw = e0;
+    } else {
+        eupw = up2f(ep, ep2);
+        if (eupw < (R)0.0f) eupw = ep;
+    }
+    R arrint = cthetab * eupw;
+    cthetab = (R)0.5f * (cm + c0);
+    if (cthetab > (R)0.0f) {
+        eupw = up2f(em, em2);
+        if (eupw < (R)0.0f) eupw = em;
+    } else {
+        eupw = up2f(e0, ep);
+        if (eupw < (R)0.0f) eupw = e0;
+    }
+    R arrmint = cthetab * eupw;
+    // zero flux through the first and last bin edges: one division of the
+    // selected numerator (arrint - 0 and 0 - arrmint are exact)
+    R num = (t == 0) ? arrint : ((t == nt - 1) ? (R)0.0f - arrmint : arrint - arrmint);
+    return num / dth;
+}
+
+// Face speeds of one cell for the x/y upwind fluxes (xadvecupwind2CPU:
+// cg at i and the x/y neighbours, u*wci and v*wci with wci of the cell).
+template <class R>
+struct Faces { R sp, sxm, sxp, sym, syp; };
+
+// The wave-action pass of rows 1..ny-2, streaming the theta planes: for each
+// bin t the x/y fluxes read the plane's neighbours (L1/L2 resident), the
+// theta flux uses a sliding register window of the cell's own bins, and the
+// advected ee / rr of the bin are parked in shared memory for the per-cell
+// chain (energint needs the sum over all bins before dissipation).
+template <class R>
+__global__ void __launch_bounds__(256, 3) k_wave_rows(Dev<R> S, Konst<R> K) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
+    const int nthr = blockDim.x * blockDim.y;
+    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
+    R* sA = (R*)smem_raw;            // [nt][nthr] advected ee
+    R* sR = sA + (size_t)nt * nthr;  // [nt][nthr] advected rr
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    R dtw = (R)3.0e38f;
+    if (ix < nx && iy <= ny - 2) {
+        const int i = ix + iy * nx;
+        const int par = clk->par;
+        const R* eeo = S.ee[par ^ 1];
+        const R* rro = S.rr[par ^ 1];
+        R* een = S.ee[par];
+        R* rrn = S.rr[par];
+        const R sg = (R)clk->sigm;
+        const R dtf = (R)clk->dt;
+        const R Trep = (R)clk->Trep;
+        const R tt = (R)clk->totaltime;
+        const R taper = (R)cmin((double)tt / 100.0, 1.0);
+        const R* St = S.St;
+        const int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
+        const int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
+        const int o_xm2 = xm2 + iy * nx, o_xm = xm + iy * nx, o_xp = xp + iy * nx, o_xp2 = xp2 + iy * nx;
+        const int o_ym2 = ix + ym2 * nx, o_ym = ix + ym * nx, o_yp = ix + yp * nx, o_yp2 = ix + yp2 * nx;
+        const R hh = ld(S.f[HH] + i);
+        const CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
+        const R wci = cc.wci;
+        const R dxplus_i = (R)1.0f / K.dx;
+        const R dth = K.dtheta;
+        const R* cgp = S.f[CG];
+        const R* cp = S.f[CC_];
+        Faces<R> fe{ld(cgp + i), ld(cgp + o_xm), ld(cgp + o_xp), ld(cgp + o_ym), ld(cgp + o_yp)};
+        Faces<R> fr{ld(cp + i), ld(cp + o_xm), ld(cp + o_xp), ld(cp + o_ym), ld(cp + o_yp)};
+        const R* uu = S.f[UU]; const R* vv = S.f[VV];
+        const R uui = ld(uu + i) * wci, uuixmin = ld(uu + o_xm) * wci, uuixmax = ld(uu + o_xp) * wci;
+        const R vvi = wci * ld(vv + i), vviymin = wci * ld(vv + o_ym), vviymax = wci * ld(vv + o_yp);
+        // ee after offshorebndWav + sanity + action at plane t (column 0 is St)
+        auto qe = [&](int off, int x, int y, int t) -> R {
+            R v = (x == 0) ? St[y + t * ny] * taper : ld(eeo + off + (size_t)t * C);
+            v = cmax(v, (R)0.000f);
+            return v / sg;
+        };
+        const bool roller = K.roller == 1;
+        // windows of the cell's own bins: clamp(t-2) .. clamp(t+2)
+        auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
+        R we0 = qe(i, ix, iy, cl(-2)), we1 = qe(i, ix, iy, cl(-1)), we2 = qe(i, ix, iy, 0),
+          we3 = qe(i, ix, iy, cl(1)), we4 = qe(i, ix, iy, cl(2));
+        R wr0 = ld(rro + i + (size_t)cl(-2) * C), wr1 = ld(rro + i + (size_t)cl(-1) * C), wr2 = ld(rro + i),
+          wr3 = ld(rro + i + (size_t)cl(1) * C), wr4 = ld(rro + i + (size_t)cl(2) * C);
+        R c0 = cth_eval(cc, K.cxsth[0], K.sxnth[0]);
+        R cm = c0;
+        R cpp = cth_eval(cc, K.cxsth[cl(1)], K.sxnth[cl(1)]);
+        R Etmp = (R)0.0f;
+        const bool edge_row = (iy == 1 || iy == ny - 2);
+        const int slot = (iy == 1) ? 0 : 1;
+#pragma unroll 1
+        for (int t = 0; t < nt; t++) {
+            const size_t o = (size_t)t * C;
+            const R ct = K.cxsth[t], st = K.sxnth[t];
+            dtw = DM<R>::fmin(K.cfl * dth / DM<R>::fabs(c0), dtw);
+            // ee: x and y fluxes of plane t, theta flux from the window
+            R cgx = (R)0.5f * (fe.sp * ct + uui + fe.sxp * ct + uuixmax);
+            R cgxmin = (R)0.5f * (fe.sp * ct + uui + fe.sxm * ct + uuixmin);
+            R cgy = (R)0.5f * (fe.sp * st + vvi + fe.syp * st + vviymax);
+            R cgymin = (R)0.5f * (fe.sp * st + vvi + fe.sym * st + vviymin);
+            R xa = adv2(qe(o_xm2, xm2, iy, t), qe(o_xm, xm, iy, t), we2, qe(o_xp, xp, iy, t),
+                        qe(o_xp2, xp2, iy, t), cgx, cgxmin, dxplus_i);
+            R ya = adv2(qe(o_ym2, ix, ym2, t), qe(o_ym, ix, ym, t), we2, qe(o_yp, ix, yp, t),
+                        qe(o_yp2, ix, yp2, t), cgy, cgymin, dxplus_i);
+            R ta = theta_adv(we0, we1, we2, we3, we4, cm, c0, cpp, t, nt, dth);
+            R A = we2 - dtf * (xa + ya + ta);
+            // rr with the phase speed c (Wavestep.cu:1277-1284)
+            R Ar = wr2;
+            if (roller) {
+                R cx = (R)0.5f * (fr.sp * ct + uui + fr.sxp * ct + uuixmax);
+                R cxm = (R)0.5f * (fr.sp * ct + uui + fr.sxm * ct + uuixmin);
+                R cy = (R)0.5f * (fr.sp * st + vvi + fr.syp * st + vviymax);
+                R cym = (R)0.5f * (fr.sp * st + vvi + fr.sym * st + vviymin);
+                R xr = adv2(ld(rro + o_xm2 + o), ld(rro + o_xm + o), wr2, ld(rro + o_xp + o),
+                            ld(rro + o_xp2 + o), cx, cxm, dxplus_i);
+                R yr = adv2(ld(rro + o_ym2 + o), ld(rro + o_ym + o), wr2, ld(rro + o_yp + o),
+                            ld(rro + o_yp2 + o), cy, cym, dxplus_i);
+                R tr = theta_adv(wr0, wr1, wr2, wr3, wr4, cm, c0, cpp, t, nt, dth);
+                Ar = wr2 - dtf * (xr + yr + tr);
+            }
+            sA[t * nthr + tid] = A;
+            sR[t * nthr + tid] = Ar;
+            if (edge_row) {   // advected rows 1 / ny-2 for the edge rows
+                S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = A;
+                S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = Ar;
+            }
+            Etmp = Etmp + cmax(A * sg, (R)0.0f);   // energyCPU, then the energint sum
+            // slide the windows
+            const int tn = cl(t + 3);
+            we0 = we1; we1 = we2; we2 = we3; we3 = we4; we4 = qe(i, ix, iy, tn);
+            wr0 = wr1; wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(rro + i + (size_t)tn * C);
+            cm = c0; c0 = cpp; cpp = cth_eval(cc, K.cxsth[cl(t + 2)], K.sxnth[cl(t + 2)]);
+        }
+        // energintCPU (wave_CPU.cpp:891-924)
+        const R rho = K.rho, g = K.g;
+        Etmp = Etmp * dth;
+        R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
+        const R idiv = cmax((R)1.0f, DM<R>::pow(Htmp / (K.gammax * hh), (R)2.0f));
+        Htmp = cmin(Htmp, K.gammax * hh);
+        const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
+        const R k = ld(S.f[WK] + i);
+        const R fw = ld(S.f[FWM] + i);
+        R Dv;
+        if (K.breakmodel == 1) {   // roelvinkCPU (wave_CPU.cpp:927-985)
+            R fac = (R)(8.0 / (double)rho / (double)g);
+            R Ht = DM<R>::sqrt(Eint * fac);
+            R Qb = (R)(1.0 - ::exp(cmax(-1.0 * (double)DM<R>::pow((Ht / K.gammaa / hh), K.nexp), -100.0)));
+            Qb = cmin(Qb, (R)1.0f);
+            Dv = (R)((double)Qb * 2.0 * (double)K.alpha / (double)Trep * (double)Eint * (double)Ht / (double)hh);
+            R uorb = (R)(XBG_PI * (double)Ht / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
+            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
+                                      (double)uorb * (double)uorb);
+        } else {                   // baldockCPU (wave_CPU.cpp:987-1028)
+            R khh = k * hh;
+            R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
+            R Rr = Hb / cmax(Htmp, (R)0.00001f);
+            R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
+            Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
+            R uorb = (R)(XBG_PI * (double)Htmp / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
+            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
+                                      (double)uorb * (double)uorb);
+        }
+        // dissipationCPU (wave_CPU.cpp:1030-1092), then meandir and radstress
+        // on the final bins (wave_CPU.cpp:1095-1162)
+        const R cc_i = fr.sp;
+        const R Emax = cmax(Eint, (R)0.0000001f);
+        const bool wet = hh > K.eps;
+        R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
+        R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0;
+#pragma unroll 2
+        for (int t = 0; t < nt; t++) {
+            const R cx0 = K.cxsth[t], sx0 = K.sxnth[t];
+            R eet = cmax(sA[t * nthr + tid] * sg, (R)0.0f) / idiv;
+            R rrt;
+            const R dd = eet * Dv / Emax;
+            if (wet) {
+                rrt = sR[t * nthr + tid];
+                R cx = cc_i * cx0 + uui;
+                R cy = cc_i * sx0 + vvi;
+                R rrd = (R)2.0f * g * K.beta * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+                eet = cmax(eet - dtf * dd, (R)0.0f);
+                rrt = cmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                drr = drr + rrd;
+            } else {
+                eet = (R)0.0f; rrt = (R)0.0f; drr = (R)0.0f;
+            }
+            RR = RR + rrt;
+            een[i + (size_t)t * C] = eet;
+            rrn[i + (size_t)t * C] = rrt;
+            sume = sume + eet;
+            sumethet = sumethet + eet * K.theta[t];
+            txx = txx + (((R)1.0f + cx0 * cx0) * eet);
+            tyy = tyy + (((R)1.0f + sx0 * sx0) * eet);
+            txy = txy + (sx0 * cx0 * eet);
+            rxx = rxx + ((cx0 * cx0) * rrt);
+            ryy = ryy + ((sx0 * sx0) * rrt);
+            rxy = rxy + (sx0 * cx0 * rrt);
+        }
+        const R sum2 = sume;
+        sume = cmax(sume, (R)0.00001f);
+        S.f[THM][i] = (sumethet / (R)nt) / (sume / (R)nt);
+        S.f[E][i] = sume * dth;
+        S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
+        S.f[D][i] = Dv;
+        S.f[ROL][i] = RR * dth;
+        S.f[DR][i] = drr * dth;
+        const R n = fe.sp / cc_i;
+        S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
+        S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
+        S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
+    }
+    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
+}
+
+// Tiled version of the rows pass: per theta plane, the block stages the
+// plane's (32+4) x (8+4) neighbourhood of ee (after offshore boundary, sanity
+// and action) and of rr in shared memory once, so each value is transformed
+// and fetched once per block instead of once per neighbouring thread.  Tile
+// element k holds the value at the clamped coordinate bx0-2+k (by0-2+k), so
+// the reference's clamped neighbour indices map straight into the tile.
+#define WT_X 32
+#define WT_Y 8
+#define WT_TX (WT_X + 4)
+#define WT_TY (WT_Y + 4)
+#define WT_N (WT_TX * WT_TY)
+template <class R>
+__global__ void __launch_bounds__(256, 3) k_wave_tile(Dev<R> S, Konst<R> K) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
+    const int tid = threadIdx.x + threadIdx.y * WT_X;
+    R* tE = (R*)smem_raw;                 // [WT_N] plane tile of ee/sigm
+    R* tR = tE + WT_N;                    // [WT_N] plane tile of rr
+    R* sA = tR + WT_N;                    // [nt][256] advected ee
+    R* sR = sA + (size_t)nt * 256;        // [nt][256] advected rr
+    const int bx0 = blockIdx.x * WT_X, by0 = 1 + blockIdx.y * WT_Y;
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool active = ix < nx && iy <= ny - 2;
+    const int par = clk->par;
+    const R* eeo = S.ee[par ^ 1];
+    const R* rro = S.rr[par ^ 1];
+    const R sg = (R)clk->sigm;
+    const R dtf = (R)clk->dt;
+    const R taper = (R)cmin((double)(R)clk->totaltime / 100.0, 1.0);
+    const R* St = S.St;
+    const bool roller = K.roller == 1;
+    const R dth = K.dtheta;
+    // tile element -> clamped grid offset (two elements per thread at most)
+    int eoff[2], ex0[2], ey0[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        int e = tid + k * 256;
+        int kx = e % WT_TX, ky = e / WT_TX;
+        int gx = bx0 - 2 + kx, gy = by0 - 2 + ky;
+        gx = gx < 0 ? 0 : (gx > nx - 1 ? nx - 1 : gx);
+        gy = gy < 0 ? 0 : (gy > ny - 1 ? ny - 1 : gy);
+        ex0[k] = gx; ey0[k] = gy;
+        eoff[k] = (e < WT_N) ? gx + gy * nx : -1;
+    }
+    // per-cell constants
+    R dtw = (R)3.0e38f;
+    int i = 0, pxm = 0, pxm2 = 0, pxp = 0, pxp2 = 0, pym = 0, pym2 = 0, pyp = 0, pyp2 = 0, pc = 0;
+    R hh = 0, wci = 0, uui = 0, uuixmin = 0, uuixmax = 0, vvi = 0, vviymin = 0, vviymax = 0;
+    Faces<R> fe{}, fr{};
+    CthCoef<R> cc{};
+    R we0 = 0, we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr0 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;
+    R cm = 0, c0 = 0, cpp = 0, Etmp = 0;
+    auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
+    auto qe = [&](int off, int x, int y, int t) -> R {
+        R v = (x == 0) ? St[y + t * ny] * taper : ld(eeo + off + (size_t)t * C);
+        v = cmax(v, (R)0.000f);
+        return v / sg;
+    };
+    if (active) {
+        i = ix + iy * nx;
+        const int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
+        const int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
+        const int ry = (iy - by0 + 2) * WT_TX, rx = ix - bx0 + 2;
+        pc = ry + rx;
+        pxm2 = ry + (xm2 - bx0 + 2); pxm = ry + (xm - bx0 + 2);
+        pxp = ry + (xp - bx0 + 2); pxp2 = ry + (xp2 - bx0 + 2);
+        pym2 = (ym2 - by0 + 2) * WT_TX + rx; pym = (ym - by0 + 2) * WT_TX + rx;
+        pyp = (yp - by0 + 2) * WT_TX + rx; pyp2 = (yp2 - by0 + 2) * WT_TX + rx;
+        hh = ld(S.f[HH] + i);
+        cc = cth_coef(S, K, ix, iy, sg);
+        wci = cc.wci;
+        const R* cgp = S.f[CG];
+        const R* cp = S.f[CC_];
+        fe = Faces<R>{ld(cgp + i), ld(cgp + xm + iy * nx), ld(cgp + xp + iy * nx), ld(cgp + ix + ym * nx), ld(cgp + ix + yp * nx)};
+        fr = Faces<R>{ld(cp + i), ld(cp + xm + iy * nx), ld(cp + xp + iy * nx), ld(cp + ix + ym * nx), ld(cp + ix + yp * nx)};
+        const R* uu = S.f[UU]; const R* vv = S.f[VV];
+        uui = ld(uu + i) * wci; uuixmin = ld(uu + xm + iy * nx) * wci; uuixmax = ld(uu + xp + iy * nx) * wci;
+        vvi = wci * ld(vv + i); vviymin = wci * ld(vv + ix + ym * nx); vviymax = wci * ld(vv + ix + yp * nx);
+        we0 = qe(i, ix, iy, cl(-2)); we1 = qe(i, ix, iy, cl(-1)); we2 = qe(i, ix, iy, 0);
+        we3 = qe(i, ix, iy, cl(1)); we4 = qe(i, ix, iy, cl(2));
+        wr0 = ld(rro + i + (size_t)cl(-2) * C); wr1 = ld(rro + i + (size_t)cl(-1) * C); wr2 = ld(rro + i);
+        wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
+        c0 = cth_eval(cc, K.cxsth[0], K.sxnth[0]);
+        cm = c0;
+        cpp = cth_eval(cc, K.cxsth[cl(1)], K.sxnth[cl(1)]);
+    }
+    const bool edge_row = active && (iy == 1 || iy == ny - 2);
+    const int slot = (iy == 1) ? 0 : 1;
+    const R dxplus_i = (R)1.0f / K.dx;
+#pragma unroll 1
+    for (int t = 0; t < nt; t++) {
+        const size_t o = (size_t)t * C;
+        __syncthreads();   // previous plane consumed
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            if (eoff[k] >= 0) {
+                tE[tid + k * 256] = qe(eoff[k], ex0[k], ey0[k], t);
+                if (roller) tR[tid + k * 256] = ld(rro + eoff[k] + o);
+            }
+        }
+        __syncthreads();
+        if (active) {
+            const R ct = K.cxsth[t], st = K.sxnth[t];
+            dtw = DM<R>::fmin(K.cfl * dth / DM<R>::fabs(c0), dtw);
+            R cgx = (R)0.5f * (fe.sp * ct + uui + fe.sxp * ct + uuixmax);
+            R cgxmin = (R)0.5f * (fe.sp * ct + uui + fe.sxm * ct + uuixmin);
+            R cgy = (R)0.5f * (fe.sp * st + vvi + fe.syp * st + vviymax);
+            R cgymin = (R)0.5f * (fe.sp * st + vvi + fe.sym * st + vviymin);
+            R xa = adv2(tE[pxm2], tE[pxm], we2, tE[pxp], tE[pxp2], cgx, cgxmin, dxplus_i);
+            R ya = adv2(tE[pym2], tE[pym], we2, tE[pyp], tE[pyp2], cgy, cgymin, dxplus_i);
+            R ta = theta_adv(we0, we1, we2, we3, we4, cm, c0, cpp, t, nt, dth);
+            R A = we2 - dtf * (xa + ya + ta);
+            R Ar = wr2;
+            if (roller) {
+                R cx = (R)0.5f * (fr.sp * ct + uui + fr.sxp * ct + uuixmax);
+                R cxm = (R)0.5f * (fr.sp * ct + uui + fr.sxm * ct + uuixmin);
+                R cy = (R)0.5f * (fr.sp * st + vvi + fr.syp * st + vviymax);
+                R cym = (R)0.5f * (fr.sp * st + vvi + fr.sym * st + vviymin);
+                R xr = adv2(tR[pxm2], tR[pxm], wr2, tR[pxp], tR[pxp2], cx, cxm, dxplus_i);
+                R yr = adv2(tR[pym2], tR[pym], wr2, tR[pyp], tR[pyp2], cy, cym, dxplus_i);
+                R tr = theta_adv(wr0, wr1, wr2, wr3, wr4, cm, c0, cpp, t, nt, dth);
+                Ar = wr2 - dtf * (xr + yr + tr);
+            }
+            sA[t * 256 + tid] = A;
+            sR[t * 256 + tid] = Ar;
+            if (edge_row) {
+                S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = A;
+                S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = Ar;
+            }
+            Etmp = Etmp + cmax(A * sg, (R)0.0f);
+            const int tn = cl(t + 3);
+            we0 = we1; we1 = we2; we2 = we3; we3 = we4; we4 = qe(i, ix, iy, tn);
+            wr0 = wr1; wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(rro + i + (size_t)tn * C);
+            cm = c0; c0 = cpp; cpp = cth_eval(cc, K.cxsth[cl(t + 2)], K.sxnth[cl(t + 2)]);
+        }
+    }
+    if (active) {
+        R* een = S.ee[par];
+        R* rrn = S.rr[par];
+        const R Trep = (R)clk->Trep;
+        // energintCPU (wave_CPU.cpp:891-924)
+        const R rho = K.rho, g = K.g;
+        Etmp = Etmp * dth;
+        R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
+        const R idiv = cmax((R)1.0f, DM<R>::pow(Htmp / (K.gammax * hh), (R)2.0f));
+        Htmp = cmin(Htmp, K.gammax * hh);
+        const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
+        const R k = ld(S.f[WK] + i);
+        const R fw = ld(S.f[FWM] + i);
+        R Dv;
+        if (K.breakmodel == 1) {   // roelvinkCPU (wave_CPU.cpp:927-985)
+            R fac = (R)(8.0 / (double)rho / (double)g);
+            R Ht = DM<R>::sqrt(Eint * fac);
+            R Qb = (R)(1.0 - ::exp(cmax(-1.0 * (double)DM<R>::pow((Ht / K.gammaa / hh), K.nexp), -100.0)));
+            Qb = cmin(Qb, (R)1.0f);
+            Dv = (R)((double)Qb * 2.0 * (double)K.alpha / (double)Trep * (double)Eint * (double)Ht / (double)hh);
+            R uorb = (R)(XBG_PI * (double)Ht / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
+            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
+                                      (double)uorb * (double)uorb);
+        } else {                   // baldockCPU (wave_CPU.cpp:987-1028)
+            R khh = k * hh;
+            R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
+            R Rr = Hb / cmax(Htmp, (R)0.00001f);
+            R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
+            Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
+            R uorb = (R)(XBG_PI * (double)Htmp / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
+            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
+                                      (double)uorb * (double)uorb);
+        }
+        // dissipationCPU (wave_CPU.cpp:1030-1092), meandir and radstress
+        const R cc_i = fr.sp;
+        const R Emax = cmax(Eint, (R)0.0000001f);
+        const bool wet = hh > K.eps;
+        R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
+        R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0;
+#pragma unroll 2
+        for (int t = 0; t < nt; t++) {
+            const R cx0 = K.cxsth[t], sx0 = K.sxnth[t];
+            R eet = cmax(sA[t * 256 + tid] * sg, (R)0.0f) / idiv;
+            R rrt;
+            const R dd = eet * Dv / Emax;
+            if (wet) {
+                rrt = sR[t * 256 + tid];
+                R cx = cc_i * cx0 + uui;
+                R cy = cc_i * sx0 + vvi;
+                R rrd = (R)2.0f * g * K.beta * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+                eet = cmax(eet - dtf * dd, (R)0.0f);
+                rrt = cmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                drr = drr + rrd;
+            } else {
+                eet = (R)0.0f; rrt = (R)0.0f; drr = (R)0.0f;
+            }
+            RR = RR + rrt;
+            een[i + (size_t)t * C] = eet;
+            rrn[i + (size_t)t * C] = rrt;
+            sume = sume + eet;
+            sumethet = sumethet + eet * K.theta[t];
+            txx = txx + (((R)1.0f + cx0 * cx0) * eet);
+            tyy = tyy + (((R)1.0f + sx0 * sx0) * eet);
+            txy = txy + (sx0 * cx0 * eet);
+            rxx = rxx + ((cx0 * cx0) * rrt);
+            ryy = ryy + ((sx0 * sx0) * rrt);
+            rxy = rxy + (sx0 * cx0 * rrt);
+        }
+        const R sum2 = sume;
+        sume = cmax(sume, (R)0.00001f);
+        S.f[THM][i] = (sumethet / (R)nt) / (sume / (R)nt);
+        S.f[E][i] = sume * dth;
+        S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
+        S.f[D][i] = Dv;
+        S.f[ROL][i] = RR * dth;
+        S.f[DR][i] = drr * dth;
+        const R n = fe.sp / cc_i;
+        S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
+        S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
+        S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
+    }
+    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
+}
+
+template <class R, int NMAX>
+__global__ void __launch_bounds__(128) k_wave_edge(Dev<R> S, Konst<R> K, int part_offset) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = (blockIdx.y == 0) ? 0 : ny - 1;
+    R dtw = (R)3.0e38f;
+    if (ix < nx) {
+        int i = ix + iy * nx;
+        int src = (iy == 0) ? pp(0, ny) : mm(ny - 1);
+        int slot = (iy == 0) ? 0 : 1;
+        int par = clk->par;
+        const R* rro = S.rr[par ^ 1];
+        R* een = S.ee[par];
+        R* rrn = S.rr[par];
+        R sg = (R)clk->sigm;
+        R dtf = (R)clk->dt;
+        R Trep = (R)clk->Trep;
+        CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
+        R cthv[NMAX];
+        dtw = ctheta_cell<R, NMAX>(K, cc, cthv);
+        R w = ld(S.f[HH] + i) > K.eps ? (R)1.0f : (R)0.0f;
+        R e[NMAX], r[NMAX];
+#pragma unroll
+        for (int t = 0; t < NMAX; t++) {
+            if (t < nt) {
+                e[t] = S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] * w;
+                r[t] = (K.roller == 1) ? S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] * w
+                                       : ld(rro + i + (size_t)t * C);
+            } else {
+                e[t] = (R)0; r[t] = (R)0;
+            }
+        }
+        CellOut<R> o = chain_cell<R, NMAX>(S, K, i, sg, dtf, Trep, e, r);
+        // second rollerlatbnd(ee) after dissipation: copy of the source row
+#pragma unroll
+        for (int t = 0; t < NMAX; t++)
+            if (t < nt) e[t] = een[ix + src * nx + (size_t)t * C] * w;
+        finish_cell<R, NMAX>(S, K, i, e, r, o, een, rrn);
+    }
+    block_min_store<R>(dtw, S.part_wave + part_offset + blockIdx.x + blockIdx.y * gridDim.x);
+}
+
+// wavforce (wave_CPU.cpp:1164-1238) at cell j, before the boundary copies.
+template <class R>
+__device__ __forceinline__ void force_raw(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R& Fx, R& Fy) {
+    const int nx = K.nx, ny = K.ny;
+    const R* Sxx = S.tmp[T_SXX]; const R* Sxy = S.tmp[T_SXY]; const R* Syy = S.tmp[T_SYY];
+    int xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
+    int i = ix + iy * nx;
+    R dxf = K.dx;
+    R Sxxi = ld(Sxx + i), Sxxr = ld(Sxx + xp + iy * nx), Sxyt = ld(Sxy + ix + yp * nx);
+    R Sxytr = ld(Sxy + xp + yp * nx), Sxyb = ld(Sxy + ix + ym * nx), Sxybr = ld(Sxy + xp + ym * nx);
+    R Syyi = ld(Syy + i), Syyt = ld(Syy + ix + yp * nx), Sxyr = ld(Sxy + xp + iy * nx);
+    R Sxyl = ld(Sxy + xm + iy * nx), Sxytl = ld(Sxy + xm + yp * nx);
+    Fx = (R)-1 * (Sxxr - Sxxi) / dxf - (R)0.5f * (Sxyt + Sxytr - Sxyb - Sxybr) / ((R)2.0f * dxf);
+    Fy = (R)-1 * (Syyt - Syyi) / dxf - (R)0.5f * (Sxyr + Sxytr - Sxyl - Sxytl) / ((R)2.0f * dxf);
+}
+
+// breakerdelayCPU (wave_CPU.cpp:1333-1368) at cell j.
+template <class R>
+__device__ __forceinline__ void breaker_raw(const Dev<R>& S, const Konst<R>& K, int j, R Trep, R& urms, R& ust) {
+    R hmin = (R)0.2;
+    R g = K.g, rho = K.rho;
+    R Hi = ld(S.f[H] + j), ki = ld(S.f[WK] + j);
+    R hhi = cmax(ld(S.f[HH] + j), hmin);
+    R ci = cmax(ld(S.f[CC_] + j), DM<R>::sqrt(hmin * g));
+    R Rl = ld(S.f[ROL] + j);
+    R uorb = (R)(XBG_PI * (double)Hi / (double)Trep / (double)DM<R>::sinh(cmin(cmax(ki, (R)0.01f) * hhi, (R)10.0f)));
+    urms = uorb / (DM<R>::sqrt((R)2.0f));
+    R ustw = ld(S.f[E] + j) / ci / rho / hhi;
+    R ustr = (R)2.0f * Rl / ci / rho / hhi;
+    ust = ustw + ustr;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_wave_force(Dev<R> S, Konst<R> K) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = ix + iy * nx;
+    R Trep = (R)clk->Trep;
+    R w = ld(S.f[HH] + i) > K.eps ? (R)1.0f : (R)0.0f;
+    // twodimbndnoixCPU(Fx): rows only; twodimbndCPU(Fy, ust): rows then ix = 0
+    int sy = iy;
+    if (iy == 0) sy = pp(0, ny);
+    if (iy == ny - 1) sy = mm(ny - 1);
+    int fx_src_x = ix, fx_src_y = sy;
+    int fy_src_x = (ix == 0) ? pp(0, nx) : ix;
+    int fy_src_y = (ix == 0) ? iy : sy;
+    bool rowb = (iy == 0 || iy == ny - 1);
+    bool anyb = rowb || ix == 0;
+    R Fx, Fy, tmp;
+    force_raw(S, K, fx_src_x, fx_src_y, Fx, tmp);
+    if (rowb) Fx = Fx * w;
+    force_raw(S, K, fy_src_x, fy_src_y, tmp, Fy);
+    if (anyb) Fy = Fy * w;
+    S.f[FX][i] = Fx;
+    S.f[FY][i] = Fy;
+    R urms, ust, u2;
+    breaker_raw(S, K, i, Trep, urms, ust);
+    if (anyb) {
+        breaker_raw(S, K, fy_src_x + fy_src_y * nx, Trep, u2, ust);
+        ust = ust * w;
+    }
+    S.f[URMS][i] = urms;
+    S.f[UST][i] = ust;
+}
+
+// ---------------------------------------------------------------- launchers
+template <class R>
+int wave_parts(const Konst<R>& K) {
+    int gx = (K.nx + 31) / 32, gy = (K.ny - 2 + 7) / 8;
+    int ex = (K.nx + 127) / 128;
+    return gx * gy + ex * 2;
+}
+
+template <class R, int NMAX>
+void launch_wave_main(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+    dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
+    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256) * sizeof(R);
+    k_wave_tile<R><<<g, b, smem, st>>>(S, K);
+    PMARK(pf, "k_wave_main");
+    dim3 be(128), ge((K.nx + 127) / 128, 2);
+    k_wave_edge<R, NMAX><<<ge, be, 0, st>>>(S, K, g.x * g.y);
+    PMARK(pf, "k_wave_edge");
+}
+
+template <class R>
+int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+    int n = 0;
+    k_disp<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, K); n++;
+    PMARK(pf, "k_disp");
+    if (K.nt <= 4) launch_wave_main<R, 4>(S, K, st, pf);
+    else if (K.nt <= 8) launch_wave_main<R, 8>(S, K, st, pf);
+    else if (K.nt <= 12) launch_wave_main<R, 12>(S, K, st, pf);
+    else if (K.nt <= 16) launch_wave_main<R, 16>(S, K, st, pf);
+    else if (K.nt <= 20) launch_wave_main<R, 20>(S, K, st, pf);
+    else if (K.nt <= 24) launch_wave_main<R, 24>(S, K, st, pf);
+    else launch_wave_main<R, 32>(S, K, st, pf);
+    n += 2;
+    dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
+    k_wave_force<R><<<g, b, 0, st>>>(S, K); n++;
+    PMARK(pf, "k_wave_force");
+    return n;
+}
+
+// One-time kernel attributes (dynamic shared memory above 48 KB for wide
+// theta sets in FP64).
+template <class R>
+int wave_prepare(const Konst<R>& K) {
+    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256) * sizeof(R);
+    cudaError_t e = cudaFuncSetAttribute(k_wave_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return e == cudaSuccess ? 0 : 1;
+}
+template int wave_prepare<float>(const Konst<float>&);
+template int wave_prepare<double>(const Konst<double>&);
+
+template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
+template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
+template int wave_parts<float>(const Konst<float>&);
+template int wave_parts<double>(const Konst<double>&);
+
+}  // namespace xbg

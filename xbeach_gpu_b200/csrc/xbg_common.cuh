@@ -1,0 +1,169 @@
+// xbg_common.cuh -- device-side state, constants and helpers shared by the
+// wave, flow, sediment and time-step kernels.
+//
+// Layout in HBM (one handle): structure of arrays, cell i = ix + iy*nx, every
+// 2-D field a separate cudaMalloc'd array of nx*ny elements (float or double),
+// directional fields as ntheta planes of nx*ny (the reference's layout,
+// Wave_kernel.cu:264).  ee and rr have two planes sets each; the step whose
+// device clock flips `par` reads set par^1 and writes set par, so a captured
+// CUDA graph can replay any number of steps without pointer swaps.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define XBG_PI 3.14159265          /* the reference's `pi` macro (double) */
+#define XBG_MAX_THETA 32
+
+namespace xbg {
+
+// --------------------------------------------------------------- math
+// Float functions for float, double functions for double: the FP64 build is
+// the same kernels instantiated on double.
+template <class R> struct DM;
+template <> struct DM<float> {
+    static __device__ __forceinline__ float sqrt(float x) { return sqrtf(x); }
+    static __device__ __forceinline__ float sinh(float x) { return sinhf(x); }
+    static __device__ __forceinline__ float tanh(float x) { return tanhf(x); }
+    static __device__ __forceinline__ float pow(float x, float y) { return powf(x, y); }
+    static __device__ __forceinline__ float exp(float x) { return expf(x); }
+    static __device__ __forceinline__ float log(float x) { return logf(x); }
+    static __device__ __forceinline__ float log10(float x) { return log10f(x); }
+    static __device__ __forceinline__ float cos(float x) { return cosf(x); }
+    static __device__ __forceinline__ float sin(float x) { return sinf(x); }
+    static __device__ __forceinline__ float fabs(float x) { return fabsf(x); }
+    static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
+    static __device__ __forceinline__ float fmax(float a, float b) { return fmaxf(a, b); }
+    static __device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
+    static __device__ __forceinline__ float atan(float x) { return atanf(x); }
+};
+template <> struct DM<double> {
+    static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double sinh(double x) { return ::sinh(x); }
+    static __device__ __forceinline__ double tanh(double x) { return ::tanh(x); }
+    static __device__ __forceinline__ double pow(double x, double y) { return ::pow(x, y); }
+    static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+    static __device__ __forceinline__ double log(double x) { return ::log(x); }
+    static __device__ __forceinline__ double log10(double x) { return ::log10(x); }
+    static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
+    static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
+    static __device__ __forceinline__ double fabs(double x) { return ::fabs(x); }
+    static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
+    static __device__ __forceinline__ double fmax(double a, double b) { return ::fmax(a, b); }
+    static __device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
+    static __device__ __forceinline__ double atan(double x) { return ::atan(x); }
+};
+
+// min/max as the reference's CPU wave code defines them (wave_CPU.cpp:10-16);
+// the flow and sediment kernels use CUDA's fminf/fmaxf semantics (DM::fmin).
+template <class T> __device__ __forceinline__ T cmax(T a, T b) { return (a < b) ? b : a; }
+template <class T> __device__ __forceinline__ T cmin(T a, T b) { return !(b < a) ? a : b; }
+
+// Clamped neighbours (Wave_kernel.cu:23-77, Flow_CPU.cpp:16-70).
+__device__ __forceinline__ int mm(int i) { return i <= 0 ? 0 : i - 1; }
+__device__ __forceinline__ int pp(int i, int n) { return i >= n - 1 ? n - 1 : i + 1; }
+__device__ __forceinline__ int mm2(int i) { return i <= 1 ? 0 : i - 2; }
+__device__ __forceinline__ int pp2(int i, int n) { return i >= n - 2 ? n - 1 : i + 2; }
+
+template <class T> __device__ __forceinline__ T ld(const T* p) { return __ldg(p); }
+
+// --------------------------------------------------------------- state
+enum Fld {
+    ZB = 0, ZS, HH, UU, VV, HU, HV, HUM, HVM, QX, QY, UEU, VEV, VMAGEU, VMAGEV, VU, UV,
+    UUOLD, VVOLD, ZSOLD, DZSDT, H, E, D, DR, ROL, WK, CC_, CG, FX, FY, URMS, UST, THM,
+    CFM, FWM, CSED, CEQSG, STDEP, DZB, ROLTHICK, KTURB, HMEAN, UUMEAN, VVMEAN, HHMEAN,
+    ZSMEAN, CMEAN, ZSMAX, NF2D
+};
+// Per-step temporaries (never read across steps).
+enum Tmp {
+    T_UU = 0, T_VV, T_ZS, T_NUH, T_SXX, T_SXY, T_SYY, T_CEQBG, T_TSG, T_UA, T_FACERO,
+    T_ERO, T_DEPO, T_ZB, T_STDEP, T_HH, NTMP
+};
+
+template <class R>
+struct Dev {
+    int nx, ny, nt, C;
+    R* f[NF2D];
+    R* tmp[NTMP];
+    int* wetu;
+    int* wetv;
+    R* umeanbnd;          // ny
+    R* ee[2];             // two plane sets of nt*C
+    R* rr[2];
+    R* edge;              // advected ee/rr of rows 1 and ny-2: 4*nx*nt
+    R* St;                // interpolated offshore boundary, nt*ny
+    R* stfile[2];         // boundary chunk slots: nrec*nt*ny
+    R* qfile[2];          // nrec*4*ny
+    R* part_flow;         // per-block FLOWDT minima
+    R* part_wave;         // per-block WAVEDT minima
+    R* zsold[2];          // zsold ping-pong, selected by the clock's par
+    unsigned* counter;    // last-block-done counter of the dt reduction
+    struct Clock* clk;
+};
+
+// Device clock and boundary cursors: the globals of mainloopGPU, wavebnd and
+// flowbnd (Wave_gpu.cu:26-241, Wavestep.cu:512-753) kept in device memory.
+struct Clock {
+    double totaltime, dt, nextoutputtime;
+    float wdt;                 // previous dt, a float in the reference (Wave_gpu.cu:78)
+    int par;                   // which ee/rr plane set holds the current state
+    int halt;                  // 1: the rest of this step is skipped
+    int flags;                 // XBG_FLAG_*
+    int status;                // XBG_OK or XBG_ERR_*
+    int do_sed;                // sedimentstep runs this step
+    long long nstep, nstep_total;
+    // wave boundary
+    int cur_slot;
+    int slot_valid[2];
+    int slot_nrec[2];
+    double slot_t0[2], slot_tend[2], slot_Trep[2];
+    int WAVstep;               // wavebndtype 1 record cursor
+    int nwbndstep;
+    double timenext_w, timesincelast_w;
+    double Trep;               // float in the reference, stored rounded
+    double sigm;               // 2 pi / Trep rounded to the element type
+    // sea level and wind
+    int SLstep, WNDstep, nsl, nwnd;
+    double zsbndi, zsbndn, windu, windv;
+    int n_wave_parts;          // number of valid WAVEDT partials (0 = none)
+    int pad;
+};
+#define XBG_MAX_SERIES 4096
+struct Series {
+    double slt[XBG_MAX_SERIES], sla[XBG_MAX_SERIES], slb[XBG_MAX_SERIES];
+    double wt[XBG_MAX_SERIES], wa[XBG_MAX_SERIES], wb[XBG_MAX_SERIES];
+    double wavet[XBG_MAX_SERIES];   // wavebndtype 1 record times
+};
+
+// Constants of one handle, passed by value to every kernel.
+template <class R>
+struct Konst {
+    int nx, ny, nt;
+    int swave, flow, roller, breakmodel, usesmago, wavebndtype, means;
+    R dx, eps, g, rho, cfl, dtheta, gammax, gammaa, alpha, nexp, beta, wci, hwci;
+    R nuh, nuhfac, fc, Cd, D50, D90, rhosed, wws, drydzmax, wetdzmax, maxslpchg, por,
+        morfac, sus, facsk, facas, cfsand, cfreef, fwsand, fwreef;
+    R twopi, aphi, bphi;
+    double endtime, outputtimestep, sedstart, dtbc, eps_d;
+    int sedtrans;
+    R cxsth[XBG_MAX_THETA], sxnth[XBG_MAX_THETA], theta[XBG_MAX_THETA];
+};
+
+// Per-kernel timing of a non-graph step (xbg_profile_step): an event after
+// every launch on the handle's stream.
+struct Prof {
+    cudaEvent_t ev[65];
+    const char* name[64];
+    int n = 0;
+    cudaStream_t st = nullptr;
+    void mark(const char* nm) {
+        if (n < 64) { name[n] = nm; cudaEventRecord(ev[n + 1], st); n++; }
+    }
+};
+#define PMARK(pf, nm) do { if (pf) (pf)->mark(nm); } while (0)
+
+// Early exit of a kernel in a step that the device clock has halted.
+__device__ __forceinline__ bool halted(const Clock* c) {
+    return *((volatile const int*)&c->halt) != 0;
+}
+
+}  // namespace xbg

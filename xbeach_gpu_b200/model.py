@@ -1,0 +1,206 @@
+"""Python handle on libxbg_b200.so, the CUDA implementation of the coupled step.
+
+`Model` mirrors the reference's host step interface (XBeachGPU.h:348-353):
+wavebnd -> wave_boundary, flowbnd -> flow_boundary, wavestep -> wave_step,
+flowstep -> flow_step, sedimentstep -> sediment_step, plus the dt logic and
+running means of mainloopGPU (compute_dt, accumulate_means) and whole graph-
+replayed steps (step / advance).  Every call goes through the C ABI of
+include/xbg.h; there is no other implementation behind it: if the library is
+missing or no GPU is visible, construction raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import FIELD, INT_FIELDS, Params, STATUS_NAMES, XBG_FP32
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libxbg_b200.so")
+_lib = None
+
+# Every entry point of include/xbg.h (checked by the tests against the header).
+EXPORTS = [
+    "xbg_params_default", "xbg_params_sanity", "xbg_create", "xbg_destroy", "xbg_status_string",
+    "xbg_init_state", "xbg_field_count", "xbg_set_field", "xbg_get_field", "xbg_field_device_ptr",
+    "xbg_set_wave_boundary", "xbg_set_sealevel", "xbg_set_wind", "xbg_compute_dt",
+    "xbg_wave_boundary", "xbg_flow_boundary", "xbg_wave_step", "xbg_flow_step",
+    "xbg_sediment_step", "xbg_accumulate_means", "xbg_step", "xbg_advance", "xbg_get_time",
+    "xbg_output_done", "xbg_reset_means", "xbg_set_time", "xbg_sync", "xbg_launch_count",
+    "xbg_mass", "xbg_put_wave_records", "xbg_get_stream", "xbg_profile_step",
+]
+
+
+class XbgError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the in-tree CUDA library (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise XbgError(f"{LIB_PATH} is not built: run `python -m xbeach_gpu_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp, ip, dp = C.c_void_p, C.c_int, C.POINTER(C.c_double)
+    L.xbg_params_default.argtypes = [C.POINTER(Params)]
+    L.xbg_params_default.restype = None
+    L.xbg_params_sanity.argtypes = [C.POINTER(Params), C.c_double]
+    L.xbg_create.argtypes = [C.POINTER(Params), ip, C.POINTER(vp)]
+    L.xbg_status_string.argtypes = [ip]
+    L.xbg_status_string.restype = C.c_char_p
+    for n in ["destroy", "compute_dt", "wave_boundary", "flow_boundary", "wave_step", "flow_step",
+              "sediment_step", "accumulate_means", "step", "output_done", "reset_means", "sync"]:
+        getattr(L, "xbg_" + n).argtypes = [vp]
+    L.xbg_init_state.argtypes = [vp, vp, C.c_double, C.c_double]
+    L.xbg_field_count.argtypes = [vp, ip, C.POINTER(C.c_size_t)]
+    L.xbg_set_field.argtypes = [vp, ip, vp, C.c_size_t]
+    L.xbg_get_field.argtypes = [vp, ip, vp, C.c_size_t]
+    L.xbg_field_device_ptr.argtypes = [vp, ip, C.POINTER(vp), C.POINTER(C.c_size_t)]
+    L.xbg_set_wave_boundary.argtypes = [vp, ip, vp, vp, ip, vp, C.c_double, C.c_double, C.c_double]
+    L.xbg_set_sealevel.argtypes = [vp, vp, vp, vp, ip]
+    L.xbg_set_wind.argtypes = [vp, vp, vp, vp, ip]
+    L.xbg_advance.argtypes = [vp, ip]
+    L.xbg_get_time.argtypes = [vp, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
+    L.xbg_set_time.argtypes = [vp, C.c_double, C.c_double, C.c_double]
+    L.xbg_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.xbg_mass.argtypes = [vp, dp, dp, dp]
+    L.xbg_put_wave_records.argtypes = [vp, ip, ip, ip, vp, vp]
+    L.xbg_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.xbg_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
+    _lib = L
+    return L
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise XbgError(f"{what}: status {rc} ({STATUS_NAMES.get(rc, '?')})")
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Model:
+    """One device-resident model (one xbg_handle)."""
+
+    def __init__(self, params, precision=XBG_FP32):
+        self.L = load()
+        self.p = params
+        self.dtype = np.float32 if precision == XBG_FP32 else np.float64
+        self.h = C.c_void_p()
+        _check(self.L.xbg_create(C.byref(params), precision, C.byref(self.h)), "xbg_create")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.xbg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def count(self, name):
+        n = C.c_size_t()
+        _check(self.L.xbg_field_count(self.h, FIELD[name], C.byref(n)), "count")
+        return n.value
+
+    def set(self, name, arr):
+        dt = np.int32 if name in INT_FIELDS else self.dtype
+        a = np.ascontiguousarray(arr, dtype=dt).ravel()
+        _check(self.L.xbg_set_field(self.h, FIELD[name], _ptr(a), a.size), f"set {name}")
+
+    def get(self, name, out=None):
+        dt = np.int32 if name in INT_FIELDS else self.dtype
+        a = out if out is not None else np.empty(self.count(name), dtype=dt)
+        _check(self.L.xbg_get_field(self.h, FIELD[name], _ptr(a), a.size), f"get {name}")
+        return a
+
+    def device_ptr(self, name):
+        p, n = C.c_void_p(), C.c_size_t()
+        _check(self.L.xbg_field_device_ptr(self.h, FIELD[name], C.byref(p), C.byref(n)), "device_ptr")
+        return p.value, n.value
+
+    def init_state(self, zb, zs0=0.0, zs1=0.0):
+        z = np.ascontiguousarray(zb, dtype=self.dtype).ravel()
+        _check(self.L.xbg_init_state(self.h, _ptr(z), zs0, zs1), "init_state")
+
+    def set_wave_boundary(self, slot, St, q, times=None, t0=0.0, tend=0.0, Trep=10.0):
+        St = np.ascontiguousarray(St, dtype=np.float64)
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        tp = None
+        if times is not None:
+            times = np.ascontiguousarray(times, dtype=np.float64)
+            tp = _ptr(times)
+        _check(self.L.xbg_set_wave_boundary(self.h, slot, _ptr(St), _ptr(q), St.shape[0], tp, t0, tend, Trep),
+               "set_wave_boundary")
+
+    def set_sealevel(self, t, w0, w1):
+        t, w0, w1 = (np.ascontiguousarray(x, dtype=np.float64) for x in (t, w0, w1))
+        _check(self.L.xbg_set_sealevel(self.h, _ptr(t), _ptr(w0), _ptr(w1), t.size), "sealevel")
+
+    def set_wind(self, t, u, v):
+        t, u, v = (np.ascontiguousarray(x, dtype=np.float64) for x in (t, u, v))
+        _check(self.L.xbg_set_wind(self.h, _ptr(t), _ptr(u), _ptr(v), t.size), "wind")
+
+    def call(self, name):
+        _check(getattr(self.L, "xbg_" + name)(self.h), name)
+
+    # the reference's step names
+    def compute_dt(self): self.call("compute_dt")
+    def wave_boundary(self): self.call("wave_boundary")
+    def flow_boundary(self): self.call("flow_boundary")
+    def wave_step(self): self.call("wave_step")
+    def flow_step(self): self.call("flow_step")
+    def sediment_step(self): self.call("sediment_step")
+    def accumulate_means(self): self.call("accumulate_means")
+
+    def step(self):
+        self.call("step")
+
+    def advance(self, n):
+        _check(self.L.xbg_advance(self.h, n), "advance")
+
+    def sync(self):
+        self.call("sync")
+
+    def time(self):
+        t, dt, n, fl = C.c_double(), C.c_double(), C.c_int64(), C.c_int()
+        rc = self.L.xbg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(n), C.byref(fl))
+        return t.value, dt.value, n.value, fl.value, rc
+
+    def set_time(self, t, dt, wdt):
+        _check(self.L.xbg_set_time(self.h, t, dt, wdt), "set_time")
+
+    def launches(self):
+        n = C.c_int64()
+        _check(self.L.xbg_launch_count(self.h, C.byref(n)), "launch_count")
+        return n.value
+
+    def put_wave_records(self, slot, first, St, q):
+        """Stream records into a chunk (no synchronisation); St/q must stay
+        alive until the stream has consumed them (pinned memory for overlap)."""
+        _check(self.L.xbg_put_wave_records(self.h, slot, first, St.shape[0], _ptr(St), _ptr(q)),
+               "put_wave_records")
+
+    def stream(self):
+        s = C.c_void_p()
+        _check(self.L.xbg_get_stream(self.h, C.byref(s)), "get_stream")
+        return s.value
+
+    def profile_step(self):
+        """One non-graph step with an event after every kernel: [(name, ms)]."""
+        cap = 64
+        ms = (C.c_float * cap)()
+        names = (C.c_char_p * cap)()
+        n = C.c_int(cap)
+        _check(self.L.xbg_profile_step(self.h, ms, names, C.byref(n)), "profile_step")
+        return [(names[k].decode(), float(ms[k])) for k in range(n.value)]
+
+    def mass(self):
+        w, s, b = C.c_double(), C.c_double(), C.c_double()
+        _check(self.L.xbg_mass(self.h, C.byref(w), C.byref(s), C.byref(b)), "mass")
+        return w.value, s.value, b.value
