@@ -5,9 +5,9 @@
 Each .cu file of csrc/ compiles in parallel to an object under _build/ (kept
 only if its source or a header changed), then nvcc links the shared library
 next to this file.  Flags: -gencode arch=compute_100a,code=sm_100a, -O3,
--lineinfo, and -fmad=false so that the float arithmetic rounds operation by
-operation as the reference's CPU judge does (memory-bound kernels lose
-nothing measurable by it).
+-lineinfo.  Multiply-add contraction stays on: the FP32 path is held to the
+reference within 1e-5 per step (not bit-exact), and the FP64 build agrees
+with the FP64 oracle to rounding.
 """
 import concurrent.futures as cf
 import glob
@@ -22,7 +22,7 @@ LIB = os.path.join(HERE, "libxbg_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-I", INCLUDE]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INCLUDE]
 
 
 def _headers():

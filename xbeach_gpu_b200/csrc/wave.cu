@@ -222,7 +222,7 @@ __device__ __forceinline__ CellOut<R> chain_cell(const Dev<R>& S, const Konst<R>
     // energyCPU
 #pragma unroll
     for (int t = 0; t < NMAX; t++)
-        if (t < nt) e[t] = cmax(e[t] * sg, (R)0.0f);
+        if (t < nt) e[t] = cmax(e[t], (R)0.0f);   // advected ee arrive in energy units
     // energintCPU
     R Etmp = (R)0.0f;
 #pragma unroll
@@ -868,6 +868,262 @@ __global__ void __launch_bounds__(256, 3) k_wave_tile(Dev<R> S, Konst<R> K) {
     block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
 }
 
+// ------------------------------------------------------------------------
+// Fast rows pass.  Same algorithm as k_wave_tile, arranged for instruction
+// throughput (the pass is issue-bound, not HBM-bound):
+//  - ee is advected in energy units: action (ee/sigm), the Euler step and
+//    energy (*sigm) of the reference cancel for the uniform sigm, and the
+//    upwind selection is scale invariant, so A*sigm = ee - dt*(fluxes of ee);
+//  - upwind choices are selects instead of branches (no divergence);
+//  - reciprocals of the uniform divisors (dtheta, idiv, D/E) multiply;
+//  - WAVEDT's min over bins of a/|ctheta| is a/max|ctheta| (one division);
+//  - the theta tables live in shared memory, plane pointers advance by C.
+// Results agree with the reference arithmetic to a few ulps per operation.
+template <class R>
+__device__ __forceinline__ R upw(R a, R b) {   // 1.5a - 0.5b, first-order fallback
+    R v = DM<R>::fma((R)1.5, a, (R)-0.5 * b);
+    return v < (R)0 ? a : v;
+}
+template <class R>
+__device__ __forceinline__ R flux2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin) {
+    R arrin = (cf > (R)0 ? upw(qi, qm) : upw(qp, qp2)) * cf;
+    R arrmin = (cfmin > (R)0 ? upw(qm, qm2) : upw(qi, qp)) * cfmin;
+    return arrin - arrmin;
+}
+template <class R>
+__device__ __forceinline__ R flux_theta(R em2, R em, R e0, R ep, R ep2, R cm, R c0, R cp, bool first, bool last) {
+    R cb = (R)0.5f * (c0 + cp);
+    R u1 = (R)1.5f * e0 - (R)0.5f * em;   u1 = u1 < (R)0 ? e0 : u1;
+    R u2 = (R)1.5f * ep - (R)0.5f * ep2;  u2 = u2 < (R)0 ? ep : u2;
+    R arrint = cb * (cb > (R)0 ? u1 : u2);
+    R cb2 = (R)0.5f * (cm + c0);
+    R u3 = (R)1.5f * em - (R)0.5f * em2;  u3 = u3 < (R)0 ? em : u3;
+    R u4 = (R)1.5f * e0 - (R)0.5f * ep;   u4 = u4 < (R)0 ? e0 : u4;
+    R arrmint = cb2 * (cb2 > (R)0 ? u3 : u4);
+    return first ? arrint : (last ? -arrmint : arrint - arrmint);
+}
+
+template <class R, bool ROLLER>
+__global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
+    const int tid = threadIdx.x + threadIdx.y * WT_X;
+    R* tE = (R*)smem_raw;                 // [WT_N] plane tile of ee
+    R* tR = tE + WT_N;                    // [WT_N] plane tile of rr
+    R* sA = tR + WT_N;                    // [nt][256] advected ee (energy units)
+    R* sR = sA + (size_t)nt * 256;        // [nt][256] advected rr
+    R* sCos = sR + (size_t)nt * 256;      // [nt]
+    R* sSin = sCos + nt;                  // [nt]
+    R* sTh = sSin + nt;                   // [nt]
+    if (tid < nt) { sCos[tid] = K.cxsth[tid]; sSin[tid] = K.sxnth[tid]; sTh[tid] = K.theta[tid]; }
+    const int bx0 = blockIdx.x * WT_X, by0 = 1 + blockIdx.y * WT_Y;
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool active = ix < nx && iy <= ny - 2;
+    const int par = clk->par;
+    const R* eeo = S.ee[par ^ 1];
+    const R* rro = S.rr[par ^ 1];
+    const R dtf = (R)clk->dt;
+    const R taper = (R)cmin((double)(R)clk->totaltime / 100.0, 1.0);
+    const R* St = S.St;
+    const R dth = K.dtheta;
+    const R rdth = (R)1 / dth;
+    const R rdx = (R)1 / K.dx;
+    // tile elements of this thread (two at most), offsets into a plane
+    int eoff0 = -1, eoff1 = -1, ey0 = 0, ey1 = 0;
+    bool ez0 = false, ez1 = false;
+    {
+        int e = tid, kx = e % WT_TX, ky = e / WT_TX;
+        int gx = min(max(bx0 - 2 + kx, 0), nx - 1), gy = min(max(by0 - 2 + ky, 0), ny - 1);
+        eoff0 = gx + gy * nx; ey0 = gy; ez0 = gx == 0;
+        e = tid + 256;
+        if (e < WT_N) {
+            kx = e % WT_TX; ky = e / WT_TX;
+            gx = min(max(bx0 - 2 + kx, 0), nx - 1); gy = min(max(by0 - 2 + ky, 0), ny - 1);
+            eoff1 = gx + gy * nx; ey1 = gy; ez1 = gx == 0;
+        }
+    }
+    int i = 0, pxm = 0, pxm2 = 0, pxp = 0, pxp2 = 0, pym = 0, pym2 = 0, pyp = 0, pyp2 = 0;
+    R hh = 0, uui = 0, uuixmin = 0, uuixmax = 0, vvi = 0, vviymin = 0, vviymax = 0;
+    Faces<R> fe{}, fr{};
+    CthCoef<R> cc{};
+    R we0 = 0, we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr0 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;
+    R cm = 0, c0 = 0, cpp = 0, Etmp = 0, cabs = 0;
+    const bool own_bnd = ix == 0;
+    auto own_e = [&](int t) -> R {
+        R v = own_bnd ? St[iy + t * ny] * taper : ld(eeo + i + (size_t)t * C);
+        return DM<R>::fmax(v, (R)0);
+    };
+    const bool edge_row = active && (iy == 1 || iy == ny - 2);
+    const int slot = (iy == 1) ? 0 : 1;
+    __syncthreads();
+    if (active) {
+        i = ix + iy * nx;
+        const int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
+        const int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
+        const int ry = (iy - by0 + 2) * WT_TX, rx = ix - bx0 + 2;
+        pxm2 = ry + (xm2 - bx0 + 2); pxm = ry + (xm - bx0 + 2);
+        pxp = ry + (xp - bx0 + 2); pxp2 = ry + (xp2 - bx0 + 2);
+        pym2 = (ym2 - by0 + 2) * WT_TX + rx; pym = (ym - by0 + 2) * WT_TX + rx;
+        pyp = (yp - by0 + 2) * WT_TX + rx; pyp2 = (yp2 - by0 + 2) * WT_TX + rx;
+        hh = ld(S.f[HH] + i);
+        R sg = (R)clk->sigm;
+        cc = cth_coef(S, K, ix, iy, sg);
+        const R wci = cc.wci;
+        const R* cgp = S.f[CG];
+        const R* cp = S.f[CC_];
+        fe = Faces<R>{ld(cgp + i), ld(cgp + xm + iy * nx), ld(cgp + xp + iy * nx), ld(cgp + ix + ym * nx), ld(cgp + ix + yp * nx)};
+        fr = Faces<R>{ld(cp + i), ld(cp + xm + iy * nx), ld(cp + xp + iy * nx), ld(cp + ix + ym * nx), ld(cp + ix + yp * nx)};
+        const R* uu = S.f[UU]; const R* vv = S.f[VV];
+        uui = ld(uu + i) * wci; uuixmin = ld(uu + xm + iy * nx) * wci; uuixmax = ld(uu + xp + iy * nx) * wci;
+        vvi = wci * ld(vv + i); vviymin = wci * ld(vv + ix + ym * nx); vviymax = wci * ld(vv + ix + yp * nx);
+        auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
+        we0 = own_e(0); we1 = we0; we2 = we0; we3 = own_e(cl(1)); we4 = own_e(cl(2));
+        wr0 = ld(rro + i); wr1 = wr0; wr2 = wr0;
+        wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
+        c0 = cth_eval(cc, sCos[0], sSin[0]);
+        cm = c0;
+        cpp = cth_eval(cc, sCos[cl(1)], sSin[cl(1)]);
+    }
+    const R* pe = eeo;   // plane t of ee / rr
+    const R* pr = rro;
+#pragma unroll 1
+    for (int t = 0; t < nt; t++, pe += C, pr += C) {
+        __syncthreads();   // previous plane consumed
+        {
+            R v = ez0 ? St[ey0 + t * ny] * taper : ld(pe + eoff0);
+            tE[tid] = DM<R>::fmax(v, (R)0);
+            if (ROLLER) tR[tid] = ld(pr + eoff0);
+            if (eoff1 >= 0) {
+                R w = ez1 ? St[ey1 + t * ny] * taper : ld(pe + eoff1);
+                tE[tid + 256] = DM<R>::fmax(w, (R)0);
+                if (ROLLER) tR[tid + 256] = ld(pr + eoff1);
+            }
+        }
+        __syncthreads();
+        if (active) {
+            const R ct = sCos[t], st = sSin[t];
+            const bool first = t == 0, last = t == nt - 1, multi = nt > 1;
+            cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
+            R cgx = (R)0.5f * (fe.sp * ct + uui + fe.sxp * ct + uuixmax);
+            R cgxmin = (R)0.5f * (fe.sp * ct + uui + fe.sxm * ct + uuixmin);
+            R cgy = (R)0.5f * (fe.sp * st + vvi + fe.syp * st + vviymax);
+            R cgymin = (R)0.5f * (fe.sp * st + vvi + fe.sym * st + vviymin);
+            R fx = flux2(tE[pxm2], tE[pxm], we2, tE[pxp], tE[pxp2], cgx, cgxmin);
+            R fy = flux2(tE[pym2], tE[pym], we2, tE[pyp], tE[pyp2], cgy, cgymin);
+            R ft = multi ? flux_theta(we0, we1, we2, we3, we4, cm, c0, cpp, first, last) : (R)0;
+            R A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
+            R Ar = wr2;
+            if (ROLLER) {
+                R cx = (R)0.5f * (fr.sp * ct + uui + fr.sxp * ct + uuixmax);
+                R cxm = (R)0.5f * (fr.sp * ct + uui + fr.sxm * ct + uuixmin);
+                R cy = (R)0.5f * (fr.sp * st + vvi + fr.syp * st + vviymax);
+                R cym = (R)0.5f * (fr.sp * st + vvi + fr.sym * st + vviymin);
+                R rx = flux2(tR[pxm2], tR[pxm], wr2, tR[pxp], tR[pxp2], cx, cxm);
+                R ry = flux2(tR[pym2], tR[pym], wr2, tR[pyp], tR[pyp2], cy, cym);
+                R rt = multi ? flux_theta(wr0, wr1, wr2, wr3, wr4, cm, c0, cpp, first, last) : (R)0;
+                Ar = wr2 - dtf * ((rx + ry) * rdx + rt * rdth);
+            }
+            sA[t * 256 + tid] = A;
+            sR[t * 256 + tid] = Ar;
+            if (edge_row) {
+                S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = A;
+                S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = Ar;
+            }
+            Etmp = Etmp + DM<R>::fmax(A, (R)0);
+            const int tn = t + 3 < nt ? t + 3 : nt - 1;
+            const int t2 = t + 2 < nt ? t + 2 : nt - 1;
+            we0 = we1; we1 = we2; we2 = we3; we3 = we4; we4 = own_e(tn);
+            wr0 = wr1; wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(rro + i + (size_t)tn * C);
+            cm = c0; c0 = cpp; cpp = cth_eval(cc, sCos[t2], sSin[t2]);
+        }
+    }
+    R dtw = (R)3.0e38f;
+    if (active) {
+        // WAVEDT: min over bins of cfl*dtheta/|ctheta| (Wave_kernel.cu:232-249)
+        dtw = DM<R>::fmin(K.cfl * dth / cabs, (R)9999999.9f);
+        R* een = S.ee[par];
+        R* rrn = S.rr[par];
+        const R Trep = (R)clk->Trep;
+        const R rho = K.rho, g = K.g;
+        // energintCPU
+        Etmp = Etmp * dth;
+        R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
+        R hr = Htmp / (K.gammax * hh);
+        const R idiv = DM<R>::fmax((R)1.0f, hr * hr);
+        const R ridiv = (R)1 / idiv;
+        Htmp = DM<R>::fmin(Htmp, K.gammax * hh);
+        const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
+        const R k = ld(S.f[WK] + i);
+        const R fw = ld(S.f[FWM] + i);
+        R Dv;
+        if (K.breakmodel == 1) {   // roelvinkCPU
+            R Ht = DM<R>::sqrt(Eint * (R)(8.0 / (double)rho / (double)g));
+            R x = Ht / K.gammaa / hh;
+            R Qb = (R)1 - DM<R>::exp(DM<R>::fmax(-DM<R>::pow(x, K.nexp), (R)-100));
+            Qb = DM<R>::fmin(Qb, (R)1.0f);
+            Dv = Qb * (R)2 * K.alpha / Trep * Eint * Ht / hh;
+            R uorb = (R)XBG_PI * Ht / (Trep * DM<R>::sinh(DM<R>::fmin(k * hh, (R)10.0f)));
+            Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
+        } else {                   // baldockCPU
+            R khh = k * hh;
+            R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
+            R Rr = Hb / DM<R>::fmax(Htmp, (R)0.00001f);
+            R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
+            Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
+            R uorb = (R)XBG_PI * Htmp / (Trep * DM<R>::sinh(DM<R>::fmin(k * hh, (R)10.0f)));
+            Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
+        }
+        // dissipationCPU, meandir, radstress
+        const R cc_i = fr.sp;
+        const R Dq = Dv / DM<R>::fmax(Eint, (R)0.0000001f);
+        const R twogb = (R)2.0f * g * K.beta;
+        const bool wet = hh > K.eps;
+        R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
+        R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0;
+        R* pe_n = een + i;
+        R* pr_n = rrn + i;
+#pragma unroll 2
+        for (int t = 0; t < nt; t++) {
+            const R cx0 = sCos[t], sx0 = sSin[t];
+            R eet = DM<R>::fmax(sA[t * 256 + tid], (R)0.0f) * ridiv;
+            R rrt = sR[t * 256 + tid];
+            const R dd = eet * Dq;
+            R cx = cc_i * cx0 + uui;
+            R cy = cc_i * sx0 + vvi;
+            R rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+            eet = wet ? DM<R>::fmax(eet - dtf * dd, (R)0.0f) : (R)0;
+            rrt = wet ? DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f) : (R)0;
+            drr = wet ? drr + rrd : (R)0;
+            RR = RR + rrt;
+            pe_n[(size_t)t * C] = eet;
+            pr_n[(size_t)t * C] = rrt;
+            sume = sume + eet;
+            sumethet = sumethet + eet * sTh[t];
+            txx = txx + (((R)1.0f + cx0 * cx0) * eet);
+            tyy = tyy + (((R)1.0f + sx0 * sx0) * eet);
+            txy = txy + (sx0 * cx0 * eet);
+            rxx = rxx + ((cx0 * cx0) * rrt);
+            ryy = ryy + ((sx0 * sx0) * rrt);
+            rxy = rxy + (sx0 * cx0 * rrt);
+        }
+        const R sum2 = sume;
+        sume = DM<R>::fmax(sume, (R)0.00001f);
+        S.f[THM][i] = sumethet / sume;
+        S.f[E][i] = sume * dth;
+        S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
+        S.f[D][i] = Dv;
+        S.f[ROL][i] = RR * dth;
+        S.f[DR][i] = drr * dth;
+        const R n = fe.sp / cc_i;
+        S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
+        S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
+        S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
+    }
+    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
+}
+
 template <class R, int NMAX>
 __global__ void __launch_bounds__(128) k_wave_edge(Dev<R> S, Konst<R> K, int part_offset) {
     const Clock* clk = S.clk;
@@ -992,8 +1248,9 @@ int wave_parts(const Konst<R>& K) {
 template <class R, int NMAX>
 void launch_wave_main(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
-    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256) * sizeof(R);
-    k_wave_tile<R><<<g, b, smem, st>>>(S, K);
+    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
+    if (K.roller == 1) k_wave_fast<R, true><<<g, b, smem, st>>>(S, K);
+    else k_wave_fast<R, false><<<g, b, smem, st>>>(S, K);
     PMARK(pf, "k_wave_main");
     dim3 be(128), ge((K.nx + 127) / 128, 2);
     k_wave_edge<R, NMAX><<<ge, be, 0, st>>>(S, K, g.x * g.y);
@@ -1023,9 +1280,10 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
 // theta sets in FP64).
 template <class R>
 int wave_prepare(const Konst<R>& K) {
-    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256) * sizeof(R);
-    cudaError_t e = cudaFuncSetAttribute(k_wave_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return e == cudaSuccess ? 0 : 1;
+    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
+    cudaError_t e = cudaFuncSetAttribute(k_wave_fast<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e2 = cudaFuncSetAttribute(k_wave_fast<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return (e == cudaSuccess && e2 == cudaSuccess) ? 0 : 1;
 }
 template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);
