@@ -281,7 +281,7 @@ def main():
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded barred beach, JONSWAP-shaped groups)",
         "config": {"workload": f"barred_beach {p.nx}x{p.ny} ntheta={nt} (large single domain)",
                    "nx": p.nx, "ny": p.ny, "ntheta": nt, "cells": C, "parallelism": f"replicas x{world}",
-                   "l2": "state ~2 GB per GPU, larger than the 126 MB L2 (no flush needed)",
+                   "l2": "state ~1.2 GB per GPU, larger than the 126 MB L2 (no flush needed)",
                    "sim_time_s": t_end},
         "roofline": roof,
         "roofline_step": {"bound": "hbm", "achieved": step_gbs, "peak": peak, "unit": "GB/s",
