@@ -198,6 +198,27 @@ int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
 int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,
               double* bed);
 
+/* ---- no-allocation entry point ------------------------------------------
+ * No counterpart in the reference.  For callers that may not allocate
+ * device memory: a coupler or framework that owns the device through its
+ * own pool allocator, or code that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  Computes, on `stream`, the flow
+ * time-step candidate that xbg_compute_dt derives from the water depth:
+ * *dt_out = 0.5 * min over cells of cfl*dx/sqrt(9.81*hh), with hh (nx*ny
+ * values) and dt_out caller-owned device memory of the given precision.
+ * It allocates nothing: its only scratch (per-block minima and a counter)
+ * is a fixed XBG_NOALLOC_SCRATCH_BYTES array inside the library that every
+ * GPU loading the library holds until exit.  Grids above
+ * XBG_NOALLOC_MAX_CELLS cells return XBG_ERR_ARG.  All calls on a device
+ * share that array, so calls that may overlap on the GPU race: order them.
+ * The first call on a device looks the array's address up; make it before
+ * any stream capture.  Does not synchronise.                              */
+#define XBG_NOALLOC_MAX_BLOCKS     1184          /* 8 blocks x 148 SMs    */
+#define XBG_NOALLOC_SCRATCH_BYTES  (256 + 8 * XBG_NOALLOC_MAX_BLOCKS)
+#define XBG_NOALLOC_MAX_CELLS      (1LL << 30)
+int  xbg_flow_dt_noalloc(int precision, const void* hh, int nx, int ny,
+                         double dx, double cfl, void* dt_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -28,6 +28,7 @@ EXPORTS = [
     "xbg_sediment_step", "xbg_accumulate_means", "xbg_step", "xbg_advance", "xbg_get_time",
     "xbg_output_done", "xbg_reset_means", "xbg_set_time", "xbg_sync", "xbg_launch_count",
     "xbg_mass", "xbg_put_wave_records", "xbg_get_stream", "xbg_profile_step",
+    "xbg_flow_dt_noalloc",
 ]
 
 
@@ -69,6 +70,7 @@ def load():
     L.xbg_put_wave_records.argtypes = [vp, ip, ip, ip, vp, vp]
     L.xbg_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.xbg_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
+    L.xbg_flow_dt_noalloc.argtypes = [ip, vp, ip, ip, C.c_double, C.c_double, vp, vp]
     _lib = L
     return L
 
