@@ -199,6 +199,18 @@ struct Handle : public xbg_handle {
         R phi = (R)((1.0f + (R)std::sqrt((R)5.0f)) / 2);
         K.aphi = 1 / (phi + 1); K.bphi = phi / (phi + 1);
         K.twopi = 8 * (R)std::atan((R)1.0f);
+        {
+            R drho = (K.rhosed - K.rho) / K.rho;
+            R dester = (R)std::pow(drho * K.g, (R)(1.0f / 3.0f)) / (R)0.0001f * K.D50;
+            K.sed_drho = drho;
+            K.sed_drhog = drho * K.g;
+            K.sed_Ass = (R)0.012f * K.D50 * (R)std::pow(dester, (R)-0.6f) / (R)std::pow(drho * K.g * K.D50, (R)1.2f);
+            K.sed_ucr = K.D50 <= (R)0.0005f ? (R)0.19f * (R)std::pow(K.D50, (R)0.1f)
+                                             : (R)8.50f * (R)std::pow(K.D50, (R)0.6f);
+            K.rvr_alpha = (R)-1.0f * (R)std::log10((R)std::exp((R)1.0f)) / (R)0.3539f;
+            K.rvr_beta = (R)std::exp((R)-0.6065f / (R)0.3539f);
+            K.rdx = (R)1 / K.dx;
+        }
         K.endtime = P.endtime; K.outputtimestep = P.outputtimestep; K.sedstart = P.sedstart;
         K.dtbc = P.dtbc; K.eps_d = P.eps; K.sedtrans = P.sedtrans;
         for (int i = 0; i < nt; i++) {   // Wavestep.cu:79-86

@@ -38,13 +38,13 @@ __device__ __forceinline__ R smago_cell(const Dev<R>& S, const Konst<R>& K, int 
     const R* uu = S.f[UU]; const R* vv = S.f[VV];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
     R dx = K.dx, nuh = K.nuh, nuhfac = K.nuhfac, rho = K.rho;
-    R b = nuhfac * ld(S.f[HH] + i) * DM<R>::pow(ld(S.f[DR] + i) / rho, (R)(1.0f / 3.0f));
+    R b = nuhfac * ld(S.f[HH] + i) * DM<R>::pow13(ld(S.f[DR] + i) / rho);
     if (K.usesmago == 1) {
         R dudx = (ld(uu + i) - ld(uu + IDX(xm, iy))) / dx;
         R dudy = (R)0.50f * (ld(uu + IDX(ix, yp)) - ld(uu + IDX(ix, ym)) + ld(uu + IDX(xm, yp)) - ld(uu + IDX(xm, ym))) / dx;
         R dvdy = (ld(vv + i) - ld(vv + IDX(ix, ym))) / dx;
         R dvdx = (R)0.50f * (ld(vv + IDX(xp, iy)) - ld(vv + IDX(xm, iy)) + ld(vv + IDX(xp, ym)) - ld(vv + IDX(xm, ym))) / dx;
-        R tau = DM<R>::sqrt((R)2.0f * dudx * dudx + (R)2.0f * dvdy * dvdy + DM<R>::pow(dudy + dvdx, (R)2.0f));
+        R tau = DM<R>::sqrt((R)2.0f * dudx * dudx + (R)2.0f * dvdy * dvdy + (dudy + dvdx) * (dudy + dvdx));
         return DM<R>::fmax(nuh * nuh * dx * dx * tau, b);
     }
     return DM<R>::fmax(nuh, b);

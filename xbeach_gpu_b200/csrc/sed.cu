@@ -38,8 +38,7 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
     // Sbvr (:167-326); kturb is 0 after longturb
     R zo = (R)0.006f, sedcal = (R)1.0f, bulk = (R)1.0f;
     R D50 = K.D50, D90 = K.D90;
-    R drho = (K.rhosed - rho) / rho;
-    R dester = DM<R>::pow(drho * g, (R)(1.0f / 3.0f)) / (R)0.0001f * D50;
+    const R drhog = K.sed_drhog;
     R hh = ld(S.f[HH] + i);
     R hhi = DM<R>::fmax(hh, (R)0.01f);
     R ue = (R)(0.5 * (double)(ld(S.f[UEU] + IDX(xm, iy)) + ld(S.f[UEU] + i)));
@@ -48,20 +47,19 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
     R ML = DM<R>::fmax(DM<R>::fmin(DM<R>::sqrt((R)2.0f * ld(S.f[ROL] + i) * Trep / (rho * c)), hhi), (R)0.01f);
     R dcfin = DM<R>::exp(DM<R>::fmin(hhi, (R)100.0f) / ML);
     R dcf = DM<R>::fmin((R)1 / (dcfin - (R)1), (R)1.0f);
-    R kb = K.nuhfac * DM<R>::pow(ld(S.f[DR] + i) / rho, (R)0.66666666667f) * dcf;
+    R kb = K.nuhfac * DM<R>::pow23(ld(S.f[DR] + i) / rho) * dcf;
     R urms = ld(S.f[URMS] + i);
     R Urms2 = urms * urms + (R)1.45f * (kb + (R)0.0f);
     R Tsg = DM<R>::fmax((R)0.1f * hhi / K.wws, (R)0.5f);
     R Ucr;
-    if (D50 <= (R)0.0005f) Ucr = (R)0.19f * DM<R>::pow(D50, (R)0.1f) * DM<R>::log10((R)4.0f * hhi / D90);
-    else Ucr = (R)8.50f * DM<R>::pow(D50, (R)0.6f) * DM<R>::log10((R)4.0f * hhi / D90);
+    Ucr = K.sed_ucr * DM<R>::log10((R)4.0f * hhi / D90);
     R hdrag = DM<R>::fmax(hhi, (R)10.0f * zo);
     R Cd = (R)0.4f / (DM<R>::log(hdrag / zo) - (R)1.0f);
     Cd = Cd * Cd;
-    R Asb = (R)0.005f * hhi * DM<R>::pow((R)1 / hhi / (drho * g), (R)1.2f);
-    R Ass = (R)0.012f * D50 * DM<R>::pow(dester, (R)-0.6f) / (DM<R>::pow(drho * g * D50, (R)1.2f));
+    R Asb = (R)0.005f * hhi * DM<R>::pow((R)1 / hhi / drhog, (R)1.2f);
+    R Ass = K.sed_Ass;
     R T1 = vmags + (R)0.018f / Cd * Urms2;
-    T1 = DM<R>::fmin(T1, (R)100000.0f * g / ld(S.f[CFM] + i) * D50 * drho);
+    T1 = DM<R>::fmin(T1, (R)100000.0f * g / ld(S.f[CFM] + i) * D50 * K.sed_drho);
     T1 = DM<R>::sqrt(T1);
     R wetz = hhi > eps ? (R)1 : (R)0;
     R T2 = (R)0.0f;
@@ -77,10 +75,10 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
     // Rvr (:477-509)
     {
         R m1 = (R)0.0f, m2 = (R)0.7939f, m3 = (R)-0.6065f, m4 = (R)0.3539f, m5 = (R)0.6373f, m6 = (R)0.5995f;
-        R alpha = (R)-1.0f * DM<R>::log10(DM<R>::exp((R)1.0f)) / m4;
-        R beta = DM<R>::exp(m3 / m4);
+        R alpha = K.rvr_alpha;
+        R beta = K.rvr_beta;
         R k = (R)(2 * XBG_PI / (double)(c * Trep));
-        R Ur = (R)3.0f / (R)8.0f * DM<R>::sqrt((R)2.0f) * ld(S.f[H] + i) * k / DM<R>::pow(k * hh, (R)3.0f);
+        R Ur = (R)3.0f / (R)8.0f * DM<R>::sqrt((R)2.0f) * ld(S.f[H] + i) * k / ((k * hh) * (k * hh) * (k * hh));
         Ur = DM<R>::fmax(Ur, (R)0.00001f);
         R Bm = m1 + (m2 - m1) / ((R)1.0f + beta * DM<R>::pow(Ur, alpha));
         R B1 = (R)((double)((R)-90.0f + (R)90.0f * DM<R>::tanh(m5 / DM<R>::pow(Ur, m6))) * XBG_PI / 180.0f);
@@ -111,11 +109,11 @@ __device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, in
     R uav = (R)(0.5 * stm * (double)(uar + uai));
     R uv = ld(S.f[UV] + i), vu = ld(S.f[VU] + i);
     R urep = ld(S.f[UEU] + i) + uau;
-    R vmagu = DM<R>::sqrt(DM<R>::pow((uui + uau), (R)2.0f) + DM<R>::pow((vu + uav), (R)2.0f));
+    R vmagu = DM<R>::sqrt((uui + uau) * (uui + uau) + (vu + uav) * (vu + uav));
     uau = (R)(0.5 * ctm * (double)(uai + uat));
     uav = (R)(0.5 * stm * (double)(uat + uai));
     R vrep = ld(S.f[VEV] + i) + uav;
-    R vmagv = DM<R>::sqrt(DM<R>::pow(uv + uau, (R)2.0f) + DM<R>::pow(vvi + uav, (R)2.0f));
+    R vmagv = DM<R>::sqrt((uv + uau) * (uv + uau) + (vvi + uav) * (vvi + uav));
     R dzbdx = (R)-1.0f * (zbr - zbi) / dx;
     R dzbdy = (R)-1.0f * (zbt - zbi) / dx;
     R hu = ld(S.f[HU] + i), hv = ld(S.f[HV] + i);
@@ -130,21 +128,17 @@ __device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, in
     else if (vrep < (R)0.0f) cv = cct;
     else cv = (R)0.50f * (cci + cct);
     R dcsdy = (cct - cci) / dx;
-    R Dc = K.nuh + K.nuhfac * hhi * DM<R>::pow(ld(S.f[DR] + i) / K.rho, (R)(1.0f / 3.0f));
+    R Dc = K.nuh + K.nuhfac * hhi * DM<R>::pow13(ld(S.f[DR] + i) / K.rho);
     Sus = K.sus * (cu * urep * hu - Dc * hu * dcsdx - facsl * cu * vmagu * hu * dzbdx) * wu;
     Svs = K.sus * (cv * vrep * hv - Dc * hv * dcsdy - facsl * cv * vmagv * hv * dzbdy) * wv;
 }
 
-// Conc (Sediment_kernel.cu:721-780) at (ix, iy): new C, ero, depo
+// Conc (Sediment_kernel.cu:721-780) at cell i from the suspended fluxes of
+// the cell (Susi, Svsi), its left face neighbour (Susl) and the one below
+// (Svsb): new C, ero, depo.
 template <class R>
-__device__ __forceinline__ R conc_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R& ero, R& depo) {
-    const int nx = K.nx;
-    int i = IDX(ix, iy);
-    R Susi, Svsi, Susl, t0, t1, Svsb;
-    susp_cell(S, K, ix, iy, Susi, Svsi);
-    int xm = mm(ix), ym = mm(iy);
-    if (xm != ix) susp_cell(S, K, xm, iy, Susl, t0); else Susl = Susi;
-    if (ym != iy) susp_cell(S, K, ix, ym, t1, Svsb); else Svsb = Svsi;
+__device__ __forceinline__ R conc_from(const Dev<R>& S, const Konst<R>& K, int i, R dtf, R Susi, R Svsi, R Susl,
+                                       R Svsb, R& ero, R& depo) {
     R hhi = ld(S.f[HH] + i);
     R wetz = hhi > K.eps ? (R)1.0f : (R)0.0f;
     R Tsg = ld(S.tmp[T_TSG] + i);
@@ -158,17 +152,47 @@ __device__ __forceinline__ R conc_cell(const Dev<R>& S, const Konst<R>& K, int i
     return cs / hhi;
 }
 
+// Conc at (ix, iy) evaluating the three Susp it needs (lateral rows only).
+template <class R>
+__device__ __forceinline__ R conc_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R& ero, R& depo) {
+    R Susi, Svsi, Susl, t0, t1, Svsb;
+    susp_cell(S, K, ix, iy, Susi, Svsi);
+    int xm = mm(ix), ym = mm(iy);
+    if (xm != ix) susp_cell(S, K, xm, iy, Susl, t0); else Susl = Susi;
+    if (ym != iy) susp_cell(S, K, ix, ym, t1, Svsb); else Svsb = Svsi;
+    return conc_from(S, K, ix + iy * K.nx, dtf, Susi, Svsi, Susl, Svsb, ero, depo);
+}
+
+// Susp once per cell of the block's 32 x 8 tile plus the column to its left
+// and the row below it (clamped at the grid edge, where mm() maps a cell to
+// itself), then Conc from shared memory.  The lateral rows 0 and ny-1 take
+// Conc of rows 1 and ny-2 (CClatbnd), evaluated directly.
+constexpr int SB_X = 32, SB_Y = 8, SB_TX = SB_X + 1, SB_TY = SB_Y + 1;
+
 template <class R>
 __global__ void __launch_bounds__(256) k_sed_b(Dev<R> S, Konst<R> K) {
     const Clock* clk = S.clk;
     if (sed_skip(clk)) return;
+    __shared__ R sSus[SB_TY * SB_TX], sSvs[SB_TY * SB_TX];
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int bx0 = blockIdx.x * SB_X, by0 = blockIdx.y * SB_Y;
+    const int tid = threadIdx.x + threadIdx.y * SB_X;
+    for (int e = tid; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
+        int kx = e % SB_TX, ky = e / SB_TX;
+        int gx = min(max(bx0 - 1 + kx, 0), nx - 1), gy = min(max(by0 - 1 + ky, 0), ny - 1);
+        R a, b;
+        susp_cell(S, K, gx, gy, a, b);
+        sSus[e] = a;
+        sSvs[e] = b;
+    }
+    __syncthreads();
+    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R dtf = (R)clk->dt;
-    R ero, depo;
-    R cnew = conc_cell(S, K, ix, iy, dtf, ero, depo);
+    R ero, depo, cnew;
+    const int c = (threadIdx.y + 1) * SB_TX + threadIdx.x + 1;
+    cnew = conc_from(S, K, i, dtf, sSus[c], sSvs[c], sSus[c - 1], sSvs[c - SB_TX], ero, depo);
     // CClatbnd (Sediment_kernel.cu:782-821)
     if (iy == 0 || iy == ny - 1) {
         R e2, d2;

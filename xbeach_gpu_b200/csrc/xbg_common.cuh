@@ -25,6 +25,12 @@ template <> struct DM<float> {
     static __device__ __forceinline__ float sinh(float x) { return sinhf(x); }
     static __device__ __forceinline__ float tanh(float x) { return tanhf(x); }
     static __device__ __forceinline__ float pow(float x, float y) { return powf(x, y); }
+    // x^(1/3) and x^(2/3) with the exponents the reference writes as float
+    // literals (1.0f/3.0f, 0.66666666667f).  FP32: cbrtf (within 1e-7
+    // relative of powf with those exponents); FP64: pow with the same
+    // float-valued exponents, as the reference evaluates them.
+    static __device__ __forceinline__ float pow13(float x) { return cbrtf(x); }
+    static __device__ __forceinline__ float pow23(float x) { float c = cbrtf(x); return c * c; }
     static __device__ __forceinline__ float exp(float x) { return expf(x); }
     static __device__ __forceinline__ float log(float x) { return logf(x); }
     static __device__ __forceinline__ float log10(float x) { return log10f(x); }
@@ -41,6 +47,8 @@ template <> struct DM<double> {
     static __device__ __forceinline__ double sinh(double x) { return ::sinh(x); }
     static __device__ __forceinline__ double tanh(double x) { return ::tanh(x); }
     static __device__ __forceinline__ double pow(double x, double y) { return ::pow(x, y); }
+    static __device__ __forceinline__ double pow13(double x) { return ::pow(x, (double)(1.0f / 3.0f)); }
+    static __device__ __forceinline__ double pow23(double x) { return ::pow(x, (double)0.66666666667f); }
     static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
     static __device__ __forceinline__ double log(double x) { return ::log(x); }
     static __device__ __forceinline__ double log10(double x) { return ::log10(x); }
@@ -143,6 +151,10 @@ struct Konst {
     R nuh, nuhfac, fc, Cd, D50, D90, rhosed, wws, drydzmax, wetdzmax, maxslpchg, por,
         morfac, sus, facsk, facas, cfsand, cfreef, fwsand, fwreef;
     R twopi, aphi, bphi;
+    // run constants of Sbvr / Rvr (Sediment_kernel.cu:167-326, 477-509),
+    // evaluated once on the host: drho*g, Ass, the Ucr prefactor
+    // (0.19 D50^0.1 or 8.5 D50^0.6), Rvr's alpha and beta; and 1/dx
+    R sed_drho, sed_drhog, sed_Ass, sed_ucr, rvr_alpha, rvr_beta, rdx;
     double endtime, outputtimestep, sedstart, dtbc, eps_d;
     int sedtrans;
     R cxsth[XBG_MAX_THETA], sxnth[XBG_MAX_THETA], theta[XBG_MAX_THETA];
