@@ -31,7 +31,7 @@ B_ALGO = lambda nt: 4 * (77 + 4 * nt)   # algorithmic bytes per coupled cell-upd
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--nx", type=int, default=2048)
@@ -50,8 +50,10 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    """nvidia-smi clocks and throttle reasons, sampled every 50 ms from before
+    the warm-up on; stop() keeps the samples whose nvidia-smi timestamp falls
+    inside the timed region [mark_start(), mark_end()]."""
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -59,11 +61,12 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.t0 = self.t1 = None
 
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.th = threading.Thread(target=self._read, daemon=True)
             self.th.start()
@@ -71,26 +74,45 @@ class ClockSampler:
             self.proc = None
 
     def _read(self):
+        import datetime
         for line in self.proc.stdout:
-            self.rows.append([x.strip() for x in line.split(",")])
+            r = [x.strip() for x in line.split(",")]
+            try:
+                ts = datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except Exception:
+                continue
+            self.rows.append([ts] + r[1:])
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.2)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        rows = [r for r in self.rows if len(r) >= 9]
-        if not rows:
+        rows = [r for r in self.rows if len(r) >= 10]
+        inside = [r for r in rows if self.t0 is not None and self.t0 - 0.025 <= r[0] <= self.t1 + 0.025]
+        use = inside
+        if not use:   # region shorter than the sampling period: the samples around it
+            after = [r for r in rows if self.t0 is not None and r[0] >= self.t0]
+            before = [r for r in rows if self.t0 is not None and r[0] < self.t0]
+            use = after[:1] + before[-1:]
+        if not use:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[2]) for r in use if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in use if r[3].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        reasons = sorted({names[k] for r in use for k in range(4) if r[6 + k].lower().startswith("active")})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(inside), "window_s": round(self.t1 - self.t0, 3)}
 
 
 def setup_model(nx, ny, seed=0):
@@ -208,19 +230,21 @@ def main():
     stream = torch.cuda.ExternalStream(m.stream())
     W = max(3, args.warmup)
     K = args.steps
+    sampler = ClockSampler(local)
+    sampler.start()
     m.advance(W)
     m.sync()
     launches0 = m.launches()
-    sampler = ClockSampler(local)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    sampler.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.mark_start()
     ev0.record(stream)
     m.advance(K)
     ev1.record(stream)
     ev1.synchronize()
+    sampler.mark_end()
     torch.cuda.synchronize()
     if dist:
         dist.barrier()

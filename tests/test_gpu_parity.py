@@ -128,26 +128,81 @@ def test_multistep_graph_vs_oracle_fp64():
     assert not bad, errs
 
 
-def test_full_run_linear_beach():
-    """The reference's CPU-runnable case (200 x 100, 10 bins, 600 s): final
-    H, zs, u, v, zb within 1e-3 of the oracle."""
-    p, m, o = _beach(200, 100, 10, sedstart=0.0, endtime=600.0, outputtimestep=600.0)
-    for _ in range(200):
-        m.advance(50)
-        t, _, _, fl, rc = m.time()
+FULL_FIELDS = ["H", "zs", "uu", "vv", "zb"]
+
+
+def _run_to_end(h, chunk):
+    while True:
+        h.advance(chunk)
+        t, _, n, fl, rc = h.time()
         assert rc == 0
         if fl & XBG_FLAG_ENDED:
-            break
-    while True:
-        o.advance(500)
-        t2, _, _, fl2, rc2 = o.time()
-        assert rc2 == 0
-        if fl2 & XBG_FLAG_ENDED:
-            break
-    assert abs(t - 600.0) < 1e-6 and abs(t2 - 600.0) < 1e-6
-    assert m.time()[2] == o.time()[2]
-    for n in ["H", "zs", "uu", "vv", "zb"]:
-        assert rel_err(m.get(n), o.get(n)) <= 1e-3, n
+            return t, n
+
+
+def _l2(a, b):
+    a = np.asarray(a, np.float64); b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def full_run_oracle():
+    """The reference's CPU-runnable case (200 x 100, 10 bins, 600 s, linear
+    beach) run by the oracle in FP32 and in FP64 (the error oracle)."""
+    out = {}
+    for prec in (XBG_FP32, XBG_FP64):
+        p, zb, bnd = make_case("linear_beach", nx=200, ny=100, ntheta=10)
+        p.sedstart, p.endtime, p.outputtimestep = 0.0, 600.0, 600.0
+        o = pyoracle.Oracle(p, prec)
+        o.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+        o.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        o.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        o.init_state(zb, 0.0, 0.0)
+        t, n = _run_to_end(o, 500)
+        out[prec] = dict(t=t, n=n, **{f: o.get(f).astype(np.float64) for f in FULL_FIELDS})
+    return out
+
+
+def _gpu_full_run(precision):
+    p, zb, bnd = make_case("linear_beach", nx=200, ny=100, ntheta=10)
+    p.sedstart, p.endtime, p.outputtimestep = 0.0, 600.0, 600.0
+    m = Model(p, precision)
+    m.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.init_state(zb, 0.0, 0.0)
+    t, n = _run_to_end(m, 50)
+    return dict(t=t, n=n, **{f: m.get(f).astype(np.float64) for f in FULL_FIELDS})
+
+
+def test_full_run_linear_beach_fp64(full_run_oracle):
+    """The FP64 build of the CUDA step over the whole 600 s run (3383 coupled
+    steps) against the FP64 oracle: same step count, end time, and final
+    H, zs, u, v, zb within 1e-8 -- the same algorithm to rounding."""
+    o = full_run_oracle[XBG_FP64]
+    g = _gpu_full_run(XBG_FP64)
+    assert g["n"] == o["n"] and abs(g["t"] - 600.0) < 1e-9
+    errs = {f: rel_err(g[f], o[f]) for f in FULL_FIELDS}
+    assert all(e <= 1e-8 for e in errs.values()), errs
+
+
+def test_full_run_linear_beach_fp32(full_run_oracle):
+    """The FP32 CUDA run over the same 600 s against the FP64 oracle.  The
+    reference algorithm's own FP32 arithmetic ends 1.2e-3 (H), 2.1e-3 (u) and
+    2.2e-2 (v) away from its FP64 result in max-norm (its threshold switches
+    amplify rounding), so the bar is relative to it: per field, in max-norm
+    and in L2, the CUDA FP32 result is within 3x the distance of the oracle's
+    FP32 result from the FP64 oracle (plus 1e-6 for fields that barely move)."""
+    o32, o64 = full_run_oracle[XBG_FP32], full_run_oracle[XBG_FP64]
+    g = _gpu_full_run(XBG_FP32)
+    assert g["n"] > 0 and abs(g["t"] - 600.0) < 1e-6
+    bad = {}
+    for f in FULL_FIELDS:
+        for name, norm in (("max", rel_err), ("l2", _l2)):
+            ref, got = norm(o32[f], o64[f]), norm(g[f], o64[f])
+            if not got <= 3.0 * ref + 1e-6:
+                bad[(f, name)] = (got, ref)
+    assert not bad, bad
 
 
 def test_deterministic():

@@ -310,12 +310,28 @@ __device__ __forceinline__ void wrk_v(const Dev<R>& S, const Konst<R>& K, int ix
     }
 }
 
+// Block tile for the passes that need per-cell intermediates of neighbours:
+// 32 x 8 cells plus one cell on every side, clamped at the grid edge exactly
+// as mm()/pp() clamp, so a neighbour read from the tile is the value the
+// reference reads.
+constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT_TX * FT_TY;
+
 template <class R>
 __global__ void __launch_bounds__(256) k_flow_corr(Dev<R> S, Konst<R> K) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
+    __shared__ R sU1[FT_N], sU2[FT_N], sV1[FT_N], sV2[FT_N];
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int bx0 = blockIdx.x * FT_X, by0 = blockIdx.y * FT_Y;
+    for (int e = threadIdx.x + threadIdx.y * FT_X; e < FT_N; e += FT_X * FT_Y) {
+        int gx = min(max(bx0 - 1 + e % FT_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / FT_TX, 0), ny - 1);
+        R a, b, c, d;
+        wrk_u(S, K, gx, gy, a, b);
+        wrk_v(S, K, gx, gy, c, d);
+        sU1[e] = a; sU2[e] = b; sV1[e] = c; sV2[e] = d;
+    }
+    __syncthreads();
+    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R dtf = (R)clk->dt, dx = K.dx;
@@ -323,21 +339,16 @@ __global__ void __launch_bounds__(256) k_flow_corr(Dev<R> S, Konst<R> K) {
     R u = ld(S.tmp[T_UU] + i), v = ld(S.tmp[T_VV] + i);
     if (ix > 0 && iy > 0) {
         int xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-        // uu2Ocorr (Flow_kernel.cu:2210-2245)
-        R w1i, w2i, w1r, t0, t1, w2b;
-        wrk_u(S, K, ix, iy, w1i, w2i);
-        wrk_u(S, K, xp, iy, w1r, t0);
-        wrk_u(S, K, ix, ym, t1, w2b);
+        const int c = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
+        // uu2Ocorr (Flow_kernel.cu:2210-2245): wrk at i, xp and ym
+        R w1i = sU1[c], w2i = sU2[c], w1r = sU1[c + 1], w2b = sU2[c - FT_TX];
         R qe = (R)0.5f * (ld(qx + IDX(xp, iy)) + ld(qx + i));
         R qw = (R)0.5f * (ld(qx + i) + ld(qx + IDX(xm, iy)));
         R qn = (R)0.5f * (ld(qy + IDX(ix, ym)) + ld(qy + IDX(xp, ym)));
         R qs = (R)0.5f * (ld(qy + i) + ld(qy + IDX(xm, iy)));
         u = u - dtf / ld(S.f[HUM] + i) * ((qe * w1r - qw * w1i) / dx + (qs * w2i - qn * w2b) / dx);
-        // vv2Ocorr (Flow_kernel.cu:2247-2282)
-        R v1i, v2i, v2l, v1t, t2, t3;
-        wrk_v(S, K, ix, iy, v1i, v2i);
-        wrk_v(S, K, xm, iy, t2, v2l);
-        wrk_v(S, K, ix, yp, v1t, t3);
+        // vv2Ocorr (Flow_kernel.cu:2247-2282): wrk at i, xm and yp
+        R v1i = sV1[c], v2i = sV2[c], v2l = sV2[c - 1], v1t = sV1[c + FT_TX];
         qe = (R)0.5f * (ld(qx + IDX(ix, yp)) + ld(qx + i));
         qw = (R)0.5f * (ld(qx + IDX(xm, iy)) + ld(qx + IDX(xm, yp)));
         qn = (R)0.5f * (ld(qy + i) + ld(qy + IDX(ix, ym)));
@@ -446,24 +457,24 @@ __device__ __forceinline__ R zs_corr(const Dev<R>& S, const Konst<R>& K, const R
     return z;
 }
 
-// calcuvvu (Flow_kernel.cu:467-544) at (ix, iy)
+// calcuvvu (Flow_kernel.cu:467-544) at (ix, iy); sS/sC hold ust*sin(thetamean)
+// and ust*cos(thetamean) of the tile, k is the tile index of (ix, iy), whose
+// right and top neighbours are k + 1 and k + FT_TX.
 template <class R>
-__device__ __forceinline__ void uvvu_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R* o6) {
+__device__ __forceinline__ void uvvu_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, const R* sS,
+                                          const R* sC, int k, R* o6) {
     const int nx = K.nx, ny = K.ny;
-    const R* uu = S.f[UU]; const R* vv = S.f[VV]; const R* ust = S.f[UST]; const R* thm = S.f[THM];
+    const R* uu = S.f[UU]; const R* vv = S.f[VV];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-    R usti = ld(ust + i), tmi = ld(thm + i);
-    R ustr = ld(ust + IDX(xp, iy)), tmr = ld(thm + IDX(xp, iy));
-    R ustt = ld(ust + IDX(ix, yp)), tmt = ld(thm + IDX(ix, yp));
     R wu = (R)ld(S.wetu + i), wv = (R)ld(S.wetv + i);
     R vu = (R)0.25f * (ld(vv + IDX(ix, ym)) + ld(vv + i) + ld(vv + IDX(xp, ym)) + ld(vv + IDX(xp, iy))) * wu;
     R uv = (R)0.25f * (ld(uu + IDX(xm, iy)) + ld(uu + i) + ld(uu + IDX(xm, yp)) + ld(uu + IDX(ix, yp))) * wv;
-    R vsu = (R)0.5f * (usti * DM<R>::sin(tmi) + ustr * DM<R>::sin(tmr)) * wu;
-    R usu = (R)0.5f * (usti * DM<R>::cos(tmi) + ustr * DM<R>::cos(tmr)) * wu;
+    R vsu = (R)0.5f * (sS[k] + sS[k + 1]) * wu;
+    R usu = (R)0.5f * (sC[k] + sC[k + 1]) * wu;
     R ue = ld(uu + i) - usu;
     R ve = vu - vsu;
-    R usv = (R)0.5f * (usti * DM<R>::cos(tmi) + ustt * DM<R>::cos(tmt)) * wv;
-    R vsv = (R)0.5f * (usti * DM<R>::sin(tmi) + ustt * DM<R>::sin(tmt)) * wv;
+    R usv = (R)0.5f * (sC[k] + sC[k + FT_TX]) * wv;
+    R vsv = (R)0.5f * (sS[k] + sS[k + FT_TX]) * wv;
     R vvv = ld(vv + i) - vsv;
     R uvv = uv - usv;
     o6[0] = vu; o6[1] = uv; o6[2] = ue; o6[3] = vvv;
@@ -471,29 +482,62 @@ __device__ __forceinline__ void uvvu_cell(const Dev<R>& S, const Konst<R>& K, in
     o6[5] = DM<R>::sqrt(uvv * uvv + vvv * vvv);
 }
 
+// zs after zs2Ocorr at the cell of tile index k (grid (ix, iy)) from the
+// tile's wrkzs2Ocorr values.
+template <class R>
+__device__ __forceinline__ R zs_corr_tile(const Dev<R>& S, const Konst<R>& K, const R* sW1, const R* sW2, int k,
+                                          int ix, int iy, R dtf) {
+    R z = ld(S.tmp[T_ZS] + ix + iy * K.nx);
+    if (ix > 0 && iy > 0) z = z - dtf * ((sW1[k] - sW1[k - 1]) / K.dx + (sW2[k] - sW2[k - FT_TX]) / K.dx);
+    return z;
+}
+
+// wrkzs2Ocorr + zs2Ocorr, latbnd(zs), hsbnd, calcuvvu + uvlatbnd.  The tile
+// holds wrkzs2Ocorr and the Stokes-drift products of every tile cell; the
+// lateral row ny-1 takes zs of row ny-2 (latbnd), whose lower neighbour is
+// outside the tile when ny-1 is the block's first row: that one case
+// evaluates zs_corr directly.
 template <class R>
 __global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
+    __shared__ R sW1[FT_N], sW2[FT_N], sS[FT_N], sC[FT_N];
     const R* zsold_in = S.zsold[clk->par ^ 1];
     R* zsold_out = S.zsold[clk->par];
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int bx0 = blockIdx.x * FT_X, by0 = blockIdx.y * FT_Y;
+    for (int e = threadIdx.x + threadIdx.y * FT_X; e < FT_N; e += FT_X * FT_Y) {
+        int gx = min(max(bx0 - 1 + e % FT_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / FT_TX, 0), ny - 1);
+        int g = IDX(gx, gy);
+        R a, b;
+        wrk_z(S, K, zsold_in, gx, gy, a, b);
+        R us = ld(S.f[UST] + g), tm = ld(S.f[THM] + g);
+        sW1[e] = a; sW2[e] = b;
+        sS[e] = us * DM<R>::sin(tm);
+        sC[e] = us * DM<R>::cos(tm);
+    }
+    __syncthreads();
+    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R dtf = (R)clk->dt;
     int sy = iy;
     if (iy == 0) sy = 1;
     if (iy == ny - 1) sy = ny - 2;
-    R w1, w2;
-    R zf = zs_corr(S, K, zsold_in, ix, iy, dtf, w1, w2);
+    const int k = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
+    const int ks = k + (sy - iy) * FT_TX;   // tile index of (ix, sy)
+    R zf = zs_corr_tile(S, K, sW1, sW2, k, ix, iy, dtf);
     if (ix > 0 && iy > 0) {   // zs2Ocorr flux update
-        S.f[QX][i] = ld(S.f[QX] + i) + w1;
-        S.f[QY][i] = ld(S.f[QY] + i) + w2;
+        S.f[QX][i] = ld(S.f[QX] + i) + sW1[k];
+        S.f[QY][i] = ld(S.f[QY] + i) + sW2[k];
     }
     if (sy != iy) {           // latbnd(zs)
-        R a, b;
-        zf = zs_corr(S, K, zsold_in, ix, sy, dtf, a, b);
+        if (ks >= FT_TX) {
+            zf = zs_corr_tile(S, K, sW1, sW2, ks, ix, sy, dtf);
+        } else {
+            R a, b;
+            zf = zs_corr(S, K, zsold_in, ix, sy, dtf, a, b);
+        }
     }
     S.f[ZS][i] = zf;
     S.f[HH][i] = DM<R>::fmax(ld(S.f[ZB] + i) + zf, K.eps);   // hsbnd
@@ -501,7 +545,7 @@ __global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
     S.f[VVOLD][i] = ld(S.f[VV] + i);
     zsold_out[i] = zf;
     R o6[6];
-    uvvu_cell(S, K, ix, sy, o6);   // calcuvvu + uvlatbnd
+    uvvu_cell(S, K, ix, sy, sS, sC, ks, o6);   // calcuvvu + uvlatbnd
     S.f[VU][i] = o6[0]; S.f[UV][i] = o6[1]; S.f[UEU][i] = o6[2]; S.f[VEV][i] = o6[3];
     S.f[VMAGEU][i] = o6[4]; S.f[VMAGEV][i] = o6[5];
 }

@@ -33,8 +33,7 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
     R c = ld(S.f[CC_] + i);
     // longturb (Sediment_kernel.cu:27-164)
     R rolth = ld(S.f[ROLTHICK] + i) + dtf * (DM<R>::fabs(ld(S.f[DZSDT] + i)) - K.beta * c);
-    S.f[ROLTHICK][i] = DM<R>::fmax(rolth, (R)0.0f);
-    S.f[KTURB][i] = (R)0.0f;
+    rolth = DM<R>::fmax(rolth, (R)0.0f);
     // Sbvr (:167-326); kturb is 0 after longturb
     R zo = (R)0.006f, sedcal = (R)1.0f, bulk = (R)1.0f;
     R D50 = K.D50, D90 = K.D90;
@@ -69,10 +68,8 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
     R ceqbg = ((R)1 - bulk) * ceqb * sedcal * wetz;
     R ceqs = DM<R>::fmin(Ass * T2 / hhi, (R)0.05f);
     R ceqsg = (ceqs + bulk * ceqb) * sedcal * wetz;
-    S.f[CEQSG][i] = ceqsg;
-    S.tmp[T_CEQBG][i] = ceqbg;
-    S.tmp[T_TSG][i] = Tsg;
     // Rvr (:477-509)
+    R ua;
     {
         R m1 = (R)0.0f, m2 = (R)0.7939f, m3 = (R)-0.6065f, m4 = (R)0.3539f, m5 = (R)0.6373f, m6 = (R)0.5995f;
         R alpha = K.rvr_alpha;
@@ -84,12 +81,20 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
         R B1 = (R)((double)((R)-90.0f + (R)90.0f * DM<R>::tanh(m5 / DM<R>::pow(Ur, m6))) * XBG_PI / 180.0f);
         R Sk = Bm * DM<R>::cos(B1);
         R As = Bm * DM<R>::sin(B1);
-        S.tmp[T_UA][i] = (K.facsk * Sk - K.facas * As) * urms;
+        ua = (K.facsk * Sk - K.facas * As) * urms;
     }
     // Erosus (:512-531)
     {
         R exp_ero = K.morfac * dtf / ((R)1.0f - K.por) * hh * (ceqsg * (R)1.0f / Tsg + ceqbg * (R)1.0f / dtf);
-        S.tmp[T_FACERO][i] = DM<R>::fmin((R)1.0f, ld(S.f[STDEP] + i) * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
+        R facero = DM<R>::fmin((R)1.0f, ld(S.f[STDEP] + i) * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
+        // all stores after all loads (the field pointers may alias as far as the compiler knows)
+        S.f[ROLTHICK][i] = rolth;
+        S.f[KTURB][i] = (R)0.0f;
+        S.f[CEQSG][i] = ceqsg;
+        S.tmp[T_CEQBG][i] = ceqbg;
+        S.tmp[T_TSG][i] = Tsg;
+        S.tmp[T_UA][i] = ua;
+        S.tmp[T_FACERO][i] = facero;
     }
 }
 
@@ -269,18 +274,42 @@ __device__ __forceinline__ R ddzb_cell(const Dev<R>& S, const Konst<R>& K, int i
     return a;
 }
 
+// zblatbnd, avalanching, updatezb, zblatbnd, updatezom.  The transfers
+// (dzbx, dzby) of every cell of the 32 x 8 tile, the column to its left and
+// the row below it go to shared memory once; a boundary cell whose zblatbnd
+// source lies elsewhere evaluates that source's bed change directly.
 template <class R>
 __global__ void __launch_bounds__(256) k_sed_c(Dev<R> S, Konst<R> K) {
     const Clock* clk = S.clk;
     if (sed_skip(clk)) return;
+    __shared__ R sBx[SB_TY * SB_TX], sBy[SB_TY * SB_TX];
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int bx0 = blockIdx.x * SB_X, by0 = blockIdx.y * SB_Y;
+    const bool morph = K.morfac > (R)0.0f;
+    const R dtf = (R)clk->dt;
+    if (morph) {
+        for (int e = threadIdx.x + threadIdx.y * SB_X; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
+            int gx = min(max(bx0 - 1 + e % SB_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / SB_TX, 0), ny - 1);
+            R a, b;
+            aval_cell(S, K, gx, gy, dtf, a, b);
+            sBx[e] = a;
+            sBy[e] = b;
+        }
+    }
+    __syncthreads();
+    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     S.f[CSED][i] = ld(S.tmp[T_UU] + i);
-    if (K.morfac > (R)0.0f) {
-        R dtf = (R)clk->dt;
-        R dd = ddzb_cell(S, K, ix, iy, dtf);
+    if (morph) {
+        // bed change gathered in the serial launch order:
+        // ((-dzby[below] - dzbx[left]) + dzbx) + dzby
+        const int c = (threadIdx.y + 1) * SB_TX + threadIdx.x + 1;
+        R dd = (R)0.0f;
+        if (iy > 0) dd = dd - sBy[c - SB_TX];
+        if (ix > 0) dd = dd - sBx[c - 1];
+        dd = dd + sBx[c];
+        dd = dd + sBy[c];
         // updatezb (:1139-1160) at the own cell
         S.f[DZB][i] = ld(S.f[DZB] + i) - dd;
         S.f[ZS][i] = ld(S.f[ZS] + i) - dd;

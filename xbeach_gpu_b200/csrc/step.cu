@@ -232,14 +232,19 @@ __global__ void __launch_bounds__(256) k_means(Dev<R> S, Konst<R> K) {
     if (halted(S.clk)) return;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= S.C) return;
-    R zs = ld(S.f[ZS] + i);
-    S.f[HMEAN][i] = S.f[HMEAN][i] + ld(S.f[H] + i);
-    S.f[UUMEAN][i] = S.f[UUMEAN][i] + ld(S.f[UU] + i);
-    S.f[VVMEAN][i] = S.f[VVMEAN][i] + ld(S.f[VV] + i);
-    S.f[HHMEAN][i] = S.f[HHMEAN][i] + ld(S.f[HH] + i);
-    S.f[ZSMEAN][i] = S.f[ZSMEAN][i] + zs;
-    S.f[ZSMAX][i] = DM<R>::fmax(S.f[ZSMAX][i], zs);
-    S.f[CMEAN][i] = S.f[CMEAN][i] + ld(S.f[CSED] + i);
+    // every load before the first store: the field pointers may alias as far
+    // as the compiler knows, so interleaved stores would serialise the loads
+    R zs = ld(S.f[ZS] + i), hr = ld(S.f[H] + i), u = ld(S.f[UU] + i), v = ld(S.f[VV] + i);
+    R h = ld(S.f[HH] + i), c = ld(S.f[CSED] + i);
+    R mH = S.f[HMEAN][i], mu = S.f[UUMEAN][i], mv = S.f[VVMEAN][i], mh = S.f[HHMEAN][i];
+    R mz = S.f[ZSMEAN][i], xz = S.f[ZSMAX][i], mc = S.f[CMEAN][i];
+    S.f[HMEAN][i] = mH + hr;
+    S.f[UUMEAN][i] = mu + u;
+    S.f[VVMEAN][i] = mv + v;
+    S.f[HHMEAN][i] = mh + h;
+    S.f[ZSMEAN][i] = mz + zs;
+    S.f[ZSMAX][i] = DM<R>::fmax(xz, zs);
+    S.f[CMEAN][i] = mc + c;
 }
 
 template <class R>

@@ -3,13 +3,16 @@
 //
 // Kernels (launch order):
 //   k_disp       dispersion (wave_CPU.cpp:154-205) per cell -> k, c, cg
-//   k_wave_main  rows 1..ny-2: offshore boundary + sanity + action, x/y/theta
-//                second-order upwind advection of ee and rr with the Euler
-//                step, energy, energint, roelvink|baldock, dissipation,
-//                meandir, radstress.  All theta bins of a cell live in
-//                registers; ctheta (propagtheta) is evaluated on the fly from
-//                per-cell slopes and never stored.  Emits the per-block
-//                WAVEDT minimum for the next step's dt.
+//   k_wave_fast  rows 1..ny-2, one thread per cell, bins streamed in order:
+//                offshore boundary + sanity + action, x/y/theta second-order
+//                upwind advection of ee and rr with the Euler step (in energy
+//                units), then energint, roelvink|baldock, dissipation,
+//                meandir, radstress.  Each bin's ee/rr plane tile (32 x 8
+//                cells + 2-cell halo) streams into shared memory by cp.async
+//                one bin ahead (three buffers, one barrier per bin); ctheta
+//                (propagtheta) is evaluated on the fly from per-cell slopes;
+//                the theta-face flux is computed once and carried to the
+//                next bin.  Emits the per-block WAVEDT minimum.
 //   k_wave_edge  rows 0 and ny-1, whose ee/rr are copies of rows 1 / ny-2
 //                (rollerlatbnd, wave_CPU.cpp:830-870) between the passes.
 //   k_wave_force wavforce + twodimbnd(noix) + breakerdelay + twodimbnd(ust).
@@ -366,508 +369,11 @@ __device__ __forceinline__ R ctheta_cell(const Konst<R>& K, const CthCoef<R>& cc
     return mindt;
 }
 
-template <class R, int NMAX>
-__global__ void __launch_bounds__(256) k_wave_main(Dev<R> S, Konst<R> K) {
-    const Clock* clk = S.clk;
-    if (halted(clk)) return;
-    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    int iy = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    R dtw = (R)3.0e38f;
-    if (ix < nx && iy <= ny - 2) {
-        int i = ix + iy * nx;
-        int par = clk->par;
-        const R* eeo = S.ee[par ^ 1];
-        const R* rro = S.rr[par ^ 1];
-        R* een = S.ee[par];
-        R* rrn = S.rr[par];
-        R sg = (R)clk->sigm;
-        R dtf = (R)clk->dt;
-        R Trep = (R)clk->Trep;
-        R tt = (R)clk->totaltime;
-        R taper = (R)cmin((double)tt / 100.0, 1.0);
-        const R* St = S.St;
-        CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
-        R cthv[NMAX];
-        dtw = ctheta_cell<R, NMAX>(K, cc, cthv);
-        // ee after offshorebndWav, sanity and action (wave_CPU.cpp:24-70, 308-326)
-        auto qe = [&](int x, int y, int t) -> R {
-            R v = (x == 0) ? St[y + t * ny] * taper : ld(eeo + x + y * nx + (size_t)t * C);
-            v = cmax(v, (R)0.000f);
-            return v / sg;
-        };
-        auto qr = [&](int x, int y, int t) -> R { return ld(rro + x + y * nx + (size_t)t * C); };
-        R e[NMAX], r[NMAX];
-        advect_cell<R, NMAX>(S, K, ix, iy, S.f[CG], cthv, qe, dtf, e);
-        if (K.roller == 1) {
-            advect_cell<R, NMAX>(S, K, ix, iy, S.f[CC_], cthv, qr, dtf, r);
-        } else {
-#pragma unroll
-            for (int t = 0; t < NMAX; t++) r[t] = (t < nt) ? qr(ix, iy, t) : (R)0;
-        }
-        if (iy == 1 || iy == ny - 2) {   // advected rows 1 / ny-2 for the edge rows
-            int slot = (iy == 1) ? 0 : 1;
-#pragma unroll
-            for (int t = 0; t < NMAX; t++) {
-                if (t < nt) {
-                    S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = e[t];
-                    S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = r[t];
-                }
-            }
-        }
-        CellOut<R> o = chain_cell<R, NMAX>(S, K, i, sg, dtf, Trep, e, r);
-        finish_cell<R, NMAX>(S, K, i, e, r, o, een, rrn);
-    }
-    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
-}
-
-// thetaadvecuw2hoCPU (wave_CPU.cpp:706-806) at bin t from the clamped bin
-// window e(t-2..t+2) and ctheta window c(t-1..t+1).
-template <class R>
-__device__ __forceinline__ R theta_adv(R em2, R em, R e0, R ep, R ep2, R cm, R c0, R cp, int t, int nt, R dth) {
-    if (nt <= 1) return (R)0.0f;
-    R cthetab = (R)0.5f * (c0 + cp);
-    R eupw;
-    if (cthetab > (R)0.0f) {
-        eupw = up2f(e0, em);
-        if (eupw < (R)0.0f) eupw = e0;
-    } else {
-        eupw = up2f(ep, ep2);
-        if (eupw < (R)0.0f) eupw = ep;
-    }
-    R arrint = cthetab * eupw;
-    cthetab = (R)0.5f * (cm + c0);
-    if (cthetab > (R)0.0f) {
-        eupw = up2f(em, em2);
-        if (eupw < (R)0.0f) eupw = em;
-    } else {
-        eupw = up2f(e0, ep);
-        if (eupw < (R)0.0f) eupw = e0;
-    }
-    R arrmint = cthetab * eupw;
-    // zero flux through the first and last bin edges: one division of the
-    // selected numerator (arrint - 0 and 0 - arrmint are exact)
-    R num = (t == 0) ? arrint : ((t == nt - 1) ? (R)0.0f - arrmint : arrint - arrmint);
-    return num / dth;
-}
-
-// Face speeds of one cell for the x/y upwind fluxes (xadvecupwind2CPU:
-// cg at i and the x/y neighbours, u*wci and v*wci with wci of the cell).
-template <class R>
-struct Faces { R sp, sxm, sxp, sym, syp; };
-
-// The wave-action pass of rows 1..ny-2, streaming the theta planes: for each
-// bin t the x/y fluxes read the plane's neighbours (L1/L2 resident), the
-// theta flux uses a sliding register window of the cell's own bins, and the
-// advected ee / rr of the bin are parked in shared memory for the per-cell
-// chain (energint needs the sum over all bins before dissipation).
-template <class R>
-__global__ void __launch_bounds__(256, 3) k_wave_rows(Dev<R> S, Konst<R> K) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Clock* clk = S.clk;
-    if (halted(clk)) return;
-    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
-    const int nthr = blockDim.x * blockDim.y;
-    const int tid = threadIdx.x + threadIdx.y * blockDim.x;
-    R* sA = (R*)smem_raw;            // [nt][nthr] advected ee
-    R* sR = sA + (size_t)nt * nthr;  // [nt][nthr] advected rr
-    int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    int iy = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    R dtw = (R)3.0e38f;
-    if (ix < nx && iy <= ny - 2) {
-        const int i = ix + iy * nx;
-        const int par = clk->par;
-        const R* eeo = S.ee[par ^ 1];
-        const R* rro = S.rr[par ^ 1];
-        R* een = S.ee[par];
-        R* rrn = S.rr[par];
-        const R sg = (R)clk->sigm;
-        const R dtf = (R)clk->dt;
-        const R Trep = (R)clk->Trep;
-        const R tt = (R)clk->totaltime;
-        const R taper = (R)cmin((double)tt / 100.0, 1.0);
-        const R* St = S.St;
-        const int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
-        const int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
-        const int o_xm2 = xm2 + iy * nx, o_xm = xm + iy * nx, o_xp = xp + iy * nx, o_xp2 = xp2 + iy * nx;
-        const int o_ym2 = ix + ym2 * nx, o_ym = ix + ym * nx, o_yp = ix + yp * nx, o_yp2 = ix + yp2 * nx;
-        const R hh = ld(S.f[HH] + i);
-        const CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
-        const R wci = cc.wci;
-        const R dxplus_i = (R)1.0f / K.dx;
-        const R dth = K.dtheta;
-        const R* cgp = S.f[CG];
-        const R* cp = S.f[CC_];
-        Faces<R> fe{ld(cgp + i), ld(cgp + o_xm), ld(cgp + o_xp), ld(cgp + o_ym), ld(cgp + o_yp)};
-        Faces<R> fr{ld(cp + i), ld(cp + o_xm), ld(cp + o_xp), ld(cp + o_ym), ld(cp + o_yp)};
-        const R* uu = S.f[UU]; const R* vv = S.f[VV];
-        const R uui = ld(uu + i) * wci, uuixmin = ld(uu + o_xm) * wci, uuixmax = ld(uu + o_xp) * wci;
-        const R vvi = wci * ld(vv + i), vviymin = wci * ld(vv + o_ym), vviymax = wci * ld(vv + o_yp);
-        // ee after offshorebndWav + sanity + action at plane t (column 0 is St)
-        auto qe = [&](int off, int x, int y, int t) -> R {
-            R v = (x == 0) ? St[y + t * ny] * taper : ld(eeo + off + (size_t)t * C);
-            v = cmax(v, (R)0.000f);
-            return v / sg;
-        };
-        const bool roller = K.roller == 1;
-        // windows of the cell's own bins: clamp(t-2) .. clamp(t+2)
-        auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
-        R we0 = qe(i, ix, iy, cl(-2)), we1 = qe(i, ix, iy, cl(-1)), we2 = qe(i, ix, iy, 0),
-          we3 = qe(i, ix, iy, cl(1)), we4 = qe(i, ix, iy, cl(2));
-        R wr0 = ld(rro + i + (size_t)cl(-2) * C), wr1 = ld(rro + i + (size_t)cl(-1) * C), wr2 = ld(rro + i),
-          wr3 = ld(rro + i + (size_t)cl(1) * C), wr4 = ld(rro + i + (size_t)cl(2) * C);
-        R c0 = cth_eval(cc, K.cxsth[0], K.sxnth[0]);
-        R cm = c0;
-        R cpp = cth_eval(cc, K.cxsth[cl(1)], K.sxnth[cl(1)]);
-        R Etmp = (R)0.0f;
-        const bool edge_row = (iy == 1 || iy == ny - 2);
-        const int slot = (iy == 1) ? 0 : 1;
-#pragma unroll 1
-        for (int t = 0; t < nt; t++) {
-            const size_t o = (size_t)t * C;
-            const R ct = K.cxsth[t], st = K.sxnth[t];
-            dtw = DM<R>::fmin(K.cfl * dth / DM<R>::fabs(c0), dtw);
-            // ee: x and y fluxes of plane t, theta flux from the window
-            R cgx = (R)0.5f * (fe.sp * ct + uui + fe.sxp * ct + uuixmax);
-            R cgxmin = (R)0.5f * (fe.sp * ct + uui + fe.sxm * ct + uuixmin);
-            R cgy = (R)0.5f * (fe.sp * st + vvi + fe.syp * st + vviymax);
-            R cgymin = (R)0.5f * (fe.sp * st + vvi + fe.sym * st + vviymin);
-            R xa = adv2(qe(o_xm2, xm2, iy, t), qe(o_xm, xm, iy, t), we2, qe(o_xp, xp, iy, t),
-                        qe(o_xp2, xp2, iy, t), cgx, cgxmin, dxplus_i);
-            R ya = adv2(qe(o_ym2, ix, ym2, t), qe(o_ym, ix, ym, t), we2, qe(o_yp, ix, yp, t),
-                        qe(o_yp2, ix, yp2, t), cgy, cgymin, dxplus_i);
-            R ta = theta_adv(we0, we1, we2, we3, we4, cm, c0, cpp, t, nt, dth);
-            R A = we2 - dtf * (xa + ya + ta);
-            // rr with the phase speed c (Wavestep.cu:1277-1284)
-            R Ar = wr2;
-            if (roller) {
-                R cx = (R)0.5f * (fr.sp * ct + uui + fr.sxp * ct + uuixmax);
-                R cxm = (R)0.5f * (fr.sp * ct + uui + fr.sxm * ct + uuixmin);
-                R cy = (R)0.5f * (fr.sp * st + vvi + fr.syp * st + vviymax);
-                R cym = (R)0.5f * (fr.sp * st + vvi + fr.sym * st + vviymin);
-                R xr = adv2(ld(rro + o_xm2 + o), ld(rro + o_xm + o), wr2, ld(rro + o_xp + o),
-                            ld(rro + o_xp2 + o), cx, cxm, dxplus_i);
-                R yr = adv2(ld(rro + o_ym2 + o), ld(rro + o_ym + o), wr2, ld(rro + o_yp + o),
-                            ld(rro + o_yp2 + o), cy, cym, dxplus_i);
-                R tr = theta_adv(wr0, wr1, wr2, wr3, wr4, cm, c0, cpp, t, nt, dth);
-                Ar = wr2 - dtf * (xr + yr + tr);
-            }
-            sA[t * nthr + tid] = A;
-            sR[t * nthr + tid] = Ar;
-            if (edge_row) {   // advected rows 1 / ny-2 for the edge rows
-                S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = A;
-                S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = Ar;
-            }
-            Etmp = Etmp + cmax(A * sg, (R)0.0f);   // energyCPU, then the energint sum
-            // slide the windows
-            const int tn = cl(t + 3);
-            we0 = we1; we1 = we2; we2 = we3; we3 = we4; we4 = qe(i, ix, iy, tn);
-            wr0 = wr1; wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(rro + i + (size_t)tn * C);
-            cm = c0; c0 = cpp; cpp = cth_eval(cc, K.cxsth[cl(t + 2)], K.sxnth[cl(t + 2)]);
-        }
-        // energintCPU (wave_CPU.cpp:891-924)
-        const R rho = K.rho, g = K.g;
-        Etmp = Etmp * dth;
-        R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
-        const R idiv = cmax((R)1.0f, DM<R>::pow(Htmp / (K.gammax * hh), (R)2.0f));
-        Htmp = cmin(Htmp, K.gammax * hh);
-        const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
-        const R k = ld(S.f[WK] + i);
-        const R fw = ld(S.f[FWM] + i);
-        R Dv;
-        if (K.breakmodel == 1) {   // roelvinkCPU (wave_CPU.cpp:927-985)
-            R fac = (R)(8.0 / (double)rho / (double)g);
-            R Ht = DM<R>::sqrt(Eint * fac);
-            R Qb = (R)(1.0 - ::exp(cmax(-1.0 * (double)DM<R>::pow((Ht / K.gammaa / hh), K.nexp), -100.0)));
-            Qb = cmin(Qb, (R)1.0f);
-            Dv = (R)((double)Qb * 2.0 * (double)K.alpha / (double)Trep * (double)Eint * (double)Ht / (double)hh);
-            R uorb = (R)(XBG_PI * (double)Ht / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
-            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
-                                      (double)uorb * (double)uorb);
-        } else {                   // baldockCPU (wave_CPU.cpp:987-1028)
-            R khh = k * hh;
-            R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
-            R Rr = Hb / cmax(Htmp, (R)0.00001f);
-            R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
-            Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
-            R uorb = (R)(XBG_PI * (double)Htmp / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
-            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
-                                      (double)uorb * (double)uorb);
-        }
-        // dissipationCPU (wave_CPU.cpp:1030-1092), then meandir and radstress
-        // on the final bins (wave_CPU.cpp:1095-1162)
-        const R cc_i = fr.sp;
-        const R Emax = cmax(Eint, (R)0.0000001f);
-        const bool wet = hh > K.eps;
-        R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
-        R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0;
-#pragma unroll 2
-        for (int t = 0; t < nt; t++) {
-            const R cx0 = K.cxsth[t], sx0 = K.sxnth[t];
-            R eet = cmax(sA[t * nthr + tid] * sg, (R)0.0f) / idiv;
-            R rrt;
-            const R dd = eet * Dv / Emax;
-            if (wet) {
-                rrt = sR[t * nthr + tid];
-                R cx = cc_i * cx0 + uui;
-                R cy = cc_i * sx0 + vvi;
-                R rrd = (R)2.0f * g * K.beta * rrt / DM<R>::sqrt(cx * cx + cy * cy);
-                eet = cmax(eet - dtf * dd, (R)0.0f);
-                rrt = cmax(rrt + dtf * (dd - rrd), (R)0.0f);
-                drr = drr + rrd;
-            } else {
-                eet = (R)0.0f; rrt = (R)0.0f; drr = (R)0.0f;
-            }
-            RR = RR + rrt;
-            een[i + (size_t)t * C] = eet;
-            rrn[i + (size_t)t * C] = rrt;
-            sume = sume + eet;
-            sumethet = sumethet + eet * K.theta[t];
-            txx = txx + (((R)1.0f + cx0 * cx0) * eet);
-            tyy = tyy + (((R)1.0f + sx0 * sx0) * eet);
-            txy = txy + (sx0 * cx0 * eet);
-            rxx = rxx + ((cx0 * cx0) * rrt);
-            ryy = ryy + ((sx0 * sx0) * rrt);
-            rxy = rxy + (sx0 * cx0 * rrt);
-        }
-        const R sum2 = sume;
-        sume = cmax(sume, (R)0.00001f);
-        S.f[THM][i] = (sumethet / (R)nt) / (sume / (R)nt);
-        S.f[E][i] = sume * dth;
-        S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
-        S.f[D][i] = Dv;
-        S.f[ROL][i] = RR * dth;
-        S.f[DR][i] = drr * dth;
-        const R n = fe.sp / cc_i;
-        S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
-        S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
-        S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
-    }
-    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
-}
-
-// Tiled version of the rows pass: per theta plane, the block stages the
-// plane's (32+4) x (8+4) neighbourhood of ee (after offshore boundary, sanity
-// and action) and of rr in shared memory once, so each value is transformed
-// and fetched once per block instead of once per neighbouring thread.  Tile
-// element k holds the value at the clamped coordinate bx0-2+k (by0-2+k), so
-// the reference's clamped neighbour indices map straight into the tile.
 #define WT_X 32
 #define WT_Y 8
 #define WT_TX (WT_X + 4)
 #define WT_TY (WT_Y + 4)
 #define WT_N (WT_TX * WT_TY)
-template <class R>
-__global__ void __launch_bounds__(256, 3) k_wave_tile(Dev<R> S, Konst<R> K) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const Clock* clk = S.clk;
-    if (halted(clk)) return;
-    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
-    const int tid = threadIdx.x + threadIdx.y * WT_X;
-    R* tE = (R*)smem_raw;                 // [WT_N] plane tile of ee/sigm
-    R* tR = tE + WT_N;                    // [WT_N] plane tile of rr
-    R* sA = tR + WT_N;                    // [nt][256] advected ee
-    R* sR = sA + (size_t)nt * 256;        // [nt][256] advected rr
-    const int bx0 = blockIdx.x * WT_X, by0 = 1 + blockIdx.y * WT_Y;
-    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    const bool active = ix < nx && iy <= ny - 2;
-    const int par = clk->par;
-    const R* eeo = S.ee[par ^ 1];
-    const R* rro = S.rr[par ^ 1];
-    const R sg = (R)clk->sigm;
-    const R dtf = (R)clk->dt;
-    const R taper = (R)cmin((double)(R)clk->totaltime / 100.0, 1.0);
-    const R* St = S.St;
-    const bool roller = K.roller == 1;
-    const R dth = K.dtheta;
-    // tile element -> clamped grid offset (two elements per thread at most)
-    int eoff[2], ex0[2], ey0[2];
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        int e = tid + k * 256;
-        int kx = e % WT_TX, ky = e / WT_TX;
-        int gx = bx0 - 2 + kx, gy = by0 - 2 + ky;
-        gx = gx < 0 ? 0 : (gx > nx - 1 ? nx - 1 : gx);
-        gy = gy < 0 ? 0 : (gy > ny - 1 ? ny - 1 : gy);
-        ex0[k] = gx; ey0[k] = gy;
-        eoff[k] = (e < WT_N) ? gx + gy * nx : -1;
-    }
-    // per-cell constants
-    R dtw = (R)3.0e38f;
-    int i = 0, pxm = 0, pxm2 = 0, pxp = 0, pxp2 = 0, pym = 0, pym2 = 0, pyp = 0, pyp2 = 0, pc = 0;
-    R hh = 0, wci = 0, uui = 0, uuixmin = 0, uuixmax = 0, vvi = 0, vviymin = 0, vviymax = 0;
-    Faces<R> fe{}, fr{};
-    CthCoef<R> cc{};
-    R we0 = 0, we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr0 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;
-    R cm = 0, c0 = 0, cpp = 0, Etmp = 0;
-    auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
-    auto qe = [&](int off, int x, int y, int t) -> R {
-        R v = (x == 0) ? St[y + t * ny] * taper : ld(eeo + off + (size_t)t * C);
-        v = cmax(v, (R)0.000f);
-        return v / sg;
-    };
-    if (active) {
-        i = ix + iy * nx;
-        const int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
-        const int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
-        const int ry = (iy - by0 + 2) * WT_TX, rx = ix - bx0 + 2;
-        pc = ry + rx;
-        pxm2 = ry + (xm2 - bx0 + 2); pxm = ry + (xm - bx0 + 2);
-        pxp = ry + (xp - bx0 + 2); pxp2 = ry + (xp2 - bx0 + 2);
-        pym2 = (ym2 - by0 + 2) * WT_TX + rx; pym = (ym - by0 + 2) * WT_TX + rx;
-        pyp = (yp - by0 + 2) * WT_TX + rx; pyp2 = (yp2 - by0 + 2) * WT_TX + rx;
-        hh = ld(S.f[HH] + i);
-        cc = cth_coef(S, K, ix, iy, sg);
-        wci = cc.wci;
-        const R* cgp = S.f[CG];
-        const R* cp = S.f[CC_];
-        fe = Faces<R>{ld(cgp + i), ld(cgp + xm + iy * nx), ld(cgp + xp + iy * nx), ld(cgp + ix + ym * nx), ld(cgp + ix + yp * nx)};
-        fr = Faces<R>{ld(cp + i), ld(cp + xm + iy * nx), ld(cp + xp + iy * nx), ld(cp + ix + ym * nx), ld(cp + ix + yp * nx)};
-        const R* uu = S.f[UU]; const R* vv = S.f[VV];
-        uui = ld(uu + i) * wci; uuixmin = ld(uu + xm + iy * nx) * wci; uuixmax = ld(uu + xp + iy * nx) * wci;
-        vvi = wci * ld(vv + i); vviymin = wci * ld(vv + ix + ym * nx); vviymax = wci * ld(vv + ix + yp * nx);
-        we0 = qe(i, ix, iy, cl(-2)); we1 = qe(i, ix, iy, cl(-1)); we2 = qe(i, ix, iy, 0);
-        we3 = qe(i, ix, iy, cl(1)); we4 = qe(i, ix, iy, cl(2));
-        wr0 = ld(rro + i + (size_t)cl(-2) * C); wr1 = ld(rro + i + (size_t)cl(-1) * C); wr2 = ld(rro + i);
-        wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
-        c0 = cth_eval(cc, K.cxsth[0], K.sxnth[0]);
-        cm = c0;
-        cpp = cth_eval(cc, K.cxsth[cl(1)], K.sxnth[cl(1)]);
-    }
-    const bool edge_row = active && (iy == 1 || iy == ny - 2);
-    const int slot = (iy == 1) ? 0 : 1;
-    const R dxplus_i = (R)1.0f / K.dx;
-#pragma unroll 1
-    for (int t = 0; t < nt; t++) {
-        const size_t o = (size_t)t * C;
-        __syncthreads();   // previous plane consumed
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            if (eoff[k] >= 0) {
-                tE[tid + k * 256] = qe(eoff[k], ex0[k], ey0[k], t);
-                if (roller) tR[tid + k * 256] = ld(rro + eoff[k] + o);
-            }
-        }
-        __syncthreads();
-        if (active) {
-            const R ct = K.cxsth[t], st = K.sxnth[t];
-            dtw = DM<R>::fmin(K.cfl * dth / DM<R>::fabs(c0), dtw);
-            R cgx = (R)0.5f * (fe.sp * ct + uui + fe.sxp * ct + uuixmax);
-            R cgxmin = (R)0.5f * (fe.sp * ct + uui + fe.sxm * ct + uuixmin);
-            R cgy = (R)0.5f * (fe.sp * st + vvi + fe.syp * st + vviymax);
-            R cgymin = (R)0.5f * (fe.sp * st + vvi + fe.sym * st + vviymin);
-            R xa = adv2(tE[pxm2], tE[pxm], we2, tE[pxp], tE[pxp2], cgx, cgxmin, dxplus_i);
-            R ya = adv2(tE[pym2], tE[pym], we2, tE[pyp], tE[pyp2], cgy, cgymin, dxplus_i);
-            R ta = theta_adv(we0, we1, we2, we3, we4, cm, c0, cpp, t, nt, dth);
-            R A = we2 - dtf * (xa + ya + ta);
-            R Ar = wr2;
-            if (roller) {
-                R cx = (R)0.5f * (fr.sp * ct + uui + fr.sxp * ct + uuixmax);
-                R cxm = (R)0.5f * (fr.sp * ct + uui + fr.sxm * ct + uuixmin);
-                R cy = (R)0.5f * (fr.sp * st + vvi + fr.syp * st + vviymax);
-                R cym = (R)0.5f * (fr.sp * st + vvi + fr.sym * st + vviymin);
-                R xr = adv2(tR[pxm2], tR[pxm], wr2, tR[pxp], tR[pxp2], cx, cxm, dxplus_i);
-                R yr = adv2(tR[pym2], tR[pym], wr2, tR[pyp], tR[pyp2], cy, cym, dxplus_i);
-                R tr = theta_adv(wr0, wr1, wr2, wr3, wr4, cm, c0, cpp, t, nt, dth);
-                Ar = wr2 - dtf * (xr + yr + tr);
-            }
-            sA[t * 256 + tid] = A;
-            sR[t * 256 + tid] = Ar;
-            if (edge_row) {
-                S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = A;
-                S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = Ar;
-            }
-            Etmp = Etmp + cmax(A * sg, (R)0.0f);
-            const int tn = cl(t + 3);
-            we0 = we1; we1 = we2; we2 = we3; we3 = we4; we4 = qe(i, ix, iy, tn);
-            wr0 = wr1; wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(rro + i + (size_t)tn * C);
-            cm = c0; c0 = cpp; cpp = cth_eval(cc, K.cxsth[cl(t + 2)], K.sxnth[cl(t + 2)]);
-        }
-    }
-    if (active) {
-        R* een = S.ee[par];
-        R* rrn = S.rr[par];
-        const R Trep = (R)clk->Trep;
-        // energintCPU (wave_CPU.cpp:891-924)
-        const R rho = K.rho, g = K.g;
-        Etmp = Etmp * dth;
-        R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
-        const R idiv = cmax((R)1.0f, DM<R>::pow(Htmp / (K.gammax * hh), (R)2.0f));
-        Htmp = cmin(Htmp, K.gammax * hh);
-        const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
-        const R k = ld(S.f[WK] + i);
-        const R fw = ld(S.f[FWM] + i);
-        R Dv;
-        if (K.breakmodel == 1) {   // roelvinkCPU (wave_CPU.cpp:927-985)
-            R fac = (R)(8.0 / (double)rho / (double)g);
-            R Ht = DM<R>::sqrt(Eint * fac);
-            R Qb = (R)(1.0 - ::exp(cmax(-1.0 * (double)DM<R>::pow((Ht / K.gammaa / hh), K.nexp), -100.0)));
-            Qb = cmin(Qb, (R)1.0f);
-            Dv = (R)((double)Qb * 2.0 * (double)K.alpha / (double)Trep * (double)Eint * (double)Ht / (double)hh);
-            R uorb = (R)(XBG_PI * (double)Ht / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
-            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
-                                      (double)uorb * (double)uorb);
-        } else {                   // baldockCPU (wave_CPU.cpp:987-1028)
-            R khh = k * hh;
-            R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
-            R Rr = Hb / cmax(Htmp, (R)0.00001f);
-            R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
-            Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
-            R uorb = (R)(XBG_PI * (double)Htmp / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
-            Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
-                                      (double)uorb * (double)uorb);
-        }
-        // dissipationCPU (wave_CPU.cpp:1030-1092), meandir and radstress
-        const R cc_i = fr.sp;
-        const R Emax = cmax(Eint, (R)0.0000001f);
-        const bool wet = hh > K.eps;
-        R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
-        R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0;
-#pragma unroll 2
-        for (int t = 0; t < nt; t++) {
-            const R cx0 = K.cxsth[t], sx0 = K.sxnth[t];
-            R eet = cmax(sA[t * 256 + tid] * sg, (R)0.0f) / idiv;
-            R rrt;
-            const R dd = eet * Dv / Emax;
-            if (wet) {
-                rrt = sR[t * 256 + tid];
-                R cx = cc_i * cx0 + uui;
-                R cy = cc_i * sx0 + vvi;
-                R rrd = (R)2.0f * g * K.beta * rrt / DM<R>::sqrt(cx * cx + cy * cy);
-                eet = cmax(eet - dtf * dd, (R)0.0f);
-                rrt = cmax(rrt + dtf * (dd - rrd), (R)0.0f);
-                drr = drr + rrd;
-            } else {
-                eet = (R)0.0f; rrt = (R)0.0f; drr = (R)0.0f;
-            }
-            RR = RR + rrt;
-            een[i + (size_t)t * C] = eet;
-            rrn[i + (size_t)t * C] = rrt;
-            sume = sume + eet;
-            sumethet = sumethet + eet * K.theta[t];
-            txx = txx + (((R)1.0f + cx0 * cx0) * eet);
-            tyy = tyy + (((R)1.0f + sx0 * sx0) * eet);
-            txy = txy + (sx0 * cx0 * eet);
-            rxx = rxx + ((cx0 * cx0) * rrt);
-            ryy = ryy + ((sx0 * sx0) * rrt);
-            rxy = rxy + (sx0 * cx0 * rrt);
-        }
-        const R sum2 = sume;
-        sume = cmax(sume, (R)0.00001f);
-        S.f[THM][i] = (sumethet / (R)nt) / (sume / (R)nt);
-        S.f[E][i] = sume * dth;
-        S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
-        S.f[D][i] = Dv;
-        S.f[ROL][i] = RR * dth;
-        S.f[DR][i] = drr * dth;
-        const R n = fe.sp / cc_i;
-        S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
-        S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
-        S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
-    }
-    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
-}
-
 // ------------------------------------------------------------------------
 // Fast rows pass.  Same algorithm as k_wave_tile, arranged for instruction
 // throughput (the pass is issue-bound, not HBM-bound):
@@ -890,18 +396,27 @@ __device__ __forceinline__ R flux2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin
     R arrmin = (cfmin > (R)0 ? upw(qm, qm2) : upw(qi, qp)) * cfmin;
     return arrin - arrmin;
 }
+// Asynchronous 4/8-byte global -> shared copies (cp.async, completion by
+// commit groups) for the plane tiles.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// theta-face flux between bins t and t+1 (the arrint of bin t, which is the
+// arrmint of bin t+1): e(t-1), e(t), e(t+1), e(t+2), ctheta(t), ctheta(t+1)
 template <class R>
-__device__ __forceinline__ R flux_theta(R em2, R em, R e0, R ep, R ep2, R cm, R c0, R cp, bool first, bool last) {
+__device__ __forceinline__ R theta_face(R em, R e0, R ep, R ep2, R c0, R cp) {
     R cb = (R)0.5f * (c0 + cp);
     R u1 = (R)1.5f * e0 - (R)0.5f * em;   u1 = u1 < (R)0 ? e0 : u1;
     R u2 = (R)1.5f * ep - (R)0.5f * ep2;  u2 = u2 < (R)0 ? ep : u2;
-    R arrint = cb * (cb > (R)0 ? u1 : u2);
-    R cb2 = (R)0.5f * (cm + c0);
-    R u3 = (R)1.5f * em - (R)0.5f * em2;  u3 = u3 < (R)0 ? em : u3;
-    R u4 = (R)1.5f * e0 - (R)0.5f * ep;   u4 = u4 < (R)0 ? e0 : u4;
-    R arrmint = cb2 * (cb2 > (R)0 ? u3 : u4);
-    return first ? arrint : (last ? -arrmint : arrint - arrmint);
+    return cb * (cb > (R)0 ? u1 : u2);
 }
+
+constexpr int WT_NB = 3;   // plane tile buffers: plane t+1 streams in while t is used
 
 template <class R, bool ROLLER>
 __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
@@ -910,9 +425,9 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
     const int tid = threadIdx.x + threadIdx.y * WT_X;
-    R* tE = (R*)smem_raw;                 // [WT_N] plane tile of ee
-    R* tR = tE + WT_N;                    // [WT_N] plane tile of rr
-    R* sA = tR + WT_N;                    // [nt][256] advected ee (energy units)
+    R* tE = (R*)smem_raw;                 // [WT_NB][WT_N] plane tiles of ee
+    R* tR = tE + WT_NB * WT_N;            // [WT_NB][WT_N] plane tiles of rr
+    R* sA = tR + WT_NB * WT_N;            // [nt][256] advected ee (energy units)
     R* sR = sA + (size_t)nt * 256;        // [nt][256] advected rr
     R* sCos = sR + (size_t)nt * 256;      // [nt]
     R* sSin = sCos + nt;                  // [nt]
@@ -930,7 +445,8 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
     const R dth = K.dtheta;
     const R rdth = (R)1 / dth;
     const R rdx = (R)1 / K.dx;
-    // tile elements of this thread (two at most), offsets into a plane
+    // tile elements of this thread (two at most): plane offsets, clamped as
+    // mm()/pp()/mm2()/pp2() clamp; column 0 is the offshore boundary St*taper
     int eoff0 = -1, eoff1 = -1, ey0 = 0, ey1 = 0;
     bool ez0 = false, ez1 = false;
     {
@@ -944,12 +460,41 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
             eoff1 = gx + gy * nx; ey1 = gy; ez1 = gx == 0;
         }
     }
-    int i = 0, pxm = 0, pxm2 = 0, pxp = 0, pxp2 = 0, pym = 0, pym2 = 0, pyp = 0, pyp2 = 0;
-    R hh = 0, uui = 0, uuixmin = 0, uuixmax = 0, vvi = 0, vviymin = 0, vviymax = 0;
-    Faces<R> fe{}, fr{};
+    // sources of this thread's tile elements in the next plane to issue
+    const R* gE0 = eeo + eoff0; const R* gR0 = rro + eoff0; const R* gS0 = St + ey0;
+    const R* gE1 = eeo + max(eoff1, 0); const R* gR1 = rro + max(eoff1, 0); const R* gS1 = St + ey1;
+    // issue the copies of the next plane into buffer b (boundary column written directly)
+    auto issue = [&](int b) {
+        R* dE = tE + b * WT_N;
+        R* dR = tR + b * WT_N;
+        if (ez0) dE[tid] = DM<R>::fmax(*gS0 * taper, (R)0);
+        else cp_async<sizeof(R)>(dE + tid, gE0);
+        if (ROLLER) cp_async<sizeof(R)>(dR + tid, gR0);
+        if (eoff1 >= 0) {
+            if (ez1) dE[tid + 256] = DM<R>::fmax(*gS1 * taper, (R)0);
+            else cp_async<sizeof(R)>(dE + tid + 256, gE1);
+            if (ROLLER) cp_async<sizeof(R)>(dR + tid + 256, gR1);
+        }
+        cp_async_commit();
+        gE0 += C; gR0 += C; gS0 += ny; gE1 += C; gR1 += C; gS1 += ny;
+    };
+    // sanity (ee = max(ee, 0)) on this thread's copied elements of buffer b
+    auto fixup = [&](int b) {
+        R* dE = tE + b * WT_N;
+        if (!ez0) dE[tid] = DM<R>::fmax(dE[tid], (R)0);
+        if (eoff1 >= 0 && !ez1) dE[tid + 256] = DM<R>::fmax(dE[tid + 256], (R)0);
+    };
+    // the cell's tile slot; the tile is clamped like mm()/pp()/mm2()/pp2(), so
+    // its x/y neighbours are at fixed offsets +-1, +-2, +-WT_TX, +-2*WT_TX
+    const int ctile = (iy - by0 + 2) * WT_TX + (ix - bx0 + 2);
+    int i = 0;
+    R hh = 0, uui = 0, vvi = 0;
+    // face speeds as ct * A + B (x faces) and st * A + B (y faces), for cg (ee) and c (rr)
+    R axp = 0, axm = 0, ayp = 0, aym = 0, rxp = 0, rxm = 0, ryp = 0, rym = 0;
+    R bxp = 0, bxm = 0, byp = 0, bym = 0, cgi = 0, cci = 0;
     CthCoef<R> cc{};
-    R we0 = 0, we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr0 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;
-    R cm = 0, c0 = 0, cpp = 0, Etmp = 0, cabs = 0;
+    R we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;   // bins t-1 .. t+2
+    R c0 = 0, cpp = 0, Etmp = 0, cabs = 0, fte = 0, ftr = 0;
     const bool own_bnd = ix == 0;
     auto own_e = [&](int t) -> R {
         R v = own_bnd ? St[iy + t * ny] * taper : ld(eeo + i + (size_t)t * C);
@@ -957,86 +502,90 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
     };
     const bool edge_row = active && (iy == 1 || iy == ny - 2);
     const int slot = (iy == 1) ? 0 : 1;
-    __syncthreads();
+    issue(0);
+    __syncthreads();   // theta tables
     if (active) {
         i = ix + iy * nx;
-        const int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
-        const int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
-        const int ry = (iy - by0 + 2) * WT_TX, rx = ix - bx0 + 2;
-        pxm2 = ry + (xm2 - bx0 + 2); pxm = ry + (xm - bx0 + 2);
-        pxp = ry + (xp - bx0 + 2); pxp2 = ry + (xp2 - bx0 + 2);
-        pym2 = (ym2 - by0 + 2) * WT_TX + rx; pym = (ym - by0 + 2) * WT_TX + rx;
-        pyp = (yp - by0 + 2) * WT_TX + rx; pyp2 = (yp2 - by0 + 2) * WT_TX + rx;
+        const int xm = mm(ix), xp = pp(ix, nx);
+        const int ym = mm(iy), yp = pp(iy, ny);
         hh = ld(S.f[HH] + i);
         R sg = (R)clk->sigm;
         cc = cth_coef(S, K, ix, iy, sg);
         const R wci = cc.wci;
         const R* cgp = S.f[CG];
         const R* cp = S.f[CC_];
-        fe = Faces<R>{ld(cgp + i), ld(cgp + xm + iy * nx), ld(cgp + xp + iy * nx), ld(cgp + ix + ym * nx), ld(cgp + ix + yp * nx)};
-        fr = Faces<R>{ld(cp + i), ld(cp + xm + iy * nx), ld(cp + xp + iy * nx), ld(cp + ix + ym * nx), ld(cp + ix + yp * nx)};
+        cgi = ld(cgp + i); cci = ld(cp + i);
+        const R h = (R)0.5f;
+        axp = h * (cgi + ld(cgp + xp + iy * nx)); axm = h * (cgi + ld(cgp + xm + iy * nx));
+        ayp = h * (cgi + ld(cgp + ix + yp * nx)); aym = h * (cgi + ld(cgp + ix + ym * nx));
+        rxp = h * (cci + ld(cp + xp + iy * nx)); rxm = h * (cci + ld(cp + xm + iy * nx));
+        ryp = h * (cci + ld(cp + ix + yp * nx)); rym = h * (cci + ld(cp + ix + ym * nx));
         const R* uu = S.f[UU]; const R* vv = S.f[VV];
-        uui = ld(uu + i) * wci; uuixmin = ld(uu + xm + iy * nx) * wci; uuixmax = ld(uu + xp + iy * nx) * wci;
-        vvi = wci * ld(vv + i); vviymin = wci * ld(vv + ix + ym * nx); vviymax = wci * ld(vv + ix + yp * nx);
+        uui = ld(uu + i) * wci; vvi = wci * ld(vv + i);
+        bxp = h * (uui + ld(uu + xp + iy * nx) * wci); bxm = h * (uui + ld(uu + xm + iy * nx) * wci);
+        byp = h * (vvi + wci * ld(vv + ix + yp * nx)); bym = h * (vvi + wci * ld(vv + ix + ym * nx));
         auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
-        we0 = own_e(0); we1 = we0; we2 = we0; we3 = own_e(cl(1)); we4 = own_e(cl(2));
-        wr0 = ld(rro + i); wr1 = wr0; wr2 = wr0;
+        we2 = own_e(0); we1 = we2; we3 = own_e(cl(1)); we4 = own_e(cl(2));
+        wr2 = ld(rro + i); wr1 = wr2;
         wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
         c0 = cth_eval(cc, sCos[0], sSin[0]);
-        cm = c0;
         cpp = cth_eval(cc, sCos[cl(1)], sSin[cl(1)]);
     }
-    const R* pe = eeo;   // plane t of ee / rr
-    const R* pr = rro;
+    // the cell's own bins ahead (window refill): plane min(t+3, nt-1)
+    const R* wE = eeo + i + (size_t)min(3, nt - 1) * C;
+    const R* wR = rro + i + (size_t)min(3, nt - 1) * C;
+    const R* wS = St + iy + min(3, nt - 1) * ny;
+    R* oA = sA + tid;
+    R* oR = sR + tid;
+    R* oEdge = S.edge + ix + (size_t)slot * nt * nx;
+    const size_t edge_rr = (size_t)2 * nt * nx;
 #pragma unroll 1
-    for (int t = 0; t < nt; t++, pe += C, pr += C) {
-        __syncthreads();   // previous plane consumed
-        {
-            R v = ez0 ? St[ey0 + t * ny] * taper : ld(pe + eoff0);
-            tE[tid] = DM<R>::fmax(v, (R)0);
-            if (ROLLER) tR[tid] = ld(pr + eoff0);
-            if (eoff1 >= 0) {
-                R w = ez1 ? St[ey1 + t * ny] * taper : ld(pe + eoff1);
-                tE[tid + 256] = DM<R>::fmax(w, (R)0);
-                if (ROLLER) tR[tid + 256] = ld(pr + eoff1);
-            }
-        }
-        __syncthreads();
+    for (int t = 0; t < nt; t++) {
+        const int b = t % WT_NB;
+        if (t + 1 < nt) issue((t + 1) % WT_NB);
+        else cp_async_commit();
+        cp_async_wait1();   // plane t has landed (this thread's copies)
+        fixup(b);
+        __syncthreads();    // ... and every thread's; buffer (t+1)%3 was last read two planes ago
         if (active) {
+            const R* qE = tE + b * WT_N + ctile;
+            const R* qR = tR + b * WT_N + ctile;
             const R ct = sCos[t], st = sSin[t];
-            const bool first = t == 0, last = t == nt - 1, multi = nt > 1;
+            const bool last = t == nt - 1;
             cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
-            R cgx = (R)0.5f * (fe.sp * ct + uui + fe.sxp * ct + uuixmax);
-            R cgxmin = (R)0.5f * (fe.sp * ct + uui + fe.sxm * ct + uuixmin);
-            R cgy = (R)0.5f * (fe.sp * st + vvi + fe.syp * st + vviymax);
-            R cgymin = (R)0.5f * (fe.sp * st + vvi + fe.sym * st + vviymin);
-            R fx = flux2(tE[pxm2], tE[pxm], we2, tE[pxp], tE[pxp2], cgx, cgxmin);
-            R fy = flux2(tE[pym2], tE[pym], we2, tE[pyp], tE[pyp2], cgy, cgymin);
-            R ft = multi ? flux_theta(we0, we1, we2, we3, we4, cm, c0, cpp, first, last) : (R)0;
+            R fx = flux2(qE[-2], qE[-1], we2, qE[1], qE[2], DM<R>::fma(ct, axp, bxp), DM<R>::fma(ct, axm, bxm));
+            R fy = flux2(qE[-2 * WT_TX], qE[-WT_TX], we2, qE[WT_TX], qE[2 * WT_TX], DM<R>::fma(st, ayp, byp),
+                         DM<R>::fma(st, aym, bym));
+            // theta flux: upper face computed here, lower face carried from bin t-1
+            R fup = last ? (R)0 : theta_face(we1, we2, we3, we4, c0, cpp);
+            R ft = fup - fte;
+            fte = fup;
             R A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
             R Ar = wr2;
             if (ROLLER) {
-                R cx = (R)0.5f * (fr.sp * ct + uui + fr.sxp * ct + uuixmax);
-                R cxm = (R)0.5f * (fr.sp * ct + uui + fr.sxm * ct + uuixmin);
-                R cy = (R)0.5f * (fr.sp * st + vvi + fr.syp * st + vviymax);
-                R cym = (R)0.5f * (fr.sp * st + vvi + fr.sym * st + vviymin);
-                R rx = flux2(tR[pxm2], tR[pxm], wr2, tR[pxp], tR[pxp2], cx, cxm);
-                R ry = flux2(tR[pym2], tR[pym], wr2, tR[pyp], tR[pyp2], cy, cym);
-                R rt = multi ? flux_theta(wr0, wr1, wr2, wr3, wr4, cm, c0, cpp, first, last) : (R)0;
+                R rx = flux2(qR[-2], qR[-1], wr2, qR[1], qR[2], DM<R>::fma(ct, rxp, bxp), DM<R>::fma(ct, rxm, bxm));
+                R ry = flux2(qR[-2 * WT_TX], qR[-WT_TX], wr2, qR[WT_TX], qR[2 * WT_TX], DM<R>::fma(st, ryp, byp),
+                             DM<R>::fma(st, rym, bym));
+                R rup = last ? (R)0 : theta_face(wr1, wr2, wr3, wr4, c0, cpp);
+                R rt = rup - ftr;
+                ftr = rup;
                 Ar = wr2 - dtf * ((rx + ry) * rdx + rt * rdth);
             }
-            sA[t * 256 + tid] = A;
-            sR[t * 256 + tid] = Ar;
+            *oA = A;
+            *oR = Ar;
+            oA += 256; oR += 256;
             if (edge_row) {
-                S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] = A;
-                S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] = Ar;
+                oEdge[0] = A;
+                oEdge[edge_rr] = Ar;
             }
+            oEdge += nx;
             Etmp = Etmp + DM<R>::fmax(A, (R)0);
-            const int tn = t + 3 < nt ? t + 3 : nt - 1;
             const int t2 = t + 2 < nt ? t + 2 : nt - 1;
-            we0 = we1; we1 = we2; we2 = we3; we3 = we4; we4 = own_e(tn);
-            wr0 = wr1; wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(rro + i + (size_t)tn * C);
-            cm = c0; c0 = cpp; cpp = cth_eval(cc, sCos[t2], sSin[t2]);
+            we1 = we2; we2 = we3; we3 = we4;
+            we4 = DM<R>::fmax(own_bnd ? *wS * taper : ld(wE), (R)0);
+            wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(wR);
+            if (t + 4 <= nt - 1) { wE += C; wR += C; wS += ny; }
+            c0 = cpp; cpp = cth_eval(cc, sCos[t2], sSin[t2]);
         }
     }
     R dtw = (R)3.0e38f;
@@ -1076,7 +625,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
             Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
         }
         // dissipationCPU, meandir, radstress
-        const R cc_i = fr.sp;
+        const R cc_i = cci;
         const R Dq = Dv / DM<R>::fmax(Eint, (R)0.0000001f);
         const R twogb = (R)2.0f * g * K.beta;
         const bool wet = hh > K.eps;
@@ -1116,7 +665,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
         S.f[D][i] = Dv;
         S.f[ROL][i] = RR * dth;
         S.f[DR][i] = drr * dth;
-        const R n = fe.sp / cc_i;
+        const R n = cgi / cc_i;
         S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
         S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
         S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
@@ -1248,7 +797,7 @@ int wave_parts(const Konst<R>& K) {
 template <class R, int NMAX>
 void launch_wave_main(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
-    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
+    size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
     if (K.roller == 1) k_wave_fast<R, true><<<g, b, smem, st>>>(S, K);
     else k_wave_fast<R, false><<<g, b, smem, st>>>(S, K);
     PMARK(pf, "k_wave_main");
@@ -1280,7 +829,7 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
 // theta sets in FP64).
 template <class R>
 int wave_prepare(const Konst<R>& K) {
-    size_t smem = ((size_t)2 * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
+    size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
     cudaError_t e = cudaFuncSetAttribute(k_wave_fast<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaError_t e2 = cudaFuncSetAttribute(k_wave_fast<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     return (e == cudaSuccess && e2 == cudaSuccess) ? 0 : 1;
