@@ -246,113 +246,113 @@ __global__ void __launch_bounds__(256) k_flow_v(Dev<R> S, Konst<R> K) {
     S.tmp[T_VV][IDX(ix, iy)] = v;
 }
 
-// wrkuu2Ocorr (Flow_kernel.cu:1960-2044) at cell (ix, iy)
-template <class R>
-__device__ __forceinline__ void wrk_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
-    const int nx = K.nx, ny = K.ny;
-    const R* zs = S.f[ZS]; const R* zb = S.f[ZB]; const R* uu = S.tmp[T_UU]; const R* uo = S.f[UUOLD];
-    const R* qx = S.f[QX]; const R* qy = S.f[QY];
-    int i = IDX(ix, iy);
-    int xm = mm(ix), xm2 = mm2(ix), xp = pp(ix, nx), xp2 = pp2(ix, nx);
-    int ym = mm(iy), yp = pp(iy, ny), yp2 = pp2(iy, ny);
-    R eps2 = K.eps * (R)2.0f;
+// Fields of the momentum-correction pass, in its shared-memory tile.
+enum { C_ZS, C_ZB, C_UU, C_VV, C_UO, C_VO, C_QX, C_QY, C_NF };
+
+// wrkuu2Ocorr (Flow_kernel.cu:1960-2044) at cell (ix, iy); a: field access
+// around the cell (uu is the post-Euler uu*, uo the previous step's).
+template <class R, class A>
+__device__ __forceinline__ void wrk_u(const A& a, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
+    const R eps2 = K.eps * (R)2.0f;
     w1 = (R)0.0f; w2 = (R)0.0f;
     if (ix > 0) {
-        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm2, iy)), ld(zs + IDX(xm, iy))), ld(zs + i)), ld(zs + IDX(xp, iy))), ld(zs + IDX(xp2, iy)));
-        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm2, iy)), ld(zb + IDX(xm, iy))), ld(zb + i)), ld(zb + IDX(xp, iy))), ld(zb + IDX(xp2, iy)));
+        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, -2, 0), a(C_ZS, -1, 0)), a(C_ZS, 0, 0)), a(C_ZS, 1, 0)), a(C_ZS, 2, 0));
+        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, -2, 0), a(C_ZB, -1, 0)), a(C_ZB, 0, 0)), a(C_ZB, 1, 0)), a(C_ZB, 2, 0));
         if (minzs + minzb > eps2) {
-            R qs = ld(qx + i) + ld(qx + IDX(xm, iy));
-            if (qs > (R)0.0f) w1 = (R)0.5f * minmod(ld(uu + i) - ld(uo + IDX(xm, iy)), ld(uu + IDX(xm, iy)) - ld(uo + IDX(xm2, iy)));
-            if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(ld(uo + i) - ld(uu + IDX(xm, iy)), ld(uo + IDX(xp, iy)) - ld(uu + i));
+            R qs = a(C_QX, 0, 0) + a(C_QX, -1, 0);
+            if (qs > (R)0.0f) w1 = (R)0.5f * minmod(a(C_UU, 0, 0) - a(C_UO, -1, 0), a(C_UU, -1, 0) - a(C_UO, -2, 0));
+            if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(a(C_UO, 0, 0) - a(C_UU, -1, 0), a(C_UO, 1, 0) - a(C_UU, 0, 0));
         }
         if (iy > 0) {
-            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(ix, iy)), ld(zs + IDX(ix, ym))), ld(zs + IDX(ix, yp))), ld(zs + IDX(ix, yp2)));
-            mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xp, iy)), ld(zs + IDX(xp, ym))), ld(zs + IDX(xp, yp))), ld(zs + IDX(xp, yp2))));
-            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(ix, iy)), ld(zb + IDX(ix, ym))), ld(zb + IDX(ix, yp))), ld(zb + IDX(ix, yp2)));
-            mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xp, iy)), ld(zb + IDX(xp, ym))), ld(zb + IDX(xp, yp))), ld(zb + IDX(xp, yp2))));
+            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, 0, 0), a(C_ZS, 0, -1)), a(C_ZS, 0, 1)), a(C_ZS, 0, 2));
+            mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, 1, 0), a(C_ZS, 1, -1)), a(C_ZS, 1, 1)), a(C_ZS, 1, 2)));
+            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, 0, 0), a(C_ZB, 0, -1)), a(C_ZB, 0, 1)), a(C_ZB, 0, 2));
+            mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, 1, 0), a(C_ZB, 1, -1)), a(C_ZB, 1, 1)), a(C_ZB, 1, 2)));
             if (mzs + mzb > eps2) {
-                R qs = ld(qy + IDX(xp, iy)) + ld(qy + i);
-                if (qs > (R)0.0f) w2 = (R)0.5f * minmod(ld(uu + IDX(ix, yp)) - ld(uo + i), ld(uu + i) - ld(uo + IDX(ix, ym)));
-                if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(ld(uo + IDX(ix, yp)) - ld(uu + i), ld(uo + IDX(ix, yp2)) - ld(uu + IDX(ix, yp)));
+                R qs = a(C_QY, 1, 0) + a(C_QY, 0, 0);
+                if (qs > (R)0.0f) w2 = (R)0.5f * minmod(a(C_UU, 0, 1) - a(C_UO, 0, 0), a(C_UU, 0, 0) - a(C_UO, 0, -1));
+                if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(a(C_UO, 0, 1) - a(C_UU, 0, 0), a(C_UO, 0, 2) - a(C_UU, 0, 1));
             }
         }
     }
 }
 
 // wrkvv2Ocorr (Flow_kernel.cu:2046-2128) at cell (ix, iy)
-template <class R>
-__device__ __forceinline__ void wrk_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
-    const int nx = K.nx, ny = K.ny;
-    const R* zs = S.f[ZS]; const R* zb = S.f[ZB]; const R* vv = S.tmp[T_VV]; const R* vo = S.f[VVOLD];
-    const R* qx = S.f[QX]; const R* qy = S.f[QY];
-    int i = IDX(ix, iy);
-    int xm = mm(ix), xp = pp(ix, nx), xp2 = pp2(ix, nx);
-    int ym = mm(iy), ym2 = mm2(iy), yp = pp(iy, ny), yp2 = pp2(iy, ny);
-    R eps2 = K.eps * (R)2.0f;
+template <class R, class A>
+__device__ __forceinline__ void wrk_v(const A& a, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
+    const R eps2 = K.eps * (R)2.0f;
     w1 = (R)0.0f; w2 = (R)0.0f;
-    if (ix > 0 && iy > 0 && iy < ny - 2) {
-        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(ix, ym2)), ld(zs + IDX(ix, ym))), ld(zs + IDX(ix, iy))), ld(zs + IDX(ix, yp))), ld(zs + IDX(ix, yp2)));
-        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(ix, ym2)), ld(zb + IDX(ix, ym))), ld(zb + IDX(ix, iy))), ld(zb + IDX(ix, yp))), ld(zb + IDX(ix, yp2)));
+    if (ix > 0 && iy > 0 && iy < K.ny - 2) {
+        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, 0, -2), a(C_ZS, 0, -1)), a(C_ZS, 0, 0)), a(C_ZS, 0, 1)), a(C_ZS, 0, 2));
+        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, 0, -2), a(C_ZB, 0, -1)), a(C_ZB, 0, 0)), a(C_ZB, 0, 1)), a(C_ZB, 0, 2));
         if (minzs + minzb > eps2) {
-            R qs = ld(qy + i) + ld(qy + IDX(ix, ym));
-            if (qs > (R)0.0f) w1 = (R)0.5f * minmod(ld(vv + i) - ld(vo + IDX(ix, ym)), ld(vv + IDX(ix, ym)) - ld(vo + IDX(ix, ym2)));
-            if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(ld(vo + i) - ld(vv + IDX(ix, ym)), ld(vo + IDX(ix, yp)) - ld(vv + i));
+            R qs = a(C_QY, 0, 0) + a(C_QY, 0, -1);
+            if (qs > (R)0.0f) w1 = (R)0.5f * minmod(a(C_VV, 0, 0) - a(C_VO, 0, -1), a(C_VV, 0, -1) - a(C_VO, 0, -2));
+            if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(a(C_VO, 0, 0) - a(C_VV, 0, -1), a(C_VO, 0, 1) - a(C_VV, 0, 0));
         }
-        R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm, iy)), ld(zs + IDX(ix, iy))), ld(zs + IDX(xp, iy))), ld(zs + IDX(xp2, iy)));
-        mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm, yp)), ld(zs + IDX(ix, yp))), ld(zs + IDX(xp, yp))), ld(zs + IDX(xp2, yp))));
-        R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm, iy)), ld(zb + IDX(ix, iy))), ld(zb + IDX(xp, iy))), ld(zb + IDX(xp2, iy)));
-        mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm, yp)), ld(zb + IDX(ix, yp))), ld(zb + IDX(xp, yp))), ld(zb + IDX(xp2, yp))));
+        R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, -1, 0), a(C_ZS, 0, 0)), a(C_ZS, 1, 0)), a(C_ZS, 2, 0));
+        mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, -1, 1), a(C_ZS, 0, 1)), a(C_ZS, 1, 1)), a(C_ZS, 2, 1)));
+        R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, -1, 0), a(C_ZB, 0, 0)), a(C_ZB, 1, 0)), a(C_ZB, 2, 0));
+        mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, -1, 1), a(C_ZB, 0, 1)), a(C_ZB, 1, 1)), a(C_ZB, 2, 1)));
         if (mzs + mzb > eps2) {
-            R qs = ld(qx + IDX(ix, yp)) + ld(qx + i);
-            if (qs > (R)0.0f) w2 = (R)0.5f * minmod(ld(vv + IDX(xp, iy)) - ld(vo + i), ld(vv + i) - ld(vo + IDX(xm, iy)));
-            if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(ld(vo + IDX(xp, iy)) - ld(vv + i), ld(vo + IDX(xp2, iy)) - ld(vv + IDX(xp, iy)));
+            R qs = a(C_QX, 0, 1) + a(C_QX, 0, 0);
+            if (qs > (R)0.0f) w2 = (R)0.5f * minmod(a(C_VV, 1, 0) - a(C_VO, 0, 0), a(C_VV, 0, 0) - a(C_VO, -1, 0));
+            if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(a(C_VO, 1, 0) - a(C_VV, 0, 0), a(C_VO, 2, 0) - a(C_VV, 1, 0));
         }
     }
 }
 
-// Block tile for the passes that need per-cell intermediates of neighbours:
-// 32 x 8 cells plus one cell on every side, clamped at the grid edge exactly
-// as mm()/pp() clamp, so a neighbour read from the tile is the value the
-// reference reads.
+// uu2Ocorr + vv2Ocorr (Flow_kernel.cu:2210-2282).  The eight input fields of
+// the block's tile (halo 3) stream into shared memory first; the wrk values of
+// the tile cells and a one-cell ring (the left, right, lower and upper
+// neighbours the corrections read) are computed once from there.
 constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT_TX * FT_TY;
+constexpr int FC_H = 3;
 
 template <class R>
 __global__ void __launch_bounds__(256) k_flow_corr(Dev<R> S, Konst<R> K) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
+    using G = TileG<FC_H>;
+    __shared__ R tile[C_NF * G::N];
     __shared__ R sU1[FT_N], sU2[FT_N], sV1[FT_N], sV2[FT_N];
     const int nx = K.nx, ny = K.ny;
     const int bx0 = blockIdx.x * FT_X, by0 = blockIdx.y * FT_Y;
+    {
+        const R* src[C_NF] = {S.f[ZS], S.f[ZB], S.tmp[T_UU], S.tmp[T_VV], S.f[UUOLD], S.f[VVOLD], S.f[QX], S.f[QY]};
+        tile_load<R, FC_H, C_NF>(tile, src, bx0, by0, nx, ny);
+    }
     for (int e = threadIdx.x + threadIdx.y * FT_X; e < FT_N; e += FT_X * FT_Y) {
-        int gx = min(max(bx0 - 1 + e % FT_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / FT_TX, 0), ny - 1);
-        R a, b, c, d;
-        wrk_u(S, K, gx, gy, a, b);
-        wrk_v(S, K, gx, gy, c, d);
-        sU1[e] = a; sU2[e] = b; sV1[e] = c; sV2[e] = d;
+        int gx, gy;
+        int k = tile_centre<FC_H>(e % FT_TX + FC_H - 1, e / FT_TX + FC_H - 1, bx0, by0, nx, ny, gx, gy);
+        TileAt<R, FC_H> a{tile, k};
+        R w1, w2, v1, v2;
+        wrk_u(a, K, gx, gy, w1, w2);
+        wrk_v(a, K, gx, gy, v1, v2);
+        sU1[e] = w1; sU2[e] = w2; sV1[e] = v1; sV2[e] = v2;
     }
     __syncthreads();
     int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R dtf = (R)clk->dt, dx = K.dx;
-    const R* qx = S.f[QX]; const R* qy = S.f[QY];
-    R u = ld(S.tmp[T_UU] + i), v = ld(S.tmp[T_VV] + i);
+    TileAt<R, FC_H> a{tile, (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H};
+    R u = a(C_UU, 0, 0), v = a(C_VV, 0, 0);
     if (ix > 0 && iy > 0) {
-        int xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
         const int c = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
-        // uu2Ocorr (Flow_kernel.cu:2210-2245): wrk at i, xp and ym
+        // uu2Ocorr: wrk at i, xp and ym
         R w1i = sU1[c], w2i = sU2[c], w1r = sU1[c + 1], w2b = sU2[c - FT_TX];
-        R qe = (R)0.5f * (ld(qx + IDX(xp, iy)) + ld(qx + i));
-        R qw = (R)0.5f * (ld(qx + i) + ld(qx + IDX(xm, iy)));
-        R qn = (R)0.5f * (ld(qy + IDX(ix, ym)) + ld(qy + IDX(xp, ym)));
-        R qs = (R)0.5f * (ld(qy + i) + ld(qy + IDX(xm, iy)));
+        R qe = (R)0.5f * (a(C_QX, 1, 0) + a(C_QX, 0, 0));
+        R qw = (R)0.5f * (a(C_QX, 0, 0) + a(C_QX, -1, 0));
+        R qn = (R)0.5f * (a(C_QY, 0, -1) + a(C_QY, 1, -1));
+        R qs = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, -1, 0));
         u = u - dtf / ld(S.f[HUM] + i) * ((qe * w1r - qw * w1i) / dx + (qs * w2i - qn * w2b) / dx);
-        // vv2Ocorr (Flow_kernel.cu:2247-2282): wrk at i, xm and yp
+        // vv2Ocorr: wrk at i, xm and yp
         R v1i = sV1[c], v2i = sV2[c], v2l = sV2[c - 1], v1t = sV1[c + FT_TX];
-        qe = (R)0.5f * (ld(qx + IDX(ix, yp)) + ld(qx + i));
-        qw = (R)0.5f * (ld(qx + IDX(xm, iy)) + ld(qx + IDX(xm, yp)));
-        qn = (R)0.5f * (ld(qy + i) + ld(qy + IDX(ix, ym)));
-        qs = (R)0.5f * (ld(qy + IDX(ix, yp)) + ld(qy + i));
+        qe = (R)0.5f * (a(C_QX, 0, 1) + a(C_QX, 0, 0));
+        qw = (R)0.5f * (a(C_QX, -1, 0) + a(C_QX, -1, 1));
+        qn = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, 0, -1));
+        qs = (R)0.5f * (a(C_QY, 0, 1) + a(C_QY, 0, 0));
         v = v - dtf / ld(S.f[HVM] + i) * ((qe * v2i - qw * v2l) / dx + (qs * v1t - qn * v1i) / dx);
     }
     S.f[UU][i] = u;
@@ -412,107 +412,103 @@ __global__ void __launch_bounds__(256) k_flow_cont(Dev<R> S, Konst<R> K) {
     S.tmp[T_ZS][i] = zs;
 }
 
-// wrkzs2Ocorr (Flow_kernel.cu:2130-2208) at cell (ix, iy); zs is the
-// post-continuity level, zsold the previous step's.
-template <class R>
-__device__ __forceinline__ void wrk_z(const Dev<R>& S, const Konst<R>& K, const R* zso, int ix, int iy, R& w1, R& w2) {
-    const int nx = K.nx, ny = K.ny;
-    const R* zs = S.tmp[T_ZS]; const R* zb = S.f[ZB];
-    int i = IDX(ix, iy);
-    int xm = mm(ix), xp = pp(ix, nx), xp2 = pp2(ix, nx), ym = mm(iy), yp = pp(iy, ny), yp2 = pp2(iy, ny);
-    R eps2 = K.eps * (R)2.0f;
+// Fields of the final pass, in its shared-memory tile: the post-continuity
+// level, bed, previous step's level, corrected velocities, Stokes drift inputs.
+enum { Z_ZS, Z_ZB, Z_ZO, Z_UU, Z_VV, Z_UST, Z_THM, Z_NF };
+
+// wrkzs2Ocorr (Flow_kernel.cu:2130-2208) at cell (ix, iy)
+template <class R, class A>
+__device__ __forceinline__ void wrk_z(const A& a, const Konst<R>& K, int ix, int iy, R& w1, R& w2) {
+    const R eps2 = K.eps * (R)2.0f;
     w1 = (R)0.0f; w2 = (R)0.0f;
     if (ix > 0) {
-        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(xm, iy)), ld(zs + i)), ld(zs + IDX(xp, iy))), ld(zs + IDX(xp2, iy)));
-        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(xm, iy)), ld(zb + i)), ld(zb + IDX(xp, iy))), ld(zb + IDX(xp2, iy)));
+        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZS, -1, 0), a(Z_ZS, 0, 0)), a(Z_ZS, 1, 0)), a(Z_ZS, 2, 0));
+        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZB, -1, 0), a(Z_ZB, 0, 0)), a(Z_ZB, 1, 0)), a(Z_ZB, 2, 0));
         if (minzs + minzb > eps2) {
-            R u = ld(S.f[UU] + i);
-            if (u > (R)0.0f) w1 = u * (R)0.5f * minmod(ld(zs + IDX(xp, iy)) - ld(zso + i), ld(zs + i) - ld(zso + IDX(xm, iy)));
-            if (u < (R)0.0f) w1 = (R)-1.0f * u * (R)0.5f * minmod(ld(zso + IDX(xp2, iy)) - ld(zs + IDX(xp, iy)), ld(zso + IDX(xp, iy)) - ld(zs + i));
+            R u = a(Z_UU, 0, 0);
+            if (u > (R)0.0f) w1 = u * (R)0.5f * minmod(a(Z_ZS, 1, 0) - a(Z_ZO, 0, 0), a(Z_ZS, 0, 0) - a(Z_ZO, -1, 0));
+            if (u < (R)0.0f) w1 = (R)-1.0f * u * (R)0.5f * minmod(a(Z_ZO, 2, 0) - a(Z_ZS, 1, 0), a(Z_ZO, 1, 0) - a(Z_ZS, 0, 0));
         }
         if (iy > 0) {
-            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zs + IDX(ix, ym)), ld(zs + i)), ld(zs + IDX(ix, yp))), ld(zs + IDX(ix, yp2)));
-            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(ld(zb + IDX(ix, ym)), ld(zb + i)), ld(zb + IDX(ix, yp))), ld(zb + IDX(ix, yp2)));
+            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZS, 0, -1), a(Z_ZS, 0, 0)), a(Z_ZS, 0, 1)), a(Z_ZS, 0, 2));
+            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZB, 0, -1), a(Z_ZB, 0, 0)), a(Z_ZB, 0, 1)), a(Z_ZB, 0, 2));
             if (mzs + mzb > eps2) {
-                R v = ld(S.f[VV] + i);
-                if (v > (R)0.0f) w2 = v * (R)0.5f * minmod(ld(zs + IDX(ix, yp)) - ld(zso + i), ld(zs + i) - ld(zso + IDX(ix, ym)));
-                if (v < (R)0.0f) w2 = v * (R)0.5f * minmod(ld(zso + IDX(ix, yp2)) - ld(zs + IDX(ix, yp)), ld(zso + IDX(ix, yp)) - ld(zs + i));
+                R v = a(Z_VV, 0, 0);
+                if (v > (R)0.0f) w2 = v * (R)0.5f * minmod(a(Z_ZS, 0, 1) - a(Z_ZO, 0, 0), a(Z_ZS, 0, 0) - a(Z_ZO, 0, -1));
+                if (v < (R)0.0f) w2 = v * (R)0.5f * minmod(a(Z_ZO, 0, 2) - a(Z_ZS, 0, 1), a(Z_ZO, 0, 1) - a(Z_ZS, 0, 0));
             }
         }
     }
 }
 
-// zs after zs2Ocorr (Flow_kernel.cu:2284-2317) at (ix, iy); w1, w2: its wrk.
+// zs after zs2Ocorr (Flow_kernel.cu:2284-2317) at (ix, iy), every wrk
+// evaluated from global memory (the one lateral cell the tile cannot serve).
 template <class R>
-__device__ __forceinline__ R zs_corr(const Dev<R>& S, const Konst<R>& K, const R* zso, int ix, int iy, R dtf, R& w1, R& w2) {
-    const int nx = K.nx;
-    wrk_z(S, K, zso, ix, iy, w1, w2);
-    R z = ld(S.tmp[T_ZS] + IDX(ix, iy));
+__device__ R zs_corr_global(const Dev<R>& S, const Konst<R>& K, const R* zso, int ix, int iy, R dtf) {
+    auto at = [&](int x, int y) {
+        return GlobalAt<R, Z_NF>{{S.tmp[T_ZS], S.f[ZB], zso, S.f[UU], S.f[VV], S.f[UST], S.f[THM]}, x, y, K.nx, K.ny};
+    };
+    R w1, w2, w1l, w2b, t0, t1;
+    wrk_z(at(ix, iy), K, ix, iy, w1, w2);
+    R z = ld(S.tmp[T_ZS] + ix + iy * K.nx);
     if (ix > 0 && iy > 0) {
-        R w1l, t0, t1, w2b;
-        wrk_z(S, K, zso, mm(ix), iy, w1l, t0);
-        wrk_z(S, K, zso, ix, mm(iy), t1, w2b);
+        wrk_z(at(ix - 1, iy), K, ix - 1, iy, w1l, t0);
+        wrk_z(at(ix, iy - 1), K, ix, iy - 1, t1, w2b);
         z = z - dtf * ((w1 - w1l) / K.dx + (w2 - w2b) / K.dx);
     }
     return z;
 }
 
-// calcuvvu (Flow_kernel.cu:467-544) at (ix, iy); sS/sC hold ust*sin(thetamean)
-// and ust*cos(thetamean) of the tile, k is the tile index of (ix, iy), whose
-// right and top neighbours are k + 1 and k + FT_TX.
-template <class R>
-__device__ __forceinline__ void uvvu_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, const R* sS,
-                                          const R* sC, int k, R* o6) {
-    const int nx = K.nx, ny = K.ny;
-    const R* uu = S.f[UU]; const R* vv = S.f[VV];
-    int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-    R wu = (R)ld(S.wetu + i), wv = (R)ld(S.wetv + i);
-    R vu = (R)0.25f * (ld(vv + IDX(ix, ym)) + ld(vv + i) + ld(vv + IDX(xp, ym)) + ld(vv + IDX(xp, iy))) * wu;
-    R uv = (R)0.25f * (ld(uu + IDX(xm, iy)) + ld(uu + i) + ld(uu + IDX(xm, yp)) + ld(uu + IDX(ix, yp))) * wv;
+// calcuvvu (Flow_kernel.cu:467-544) at (ix, iy); a: the final-pass tile around
+// the cell; sS/sC hold ust*sin(thetamean) and ust*cos(thetamean) of the ring
+// tile, k is the ring index of (ix, iy), whose right and top neighbours are
+// k + 1 and k + FT_TX.
+template <class R, class A>
+__device__ __forceinline__ void uvvu_cell(const A& a, R wu, R wv, const R* sS, const R* sC, int k, R* o6) {
+    R vu = (R)0.25f * (a(Z_VV, 0, -1) + a(Z_VV, 0, 0) + a(Z_VV, 1, -1) + a(Z_VV, 1, 0)) * wu;
+    R uv = (R)0.25f * (a(Z_UU, -1, 0) + a(Z_UU, 0, 0) + a(Z_UU, -1, 1) + a(Z_UU, 0, 1)) * wv;
     R vsu = (R)0.5f * (sS[k] + sS[k + 1]) * wu;
     R usu = (R)0.5f * (sC[k] + sC[k + 1]) * wu;
-    R ue = ld(uu + i) - usu;
+    R ue = a(Z_UU, 0, 0) - usu;
     R ve = vu - vsu;
     R usv = (R)0.5f * (sC[k] + sC[k + FT_TX]) * wv;
     R vsv = (R)0.5f * (sS[k] + sS[k + FT_TX]) * wv;
-    R vvv = ld(vv + i) - vsv;
+    R vvv = a(Z_VV, 0, 0) - vsv;
     R uvv = uv - usv;
     o6[0] = vu; o6[1] = uv; o6[2] = ue; o6[3] = vvv;
     o6[4] = DM<R>::sqrt(ue * ue + ve * ve);
     o6[5] = DM<R>::sqrt(uvv * uvv + vvv * vvv);
 }
 
-// zs after zs2Ocorr at the cell of tile index k (grid (ix, iy)) from the
-// tile's wrkzs2Ocorr values.
-template <class R>
-__device__ __forceinline__ R zs_corr_tile(const Dev<R>& S, const Konst<R>& K, const R* sW1, const R* sW2, int k,
-                                          int ix, int iy, R dtf) {
-    R z = ld(S.tmp[T_ZS] + ix + iy * K.nx);
-    if (ix > 0 && iy > 0) z = z - dtf * ((sW1[k] - sW1[k - 1]) / K.dx + (sW2[k] - sW2[k - FT_TX]) / K.dx);
-    return z;
-}
-
-// wrkzs2Ocorr + zs2Ocorr, latbnd(zs), hsbnd, calcuvvu + uvlatbnd.  The tile
-// holds wrkzs2Ocorr and the Stokes-drift products of every tile cell; the
-// lateral row ny-1 takes zs of row ny-2 (latbnd), whose lower neighbour is
-// outside the tile when ny-1 is the block's first row: that one case
-// evaluates zs_corr directly.
+// wrkzs2Ocorr + zs2Ocorr, latbnd(zs), hsbnd, calcuvvu + uvlatbnd.  The seven
+// input fields of the block's tile (halo 3) stream into shared memory; the
+// wrk values and Stokes-drift products of the tile cells and a one-cell ring
+// are computed once from there.  The lateral row ny-1 takes zs of row ny-2
+// (latbnd), whose lower neighbour is outside the ring when ny-1 is the block's
+// first row: that one case evaluates zs from global memory.
 template <class R>
 __global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
+    using G = TileG<FC_H>;
+    __shared__ R tile[Z_NF * G::N];
     __shared__ R sW1[FT_N], sW2[FT_N], sS[FT_N], sC[FT_N];
     const R* zsold_in = S.zsold[clk->par ^ 1];
     R* zsold_out = S.zsold[clk->par];
     const int nx = K.nx, ny = K.ny;
     const int bx0 = blockIdx.x * FT_X, by0 = blockIdx.y * FT_Y;
+    {
+        const R* src[Z_NF] = {S.tmp[T_ZS], S.f[ZB], zsold_in, S.f[UU], S.f[VV], S.f[UST], S.f[THM]};
+        tile_load<R, FC_H, Z_NF>(tile, src, bx0, by0, nx, ny);
+    }
     for (int e = threadIdx.x + threadIdx.y * FT_X; e < FT_N; e += FT_X * FT_Y) {
-        int gx = min(max(bx0 - 1 + e % FT_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / FT_TX, 0), ny - 1);
-        int g = IDX(gx, gy);
-        R a, b;
-        wrk_z(S, K, zsold_in, gx, gy, a, b);
-        R us = ld(S.f[UST] + g), tm = ld(S.f[THM] + g);
-        sW1[e] = a; sW2[e] = b;
+        int gx, gy;
+        int k = tile_centre<FC_H>(e % FT_TX + FC_H - 1, e / FT_TX + FC_H - 1, bx0, by0, nx, ny, gx, gy);
+        TileAt<R, FC_H> a{tile, k};
+        R w1, w2;
+        wrk_z(a, K, gx, gy, w1, w2);
+        R us = a(Z_UST, 0, 0), tm = a(Z_THM, 0, 0);
+        sW1[e] = w1; sW2[e] = w2;
         sS[e] = us * DM<R>::sin(tm);
         sC[e] = us * DM<R>::cos(tm);
     }
@@ -525,27 +521,33 @@ __global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
     if (iy == 0) sy = 1;
     if (iy == ny - 1) sy = ny - 2;
     const int k = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
-    const int ks = k + (sy - iy) * FT_TX;   // tile index of (ix, sy)
-    R zf = zs_corr_tile(S, K, sW1, sW2, k, ix, iy, dtf);
-    if (ix > 0 && iy > 0) {   // zs2Ocorr flux update
-        S.f[QX][i] = ld(S.f[QX] + i) + sW1[k];
-        S.f[QY][i] = ld(S.f[QY] + i) + sW2[k];
-    }
+    const int ks = k + (sy - iy) * FT_TX;   // ring index of (ix, sy)
+    const int kc = (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H;
+    TileAt<R, FC_H> a{tile, kc};                          // around (ix, iy)
+    TileAt<R, FC_H> as{tile, kc + (sy - iy) * G::TX};     // around (ix, sy)
+    auto zcorr = [&](const TileAt<R, FC_H>& c, int r, int y) {
+        R z = c(Z_ZS, 0, 0);
+        if (ix > 0 && y > 0) z = z - dtf * ((sW1[r] - sW1[r - 1]) / K.dx + (sW2[r] - sW2[r - FT_TX]) / K.dx);
+        return z;
+    };
+    R zf = zcorr(a, k, iy);
+    R qx = ld(S.f[QX] + i), qy = ld(S.f[QY] + i);
+    R wu = (R)ld(S.wetu + IDX(ix, sy)), wv = (R)ld(S.wetv + IDX(ix, sy));
     if (sy != iy) {           // latbnd(zs)
-        if (ks >= FT_TX) {
-            zf = zs_corr_tile(S, K, sW1, sW2, ks, ix, sy, dtf);
-        } else {
-            R a, b;
-            zf = zs_corr(S, K, zsold_in, ix, sy, dtf, a, b);
-        }
+        if (ks >= FT_TX) zf = zcorr(as, ks, sy);
+        else zf = zs_corr_global(S, K, zsold_in, ix, sy, dtf);
+    }
+    R o6[6];
+    uvvu_cell(as, wu, wv, sS, sC, ks, o6);   // calcuvvu + uvlatbnd
+    if (ix > 0 && iy > 0) {   // zs2Ocorr flux update
+        S.f[QX][i] = qx + sW1[k];
+        S.f[QY][i] = qy + sW2[k];
     }
     S.f[ZS][i] = zf;
-    S.f[HH][i] = DM<R>::fmax(ld(S.f[ZB] + i) + zf, K.eps);   // hsbnd
-    S.f[UUOLD][i] = ld(S.f[UU] + i);
-    S.f[VVOLD][i] = ld(S.f[VV] + i);
+    S.f[HH][i] = DM<R>::fmax(a(Z_ZB, 0, 0) + zf, K.eps);   // hsbnd
+    S.f[UUOLD][i] = a(Z_UU, 0, 0);
+    S.f[VVOLD][i] = a(Z_VV, 0, 0);
     zsold_out[i] = zf;
-    R o6[6];
-    uvvu_cell(S, K, ix, sy, sS, sC, ks, o6);   // calcuvvu + uvlatbnd
     S.f[VU][i] = o6[0]; S.f[UV][i] = o6[1]; S.f[UEU][i] = o6[2]; S.f[VEV][i] = o6[3];
     S.f[VMAGEU][i] = o6[4]; S.f[VMAGEV][i] = o6[5];
 }

@@ -396,16 +396,6 @@ __device__ __forceinline__ R flux2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin
     R arrmin = (cfmin > (R)0 ? upw(qm, qm2) : upw(qi, qp)) * cfmin;
     return arrin - arrmin;
 }
-// Asynchronous 4/8-byte global -> shared copies (cp.async, completion by
-// commit groups) for the plane tiles.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
-    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-
 // theta-face flux between bins t and t+1 (the arrint of bin t, which is the
 // arrmint of bin t+1): e(t-1), e(t), e(t+1), e(t+2), ctheta(t), ctheta(t+1)
 template <class R>

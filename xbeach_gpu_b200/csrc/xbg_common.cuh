@@ -173,6 +173,74 @@ struct Prof {
 };
 #define PMARK(pf, nm) do { if (pf) (pf)->mark(nm); } while (0)
 
+// ---------------------------------------------------------------- tiles
+// Asynchronous 4/8-byte global -> shared copies (cp.async) and their groups.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
+// A block's cell tile (32 x 8 cells, 256 threads) with a halo of H cells,
+// filled with the grid clamped at its edges: the tile element next to a cell
+// is the neighbour the reference reads through mm()/pp()/mm2()/pp2().
+template <int H>
+struct TileG {
+    static constexpr int X = 32, Y = 8, TX = X + 2 * H, TY = Y + 2 * H, N = TX * TY;
+};
+
+// Copy NF fields over the tile into t[f * N + e] (cp.async), then wait and
+// synchronise the block.
+template <class R, int H, int NF>
+__device__ __forceinline__ void tile_load(R* t, const R* const (&src)[NF], int bx0, int by0, int nx, int ny) {
+    using G = TileG<H>;
+    const int tid = threadIdx.x + threadIdx.y * G::X;
+    for (int e = tid; e < G::N; e += G::X * G::Y) {
+        int gx = min(max(bx0 - H + e % G::TX, 0), nx - 1), gy = min(max(by0 - H + e / G::TX, 0), ny - 1);
+        size_t g = (size_t)gx + (size_t)gy * nx;
+#pragma unroll
+        for (int f = 0; f < NF; f++) cp_async<sizeof(R)>(t + f * G::N + e, src[f] + g);
+    }
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+}
+
+// Tile index of the cell that tile position (kx, ky) stands for (the grid
+// clamped), and that cell's grid coordinates.
+template <int H>
+__device__ __forceinline__ int tile_centre(int kx, int ky, int bx0, int by0, int nx, int ny, int& gx, int& gy) {
+    using G = TileG<H>;
+    int vx = bx0 - H + kx, vy = by0 - H + ky;
+    gx = min(max(vx, 0), nx - 1);
+    gy = min(max(vy, 0), ny - 1);
+    return (ky + gy - vy) * G::TX + (kx + gx - vx);
+}
+
+// Field access around one cell: a(f, dx, dy) = field f at
+// (clamp(ix + dx), clamp(iy + dy)), from the shared-memory tile ...
+template <class R, int H>
+struct TileAt {
+    const R* t;
+    int k;
+    __device__ __forceinline__ R operator()(int f, int dx, int dy) const {
+        return t[f * TileG<H>::N + k + dx + dy * TileG<H>::TX];
+    }
+};
+// ... or from global memory.
+template <class R, int NF>
+struct GlobalAt {
+    const R* p[NF];
+    int ix, iy, nx, ny;
+    __device__ __forceinline__ R operator()(int f, int dx, int dy) const {
+        int x = min(max(ix + dx, 0), nx - 1), y = min(max(iy + dy, 0), ny - 1);
+        return __ldg(p[f] + x + (size_t)y * nx);
+    }
+};
+
 // Early exit of a kernel in a step that the device clock has halted.
 __device__ __forceinline__ bool halted(const Clock* c) {
     return *((volatile const int*)&c->halt) != 0;
