@@ -27,6 +27,14 @@ sys.path.insert(0, ROOT)
 
 B_ALGO = lambda nt: 4 * (77 + 4 * nt)   # algorithmic bytes per coupled cell-update
 
+# DRAM bytes (read + write) per launch of the dominant kernel, from one ncu
+# capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum; the
+# capture and its command are summarised under profiles/).  Keyed by
+# (kernel, nx, ny, ntheta); other workloads report traffic null.
+NCU_TRAFFIC = {
+    ("k_wave_fast", 2048, 1024, 18): 361393920 + 342432256,
+}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -290,13 +298,14 @@ def main():
     # dominant kernel: the fused wave-action kernel
     dom = max(kern, key=kern.get)
     nt = p.ntheta
-    algo_dom = {"k_wave_main": 4 * (4 * nt + 16)}.get(dom, None)
-    rows = p.ny - 2 if dom == "k_wave_main" else p.ny
+    algo_dom = {"k_wave_fast": 4 * (4 * nt + 16)}.get(dom, None)
+    rows = p.ny - 2 if dom == "k_wave_fast" else p.ny
     roof = None
     if algo_dom:
         achieved = algo_dom * p.nx * rows / (kern[dom] / 1e3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": NCU_TRAFFIC.get((dom, p.nx, p.ny, nt)),
                 "algorithmic_bytes_per_cell": algo_dom, "ms_per_launch": kern[dom]}
     step_gbs = B_ALGO(nt) * C * K / (ms / 1e3) / 1e9
     out = {

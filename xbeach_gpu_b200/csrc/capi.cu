@@ -222,7 +222,7 @@ struct Handle : public xbg_handle {
         // reductions and clock
         int nflow = step_begin_blocks(K);
         nwave = wave_parts(K);
-        if ((rc = alloc(&S.part_flow, (size_t)nflow)) || (rc = alloc(&S.part_wave, (size_t)nwave)) ||
+        if ((rc = alloc(&S.part_flow, (size_t)2 * nflow)) || (rc = alloc(&S.part_wave, (size_t)nwave)) ||
             (rc = alloc(&S.counter, 1)) || (rc = alloc(&clk, 1)) || (rc = alloc(&ser, 1)) ||
             (rc = alloc(&mass_buf, 3)))
             return rc;

@@ -72,15 +72,34 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const 
     __shared__ int last;
     int tid = threadIdx.x;
     R m = (R)3.0e38f;
-    for (int i = blockIdx.x * blockDim.x + tid; i < S.C; i += gridDim.x * blockDim.x)   // FLOWDT
-        m = DM<R>::fmin(m, K.cfl * K.dx / (DM<R>::sqrt((R)9.81f * ld(S.f[HH] + i))));
-    for (int o = 16; o > 0; o >>= 1) m = DM<R>::fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((tid & 31) == 0) red[tid >> 5] = m;
+    {   // FLOWDT: min of hh first (4 loads in flight per thread), one sqrt per thread
+        const R* hh = S.f[HH];
+        const int stride = gridDim.x * blockDim.x;
+        R hmax = (R)0;
+        int i = blockIdx.x * blockDim.x + tid;
+        for (; i + 3 * stride < S.C; i += 4 * stride) {
+            R a = ld(hh + i), b = ld(hh + i + stride), c = ld(hh + i + 2 * stride), d = ld(hh + i + 3 * stride);
+            hmax = DM<R>::fmax(hmax, DM<R>::fmax(DM<R>::fmax(a, b), DM<R>::fmax(c, d)));
+        }
+        for (; i < S.C; i += stride) hmax = DM<R>::fmax(hmax, ld(hh + i));
+        // cfl*dx/sqrt(g*hh) decreases with hh, so its minimum is at the deepest cell
+        if (hmax > (R)0) m = K.cfl * K.dx / (DM<R>::sqrt((R)9.81f * hmax));
+    }
+    // this block's share of the wave kernel's per-block WAVEDT minima
+    R mwv = (R)3.0e38f;
+    for (int j = blockIdx.x * blockDim.x + tid; j < nwave; j += gridDim.x * blockDim.x)
+        mwv = DM<R>::fmin(mwv, ld(S.part_wave + j));
+    for (int o = 16; o > 0; o >>= 1) {
+        m = DM<R>::fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+        mwv = DM<R>::fmin(mwv, __shfl_xor_sync(0xffffffffu, mwv, o));
+    }
+    if ((tid & 31) == 0) { red[tid >> 5] = m; rw[tid >> 5] = mwv; }
     __syncthreads();
     if (tid == 0) {
-        R b = red[0];
-        for (int w = 1; w < (int)(blockDim.x >> 5); w++) b = DM<R>::fmin(b, red[w]);
+        R b = red[0], bw = rw[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) { b = DM<R>::fmin(b, red[w]); bw = DM<R>::fmin(bw, rw[w]); }
         S.part_flow[blockIdx.x] = b;
+        S.part_flow[gridDim.x + blockIdx.x] = bw;
         __threadfence();
         unsigned prev = atomicAdd(S.counter, 1u);
         last = (prev == gridDim.x - 1);
@@ -90,8 +109,10 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const 
     __threadfence();
     // ---- last block: global minima, clock, boundaries
     R mf = (R)3.0e38f, mw = (R)3.0e38f;
-    for (int j = tid; j < nflow; j += blockDim.x) mf = DM<R>::fmin(mf, ((volatile R*)S.part_flow)[j]);
-    for (int j = tid; j < nwave; j += blockDim.x) mw = DM<R>::fmin(mw, S.part_wave[j]);
+    for (int j = tid; j < nflow; j += blockDim.x) {
+        mf = DM<R>::fmin(mf, ((volatile R*)S.part_flow)[j]);
+        mw = DM<R>::fmin(mw, ((volatile R*)S.part_flow)[nflow + j]);
+    }
     for (int o = 16; o > 0; o >>= 1) {
         mf = DM<R>::fmin(mf, __shfl_xor_sync(0xffffffffu, mf, o));
         mw = DM<R>::fmin(mw, __shfl_xor_sync(0xffffffffu, mw, o));
