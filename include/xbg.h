@@ -198,6 +198,42 @@ int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
 int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,
               double* bed);
 
+/* ---- batches of scenarios ------------------------------------------------
+ * No counterpart in the reference (it runs one grid per process).  A batch
+ * advances n scenarios -- each its own grid size, parameters, boundaries,
+ * clock and dt -- with one launch per kernel of the step for all of them,
+ * replayed from one CUDA graph.  The scenarios share precision, ntheta and
+ * the swave/flow/sedtrans/roller/means switches (XBG_ERR_ARG otherwise).
+ * Each scenario is an ordinary handle owned by the batch: set fields,
+ * boundaries and time, and read results, with the xbg_* calls above on the
+ * handle from xbg_batch_scenario (reads wait for the batch's stream);
+ * stepping a scenario's handle on its own is not supported while it is in
+ * a batch, and xbg_destroy refuses it (XBG_ERR_STATE).                    */
+typedef struct xbg_batch xbg_batch;
+#define XBG_MAX_BATCH 4096
+int  xbg_batch_create(const xbg_params* params, int n, int precision,
+                      xbg_batch** out);            /* params: n entries   */
+int  xbg_batch_destroy(xbg_batch* b);
+int  xbg_batch_scenario(xbg_batch* b, int s, xbg_handle** h);
+/* nsteps coupled steps of every scenario (each with its own dt; a scenario
+ * that reached its end time, an output time or an error skips them).  Does
+ * not synchronise.                                                          */
+int  xbg_batch_advance(xbg_batch* b, int nsteps);
+/* Synchronise and read every scenario's time, dt, steps, flags and status
+ * word (arrays of n; any may be NULL).                                      */
+int  xbg_batch_status(xbg_batch* b, double* t, double* dt, int64_t* nstep,
+                      int* flags, int* status);
+int  xbg_batch_sync(xbg_batch* b);
+int  xbg_batch_get_stream(xbg_batch* b, void** stream);
+/* As xbg_profile_step, for one batched step. */
+int  xbg_batch_profile_step(xbg_batch* b, float* ms, const char** names,
+                            int* n);
+/* Persistent blocks of the launches of one tile shape (0: 32x8 tiles,
+ * 1: wave rows, 2: 256-cell runs, 3: lateral rows, 4: one block per
+ * scenario, 5: boundary values, 6: dt reduction); used by the autotuner. */
+int  xbg_batch_set_grid(xbg_batch* b, int shape, int blocks);
+int  xbg_batch_launch_count(xbg_batch* b, int64_t* count);
+
 /* ---- no-allocation entry point ------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate
  * device memory: a coupler or framework that owns the device through its

@@ -24,6 +24,14 @@ template <class R> int launch_step_begin(const Dev<R>&, const Konst<R>&, const S
 template <class R> int launch_ubnd(const Dev<R>&, const Konst<R>&, const Series*, cudaStream_t, Prof*);
 template <class R> int launch_wavebnd(const Dev<R>&, const Konst<R>&, const Series*, cudaStream_t, Prof*, int);
 template <class R> int launch_means(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int launch_step_begin_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+template <class R> int launch_wavebnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+template <class R> int launch_ubnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+template <class R> int launch_means_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, cudaStream_t, Prof*);
+template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+template <class R> int ubnd_threads(const Konst<R>&);
 template <class R> void launch_output_done(const Dev<R>&, const Konst<R>&, cudaStream_t);
 template <class R> void launch_reset_means(const Dev<R>&, cudaStream_t);
 template <class R> void launch_mass(const Dev<R>&, double, double*, cudaStream_t);
@@ -38,6 +46,16 @@ __global__ void k_set_slot(Clock* c, int logical, int nrec, double t0, double te
     c->slot_Trep[phys] = Trep;
     if (logical == 1) c->flags &= ~XBG_FLAG_NEED_BOUNDARY;
 }
+// Copy every scenario's device clock of a batch into one array.
+template <class R>
+__global__ void k_gather_clocks(const Dev<R>* S, int n, Clock* out) {
+    int s = blockIdx.x;
+    if (s >= n) return;
+    const unsigned* src = reinterpret_cast<const unsigned*>(S[s].clk);
+    unsigned* dst = reinterpret_cast<unsigned*>(out + s);
+    for (int k = threadIdx.x; k < (int)(sizeof(Clock) / 4); k += blockDim.x) dst[k] = src[k];
+}
+
 }  // namespace xbg
 
 using namespace xbg;
@@ -109,6 +127,8 @@ struct xbg_handle {
     xbg_params P;
     int precision = XBG_FP32;
     int64_t launches = 0;
+    cudaStream_t ext = nullptr;   // a batch's stream that also works on this state
+    bool batch_owned = false;      // destroyed with its batch only
     virtual int init_state(const void* zb, double zs0, double zs1) = 0;
     virtual int field_count(int f, size_t* n) = 0;
     virtual int set_field(int f, const void* p, size_t n) = 0;
@@ -128,6 +148,19 @@ struct xbg_handle {
     virtual void* stream() = 0;
     virtual int profile(float* ms, const char** names, int* n) = 0;
     virtual int put_wave_records(int slot, int first, int n, const void* St, const void* q) = 0;
+};
+
+struct xbg_batch {
+    virtual ~xbg_batch() {}
+    int n = 0;
+    std::vector<xbg_handle*> h;
+    virtual int advance(int nsteps) = 0;
+    virtual int status(double* t, double* dt, int64_t* nstep, int* flags, int* st) = 0;
+    virtual int sync() = 0;
+    virtual void* stream() = 0;
+    virtual int profile(float* ms, const char** names, int* n) = 0;
+    virtual int set_grid(int shape, int blocks) = 0;
+    virtual int64_t launches() = 0;
 };
 
 namespace {
@@ -249,6 +282,7 @@ struct Handle : public xbg_handle {
 
     int host_cur_slot = 0;
     int read_clock(Clock& c) {
+        if (ext) CK(cudaStreamSynchronize(ext));
         CK(cudaStreamSynchronize(st));
         CK(cudaMemcpy(&c, clk, sizeof(c), cudaMemcpyDeviceToHost));
         host_cur_slot = c.cur_slot;
@@ -562,6 +596,199 @@ struct Handle : public xbg_handle {
     }
 };
 
+// A batch of scenarios advanced together: N ordinary handles (their
+// buffers, clocks and boundary data), device tables of their Dev/Konst and
+// per-scenario extras, one work list per tile shape, and one CUDA graph of
+// a whole batched step (one launch per kernel for all scenarios).
+template <class R>
+struct Batch : public xbg_batch {
+    std::vector<Handle<R>*> hs;
+    Dev<R>* dS = nullptr;
+    Konst<R>* dK = nullptr;
+    BatchAux* dA = nullptr;
+    Clock* dclk = nullptr;
+    int2* ditems[BS_N] = {};
+    BatchLaunch L{};
+    std::vector<Dev<R>> hS;
+    std::vector<cudaEvent_t> evs;
+    cudaStream_t st = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    int per_step = 0;
+    int64_t nlaunch = 0;
+    cudaError_t last_err = cudaSuccess;
+    int nt = 0, swave = 0, flow = 0, sedtrans = 0, roller = 0, means = 0;
+
+    ~Batch() override {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        for (auto e : evs) cudaEventDestroy(e);
+        cudaFree(dS); cudaFree(dK); cudaFree(dA); cudaFree(dclk);
+        for (int k = 0; k < BS_N; k++) cudaFree(ditems[k]);
+        for (auto p : hs) delete p;
+        if (st) cudaStreamDestroy(st);
+    }
+
+    int setup(const xbg_params* ps, int ns, int prec) {
+        n = ns;
+        CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        for (int s = 0; s < ns; s++) {
+            const xbg_params& p = ps[s];
+            if (s == 0) {
+                nt = p.ntheta; swave = p.swave; flow = p.flow; sedtrans = p.sedtrans; roller = p.roller; means = p.means;
+            } else if (p.ntheta != nt || p.swave != swave || p.flow != flow || p.sedtrans != sedtrans ||
+                       p.roller != roller || p.means != means) {
+                return XBG_ERR_ARG;   // one kernel sequence for the whole batch
+            }
+            auto* hp = new Handle<R>();
+            hs.push_back(hp);
+            h.push_back(hp);
+            hp->batch_owned = true;
+            hp->ext = st;
+            int rc = hp->setup(&p, prec);
+            if (rc) return rc;
+        }
+        // tables
+        std::vector<Konst<R>> hK(ns);
+        std::vector<BatchAux> hA(ns);
+        hS.resize(ns);
+        std::vector<int2> it[BS_N];
+        for (int s = 0; s < ns; s++) {
+            Handle<R>& H = *hs[s];
+            hS[s] = H.S; hK[s] = H.K;
+            const int nx = H.K.nx, ny = H.K.ny, C = nx * ny;
+            hA[s].ser = H.ser;
+            hA[s].nflow = std::min((C + 255) / 256, 32);   // within the handle's 2 * step_begin_blocks partials
+            hA[s].nwave = H.nwave;
+            hA[s].ubnd_threads = ubnd_threads(H.K);
+            hA[s].pad = 0;
+            auto add = [&](int sh, int bx, int by) { it[sh].push_back(make_int2(s, bx | (by << 16))); };
+            for (int by = 0; by < (ny + 7) / 8; by++)
+                for (int bx = 0; bx < (nx + 31) / 32; bx++) add(BS_TILE, bx, by);
+            for (int by = 0; by < (ny - 2 + 7) / 8; by++)
+                for (int bx = 0; bx < (nx + 31) / 32; bx++) add(BS_WROWS, bx, by);
+            for (int b = 0; b < (C + 255) / 256; b++) add(BS_LIN, b, 0);
+            for (int r = 0; r < 2; r++)
+                for (int b = 0; b < (nx + 127) / 128; b++) add(BS_EDGE, b, r);
+            add(BS_ONE, 0, 0);
+            for (int b = 0; b < (ny * nt + 255) / 256; b++) add(BS_BND, b, 0);
+            for (int b = 0; b < hA[s].nflow; b++) add(BS_DT, b, 0);
+        }
+        CK(cudaMalloc(&dS, ns * sizeof(Dev<R>)));
+        CK(cudaMalloc(&dK, ns * sizeof(Konst<R>)));
+        CK(cudaMalloc(&dA, ns * sizeof(BatchAux)));
+        CK(cudaMalloc(&dclk, ns * sizeof(Clock)));
+        CK(cudaMemcpy(dK, hK.data(), ns * sizeof(Konst<R>), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dA, hA.data(), ns * sizeof(BatchAux), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(dS, hS.data(), ns * sizeof(Dev<R>), cudaMemcpyHostToDevice));
+        int dev = 0, sms = 148;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        const int per_sm[BS_N] = {8, 3, 8, 8, 2, 8, 8};   // resident-block targets per SM
+        for (int k = 0; k < BS_N; k++) {
+            CK(cudaMalloc(&ditems[k], std::max<size_t>(1, it[k].size()) * sizeof(int2)));
+            CK(cudaMemcpy(ditems[k], it[k].data(), it[k].size() * sizeof(int2), cudaMemcpyHostToDevice));
+            L.items[k] = ditems[k];
+            L.n[k] = (int)it[k].size();
+            L.grid[k] = std::max(1, std::min(L.n[k], sms * per_sm[k]));
+        }
+        evs.resize(ns);
+        for (int s = 0; s < ns; s++) CK(cudaEventCreateWithFlags(&evs[s], cudaEventDisableTiming));
+        for (auto* hp : hs) CK(cudaStreamSynchronize(hp->st));
+        return XBG_OK;
+    }
+
+    BatchTab<R> tab() const { return BatchTab<R>{dS, dK, dA}; }
+
+    int enqueue(Prof* pf) {
+        BatchTab<R> T = tab();
+        int k = 0;
+        k += launch_step_begin_batch(T, L, st, pf);
+        if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
+        if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
+        if (swave == 1) k += launch_wave_batch(T, L, nt, roller, st, pf);
+        if (flow == 1) k += launch_flow_batch(T, L, st, pf);
+        if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf);
+        if (means) k += launch_means_batch(T, L, st, pf);
+        return k;
+    }
+
+    // order the batch after the scenarios' own streams and refresh the
+    // scenario table (a boundary upload may have moved a scenario's slots)
+    int prepare() {
+        for (int s = 0; s < n; s++) {
+            CK(cudaEventRecord(evs[s], hs[s]->st));
+            CK(cudaStreamWaitEvent(st, evs[s], 0));
+            hS[s] = hs[s]->S;
+        }
+        CK(cudaMemcpyAsync(dS, hS.data(), n * sizeof(Dev<R>), cudaMemcpyHostToDevice, st));
+        return XBG_OK;
+    }
+
+    int advance(int nsteps) override {
+        int rc = prepare();
+        if (rc) return rc;
+        if (!gexec) {
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            per_step = enqueue(nullptr);
+            cudaError_t e = cudaStreamEndCapture(st, &graph);
+            if (e != cudaSuccess) { last_err = e; return XBG_ERR_CUDA; }
+            CK(cudaGraphInstantiate(&gexec, graph, 0));
+        }
+        for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(gexec, st));
+        nlaunch += (int64_t)per_step * nsteps;
+        return XBG_OK;
+    }
+
+    int status(double* t, double* dt, int64_t* nstep, int* flags, int* stt) override {
+        k_gather_clocks<R><<<n, 64, 0, st>>>(dS, n, dclk);
+        CK(cudaGetLastError());
+        std::vector<Clock> c(n);
+        CK(cudaMemcpyAsync(c.data(), dclk, n * sizeof(Clock), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int s = 0; s < n; s++) {
+            if (t) t[s] = c[s].totaltime;
+            if (dt) dt[s] = c[s].dt;
+            if (nstep) nstep[s] = c[s].nstep_total;
+            if (flags) flags[s] = c[s].flags;
+            if (stt) stt[s] = c[s].status;
+        }
+        return XBG_OK;
+    }
+
+    int sync() override { CK(cudaStreamSynchronize(st)); return XBG_OK; }
+    void* stream() override { return (void*)st; }
+    int64_t launches() override { return nlaunch; }
+
+    int set_grid(int shape, int blocks) override {
+        if (shape < 0 || shape >= BS_N || blocks < 1) return XBG_ERR_ARG;
+        L.grid[shape] = std::min(blocks, std::max(1, L.n[shape]));
+        if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+        if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+        return XBG_OK;
+    }
+
+    int profile(float* ms, const char** names, int* nk) override {
+        int rc = prepare();
+        if (rc) return rc;
+        Prof pf;
+        pf.st = st;
+        for (int k = 0; k < 65; k++) CK(cudaEventCreate(&pf.ev[k]));
+        CK(cudaEventRecord(pf.ev[0], st));
+        nlaunch += enqueue(&pf);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        int m = std::min(*nk, pf.n);
+        for (int k = 0; k < m; k++) {
+            CK(cudaEventElapsedTime(&ms[k], pf.ev[k], pf.ev[k + 1]));
+            if (names) names[k] = pf.name[k];
+        }
+        *nk = m;
+        for (int k = 0; k < 65; k++) cudaEventDestroy(pf.ev[k]);
+        return XBG_OK;
+    }
+};
+
 }  // namespace
 
 // ------------------------------------------------------------------ C ABI
@@ -579,7 +806,11 @@ int xbg_create(const xbg_params* p, int precision, xbg_handle** out) {
     *out = h;
     return XBG_OK;
 }
-int xbg_destroy(xbg_handle* h) { delete h; return XBG_OK; }
+int xbg_destroy(xbg_handle* h) {
+    if (h && h->batch_owned) return XBG_ERR_STATE;   // freed with its batch
+    delete h;
+    return XBG_OK;
+}
 int xbg_init_state(xbg_handle* h, const void* zb, double zs0, double zs1) { return h ? h->init_state(zb, zs0, zs1) : XBG_ERR_ARG; }
 int xbg_field_count(const xbg_handle* h, int f, size_t* n) { return h ? const_cast<xbg_handle*>(h)->field_count(f, n) : XBG_ERR_ARG; }
 int xbg_set_field(xbg_handle* h, int f, const void* p, size_t n) { return h ? h->set_field(f, p, n) : XBG_ERR_ARG; }
@@ -615,5 +846,36 @@ int xbg_put_wave_records(xbg_handle* h, int slot, int first, int n, const void* 
     return h ? h->put_wave_records(slot, first, n, St, q) : XBG_ERR_ARG;
 }
 int xbg_mass(xbg_handle* h, double* w, double* s, double* b) { return h ? h->mass(w, s, b) : XBG_ERR_ARG; }
+
+int xbg_batch_create(const xbg_params* p, int n, int precision, xbg_batch** out) {
+    if (!p || !out || n < 1 || n > XBG_MAX_BATCH || (precision != XBG_FP32 && precision != XBG_FP64))
+        return XBG_ERR_ARG;
+    *out = nullptr;
+    xbg_batch* b = nullptr;
+    int rc;
+    if (precision == XBG_FP32) { auto* q = new Batch<float>(); b = q; rc = q->setup(p, n, precision); }
+    else { auto* q = new Batch<double>(); b = q; rc = q->setup(p, n, precision); }
+    if (rc) { delete b; return rc; }
+    *out = b;
+    return XBG_OK;
+}
+int xbg_batch_destroy(xbg_batch* b) { delete b; return XBG_OK; }
+int xbg_batch_scenario(xbg_batch* b, int s, xbg_handle** h) {
+    if (!b || !h || s < 0 || s >= b->n) return XBG_ERR_ARG;
+    *h = b->h[s];
+    return XBG_OK;
+}
+int xbg_batch_advance(xbg_batch* b, int nsteps) { return (b && nsteps >= 0) ? b->advance(nsteps) : XBG_ERR_ARG; }
+int xbg_batch_status(xbg_batch* b, double* t, double* dt, int64_t* nstep, int* flags, int* status) {
+    return b ? b->status(t, dt, nstep, flags, status) : XBG_ERR_ARG;
+}
+int xbg_batch_sync(xbg_batch* b) { return b ? b->sync() : XBG_ERR_ARG; }
+int xbg_batch_get_stream(xbg_batch* b, void** s) { if (!b || !s) return XBG_ERR_ARG; *s = b->stream(); return XBG_OK; }
+int xbg_batch_profile_step(xbg_batch* b, float* ms, const char** names, int* n) {
+    if (!b || !ms || !n) return XBG_ERR_ARG;
+    return b->profile(ms, names, n);
+}
+int xbg_batch_set_grid(xbg_batch* b, int shape, int blocks) { return b ? b->set_grid(shape, blocks) : XBG_ERR_ARG; }
+int xbg_batch_launch_count(xbg_batch* b, int64_t* n) { if (!b || !n) return XBG_ERR_ARG; *n = b->launches(); return XBG_OK; }
 
 }  // extern "C"

@@ -51,10 +51,10 @@ __device__ __forceinline__ R smago_cell(const Dev<R>& S, const Konst<R>& K, int 
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_a(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_flow_a(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     if (halted(S.clk)) return;
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R eps = K.eps;
@@ -67,6 +67,7 @@ __global__ void __launch_bounds__(256) k_flow_a(Dev<R> S, Konst<R> K) {
     S.f[HVM][i] = DM<R>::fmax(hvmi, eps);
     S.tmp[T_NUH][i] = smago_cell(S, K, ix, iy);
 }
+XBG_KERNELS(flow_a)
 
 // eulerustep (Flow_kernel.cu:1487-1544) at an interior-x cell, with the
 // advection (ududx_adv :752, vdudy_adv :887) and viscosity (viscou1 :1319,
@@ -136,11 +137,11 @@ __device__ R euler_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_u(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_flow_u(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     R dtf = (R)clk->dt, wu = (R)clk->windu;
     // latbnd(uu): rows 0 / ny-1 take the updated rows 1 / ny-2
@@ -150,6 +151,7 @@ __global__ void __launch_bounds__(256) k_flow_u(Dev<R> S, Konst<R> K) {
     R v = (ix > 0) ? euler_u(S, K, ix, sy, dtf, wu) : ld(S.f[UU] + IDX(ix, sy));
     S.tmp[T_UU][IDX(ix, iy)] = v;
 }
+XBG_KERNELS(flow_u)
 
 // vdvdy_adv (Flow_kernel.cu:1024-1074) at a row that eulervstep updates.
 template <class R>
@@ -229,11 +231,11 @@ __device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_v(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_flow_v(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     R dtf = (R)clk->dt, wv = (R)clk->windv;
     // vvlatbnd: row 0 <- row 1, row ny-2 <- row ny-3; row ny-1 keeps its value
@@ -245,6 +247,7 @@ __global__ void __launch_bounds__(256) k_flow_v(Dev<R> S, Konst<R> K) {
     else v = ld(S.f[VV] + IDX(ix, sy));
     S.tmp[T_VV][IDX(ix, iy)] = v;
 }
+XBG_KERNELS(flow_v)
 
 // Fields of the momentum-correction pass, in its shared-memory tile.
 enum { C_ZS, C_ZB, C_UU, C_VV, C_UO, C_VO, C_QX, C_QY, C_NF };
@@ -310,14 +313,14 @@ constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT
 constexpr int FC_H = 3;
 
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_corr(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     using G = TileG<FC_H>;
     __shared__ R tile[C_NF * G::N];
     __shared__ R sU1[FT_N], sU2[FT_N], sV1[FT_N], sV2[FT_N];
     const int nx = K.nx, ny = K.ny;
-    const int bx0 = blockIdx.x * FT_X, by0 = blockIdx.y * FT_Y;
+    const int bx0 = bix * FT_X, by0 = biy * FT_Y;
     {
         const R* src[C_NF] = {S.f[ZS], S.f[ZB], S.tmp[T_UU], S.tmp[T_VV], S.f[UUOLD], S.f[VVOLD], S.f[QX], S.f[QY]};
         tile_load<R, FC_H, C_NF>(tile, src, bx0, by0, nx, ny);
@@ -358,6 +361,7 @@ __global__ void __launch_bounds__(256) k_flow_corr(Dev<R> S, Konst<R> K) {
     S.f[UU][i] = u;
     S.f[VV][i] = v;
 }
+XBG_KERNELS(flow_corr)
 
 // depthhu / depthhv (Flow_kernel.cu:653-750)
 template <class R>
@@ -388,11 +392,11 @@ __device__ __forceinline__ R depth_v(const Dev<R>& S, const Konst<R>& K, int ix,
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_cont(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_flow_cont(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R dtf = (R)clk->dt;
@@ -411,6 +415,7 @@ __global__ void __launch_bounds__(256) k_flow_cont(Dev<R> S, Konst<R> K) {
     }
     S.tmp[T_ZS][i] = zs;
 }
+XBG_KERNELS(flow_cont)
 
 // Fields of the final pass, in its shared-memory tile: the post-continuity
 // level, bed, previous step's level, corrected velocities, Stokes drift inputs.
@@ -487,7 +492,7 @@ __device__ __forceinline__ void uvvu_cell(const A& a, R wu, R wv, const R* sS, c
 // (latbnd), whose lower neighbour is outside the ring when ny-1 is the block's
 // first row: that one case evaluates zs from global memory.
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     using G = TileG<FC_H>;
@@ -496,7 +501,7 @@ __global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
     const R* zsold_in = S.zsold[clk->par ^ 1];
     R* zsold_out = S.zsold[clk->par];
     const int nx = K.nx, ny = K.ny;
-    const int bx0 = blockIdx.x * FT_X, by0 = blockIdx.y * FT_Y;
+    const int bx0 = bix * FT_X, by0 = biy * FT_Y;
     {
         const R* src[Z_NF] = {S.tmp[T_ZS], S.f[ZB], zsold_in, S.f[UU], S.f[VV], S.f[UST], S.f[THM]};
         tile_load<R, FC_H, Z_NF>(tile, src, bx0, by0, nx, ny);
@@ -551,6 +556,7 @@ __global__ void __launch_bounds__(256) k_flow_final(Dev<R> S, Konst<R> K) {
     S.f[VU][i] = o6[0]; S.f[UV][i] = o6[1]; S.f[UEU][i] = o6[2]; S.f[VEV][i] = o6[3];
     S.f[VMAGEU][i] = o6[4]; S.f[VMAGEV][i] = o6[5];
 }
+XBG_KERNELS(flow_final)
 
 template <class R>
 int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
@@ -569,6 +575,29 @@ int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     PMARK(pf, "k_flow_final");
     return 6;
 }
+// the six flow kernels over every scenario of a batch
+template <class R>
+int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+    dim3 b(32, 8);
+    const int2* it = L.items[BS_TILE];
+    int n = L.n[BS_TILE], g = L.grid[BS_TILE];
+    kb_flow_a<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_flow_a");
+    kb_flow_u<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_flow_u");
+    kb_flow_v<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_flow_v");
+    kb_flow_corr<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_flow_corr");
+    kb_flow_cont<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_flow_cont");
+    kb_flow_final<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_flow_final");
+    return 6;
+}
+template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*);
+template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*);
+
 template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
 template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
 

@@ -21,11 +21,11 @@ __device__ __forceinline__ bool sed_skip(const Clock* c) {
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (sed_skip(clk)) return;
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy), xm = mm(ix), ym = mm(iy);
     R dtf = (R)clk->dt, Trep = (R)clk->Trep;
@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(256) k_sed_a(Dev<R> S, Konst<R> K) {
         S.tmp[T_FACERO][i] = facero;
     }
 }
+XBG_KERNELS(sed_a)
 
 // Susp (Sediment_kernel.cu:534-719): suspended fluxes Sus, Svs at (ix, iy)
 template <class R>
@@ -175,12 +176,12 @@ __device__ __forceinline__ R conc_cell(const Dev<R>& S, const Konst<R>& K, int i
 constexpr int SB_X = 32, SB_Y = 8, SB_TX = SB_X + 1, SB_TY = SB_Y + 1;
 
 template <class R>
-__global__ void __launch_bounds__(256) k_sed_b(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_sed_b(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (sed_skip(clk)) return;
     __shared__ R sSus[SB_TY * SB_TX], sSvs[SB_TY * SB_TX];
     const int nx = K.nx, ny = K.ny;
-    const int bx0 = blockIdx.x * SB_X, by0 = blockIdx.y * SB_Y;
+    const int bx0 = bix * SB_X, by0 = biy * SB_Y;
     const int tid = threadIdx.x + threadIdx.y * SB_X;
     for (int e = tid; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
         int kx = e % SB_TX, ky = e / SB_TX;
@@ -214,6 +215,7 @@ __global__ void __launch_bounds__(256) k_sed_b(Dev<R> S, Konst<R> K) {
         S.tmp[T_STDEP][i] = ld(S.f[STDEP] + i) - dzg;
     }
 }
+XBG_KERNELS(sed_b)
 
 // zblatbnd source cell (Sediment_kernel.cu:970-1018, pre-kernel reads)
 __device__ __forceinline__ int zbl_src(int ix, int iy, int nx, int ny) {
@@ -279,12 +281,12 @@ __device__ __forceinline__ R ddzb_cell(const Dev<R>& S, const Konst<R>& K, int i
 // the row below it go to shared memory once; a boundary cell whose zblatbnd
 // source lies elsewhere evaluates that source's bed change directly.
 template <class R>
-__global__ void __launch_bounds__(256) k_sed_c(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (sed_skip(clk)) return;
     __shared__ R sBx[SB_TY * SB_TX], sBy[SB_TY * SB_TX];
     const int nx = K.nx, ny = K.ny;
-    const int bx0 = blockIdx.x * SB_X, by0 = blockIdx.y * SB_Y;
+    const int bx0 = bix * SB_X, by0 = biy * SB_Y;
     const bool morph = K.morfac > (R)0.0f;
     const R dtf = (R)clk->dt;
     if (morph) {
@@ -328,6 +330,7 @@ __global__ void __launch_bounds__(256) k_sed_c(Dev<R> S, Konst<R> K) {
         else { S.f[CFM][i] = K.cfsand; S.f[FWM][i] = K.fwsand; }
     }
 }
+XBG_KERNELS(sed_c)
 
 template <class R>
 int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
@@ -340,6 +343,23 @@ int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     PMARK(pf, "k_sed_c");
     return 3;
 }
+// the three sediment kernels over every scenario of a batch
+template <class R>
+int launch_sed_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+    dim3 b(32, 8);
+    const int2* it = L.items[BS_TILE];
+    int n = L.n[BS_TILE], g = L.grid[BS_TILE];
+    kb_sed_a<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_sed_a");
+    kb_sed_b<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_sed_b");
+    kb_sed_c<R><<<g, b, 0, st>>>(T, it, n);
+    PMARK(pf, "k_sed_c");
+    return 3;
+}
+template int launch_sed_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*);
+template int launch_sed_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*);
+
 template int launch_sed<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
 template int launch_sed<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
 

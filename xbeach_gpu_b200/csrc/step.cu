@@ -35,7 +35,7 @@ template <class R>
 __device__ void wavebnd_cursor(Clock& c, const Konst<R>& K, const Series* ser);
 
 template <class R>
-__device__ void finalize_scalar(Dev<R>& S, const Konst<R>& K, const Series* ser, R mflow, R mwave) {
+__device__ void finalize_scalar(const Dev<R>& S, const Konst<R>& K, const Series* ser, R mflow, R mwave) {
     Clock& c = *S.clk;
     c.halt = 1;
     if (c.status != XBG_OK) return;
@@ -67,16 +67,17 @@ __device__ void finalize_scalar(Dev<R>& S, const Konst<R>& K, const Series* ser,
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const Series* ser, int nflow, int nwave) {
+__device__ __forceinline__ void b_step_begin(const Dev<R>& S, const Konst<R>& K, const Series* ser, int nflow,
+                                             int nwave, const int bi, const int nb) {
     __shared__ R red[8], rw[8];
     __shared__ int last;
     int tid = threadIdx.x;
     R m = (R)3.0e38f;
     {   // FLOWDT: min of hh first (4 loads in flight per thread), one sqrt per thread
         const R* hh = S.f[HH];
-        const int stride = gridDim.x * blockDim.x;
+        const int stride = nb * blockDim.x;
         R hmax = (R)0;
-        int i = blockIdx.x * blockDim.x + tid;
+        int i = bi * blockDim.x + tid;
         for (; i + 3 * stride < S.C; i += 4 * stride) {
             R a = ld(hh + i), b = ld(hh + i + stride), c = ld(hh + i + 2 * stride), d = ld(hh + i + 3 * stride);
             hmax = DM<R>::fmax(hmax, DM<R>::fmax(DM<R>::fmax(a, b), DM<R>::fmax(c, d)));
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const 
     }
     // this block's share of the wave kernel's per-block WAVEDT minima
     R mwv = (R)3.0e38f;
-    for (int j = blockIdx.x * blockDim.x + tid; j < nwave; j += gridDim.x * blockDim.x)
+    for (int j = bi * blockDim.x + tid; j < nwave; j += nb * blockDim.x)
         mwv = DM<R>::fmin(mwv, ld(S.part_wave + j));
     for (int o = 16; o > 0; o >>= 1) {
         m = DM<R>::fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -98,11 +99,11 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const 
     if (tid == 0) {
         R b = red[0], bw = rw[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) { b = DM<R>::fmin(b, red[w]); bw = DM<R>::fmin(bw, rw[w]); }
-        S.part_flow[blockIdx.x] = b;
-        S.part_flow[gridDim.x + blockIdx.x] = bw;
+        S.part_flow[bi] = b;
+        S.part_flow[nb + bi] = bw;
         __threadfence();
         unsigned prev = atomicAdd(S.counter, 1u);
-        last = (prev == gridDim.x - 1);
+        last = (prev == nb - 1);
     }
     __syncthreads();
     if (!last) return;
@@ -125,6 +126,16 @@ __global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const 
         *S.counter = 0;
         finalize_scalar(S, K, ser, mf, mw);
     }
+}
+template <class R>
+__global__ void __launch_bounds__(256) k_step_begin(Dev<R> S, Konst<R> K, const Series* ser, int nflow, int nwave) {
+    b_step_begin<R>(S, K, ser, nflow, nwave, blockIdx.x, gridDim.x);
+}
+template <class R>
+__global__ void __launch_bounds__(256) kb_step_begin(BatchTab<R> T, const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux& A, int bx, int) {
+        b_step_begin<R>(S, K, A.ser, A.nflow, A.nwave, bx, A.nflow);
+    });
 }
 
 // wavebnd's record cursor and chunk slot (Wavestep.cu:512-700, 684-695),
@@ -166,10 +177,10 @@ __global__ void k_wavebnd_cursor(Dev<R> S, Konst<R> K, const Series* ser) {
 
 // St interpolation in time (Wavestep.cu:703-741), one thread per (iy, bin).
 template <class R>
-__global__ void __launch_bounds__(256) k_wavebnd_interp(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_wavebnd_interp(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock& c = *S.clk;
     if (halted(&c)) return;
-    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = bix * blockDim.x + threadIdx.x;
     int nyt = K.ny * K.nt;
     if (j >= nyt) return;
     int cs = c.cur_slot, nb = c.nwbndstep;
@@ -178,9 +189,10 @@ __global__ void __launch_bounds__(256) k_wavebnd_interp(Dev<R> S, Konst<R> K) {
     R sn = sf[j + (size_t)(nb + 1) * nyt];
     S.St[j] = (R)interptime((double)sn, (double)so, c.timenext_w, c.timesincelast_w);
 }
+XBG_KERNELS(wavebnd_interp)
 
 template <class R>
-__global__ void __launch_bounds__(1024) k_ubnd(Dev<R> S, Konst<R> K, const Series* ser) {
+__device__ __forceinline__ void b_ubnd(const Dev<R>& S, const Konst<R>& K, const Series* ser, const int nthr) {
     Clock* clk = S.clk;
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny;
@@ -203,13 +215,13 @@ __global__ void __launch_bounds__(1024) k_ubnd(Dev<R> S, Konst<R> K, const Serie
     // column mean of the pre-kernel uu (sequential float sum in the reference;
     // here a tree sum)
     R s = (R)0;
-    for (int n = tid; n < ny; n += blockDim.x) s += uu[n * nx];
+    for (int n = tid; n < ny; n += nthr) s += uu[n * nx];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((tid & 31) == 0) wsum[tid >> 5] = s;
     __syncthreads();
     if (tid == 0) {
         R a = (R)0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) a += wsum[w];
+        for (int w = 0; w < (int)(nthr >> 5); w++) a += wsum[w];
         uuavg_s = a / (R)ny;
     }
     __syncthreads();
@@ -219,7 +231,7 @@ __global__ void __launch_bounds__(1024) k_ubnd(Dev<R> S, Konst<R> K, const Serie
     R zsi = (R)clk->zsbndi, zsn = (R)clk->zsbndn;
     int cs = clk->cur_slot, nb = clk->nwbndstep;
     const R* q = S.qfile[cs];
-    for (int iy = tid; iy < ny; iy += blockDim.x) {
+    for (int iy = tid; iy < ny; iy += nthr) {
         int i = iy * nx, xplus = pp(0, nx);
         R zsbnd = zsi + (zsn - zsi) * (((R)iy) / ((R)ny));
         R zsplus = zs[xplus + iy * nx];
@@ -247,11 +259,23 @@ __global__ void __launch_bounds__(1024) k_ubnd(Dev<R> S, Konst<R> K, const Serie
         vv[i] = nv;
     }
 }
+template <class R>
+__global__ void __launch_bounds__(1024) k_ubnd(Dev<R> S, Konst<R> K, const Series* ser) {
+    b_ubnd<R>(S, K, ser, blockDim.x);
+}
+// one 1024-thread block per scenario; the column sum runs over the scenario's
+// own logical thread count, so it adds in the single-domain kernel's order
+template <class R>
+__global__ void __launch_bounds__(1024) kb_ubnd(BatchTab<R> T, const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux& A, int, int) {
+        b_ubnd<R>(S, K, A.ser, A.ubnd_threads);
+    });
+}
 
 template <class R>
-__global__ void __launch_bounds__(256) k_means(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_means(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     if (halted(S.clk)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bix * blockDim.x + threadIdx.x;
     if (i >= S.C) return;
     // every load before the first store: the field pointers may alias as far
     // as the compiler knows, so interleaved stores would serialise the loads
@@ -267,6 +291,7 @@ __global__ void __launch_bounds__(256) k_means(Dev<R> S, Konst<R> K) {
     S.f[ZSMAX][i] = DM<R>::fmax(xz, zs);
     S.f[CMEAN][i] = mc + c;
 }
+XBG_KERNELS(means)
 
 template <class R>
 __global__ void k_output_done(Dev<R> S, Konst<R> K) {   // Wave_gpu.cu:786-824
@@ -338,10 +363,13 @@ int launch_step_begin(const Dev<R>& S, const Konst<R>& K, const Series* ser, int
     PMARK(pf, "k_step_begin");
     return 1;
 }
+// logical thread count of the single-domain ubnd launch
+template <class R>
+int ubnd_threads(const Konst<R>& K) { return K.ny >= 1024 ? 1024 : ((K.ny + 31) / 32) * 32; }
+
 template <class R>
 int launch_ubnd(const Dev<R>& S, const Konst<R>& K, const Series* ser, cudaStream_t st, Prof* pf) {
-    int nt = K.ny >= 1024 ? 1024 : ((K.ny + 31) / 32) * 32;
-    k_ubnd<R><<<1, nt, 0, st>>>(S, K, ser);
+    k_ubnd<R><<<1, ubnd_threads(K), 0, st>>>(S, K, ser);
     PMARK(pf, "k_ubnd");
     return 1;
 }
@@ -376,6 +404,31 @@ void launch_mass(const Dev<R>& S, double dx2, double* out, cudaStream_t st) {
     k_mass<R><<<296, 256, 0, st>>>(S, dx2, out);
 }
 
+// the step-control kernels over every scenario of a batch
+template <class R>
+int launch_step_begin_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+    kb_step_begin<R><<<L.grid[BS_DT], 256, 0, st>>>(T, L.items[BS_DT], L.n[BS_DT]);
+    PMARK(pf, "k_step_begin");
+    return 1;
+}
+template <class R>
+int launch_wavebnd_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+    kb_wavebnd_interp<R><<<L.grid[BS_BND], 256, 0, st>>>(T, L.items[BS_BND], L.n[BS_BND]);
+    PMARK(pf, "k_wavebnd");
+    return 1;
+}
+template <class R>
+int launch_ubnd_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+    kb_ubnd<R><<<L.grid[BS_ONE], 1024, 0, st>>>(T, L.items[BS_ONE], L.n[BS_ONE]);
+    PMARK(pf, "k_ubnd");
+    return 1;
+}
+template <class R>
+int launch_means_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+    kb_means<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
+    PMARK(pf, "k_means");
+    return 1;
+}
 #define INST(R)                                                                                   \
     template int step_begin_blocks<R>(const Konst<R>&);                                           \
     template int launch_step_begin<R>(const Dev<R>&, const Konst<R>&, const Series*, int, cudaStream_t, Prof*); \
@@ -384,7 +437,12 @@ void launch_mass(const Dev<R>& S, double dx2, double* out, cudaStream_t st) {
     template int launch_means<R>(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);                   \
     template void launch_output_done<R>(const Dev<R>&, const Konst<R>&, cudaStream_t);            \
     template void launch_reset_means<R>(const Dev<R>&, cudaStream_t);                             \
-    template void launch_mass<R>(const Dev<R>&, double, double*, cudaStream_t);
+    template void launch_mass<R>(const Dev<R>&, double, double*, cudaStream_t);                        \
+    template int ubnd_threads<R>(const Konst<R>&);                                                \
+    template int launch_step_begin_batch<R>(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*); \
+    template int launch_wavebnd_batch<R>(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);    \
+    template int launch_ubnd_batch<R>(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);       \
+    template int launch_means_batch<R>(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 INST(float)
 INST(double)
 

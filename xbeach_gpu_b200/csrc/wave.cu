@@ -64,9 +64,9 @@ __device__ void disp_cell(const Konst<R>& K, R sg, R h, R& k_, R& c_, R& cg_) {
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_disp(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_disp(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     if (halted(S.clk)) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int i = bix * blockDim.x + threadIdx.x;
     if (i >= S.C) return;
     R sg = (R)S.clk->sigm;
     R k_, c_, cg_;
@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(256) k_disp(Dev<R> S, Konst<R> K) {
     S.f[CC_][i] = c_;
     S.f[CG][i] = cg_;
 }
+XBG_KERNELS(disp)
 
 // Per-cell slope terms of propagtheta (wave_CPU.cpp:226-306).
 template <class R>
@@ -414,7 +415,7 @@ __device__ __forceinline__ R theta_face(R em, R e0, R ep, R ep2, R c0, R cp) {
 constexpr int WT_NB = 3;   // plane tile buffers: plane t+1 streams in while t is used
 
 template <class R, bool ROLLER>
-__global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Clock* clk = S.clk;
     if (halted(clk)) return;
@@ -428,7 +429,7 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
     R* sSin = sCos + nt;                  // [nt]
     R* sTh = sSin + nt;                   // [nt]
     if (tid < nt) { sCos[tid] = K.cxsth[tid]; sSin[tid] = K.sxnth[tid]; sTh[tid] = K.theta[tid]; }
-    const int bx0 = blockIdx.x * WT_X, by0 = 1 + blockIdx.y * WT_Y;
+    const int bx0 = bix * WT_X, by0 = 1 + biy * WT_Y;
     const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     const bool active = ix < nx && iy <= ny - 2;
     const int par = clk->par;
@@ -665,16 +666,26 @@ __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
         S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
         S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
     }
-    block_min_store<R>(dtw, S.part_wave + blockIdx.x + blockIdx.y * gridDim.x);
+    block_min_store<R>(dtw, S.part_wave + bix + biy * ((K.nx + 31) / 32));
+}
+template <class R, bool ROLLER>
+__global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
+    b_wave_fast<R, ROLLER>(S, K, blockIdx.x, blockIdx.y);
+}
+template <class R, bool ROLLER>
+__global__ void __launch_bounds__(256, 3) kb_wave_fast(BatchTab<R> T, const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux&, int bx, int by) {
+        b_wave_fast<R, ROLLER>(S, K, bx, by);
+    });
 }
 
 template <class R, int NMAX>
-__global__ void __launch_bounds__(128) k_wave_edge(Dev<R> S, Konst<R> K, int part_offset) {
+__device__ __forceinline__ void b_wave_edge(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    int iy = (blockIdx.y == 0) ? 0 : ny - 1;
+    int ix = bix * blockDim.x + threadIdx.x;
+    int iy = (biy == 0) ? 0 : ny - 1;
     R dtw = (R)3.0e38f;
     if (ix < nx) {
         int i = ix + iy * nx;
@@ -709,7 +720,17 @@ __global__ void __launch_bounds__(128) k_wave_edge(Dev<R> S, Konst<R> K, int par
             if (t < nt) e[t] = een[ix + src * nx + (size_t)t * C] * w;
         finish_cell<R, NMAX>(S, K, i, e, r, o, een, rrn);
     }
-    block_min_store<R>(dtw, S.part_wave + part_offset + blockIdx.x + blockIdx.y * gridDim.x);
+    block_min_store<R>(dtw, S.part_wave + ((K.nx + 31) / 32) * ((K.ny - 2 + 7) / 8) + bix + biy * ((K.nx + 127) / 128));
+}
+template <class R, int NMAX>
+__global__ void __launch_bounds__(128) k_wave_edge(Dev<R> S, Konst<R> K) {
+    b_wave_edge<R, NMAX>(S, K, blockIdx.x, blockIdx.y);
+}
+template <class R, int NMAX>
+__global__ void __launch_bounds__(128) kb_wave_edge(BatchTab<R> T, const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux&, int bx, int by) {
+        b_wave_edge<R, NMAX>(S, K, bx, by);
+    });
 }
 
 // wavforce (wave_CPU.cpp:1164-1238) at cell j, before the boundary copies.
@@ -745,12 +766,12 @@ __device__ __forceinline__ void breaker_raw(const Dev<R>& S, const Konst<R>& K, 
 }
 
 template <class R>
-__global__ void __launch_bounds__(256) k_wave_force(Dev<R> S, Konst<R> K) {
+__device__ __forceinline__ void b_wave_force(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
     if (halted(clk)) return;
     const int nx = K.nx, ny = K.ny;
-    int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    int ix = bix * blockDim.x + threadIdx.x;
+    int iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = ix + iy * nx;
     R Trep = (R)clk->Trep;
@@ -780,6 +801,7 @@ __global__ void __launch_bounds__(256) k_wave_force(Dev<R> S, Konst<R> K) {
     S.f[URMS][i] = urms;
     S.f[UST][i] = ust;
 }
+XBG_KERNELS(wave_force)
 
 // ---------------------------------------------------------------- launchers
 template <class R>
@@ -797,7 +819,7 @@ void launch_wave_main(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof*
     else k_wave_fast<R, false><<<g, b, smem, st>>>(S, K);
     PMARK(pf, "k_wave_fast");
     dim3 be(128), ge((K.nx + 127) / 128, 2);
-    k_wave_edge<R, NMAX><<<ge, be, 0, st>>>(S, K, g.x * g.y);
+    k_wave_edge<R, NMAX><<<ge, be, 0, st>>>(S, K);
     PMARK(pf, "k_wave_edge");
 }
 
@@ -820,6 +842,37 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     return n;
 }
 
+// the wave kernels over every scenario of a batch (one ntheta and roller
+// setting for the whole batch)
+template <class R, int NMAX>
+void launch_wave_main_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, cudaStream_t st, Prof* pf) {
+    dim3 b(32, 8);
+    size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * nt * 256 + 3 * nt) * sizeof(R);
+    if (roller == 1) kb_wave_fast<R, true><<<L.grid[BS_WROWS], b, smem, st>>>(T, L.items[BS_WROWS], L.n[BS_WROWS]);
+    else kb_wave_fast<R, false><<<L.grid[BS_WROWS], b, smem, st>>>(T, L.items[BS_WROWS], L.n[BS_WROWS]);
+    PMARK(pf, "k_wave_fast");
+    kb_wave_edge<R, NMAX><<<L.grid[BS_EDGE], 128, 0, st>>>(T, L.items[BS_EDGE], L.n[BS_EDGE]);
+    PMARK(pf, "k_wave_edge");
+}
+
+template <class R>
+int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, cudaStream_t st, Prof* pf) {
+    kb_disp<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
+    PMARK(pf, "k_disp");
+    if (nt <= 4) launch_wave_main_batch<R, 4>(T, L, nt, roller, st, pf);
+    else if (nt <= 8) launch_wave_main_batch<R, 8>(T, L, nt, roller, st, pf);
+    else if (nt <= 12) launch_wave_main_batch<R, 12>(T, L, nt, roller, st, pf);
+    else if (nt <= 16) launch_wave_main_batch<R, 16>(T, L, nt, roller, st, pf);
+    else if (nt <= 20) launch_wave_main_batch<R, 20>(T, L, nt, roller, st, pf);
+    else if (nt <= 24) launch_wave_main_batch<R, 24>(T, L, nt, roller, st, pf);
+    else launch_wave_main_batch<R, 32>(T, L, nt, roller, st, pf);
+    kb_wave_force<R><<<L.grid[BS_TILE], dim3(32, 8), 0, st>>>(T, L.items[BS_TILE], L.n[BS_TILE]);
+    PMARK(pf, "k_wave_force");
+    return 4;
+}
+template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, cudaStream_t, Prof*);
+template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, cudaStream_t, Prof*);
+
 // One-time kernel attributes (dynamic shared memory above 48 KB for wide
 // theta sets in FP64).
 template <class R>
@@ -827,7 +880,9 @@ int wave_prepare(const Konst<R>& K) {
     size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
     cudaError_t e = cudaFuncSetAttribute(k_wave_fast<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaError_t e2 = cudaFuncSetAttribute(k_wave_fast<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return (e == cudaSuccess && e2 == cudaSuccess) ? 0 : 1;
+    cudaError_t e3 = cudaFuncSetAttribute(kb_wave_fast<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e4 = cudaFuncSetAttribute(kb_wave_fast<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return (e == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess) ? 0 : 1;
 }
 template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);

@@ -241,6 +241,88 @@ struct GlobalAt {
     }
 };
 
+// ---------------------------------------------------------------- batches
+// A batch advances many scenarios (each with its own grid, parameters, clock
+// and dt) with one launch per kernel of the step.  Each kernel is a body
+// b_NAME(S, K, bx, by) over one block-sized tile; the single-domain kernel
+// k_NAME runs it at (blockIdx.x, blockIdx.y), the batched kernel kb_NAME runs
+// it for each (scenario, tile) work item of its list, persistent blocks
+// taking contiguous runs of items.
+
+// Per-scenario extras that single-domain kernels get as launch arguments.
+struct BatchAux {
+    const Series* ser;
+    int nflow;          // blocks of the dt reduction
+    int nwave;          // WAVEDT partials
+    int ubnd_threads;   // logical thread count of the ubnd block
+    int pad;
+};
+
+template <class R>
+struct BatchTab {
+    const Dev<R>* S;
+    const Konst<R>* K;
+    const BatchAux* A;
+};
+
+// Work-item lists, one per tile shape: (scenario, bx | by << 16)
+enum BatchShape {
+    BS_TILE,    // 32 x 8 tiles over nx x ny
+    BS_WROWS,   // 32 x 8 tiles over nx x rows 1..ny-2 (wave pass)
+    BS_LIN,     // 256-cell runs of the C cells
+    BS_EDGE,    // 128-cell runs of rows 0 and ny-1
+    BS_ONE,     // one block per scenario
+    BS_BND,     // 256-value runs of the ny*ntheta boundary values
+    BS_DT,      // the blocks of the dt reduction
+    BS_N
+};
+struct BatchLaunch {
+    const int2* items[BS_N];
+    int n[BS_N];
+    int grid[BS_N];
+};
+
+template <class R, class F>
+__device__ __forceinline__ void batch_items(const BatchTab<R>& T, const int2* items, int n, F&& f) {
+    constexpr int WD = (int)(sizeof(Dev<R>) / 4), WK = (int)(sizeof(Konst<R>) / 4), WA = (int)(sizeof(BatchAux) / 4);
+    __shared__ __align__(16) unsigned sbuf[WD + WK + WA];
+    const Dev<R>& sS = *reinterpret_cast<const Dev<R>*>(sbuf);
+    const Konst<R>& sK = *reinterpret_cast<const Konst<R>*>(sbuf + WD);
+    const BatchAux& sA = *reinterpret_cast<const BatchAux*>(sbuf + WD + WK);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int nth = blockDim.x * blockDim.y;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int lo = blockIdx.x * per, hi = min(n, lo + per);
+    int cur = -1;
+    for (int it = lo; it < hi; it++) {
+        const int2 w = items[it];
+        if (w.x != cur) {   // stage the scenario's state and constants
+            __syncthreads();
+            const unsigned* gS = reinterpret_cast<const unsigned*>(T.S + w.x);
+            const unsigned* gK = reinterpret_cast<const unsigned*>(T.K + w.x);
+            const unsigned* gA = reinterpret_cast<const unsigned*>(T.A + w.x);
+            for (int k = tid; k < WD + WK + WA; k += nth)
+                sbuf[k] = k < WD ? gS[k] : (k < WD + WK ? gK[k - WD] : gA[k - WD - WK]);
+            __syncthreads();
+            cur = w.x;
+        }
+        f(sS, sK, sA, w.y & 0xffff, w.y >> 16);
+        __syncthreads();
+    }
+}
+
+// Single-domain and batched kernels of a 256-thread body b_NAME(S, K, bx, by).
+#define XBG_KERNELS(NAME)                                                                              \
+    template <class R>                                                                                 \
+    __global__ void __launch_bounds__(256) k_##NAME(Dev<R> S, Konst<R> K) {                            \
+        b_##NAME<R>(S, K, blockIdx.x, blockIdx.y);                                                     \
+    }                                                                                                  \
+    template <class R>                                                                                 \
+    __global__ void __launch_bounds__(256) kb_##NAME(BatchTab<R> T, const int2* items, int n) {        \
+        batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux&, int bx,   \
+                                        int by) { b_##NAME<R>(S, K, bx, by); });                       \
+    }
+
 // Early exit of a kernel in a step that the device clock has halted.
 __device__ __forceinline__ bool halted(const Clock* c) {
     return *((volatile const int*)&c->halt) != 0;

@@ -29,6 +29,9 @@ EXPORTS = [
     "xbg_output_done", "xbg_reset_means", "xbg_set_time", "xbg_sync", "xbg_launch_count",
     "xbg_mass", "xbg_put_wave_records", "xbg_get_stream", "xbg_profile_step",
     "xbg_flow_dt_noalloc",
+    "xbg_batch_create", "xbg_batch_destroy", "xbg_batch_scenario", "xbg_batch_advance", "xbg_batch_status",
+    "xbg_batch_sync", "xbg_batch_get_stream", "xbg_batch_profile_step", "xbg_batch_set_grid",
+    "xbg_batch_launch_count",
 ]
 
 
@@ -71,6 +74,16 @@ def load():
     L.xbg_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.xbg_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
     L.xbg_flow_dt_noalloc.argtypes = [ip, vp, ip, ip, C.c_double, C.c_double, vp, vp]
+    L.xbg_batch_create.argtypes = [C.POINTER(Params), ip, ip, C.POINTER(vp)]
+    L.xbg_batch_destroy.argtypes = [vp]
+    L.xbg_batch_scenario.argtypes = [vp, ip, C.POINTER(vp)]
+    L.xbg_batch_advance.argtypes = [vp, ip]
+    L.xbg_batch_status.argtypes = [vp, vp, vp, vp, vp, vp]
+    L.xbg_batch_sync.argtypes = [vp]
+    L.xbg_batch_get_stream.argtypes = [vp, C.POINTER(vp)]
+    L.xbg_batch_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
+    L.xbg_batch_set_grid.argtypes = [vp, ip, ip]
+    L.xbg_batch_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
     _lib = L
     return L
 
@@ -87,16 +100,21 @@ def _ptr(a):
 class Model:
     """One device-resident model (one xbg_handle)."""
 
-    def __init__(self, params, precision=XBG_FP32):
+    def __init__(self, params, precision=XBG_FP32, _handle=None):
         self.L = load()
         self.p = params
         self.dtype = np.float32 if precision == XBG_FP32 else np.float64
+        self.owned = _handle is None
+        if _handle is not None:   # a batch's scenario: the batch frees it
+            self.h = _handle
+            return
         self.h = C.c_void_p()
         _check(self.L.xbg_create(C.byref(params), precision, C.byref(self.h)), "xbg_create")
 
     def close(self):
         if getattr(self, "h", None):
-            self.L.xbg_destroy(self.h)
+            if self.owned:
+                self.L.xbg_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -206,3 +224,72 @@ class Model:
         w, s, b = C.c_double(), C.c_double(), C.c_double()
         _check(self.L.xbg_mass(self.h, C.byref(w), C.byref(s), C.byref(b)), "mass")
         return w.value, s.value, b.value
+
+
+class Batch:
+    """n scenarios advanced together, one launch per kernel for all of them
+    (xbg_batch_*).  batch.scenario(s) is a Model on the batch's handle s for
+    fields, boundaries and time; advance() steps all of them."""
+
+    def __init__(self, params_list, precision=XBG_FP32):
+        self.L = load()
+        self.n = len(params_list)
+        arr = (Params * self.n)(*params_list)
+        self.b = C.c_void_p()
+        _check(self.L.xbg_batch_create(arr, self.n, precision, C.byref(self.b)), "xbg_batch_create")
+        self.models = []
+        for s, p in enumerate(params_list):
+            h = C.c_void_p()
+            _check(self.L.xbg_batch_scenario(self.b, s, C.byref(h)), "xbg_batch_scenario")
+            self.models.append(Model(p, precision, _handle=h))
+
+    def scenario(self, s):
+        return self.models[s]
+
+    def advance(self, nsteps):
+        _check(self.L.xbg_batch_advance(self.b, nsteps), "xbg_batch_advance")
+
+    def sync(self):
+        _check(self.L.xbg_batch_sync(self.b), "xbg_batch_sync")
+
+    def status(self):
+        n = self.n
+        t, dt = np.zeros(n), np.zeros(n)
+        ns = np.zeros(n, np.int64)
+        fl, st = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        _check(self.L.xbg_batch_status(self.b, _ptr(t), _ptr(dt), _ptr(ns), _ptr(fl), _ptr(st)), "xbg_batch_status")
+        return dict(t=t, dt=dt, nstep=ns, flags=fl, status=st)
+
+    def stream(self):
+        s = C.c_void_p()
+        _check(self.L.xbg_batch_get_stream(self.b, C.byref(s)), "xbg_batch_get_stream")
+        return s.value
+
+    def set_grid(self, shape, blocks):
+        _check(self.L.xbg_batch_set_grid(self.b, shape, blocks), "xbg_batch_set_grid")
+
+    def launches(self):
+        n = C.c_int64()
+        _check(self.L.xbg_batch_launch_count(self.b, C.byref(n)), "xbg_batch_launch_count")
+        return n.value
+
+    def profile_step(self):
+        cap = 64
+        ms = (C.c_float * cap)()
+        names = (C.c_char_p * cap)()
+        n = C.c_int(cap)
+        _check(self.L.xbg_batch_profile_step(self.b, ms, names, C.byref(n)), "xbg_batch_profile_step")
+        return [(names[k].decode(), ms[k]) for k in range(n.value)]
+
+    def close(self):
+        if getattr(self, "b", None):
+            for m in self.models:
+                m.h = None
+            self.L.xbg_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

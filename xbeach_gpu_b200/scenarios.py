@@ -17,6 +17,13 @@ Cases
                  wide) whose crest varies alongshore (250 m, 0.5 m), 5 cm
                  seeded noise, 18 bins over -90..90 deg, Hm0 2.5 m, Tp 12 s,
                  D50 0.25 mm, morfac 10 (the large single domain).
+  ensemble       (make_ensemble) n scenarios of uneven grids: nx uniform on
+                 [128, 1024], ny on [64, 512] in multiples of 32, dx=4 m, 12
+                 bins over -90..90 deg; per scenario a slope uniform on
+                 [1/100, 1/20] (depth capped at 12 m offshore, land at -3 m),
+                 a Gaussian bar with probability 0.5, Hm0 on [0.5, 4] m, Tp on
+                 [6, 14] s, mean direction on [-30, 30] deg, D50 on
+                 [0.15, 0.4] mm, 1800 s, boundary seed = seed + k.
 The wave boundary is a seeded wave-group series on the bins: a cos^2s
 directional spreading of the JONSWAP energy Hm0^2 rho g / 16 (as GenCstWave,
 makjonswap.cpp:24-70, spreads it) modulated in time by a sum of random-phase
@@ -151,3 +158,45 @@ def random_state(p, seed=0, wet_fraction=0.85):
     dry = rng.random((ny, nx)) > wet_fraction
     f["hh"] = np.where(dry, p.eps, f["hh"])
     return f
+
+
+def make_ensemble(n, seed=0, **kw):
+    """n scenarios of the ragged ensemble: a list of (params, zb, boundary)."""
+    return list(iter_ensemble(n, seed, **kw))
+
+
+def iter_ensemble(n, seed=0, nx_range=(128, 1024), ny_range=(64, 512), step=32, dx=4.0, ntheta=12,
+                  endtime=1800.0, dtbc=5.0):
+    """The scenarios of make_ensemble one at a time.  The boundary records are
+    dtbc apart (the groups' time scales are tens of seconds), which keeps a
+    scenario's chunk a few MB."""
+    rng = np.random.default_rng(seed)
+    for k in range(n):
+        p = default_params()
+        p.nx = int(rng.integers(nx_range[0] // step, nx_range[1] // step + 1)) * step
+        p.ny = int(rng.integers(ny_range[0] // step, ny_range[1] // step + 1)) * step
+        p.dx = dx
+        p.thetamin, p.thetamax = -90 * PI / 180, 90 * PI / 180
+        p.dtheta = (p.thetamax - p.thetamin) / ntheta
+        slope = rng.uniform(1 / 100, 1 / 20)
+        x = np.arange(p.nx) * p.dx
+        y = np.arange(p.ny) * p.dx
+        xw = 0.8 * p.nx * p.dx
+        zb = np.clip((xw - x) * slope, -3.0, 12.0)[None, :].repeat(p.ny, axis=0)
+        if rng.random() < 0.5:
+            xb = xw - rng.uniform(0.1, 0.3) * xw
+            zb = zb - 1.5 * np.exp(-(((x - xb) / 40.0) ** 2) / 2)[None, :]
+        Hs, Tp = rng.uniform(0.5, 4.0), rng.uniform(6.0, 14.0)
+        mdir = rng.uniform(-30.0, 30.0) * PI / 180
+        p.D50 = rng.uniform(0.00015, 0.0004)
+        p.D90 = 1.5 * p.D50
+        p.morfac, p.endtime = 1.0, endtime
+        p.wavebndtype = 4
+        p.sedtrans, p.morphology, p.sedstart = 1, 1, 0.0
+        p.CFL, p.eps = 0.7, 0.01
+        p.dtbc, p.rtlength = dtbc, endtime
+        p = sanity(p, endbnd=1e9)
+        nrec = int(math.ceil(p.rtlength / p.dtbc)) + 1
+        St, q = wave_group_boundary(p, nrec, Hs, Tp, mdir, seed=seed + 1 + k, dtbc=dtbc)
+        bnd = dict(St=St, q=q, t0=0.0, tend=p.rtlength, Trep=Tp / 1.1, Hs=Hs, Tp=Tp)
+        yield p, zb, bnd
