@@ -166,10 +166,11 @@ def make_ensemble(n, seed=0, **kw):
 
 
 def iter_ensemble(n, seed=0, nx_range=(128, 1024), ny_range=(64, 512), step=32, dx=4.0, ntheta=12,
-                  endtime=1800.0, dtbc=5.0):
+                  endtime=1800.0, dtbc=5.0, boundary=True):
     """The scenarios of make_ensemble one at a time.  The boundary records are
     dtbc apart (the groups' time scales are tens of seconds), which keeps a
-    scenario's chunk a few MB."""
+    scenario's chunk a few MB.  boundary=False yields the parameters and bed
+    only (boundary None) with the same random draws."""
     rng = np.random.default_rng(seed)
     for k in range(n):
         p = default_params()
@@ -197,6 +198,9 @@ def iter_ensemble(n, seed=0, nx_range=(128, 1024), ny_range=(64, 512), step=32, 
         p.dtbc, p.rtlength = dtbc, endtime
         p = sanity(p, endbnd=1e9)
         nrec = int(math.ceil(p.rtlength / p.dtbc)) + 1
+        if not boundary:
+            yield p, zb, None
+            continue
         St, q = wave_group_boundary(p, nrec, Hs, Tp, mdir, seed=seed + 1 + k, dtbc=dtbc)
         bnd = dict(St=St, q=q, t0=0.0, tend=p.rtlength, Trep=Tp / 1.1, Hs=Hs, Tp=Tp)
         yield p, zb, bnd
