@@ -49,7 +49,20 @@ def parse():
                     help="large: the 2048x1024 single domain (the headline line); ensemble: the batched "
                          "ragged ensemble (256 scenarios, one launch per kernel for all)")
     ap.add_argument("--scenarios", type=int, default=256)
+    ap.add_argument("--no-autotune", action="store_true", help="ensemble: keep the default persistent grids")
     return ap.parse_args()
+
+
+def over_ranks(dist, maxed, summed, device):
+    """Max over ranks of `maxed` (times) and sum of `summed` (work), one
+    all-reduce each; every rank calls it with lists of the same lengths."""
+    import torch
+    mx = torch.tensor([float(v) for v in maxed], device=device, dtype=torch.float64)
+    sm = torch.tensor([float(v) for v in summed], device=device, dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(sm, op=dist.ReduceOp.SUM)
+    return [float(v) for v in mx], [float(v) for v in sm]
 
 
 def peaks():
@@ -233,6 +246,10 @@ def run_ensemble(args, rank, world, local):
         m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
         m.init_state(zb, 0.0, 0.0)
         cells += p.nx * p.ny
+    tuned = None
+    if not args.no_autotune:
+        from xbeach_gpu_b200.autotune import tune
+        tuned = tune(b, reps=2)
     stream = torch.cuda.ExternalStream(b.stream())
     W, K = max(3, args.warmup), args.steps
     sampler = ClockSampler(local)
@@ -284,6 +301,7 @@ def run_ensemble(args, rank, world, local):
                           "peak_kind": peak_kind},
         "kernels_ms": kern, "gpu_launches": int(launches), "clocks": clocks,
         "sim_time_s": [float(st["t"].min()), float(st["t"].max())],
+        "autotuned_blocks": {str(k): v for k, v in (tuned or {}).items()},
     }
     b.close()
     return out
@@ -314,12 +332,9 @@ def main():
     if args.workload == "ensemble":
         out = run_ensemble(args, rank, world, local)
         if dist:
-            tt = torch.tensor([out["ms_per_step"]], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            cc = torch.tensor([float(out["config"]["cells"])], device="cuda", dtype=torch.float64)
-            dist.all_reduce(cc, op=dist.ReduceOp.SUM)
-            out["ms_per_step"] = float(tt[0])
-            out["value"] = float(cc[0]) / (out["ms_per_step"] / 1e3)
+            (msx,), (cells,) = over_ranks(dist, [out["ms_per_step"]], [out["config"]["cells"]], "cuda")
+            out["ms_per_step"] = msx
+            out["value"] = cells / (msx / 1e3)
         if rank == 0:
             print(json.dumps(out), flush=True)
         if dist:
@@ -382,9 +397,7 @@ def main():
     d2h = 232   # the device clock struct read by xbg_get_time
     # max over ranks
     if dist:
-        tt = torch.tensor([ms, e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(tt[0]), float(tt[1])
+        (ms, e2e_s), _ = over_ranks(dist, [ms, e2e_s], [C], "cuda")
     value = C * K * world / (ms / 1e3)
     e2e = C * Ke * world / e2e_s
     peak, peak_kind = peaks()

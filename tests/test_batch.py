@@ -74,3 +74,28 @@ def test_batch_scenarios_end_on_their_own():
         assert np.array_equal(b.scenario(2).get(f), m.get(f)), f
     m.close()
     b.close()
+
+
+def test_batch_grid_choice_does_not_change_results(tmp_path):
+    """The autotuner's knob (persistent blocks per tile shape) only changes
+    which block runs which tile: two batches with different block counts end
+    bit for bit the same."""
+    from xbeach_gpu_b200.autotune import tune
+    sc = _cases(4, 21)
+    runs = []
+    for variant in ("default", "tuned"):
+        b = Batch([p for p, _, _ in sc], XBG_FP32)
+        for s, (p, zb, bnd) in enumerate(sc):
+            _setup(b.scenario(s), p, zb, bnd)
+        if variant == "tuned":
+            for shape, blocks in ((0, 7), (1, 3), (2, 5), (6, 2)):
+                b.set_grid(shape, blocks)
+        b.advance(25)
+        runs.append({s: {f: b.scenario(s).get(f).copy() for f in ("zs", "uu", "H", "ee")} for s in range(len(sc))})
+        if variant == "tuned":
+            choice = tune(b, cache=str(tmp_path / "tune.json"), reps=1)
+            assert set(choice) == {0, 1, 2, 6} and all(v >= 1 for v in choice.values())
+        b.close()
+    for s in runs[0]:
+        for f in runs[0][s]:
+            assert np.array_equal(runs[0][s][f], runs[1][s][f]), (s, f)
