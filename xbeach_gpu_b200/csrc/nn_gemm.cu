@@ -1,0 +1,240 @@
+// nn_gemm.cu -- the tensor-core GEMM of the wave surrogate (5th-generation
+// tensor cores, tcgen05, accumulators in tensor memory).
+//
+//   C[M x N] = act(A[M x K] . B[N x K]^T + bias[N])
+//
+// A and B are bf16, row-major with K contiguous ("K-major"); C is fp32 or bf16
+// row-major; the products accumulate in fp32.  One CTA computes a 128 x BN
+// tile (BN = N, 16..256, a multiple of 16; M is padded by the caller to a
+// multiple of 128 and K to a multiple of 64).
+//
+// Per 64-wide K chunk: all 256 threads copy the A and B chunk into shared
+// memory (cp.async, 16 B) in the canonical K-major 128-byte-swizzle layout
+// (row pitch 128 B, the 16-byte chunk index XOR the row within its 8-row
+// group, 1024-B aligned tiles), fence the async proxy and sync; one thread
+// issues four tcgen05.mma of 128 x BN x 16 (smem descriptors advanced by
+// 32 B) and commits them to the stage's mbarrier.  Two stages: the copy of
+// chunk k overlaps the MMAs of chunk k-1.  The epilogue waits for the last
+// commit, reads the accumulators with tcgen05.ld (warp w reads TMEM lanes
+// 32*(w%4).. and half of the columns), adds the bias, applies ReLU and
+// stores.  Every mbarrier wait is bounded: on time-out the kernel records an
+// error code and leaves (the host reads it).
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "../../include/xbg.h"
+#include "../../include/xbg_nn.h"
+
+namespace xbg {
+namespace nn {
+
+constexpr int GM = 128;          // rows of a CTA tile (TMEM lanes)
+constexpr int GK = 64;           // K chunk: 64 bf16 = one 128-B swizzle row
+constexpr int GSTAGES = 2;
+constexpr unsigned WAIT_LIMIT = 1u << 22;   // try_wait polls before giving up
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp16(unsigned dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src));
+}
+
+// K-major, 128-B swizzle shared-memory matrix descriptor (start address and
+// strides in 16-B units; SBO = 1024 B between 8-row groups; version 1).
+__device__ __forceinline__ uint64_t sw128_desc(unsigned saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // LBO (unused with this swizzle)
+    d |= (uint64_t)(1024 >> 4) << 32;       // SBO
+    d |= (uint64_t)1 << 46;                 // descriptor version
+    d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+    return d;
+}
+
+// kind::f16 instruction descriptor: bf16 x bf16 -> f32, both K-major, M x N
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned a, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count));
+}
+// bounded wait for the phase with the given parity; false on time-out
+__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity) {
+    for (unsigned it = 0; it < WAIT_LIMIT; it++) {
+        unsigned ok;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+template <int BN>
+__global__ void __launch_bounds__(256, 1) k_gemm_tc(const __nv_bfloat16* __restrict__ A,
+                                                    const __nv_bfloat16* __restrict__ B,
+                                                    const float* __restrict__ bias, void* C, int M, int N, int K,
+                                                    int lda, int ldb, int ldc, int flags, int* err) {
+    constexpr int A_BYTES = GM * GK * 2;       // 16 KB
+    constexpr int B_BYTES = BN * GK * 2;
+    constexpr int STAGE = A_BYTES + B_BYTES;   // multiple of 1024
+    constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long mbar[GSTAGES];
+    __shared__ unsigned tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * GM;
+    // split-K: this CTA reduces K chunks [kb, ke) (whole K unless gridDim.y > 1)
+    const int nk_all = K / GK;
+    const int per = (nk_all + gridDim.y - 1) / gridDim.y;
+    const int kb = blockIdx.y * per, ke = min(nk_all, kb + per);
+    // 1024-B aligned stage buffers
+    const unsigned base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - smem_u32(smem_raw));
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < GSTAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_slot;
+    const uint32_t idesc = idesc_bf16(GM, BN);
+    const int nk = max(0, ke - kb);
+    bool ok = true;
+
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc & 1;
+        if (kc >= GSTAGES) {   // the MMAs that read this stage are done (the block leaves together if not)
+            const bool w = mbar_wait(smem_u32(&mbar[s]), ((kc - GSTAGES) >> 1) & 1);
+            if (!__syncthreads_and(w)) { ok = false; break; }
+        }
+        const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+        const int k0 = (kb + kc) * GK;
+        for (int q = tid; q < GM * 8; q += 256) {   // A: 128 rows x 8 chunks
+            int r = q >> 3, c = q & 7;
+            int m = m0 + r;
+            unsigned dst = sa + r * 128 + ((c ^ (r & 7)) << 4);
+            if (m < M) cp16(dst, A + (size_t)m * lda + k0 + c * 8);
+            else *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
+        }
+        for (int q = tid; q < BN * 8; q += 256) {   // B: BN rows x 8 chunks
+            int r = q >> 3, c = q & 7;
+            unsigned dst = sb + r * 128 + ((c ^ (r & 7)) << 4);
+            if (r < N) cp16(dst, B + (size_t)r * ldb + k0 + c * 8);
+            else *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
+        }
+        asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
+#pragma unroll
+            for (int j = 0; j < GK / 16; j++) {
+                const unsigned acc = (kc > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da + (uint64_t)(2 * j)), "l"(db + (uint64_t)(2 * j)), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&mbar[s]))
+                         : "memory");
+        }
+    }
+    if (ok && nk > 0) ok = mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), ((nk - 1) >> 1) & 1);
+    ok = __syncthreads_and(ok) != 0;   // the TMEM loads below are warp-collective
+    tc_fence_after();
+
+    if (ok) {   // epilogue: warp w -> lanes 32*(w%4).., column half w/4
+        const int q = warp & 3, h = warp >> 2;
+        const int row = m0 + q * 32 + lane;
+        const int half = BN / 2;
+        for (int c0 = h * half; c0 < (h + 1) * half; c0 += 8) {
+            unsigned r[8];
+            const unsigned taddr = tmem + ((unsigned)(q * 32) << 16) + (unsigned)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (row < M) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const int n = c0 + j;
+                    if (n >= N) break;
+                    float v = nk > 0 ? __uint_as_float(r[j]) : 0.0f;
+                    if (flags & XBG_NN_ATOMIC) {   // split-K partial: add into f32 C
+                        atomicAdd((float*)C + (size_t)row * ldc + n, v);
+                        continue;
+                    }
+                    if (bias) v += bias[n];
+                    if (flags & XBG_NN_RELU) v = fmaxf(v, 0.0f);
+                    if (flags & XBG_NN_OUT_BF16) ((__nv_bfloat16*)C)[(size_t)row * ldc + n] = __float2bfloat16(v);
+                    else ((float*)C)[(size_t)row * ldc + n] = v;
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, XBG_ERR_TIMEOUT);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
+template <int BN>
+int gemm_launch(const void* A, const void* B, const float* bias, void* C, int M, int N, int K, int lda, int ldb,
+                int ldc, int flags, int ksplit, int* err, cudaStream_t st) {
+    constexpr int STAGE = GM * GK * 2 + BN * GK * 2;
+    const size_t smem = (size_t)GSTAGES * STAGE + 1024;
+    static bool attr = false;   // per process; the attribute is per function
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_gemm_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return XBG_ERR_CUDA;
+        attr = true;
+    }
+    dim3 grid((M + GM - 1) / GM, ksplit);
+    k_gemm_tc<BN><<<grid, 256, smem, st>>>((const __nv_bfloat16*)A, (const __nv_bfloat16*)B, bias, C, M, N, K, lda,
+                                           ldb, ldc, flags, err);
+    return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA;
+}
+
+}  // namespace nn
+}  // namespace xbg
+
+extern "C" int xbg_nn_gemm(const void* A, const void* B, const float* bias, void* C, int M, int N, int K, int lda,
+                           int ldb, int ldc, int flags, int ksplit, int* err, void* stream) {
+    using namespace xbg::nn;
+    if (!A || !B || !C || !err || M < 1 || K < GK || (K % GK) || N < 16 || N > 256 || (N % 16) || (lda % 8) ||
+        (ldb % 8) || lda < K || ldb < K || ldc < N || ksplit < 1 || ksplit > 65535)
+        return XBG_ERR_ARG;
+    if ((flags & XBG_NN_ATOMIC) && (flags & XBG_NN_OUT_BF16)) return XBG_ERR_ARG;
+    if (ksplit > 1 && !(flags & XBG_NN_ATOMIC)) return XBG_ERR_ARG;
+    if (((uintptr_t)A | (uintptr_t)B) & 15) return XBG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (N) {
+        case 16: return gemm_launch<16>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 32: return gemm_launch<32>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 48: return gemm_launch<48>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 64: return gemm_launch<64>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 96: return gemm_launch<96>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 128: return gemm_launch<128>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 192: return gemm_launch<192>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+        case 256: return gemm_launch<256>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+    }
+    return XBG_ERR_ARG;
+}
