@@ -33,6 +33,49 @@ int xbg_nn_gemm(const void* A, const void* B, const float* bias, void* C,
 /* ksplit > 1 (requires XBG_NN_ATOMIC): the K chunks are split over ksplit
  * CTAs per row tile, each adding its partial product into C.              */
 
+/* ---- layers around the GEMM (NHWC bf16 tensors, [pixels][channels], the
+ * channel counts multiples of 8) ------------------------------------------ */
+/* col[p][tap*C + c] = x[b, y+dy, x+dx, c] (0 outside the image; tap = (dy+1)*3
+ * + dx+1); columns 9C..Kp-1 and rows B*H*W..Mpad-1 are zero.  Kp % 64 == 0. */
+int xbg_nn_im2col3x3(const void* x, void* col, int B, int H, int W, int C,
+                     int Kp, int Mpad, void* stream);
+/* dx (+)= the gather of dcol back onto the pixels it was taken from. */
+int xbg_nn_col2im3x3(const void* dcol, void* dx, int B, int H, int W, int C,
+                     int Kp, int accumulate, void* stream);
+/* dst[c][r] = src[r][c], r < R, c < Cc (bf16). */
+int xbg_nn_transpose(const void* src, void* dst, int R, int Cc, int lds,
+                     int ldd, void* stream);
+/* dx = dy where y > 0 (n values, a multiple of 8). */
+int xbg_nn_relu_bwd(const void* dy, const void* y, void* dx, long long n,
+                    void* stream);
+/* db[n] += sum over p < P of dy[p][n] (f32 db, N <= 256). */
+int xbg_nn_bias_grad(const void* dy, float* db, int P, int N, int ld,
+                     void* stream);
+/* 2x2 average pooling and its backward (dx (+)= dy / 4 on each child). */
+int xbg_nn_pool2(const void* x, void* y, int B, int H, int W, int C,
+                 void* stream);
+int xbg_nn_pool2_bwd(const void* dy, void* dx, int B, int H, int W, int C,
+                     int accumulate, void* stream);
+/* nearest 2x upsampling of x[B,h,w,C] into channels [c0, c0+C) of
+ * y[B,2h,2w,ldy], and its backward (sum of the four children). */
+int xbg_nn_up2(const void* x, void* y, int B, int h, int w, int C, int ldy,
+               int c0, void* stream);
+int xbg_nn_up2_bwd(const void* dy, void* dx, int B, int h, int w, int C,
+                   int ldy, int c0, void* stream);
+/* x[P][C] -> channels [c0, c0+C) of y[P][ldy] (concatenation), or back
+ * (reverse = 1, optionally adding into x). */
+int xbg_nn_chan_copy(void* x, void* y, long long P, int C, int ldy, int c0,
+                     int reverse, int accumulate, void* stream);
+/* mean squared error of pred[P][ldp] (f32) against tgt[P][nc] (f32):
+ * *loss += mean, dpred[P][ldg] (bf16) = its gradient (0 in padding). */
+int xbg_nn_mse(const float* pred, const float* tgt, void* dpred, float* loss,
+               int P, int nc, int ldp, int ldg, void* stream);
+/* Adam step `step` (1-based) on f32 master weights p with bf16 copy pb. */
+int xbg_nn_adam(float* p, void* pb, const float* g, float* m, float* v,
+                long long n, float lr, float b1, float b2, float eps, int step,
+                void* stream);
+int xbg_nn_to_bf16(const float* a, void* b, long long n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
