@@ -55,8 +55,8 @@ import math  # noqa: E402
 
 import numpy as np  # noqa: E402
 
-IN_CH = 8            # zb, h, u, v, E, R (prior), Hm0, Tp/dir planes
-OUT_CH = 6           # E, H, D, DR, Fx, Fy at t + k
+IN_CH = 16           # zb, h, u, v, E, R, Hm0, Tp planes + the six wave fields at t + 2 zero planes
+OUT_CH = 6           # change of E, H, D, DR, Fx, Fy over k steps
 GEMM_N = (16, 32, 48, 64, 96, 128, 192, 256)
 
 
