@@ -198,6 +198,18 @@ int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
 int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,
               double* bed);
 
+/* ---- wave forcing from outside the wave solver ---------------------------
+ * No counterpart in the reference.  Sets the wave forcing fields E, H, D,
+ * DR, Fx, Fy to f0 + w (f1 - f0) (E, H, D, DR clipped at 0), where f0 and f1
+ * are host arrays of six DEVICE plane pointers of the handle's precision
+ * (the surrogate's predictions); with rescale != 0 the wave action of every
+ * bin and the roller energy are scaled per cell to the new E and DR, so a
+ * later plain wave step continues from the state the forcing describes.
+ * Enqueued on the handle's stream; used between xbg_flow_boundary and
+ * xbg_flow_step in place of xbg_wave_step.                                   */
+int  xbg_set_wave_forcing(xbg_handle* h, const void* const* f0,
+                          const void* const* f1, double w, int rescale);
+
 /* ---- batches of scenarios ------------------------------------------------
  * No counterpart in the reference (it runs one grid per process).  A batch
  * advances n scenarios -- each its own grid size, parameters, boundaries,

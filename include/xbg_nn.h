@@ -75,6 +75,19 @@ int xbg_nn_adam(float* p, void* pb, const float* g, float* m, float* v,
                 long long n, float lr, float b1, float b2, float eps, int step,
                 void* stream);
 int xbg_nn_to_bf16(const float* a, void* b, long long n, void* stream);
+/* dst[c][p] = src[c][p] for nc planes (DEVICE arrays of plane pointers). */
+int xbg_nn_copy_planes(const float* const* src, float* const* dst, int nc,
+                       long long P, void* stream);
+/* network input from model planes: x[p][c] = bf16((planes[c][p] - mean[c])
+ * * inv_std[c]); planes is a DEVICE array of nc f32 plane pointers (NULL =
+ * a zero plane).                                                           */
+int xbg_nn_encode(const float* const* planes, int nc, const float* mean,
+                  const float* inv_std, void* x, long long P, void* stream);
+/* network output to model planes: dst[c][p] = hold[c][p] + out[p][c] *
+ * ys[c] + ym[c]; hold and dst are DEVICE arrays of nc f32 plane pointers. */
+int xbg_nn_decode(const float* out, int ldo, const float* const* hold,
+                  const float* ym, const float* ys, float* const* dst, int nc,
+                  long long P, void* stream);
 
 #ifdef __cplusplus
 }

@@ -46,6 +46,39 @@ __global__ void k_set_slot(Clock* c, int logical, int nrec, double t0, double te
     c->slot_Trep[phys] = Trep;
     if (logical == 1) c->flags &= ~XBG_FLAG_NEED_BOUNDARY;
 }
+// Wave forcing from outside the wave solver (the surrogate): E, H, D, DR, Fx,
+// Fy = f0 + w (f1 - f0) (E, H, D, DR clipped at 0).  With rescale, the wave
+// action of every bin in both plane sets (still the state that f0 describes)
+// scales by E_new / E0 and the roller energy (both sets and R) by DR_new /
+// DR0, so a later plain wave step starts from the state the forcing
+// describes.
+template <class R>
+struct Forcing6 { const R* p[6]; };
+
+template <class R>
+__global__ void k_set_forcing(Dev<R> S, R* ee0, R* ee1, R* rr0, R* rr1, Forcing6<R> f0, Forcing6<R> f1, R w,
+                              int rescale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.C) return;
+    R v[6];
+#pragma unroll
+    for (int c = 0; c < 6; c++) v[c] = f0.p[c][i] + w * (f1.p[c][i] - f0.p[c][i]);
+#pragma unroll
+    for (int c = 0; c < 4; c++) v[c] = v[c] > (R)0 ? v[c] : (R)0;
+    if (rescale) {   // ee, rr still hold the state of f0 (the segment start)
+        const R Eo = f0.p[0][i], DRo = f0.p[3][i];
+        const R re = Eo > (R)1e-12 ? v[0] / Eo : (R)1;
+        const R rr = DRo > (R)1e-12 ? v[3] / DRo : (R)1;
+        for (int t = 0; t < S.nt; t++) {
+            const size_t j = (size_t)i + (size_t)t * S.C;
+            ee0[j] *= re; ee1[j] *= re;
+            rr0[j] *= rr; rr1[j] *= rr;
+        }
+        S.f[ROL][i] *= rr;
+    }
+    S.f[E][i] = v[0]; S.f[H][i] = v[1]; S.f[D][i] = v[2]; S.f[DR][i] = v[3]; S.f[FX][i] = v[4]; S.f[FY][i] = v[5];
+}
+
 // Copy every scenario's device clock of a batch into one array.
 template <class R>
 __global__ void k_gather_clocks(const Dev<R>* S, int n, Clock* out) {
@@ -148,6 +181,7 @@ struct xbg_handle {
     virtual void* stream() = 0;
     virtual int profile(float* ms, const char** names, int* n) = 0;
     virtual int put_wave_records(int slot, int first, int n, const void* St, const void* q) = 0;
+    virtual int set_forcing(const void* const* f0, const void* const* f1, double w, int rescale) = 0;
 };
 
 struct xbg_batch {
@@ -591,6 +625,19 @@ struct Handle : public xbg_handle {
     int sync() override { CK(cudaStreamSynchronize(st)); return XBG_OK; }
     void* stream() override { return (void*)st; }
     int profile(float* ms, const char** names, int* n) override { return profile_step(ms, names, n); }
+    int set_forcing(const void* const* f0, const void* const* f1, double w, int rescale) override {
+        Forcing6<R> a, b;
+        for (int c = 0; c < 6; c++) {
+            if (!f0[c] || !f1[c]) return XBG_ERR_ARG;
+            a.p[c] = (const R*)f0[c];
+            b.p[c] = (const R*)f1[c];
+        }
+        k_set_forcing<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, ee_buf[0], ee_buf[1], rr_buf[0], rr_buf[1], a, b, (R)w,
+                                                            rescale);
+        launches++;
+        CK(cudaGetLastError());
+        return XBG_OK;
+    }
     int put_wave_records(int slot, int first, int n, const void* St, const void* q) override {
         return put_records(slot, first, n, St, q);
     }
@@ -846,6 +893,9 @@ int xbg_put_wave_records(xbg_handle* h, int slot, int first, int n, const void* 
     return h ? h->put_wave_records(slot, first, n, St, q) : XBG_ERR_ARG;
 }
 int xbg_mass(xbg_handle* h, double* w, double* s, double* b) { return h ? h->mass(w, s, b) : XBG_ERR_ARG; }
+int xbg_set_wave_forcing(xbg_handle* h, const void* const* f0, const void* const* f1, double w, int rescale) {
+    return (h && f0 && f1) ? h->set_forcing(f0, f1, w, rescale) : XBG_ERR_ARG;
+}
 
 int xbg_batch_create(const xbg_params* p, int n, int precision, xbg_batch** out) {
     if (!p || !out || n < 1 || n > XBG_MAX_BATCH || (precision != XBG_FP32 && precision != XBG_FP64))

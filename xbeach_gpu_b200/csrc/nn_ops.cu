@@ -270,6 +270,39 @@ __global__ void k_to_bf16(const float* __restrict__ a, bf* __restrict__ b, long 
     if (i < n) b[i] = __float2bfloat16(a[i]);
 }
 
+// x[p][c] = bf16((planes[c][p] - mean[c]) * inv_std[c]) (a NULL plane is 0)
+__global__ void k_encode(const float* const* __restrict__ planes, int nc, const float* __restrict__ mean,
+                         const float* __restrict__ inv_std, bf* __restrict__ x, long long P) {
+    long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+    if (idx >= P * nc) return;
+    const long long p = idx / nc;
+    const int c = (int)(idx % nc);
+    const float* pl = planes[c];
+    float v = pl ? (pl[p] - mean[c]) * inv_std[c] : 0.0f;
+    x[idx] = __float2bfloat16(v);
+}
+
+// dst[c][p] = hold[c][p] + out[p][c] * ys[c] + ym[c]
+__global__ void k_decode(const float* __restrict__ out, int ldo, const float* const* __restrict__ hold,
+                         const float* __restrict__ ym, const float* __restrict__ ys, float* const* __restrict__ dst,
+                         int nc, long long P) {
+    long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+    if (idx >= P * nc) return;
+    const int c = (int)(idx / P);
+    const long long p = idx % P;
+    dst[c][p] = hold[c][p] + out[p * ldo + c] * ys[c] + ym[c];
+}
+
+// dst[c][p] = src[c][p] (device arrays of nc plane pointers)
+__global__ void k_copy_planes(const float* const* __restrict__ src, float* const* __restrict__ dst, int nc,
+                              long long P) {
+    long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+    if (idx >= P * nc) return;
+    const int c = (int)(idx / P);
+    const long long p = idx % P;
+    dst[c][p] = src[c][p];
+}
+
 }  // namespace nn
 }  // namespace xbg
 
@@ -365,6 +398,26 @@ int xbg_nn_adam(float* p, void* pb, const float* g, float* m, float* v, long lon
     NN_LAUNCH(n);
     float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
     k_adam<<<blocks_for(n), TPB, 0, st_>>>(p, (bf*)pb, g, m, v, n, lr / bc1, b1, b2, eps, 1.0f / bc2);
+    NN_DONE;
+}
+int xbg_nn_encode(const float* const* planes, int nc, const float* mean, const float* inv_std, void* x, long long P,
+                  void* stream) {
+    if (!planes || !mean || !inv_std || !x || nc < 1 || P < 1) return XBG_ERR_ARG;
+    NN_LAUNCH(P * nc);
+    k_encode<<<blocks_for(P * nc), TPB, 0, st_>>>(planes, nc, mean, inv_std, (bf*)x, P);
+    NN_DONE;
+}
+int xbg_nn_decode(const float* out, int ldo, const float* const* hold, const float* ym, const float* ys,
+                  float* const* dst, int nc, long long P, void* stream) {
+    if (!out || !hold || !ym || !ys || !dst || nc < 1 || ldo < nc || P < 1) return XBG_ERR_ARG;
+    NN_LAUNCH(P * nc);
+    k_decode<<<blocks_for(P * nc), TPB, 0, st_>>>(out, ldo, hold, ym, ys, dst, nc, P);
+    NN_DONE;
+}
+int xbg_nn_copy_planes(const float* const* src, float* const* dst, int nc, long long P, void* stream) {
+    if (!src || !dst || nc < 1 || P < 1) return XBG_ERR_ARG;
+    NN_LAUNCH(P * nc);
+    k_copy_planes<<<blocks_for(P * nc), TPB, 0, st_>>>(src, dst, nc, P);
     NN_DONE;
 }
 int xbg_nn_to_bf16(const float* a, void* b, long long n, void* stream) {

@@ -86,6 +86,9 @@ def _bind_ops(L):
     L.xbg_nn_mse.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, vp]
     L.xbg_nn_adam.argtypes = [vp, vp, vp, vp, vp, ll, fl, fl, fl, fl, ip, vp]
     L.xbg_nn_to_bf16.argtypes = [vp, vp, ll, vp]
+    L.xbg_nn_encode.argtypes = [vp, ip, vp, vp, vp, ll, vp]
+    L.xbg_nn_decode.argtypes = [vp, ip, vp, vp, vp, vp, ip, ll, vp]
+    L.xbg_nn_copy_planes.argtypes = [vp, vp, ip, ll, vp]
 
 
 def _ok(rc, what):
