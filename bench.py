@@ -45,7 +45,7 @@ def parse():
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--ny", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="large", choices=["large", "ensemble"],
+    ap.add_argument("--workload", default="large", choices=["large", "ensemble", "surrogate"],
                     help="large: the 2048x1024 single domain (the headline line); ensemble: the batched "
                          "ragged ensemble (256 scenarios, one launch per kernel for all)")
     ap.add_argument("--scenarios", type=int, default=256)
@@ -307,6 +307,104 @@ def run_ensemble(args, rank, world, local):
     return out
 
 
+def run_surrogate(args, rank, world, local):
+    """The wave surrogate: train on snapshot pairs of plain runs, infer on a
+    1024 x 512 domain, and run the coupled step with the wave sub-steps from
+    the surrogate (judged by the plain solver every 50 steps, 2% H bar)
+    beside the plain step on the same held-out beach."""
+    import torch
+    from xbeach_gpu_b200 import surrogate_train as st
+    from xbeach_gpu_b200.surrogate import UNet
+    from xbeach_gpu_b200.surrogate_couple import SurrogateRun
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    train_d = st.collect(nx=512, ny=256, seeds=(0, 1, 2), Hs_list=(1.5, 2.5, 3.5), warm=300, every=15, count=12, k=10)
+    test_d = st.collect(nx=512, ny=256, seeds=(7,), Hs_list=(2.0,), warm=300, every=15, count=6, k=10)
+    t_collect = time.perf_counter() - t0
+    norm = st.Normalizer(train_d)
+    net = UNet(seed=0, base=32)
+    steps = max(200, args.steps * 3)
+    t0 = time.perf_counter()
+    hist = st.train(net, train_d, norm, steps=steps, batch=16, crop=128, lr=5e-4, log_every=max(1, steps // 6))
+    t_train = time.perf_counter() - t0
+    res, _ = st.evaluate(net, norm, test_d)
+    # useful FLOPs of one forward pass per pixel (3x3 convolutions, by level)
+    scale = {"e1a": 1, "e1b": 1, "d1a": 1, "d1b": 1, "head": 1, "e2a": 4, "e2b": 4, "d2a": 4, "d2b": 4,
+             "e3a": 16, "e3b": 16, "d3a": 16, "d3b": 16, "e4a": 64, "e4b": 64}
+    fwd_per_px = sum(2.0 * 9 * l.cin * l.cout / scale[n] for n, l in net.L.items())
+    xb, yb = next(st.batches(train_d, norm, 16, 128, np.random.default_rng(3)))
+    for _ in range(3):
+        net.train_step(xb, yb, 16, 128, 128)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        net.train_step(xb, yb, 16, 128, 128)
+    e1.record(); e1.synchronize()
+    train_ms = e0.elapsed_time(e1) / 10
+    train_tflops = 3 * fwd_per_px * 16 * 128 * 128 / (train_ms / 1e3) / 1e12
+    nyi, nxi = 512, 1024
+    xi = torch.zeros(nyi * nxi, xb.shape[1], dtype=torch.bfloat16, device="cuda")
+    for _ in range(3):
+        net.forward(xi, 1, nyi, nxi)
+    e0.record()
+    for _ in range(10):
+        net.forward(xi, 1, nyi, nxi)
+    e1.record(); e1.synchronize()
+    infer_ms = e0.elapsed_time(e1) / 10
+    infer_tflops = fwd_per_px * nyi * nxi / (infer_ms / 1e3) / 1e12
+    net.check()
+    # coupled: plain vs surrogate-assisted on a held-out 1024 x 512 beach
+    nsteps = 400
+
+    def timed(fn):   # CUDA events on the default stream around host-driven steps
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record(); e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    a, Tp = st.beach_model(2.2, seed=9, nx=1024, ny=512, warm=300)
+    b, _ = st.beach_model(2.2, seed=9, nx=1024, ny=512, warm=300)
+    c, _ = st.beach_model(2.2, seed=9, nx=1024, ny=512, warm=300)
+
+    def plain():
+        a.advance(nsteps); a.sync()
+    t_plain = timed(plain)
+    run = SurrogateRun(b, net, norm, Hs=2.2, Tp=Tp, k=10, judge_every=50, threshold=0.02)
+    t_judged = timed(lambda: run.advance(nsteps))
+    free = SurrogateRun(c, net, norm, Hs=2.2, Tp=Tp, k=10, judge_every=50, threshold=float("inf"))
+    t_sur = timed(lambda: free.advance(nsteps))
+    final = {f: st.rel_err(b.get(f), a.get(f)) for f in ("H", "zb", "zs")}
+    final_free = {f: st.rel_err(c.get(f), a.get(f)) for f in ("H", "zb", "zs")}
+    peak_tc = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_tc = float(json.load(f)["bf16_tflops"])
+    except Exception:
+        peak_tc = 1590.0
+    cells = 1024 * 512
+    return {
+        "metric": "coupled cell-updates/s", "value": cells * nsteps / t_sur, "unit": "cell-updates/s",
+        "impl": "surrogate", "n_gpus": world, "steps": nsteps, "higher_is_better": True, "dtype": "bf16/f32",
+        "data": "synthetic (plain-run snapshots of seeded barred beaches)",
+        "config": {"workload": "surrogate-assisted coupled step, 1024x512 barred beach, k=10, judge every 50 "
+                               "(value: judge without a bar, 80% surrogate steps)",
+                   "train_crops": "16 x 128 x 128", "net": "U-Net 4 levels, 32 base channels, 3x3"},
+        "plain_value": cells * nsteps / t_plain,
+        "speedup_vs_plain": t_plain / t_sur,
+        "unjudged_final_rel_err_vs_plain": final_free,
+        "judged_2pct": {"judged": run.judged, "fallback": run.fallback, "surrogate_steps": run.surrogate_steps,
+                        "value": cells * nsteps / t_judged, "final_rel_err_vs_plain": final},
+        "heldout_rel_err": res,
+        "train": {"steps": steps, "seconds": t_train, "loss": hist, "ms_per_step": train_ms,
+                  "achieved_tflops": train_tflops, "peak_tflops": peak_tc, "frac": train_tflops / peak_tc,
+                  "bound": "tensor"},
+        "infer_1024x512": {"ms": infer_ms, "achieved_tflops": infer_tflops, "frac": infer_tflops / peak_tc},
+        "collect_s": t_collect,
+    }
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -329,6 +427,14 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
+    if args.workload == "surrogate":
+        out = run_surrogate(args, rank, world, local) if rank == 0 else None
+        if out is not None:
+            print(json.dumps(out), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload == "ensemble":
         out = run_ensemble(args, rank, world, local)
         if dist:

@@ -22,6 +22,23 @@ IN_FIELDS = ["zb", "hh", "uu", "vv", "E", "R"]        # + Hm0, Tp planes
 OUT_FIELDS = ["E", "H", "D", "DR", "Fx", "Fy"]
 
 
+def beach_model(Hs, seed=5, nx=256, ny=128, warm=200):
+    """A plain FP32 model of a barred beach (seeded bathymetry, wave height
+    Hs) after `warm` coupled steps; returns (model, Tp)."""
+    from .abi import XBG_FP32
+    from .model import Model
+    from .scenarios import make_case, wave_group_boundary
+    p, zb, bnd = make_case("barred_beach", seed=seed, nx=nx, ny=ny)
+    St, q = wave_group_boundary(p, bnd["St"].shape[0], Hs, bnd["Tp"], 10 * np.pi / 180, seed=seed + 1)
+    m = Model(p, XBG_FP32)
+    m.set_wave_boundary(0, St, q, t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.init_state(zb, 0.0, 0.0)
+    m.advance(warm)
+    return m, bnd["Tp"]
+
+
 def collect(nx=512, ny=256, seeds=(0, 1), Hs_list=(1.5, 2.5), warm=300, every=20, count=10, k=10):
     """Run the plain model and return snapshots {x: [S, ny, nx, IN_CH],
     y: [S, ny, nx, 6] at t + k, hold: [S, ny, nx, 6] at t} (float32)."""
