@@ -28,7 +28,7 @@ template <class R> int launch_step_begin_batch(const BatchTab<R>&, const BatchLa
 template <class R> int launch_wavebnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_ubnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_means_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
-template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, cudaStream_t, Prof*);
+template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*);
 template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int ubnd_threads(const Konst<R>&);
@@ -664,7 +664,7 @@ struct Batch : public xbg_batch {
     int per_step = 0;
     int64_t nlaunch = 0;
     cudaError_t last_err = cudaSuccess;
-    int nt = 0, swave = 0, flow = 0, sedtrans = 0, roller = 0, means = 0;
+    int nt = 0, swave = 0, flow = 0, sedtrans = 0, roller = 0, means = 0, wci = 0;   // wci: any scenario with wave-current interaction
 
     ~Batch() override {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -687,6 +687,7 @@ struct Batch : public xbg_batch {
                        p.roller != roller || p.means != means) {
                 return XBG_ERR_ARG;   // one kernel sequence for the whole batch
             }
+            if (p.wci != 0.0) wci = 1;
             auto* hp = new Handle<R>();
             hs.push_back(hp);
             h.push_back(hp);
@@ -753,7 +754,7 @@ struct Batch : public xbg_batch {
         k += launch_step_begin_batch(T, L, st, pf);
         if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
         if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
-        if (swave == 1) k += launch_wave_batch(T, L, nt, roller, st, pf);
+        if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf);
         if (flow == 1) k += launch_flow_batch(T, L, st, pf);
         if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf);
         if (means) k += launch_means_batch(T, L, st, pf);

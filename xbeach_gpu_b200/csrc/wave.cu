@@ -414,7 +414,7 @@ __device__ __forceinline__ R theta_face(R em, R e0, R ep, R ep2, R c0, R cp) {
 
 constexpr int WT_NB = 3;   // plane tile buffers: plane t+1 streams in while t is used
 
-template <class R, bool ROLLER>
+template <class R, bool ROLLER, bool WCI>
 __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Clock* clk = S.clk;
@@ -428,7 +428,14 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
     R* sCos = sR + (size_t)nt * 256;      // [nt]
     R* sSin = sCos + nt;                  // [nt]
     R* sTh = sSin + nt;                   // [nt]
-    if (tid < nt) { sCos[tid] = K.cxsth[tid]; sSin[tid] = K.sxnth[tid]; sTh[tid] = K.theta[tid]; }
+    R* sC2 = sTh + nt;                    // [nt] cos^2, sin^2, sin cos of the bins
+    R* sS2 = sC2 + nt;
+    R* sCS = sS2 + nt;
+    if (tid < nt) {
+        const R c = K.cxsth[tid], sn = K.sxnth[tid];
+        sCos[tid] = c; sSin[tid] = sn; sTh[tid] = K.theta[tid];
+        sC2[tid] = c * c; sS2[tid] = sn * sn; sCS[tid] = sn * c;
+    }
     const int bx0 = bix * WT_X, by0 = 1 + biy * WT_Y;
     const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     const bool active = ix < nx && iy <= ny - 2;
@@ -491,6 +498,14 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
     CthCoef<R> cc{};
     R we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;   // bins t-1 .. t+2
     R c0 = 0, cpp = 0, Etmp = 0, cabs = 0, fte = 0, ftr = 0;
+    // ctheta of a bin (propagtheta); without wave-current interaction only the
+    // depth-refraction term remains: s (dhdx sin - dhdy cos)
+    R cthP = 0, cthQ = 0;
+    auto cth = [&](R cx, R sx) -> R {
+        if (WCI) return cth_eval(cc, cx, sx);
+        const R ctht = DM<R>::fma(cthP, sx, cthQ * cx);
+        return cmin(cmax(ctht, (R)(-0.25f * cc.sg)), (R)(0.25f * cc.sg));
+    };
     const bool own_bnd = ix == 0;
     auto own_e = [&](int t) -> R {
         R v = own_bnd ? St[iy + t * ny] * taper : ld(eeo + i + (size_t)t * C);
@@ -524,8 +539,9 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         we2 = own_e(0); we1 = we2; we3 = own_e(cl(1)); we4 = own_e(cl(2));
         wr2 = ld(rro + i); wr1 = wr2;
         wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
-        c0 = cth_eval(cc, sCos[0], sSin[0]);
-        cpp = cth_eval(cc, sCos[cl(1)], sSin[cl(1)]);
+        if (!WCI) { cthP = cc.s * cc.dhdx; cthQ = -(cc.s * cc.dhdy); }
+        c0 = cth(sCos[0], sSin[0]);
+        cpp = cth(sCos[cl(1)], sSin[cl(1)]);
     }
     // the cell's own bins ahead (window refill): plane min(t+3, nt-1)
     const R* wE = eeo + i + (size_t)min(3, nt - 1) * C;
@@ -581,7 +597,7 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
             we4 = DM<R>::fmax(own_bnd ? *wS * taper : ld(wE), (R)0);
             wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(wR);
             if (t + 4 <= nt - 1) { wE += C; wR += C; wS += ny; }
-            c0 = cpp; cpp = cth_eval(cc, sCos[t2], sSin[t2]);
+            c0 = cpp; cpp = cth(sCos[t2], sSin[t2]);
         }
     }
     R dtw = (R)3.0e38f;
@@ -624,20 +640,25 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         const R cc_i = cci;
         const R Dq = Dv / DM<R>::fmax(Eint, (R)0.0000001f);
         const R twogb = (R)2.0f * g * K.beta;
+        const R rcoef = twogb / cc_i;   // without wave-current interaction |c (cos, sin)| = c
         const bool wet = hh > K.eps;
         R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
-        R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0;
+        R ec = 0, es = 0, ecs = 0, rc = 0, rs = 0, rcs = 0;   // sums of cos^2, sin^2, sin cos times e / r
         R* pe_n = een + i;
         R* pr_n = rrn + i;
 #pragma unroll 2
         for (int t = 0; t < nt; t++) {
-            const R cx0 = sCos[t], sx0 = sSin[t];
             R eet = DM<R>::fmax(sA[t * 256 + tid], (R)0.0f) * ridiv;
             R rrt = sR[t * 256 + tid];
             const R dd = eet * Dq;
-            R cx = cc_i * cx0 + uui;
-            R cy = cc_i * sx0 + vvi;
-            R rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+            R rrd;
+            if (WCI) {
+                const R cx = cc_i * sCos[t] + uui;
+                const R cy = cc_i * sSin[t] + vvi;
+                rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+            } else {
+                rrd = rrt * rcoef;
+            }
             eet = wet ? DM<R>::fmax(eet - dtf * dd, (R)0.0f) : (R)0;
             rrt = wet ? DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f) : (R)0;
             drr = wet ? drr + rrd : (R)0;
@@ -646,12 +667,13 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
             pr_n[(size_t)t * C] = rrt;
             sume = sume + eet;
             sumethet = sumethet + eet * sTh[t];
-            txx = txx + (((R)1.0f + cx0 * cx0) * eet);
-            tyy = tyy + (((R)1.0f + sx0 * sx0) * eet);
-            txy = txy + (sx0 * cx0 * eet);
-            rxx = rxx + ((cx0 * cx0) * rrt);
-            ryy = ryy + ((sx0 * sx0) * rrt);
-            rxy = rxy + (sx0 * cx0 * rrt);
+            const R c2 = sC2[t], s2 = sS2[t], cs = sCS[t];
+            ec = DM<R>::fma(c2, eet, ec);
+            es = DM<R>::fma(s2, eet, es);
+            ecs = DM<R>::fma(cs, eet, ecs);
+            rc = DM<R>::fma(c2, rrt, rc);
+            rs = DM<R>::fma(s2, rrt, rs);
+            rcs = DM<R>::fma(cs, rrt, rcs);
         }
         const R sum2 = sume;
         sume = DM<R>::fmax(sume, (R)0.00001f);
@@ -662,22 +684,51 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         S.f[ROL][i] = RR * dth;
         S.f[DR][i] = drr * dth;
         const R n = cgi / cc_i;
-        S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
-        S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
-        S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
+        // radstress: sum (1 + cos^2) e = sum e + sum cos^2 e, ...
+        S.tmp[T_SXX][i] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
+        S.tmp[T_SYY][i] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
+        S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
     }
     block_min_store<R>(dtw, S.part_wave + bix + biy * ((K.nx + 31) / 32));
 }
-template <class R, bool ROLLER>
+template <class R, bool ROLLER, bool WCI>
 __global__ void __launch_bounds__(256, 3) k_wave_fast(Dev<R> S, Konst<R> K) {
-    b_wave_fast<R, ROLLER>(S, K, blockIdx.x, blockIdx.y);
+    b_wave_fast<R, ROLLER, WCI>(S, K, blockIdx.x, blockIdx.y);
 }
-template <class R, bool ROLLER>
+template <class R, bool ROLLER, bool WCI>
 __global__ void __launch_bounds__(256, 3) kb_wave_fast(BatchTab<R> T, const int2* items, int n) {
     batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux&, int bx, int by) {
-        b_wave_fast<R, ROLLER>(S, K, bx, by);
+        b_wave_fast<R, ROLLER, WCI>(S, K, bx, by);
     });
 }
+// the four variants (roller on/off, wave-current interaction on/off)
+template <class R>
+void launch_wave_fast(const Dev<R>& S, const Konst<R>& K, dim3 g, dim3 b, size_t smem, cudaStream_t st) {
+    const bool w = K.wci != (R)0;
+    if (K.roller == 1) {
+        if (w) k_wave_fast<R, true, true><<<g, b, smem, st>>>(S, K);
+        else k_wave_fast<R, true, false><<<g, b, smem, st>>>(S, K);
+    } else {
+        if (w) k_wave_fast<R, false, true><<<g, b, smem, st>>>(S, K);
+        else k_wave_fast<R, false, false><<<g, b, smem, st>>>(S, K);
+    }
+}
+template <class R>
+void launch_wave_fast_batch(const BatchTab<R>& T, const BatchLaunch& L, int roller, int wci, size_t smem,
+                            cudaStream_t st) {
+    dim3 b(32, 8);
+    const int g = L.grid[BS_WROWS], n = L.n[BS_WROWS];
+    const int2* it = L.items[BS_WROWS];
+    if (roller == 1) {
+        if (wci) kb_wave_fast<R, true, true><<<g, b, smem, st>>>(T, it, n);
+        else kb_wave_fast<R, true, false><<<g, b, smem, st>>>(T, it, n);
+    } else {
+        if (wci) kb_wave_fast<R, false, true><<<g, b, smem, st>>>(T, it, n);
+        else kb_wave_fast<R, false, false><<<g, b, smem, st>>>(T, it, n);
+    }
+}
+template <class R>
+size_t wave_fast_smem(int nt) { return ((size_t)2 * WT_NB * WT_N + (size_t)2 * nt * 256 + 6 * nt) * sizeof(R); }
 
 template <class R, int NMAX>
 __device__ __forceinline__ void b_wave_edge(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
@@ -814,9 +865,7 @@ int wave_parts(const Konst<R>& K) {
 template <class R, int NMAX>
 void launch_wave_main(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
-    size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
-    if (K.roller == 1) k_wave_fast<R, true><<<g, b, smem, st>>>(S, K);
-    else k_wave_fast<R, false><<<g, b, smem, st>>>(S, K);
+    launch_wave_fast(S, K, g, b, wave_fast_smem<R>(K.nt), st);
     PMARK(pf, "k_wave_fast");
     dim3 be(128), ge((K.nx + 127) / 128, 2);
     k_wave_edge<R, NMAX><<<ge, be, 0, st>>>(S, K);
@@ -845,44 +894,47 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
 // the wave kernels over every scenario of a batch (one ntheta and roller
 // setting for the whole batch)
 template <class R, int NMAX>
-void launch_wave_main_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, cudaStream_t st, Prof* pf) {
-    dim3 b(32, 8);
-    size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * nt * 256 + 3 * nt) * sizeof(R);
-    if (roller == 1) kb_wave_fast<R, true><<<L.grid[BS_WROWS], b, smem, st>>>(T, L.items[BS_WROWS], L.n[BS_WROWS]);
-    else kb_wave_fast<R, false><<<L.grid[BS_WROWS], b, smem, st>>>(T, L.items[BS_WROWS], L.n[BS_WROWS]);
+void launch_wave_main_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
+                            Prof* pf) {
+    launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
     PMARK(pf, "k_wave_fast");
     kb_wave_edge<R, NMAX><<<L.grid[BS_EDGE], 128, 0, st>>>(T, L.items[BS_EDGE], L.n[BS_EDGE]);
     PMARK(pf, "k_wave_edge");
 }
 
 template <class R>
-int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, cudaStream_t st, Prof* pf) {
+int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
+                      Prof* pf) {
     kb_disp<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
     PMARK(pf, "k_disp");
-    if (nt <= 4) launch_wave_main_batch<R, 4>(T, L, nt, roller, st, pf);
-    else if (nt <= 8) launch_wave_main_batch<R, 8>(T, L, nt, roller, st, pf);
-    else if (nt <= 12) launch_wave_main_batch<R, 12>(T, L, nt, roller, st, pf);
-    else if (nt <= 16) launch_wave_main_batch<R, 16>(T, L, nt, roller, st, pf);
-    else if (nt <= 20) launch_wave_main_batch<R, 20>(T, L, nt, roller, st, pf);
-    else if (nt <= 24) launch_wave_main_batch<R, 24>(T, L, nt, roller, st, pf);
-    else launch_wave_main_batch<R, 32>(T, L, nt, roller, st, pf);
+    if (nt <= 4) launch_wave_main_batch<R, 4>(T, L, nt, roller, wci, st, pf);
+    else if (nt <= 8) launch_wave_main_batch<R, 8>(T, L, nt, roller, wci, st, pf);
+    else if (nt <= 12) launch_wave_main_batch<R, 12>(T, L, nt, roller, wci, st, pf);
+    else if (nt <= 16) launch_wave_main_batch<R, 16>(T, L, nt, roller, wci, st, pf);
+    else if (nt <= 20) launch_wave_main_batch<R, 20>(T, L, nt, roller, wci, st, pf);
+    else if (nt <= 24) launch_wave_main_batch<R, 24>(T, L, nt, roller, wci, st, pf);
+    else launch_wave_main_batch<R, 32>(T, L, nt, roller, wci, st, pf);
     kb_wave_force<R><<<L.grid[BS_TILE], dim3(32, 8), 0, st>>>(T, L.items[BS_TILE], L.n[BS_TILE]);
     PMARK(pf, "k_wave_force");
     return 4;
 }
-template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, cudaStream_t, Prof*);
-template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, cudaStream_t, Prof*);
+template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*);
+template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*);
 
 // One-time kernel attributes (dynamic shared memory above 48 KB for wide
 // theta sets in FP64).
 template <class R>
 int wave_prepare(const Konst<R>& K) {
-    size_t smem = ((size_t)2 * WT_NB * WT_N + (size_t)2 * K.nt * 256 + 3 * K.nt) * sizeof(R);
-    cudaError_t e = cudaFuncSetAttribute(k_wave_fast<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaError_t e2 = cudaFuncSetAttribute(k_wave_fast<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaError_t e3 = cudaFuncSetAttribute(kb_wave_fast<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaError_t e4 = cudaFuncSetAttribute(kb_wave_fast<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return (e == cudaSuccess && e2 == cudaSuccess && e3 == cudaSuccess && e4 == cudaSuccess) ? 0 : 1;
+    const int smem = (int)wave_fast_smem<R>(K.nt);
+    const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    cudaError_t e[8] = {
+        cudaFuncSetAttribute(k_wave_fast<R, true, true>, a, smem), cudaFuncSetAttribute(k_wave_fast<R, true, false>, a, smem),
+        cudaFuncSetAttribute(k_wave_fast<R, false, true>, a, smem), cudaFuncSetAttribute(k_wave_fast<R, false, false>, a, smem),
+        cudaFuncSetAttribute(kb_wave_fast<R, true, true>, a, smem), cudaFuncSetAttribute(kb_wave_fast<R, true, false>, a, smem),
+        cudaFuncSetAttribute(kb_wave_fast<R, false, true>, a, smem), cudaFuncSetAttribute(kb_wave_fast<R, false, false>, a, smem)};
+    for (auto x : e)
+        if (x != cudaSuccess) return 1;
+    return 0;
 }
 template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);
