@@ -241,8 +241,8 @@ int  xbg_batch_get_stream(xbg_batch* b, void** stream);
 int  xbg_batch_profile_step(xbg_batch* b, float* ms, const char** names,
                             int* n);
 /* Persistent blocks of the launches of one tile shape (0: 32x8 tiles,
- * 1: wave rows, 2: 256-cell runs, 3: lateral rows, 4: one block per
- * scenario, 5: boundary values, 6: dt reduction); used by the autotuner. */
+ * 1: wave rows, 2: 256-cell runs, 3: one block per scenario, 4: boundary
+ * values, 5: dt reduction); used by the autotuner. */
 int  xbg_batch_set_grid(xbg_batch* b, int shape, int blocks);
 int  xbg_batch_launch_count(xbg_batch* b, int64_t* count);
 

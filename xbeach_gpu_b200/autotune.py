@@ -21,7 +21,7 @@ SHAPES = {
                  "k_flow_final", "k_sed_a", "k_sed_b", "k_sed_c"}),
     1: ("wave_rows", {"k_wave_fast"}),
     2: ("lin", {"k_disp", "k_means"}),
-    6: ("dt", {"k_step_begin"}),
+    5: ("dt", {"k_step_begin"}),
 }
 FACTORS = (1, 2, 3, 4, 6, 8, 12, 16)
 

@@ -14,7 +14,7 @@
 #include "../../include/xbg.h"
 
 namespace xbg {
-template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t);
 template <class R> int wave_parts(const Konst<R>&);
 template <class R> int wave_prepare(const Konst<R>&);
 template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
@@ -28,7 +28,8 @@ template <class R> int launch_step_begin_batch(const BatchTab<R>&, const BatchLa
 template <class R> int launch_wavebnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_ubnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_means_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
-template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*);
+template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
+                                         cudaEvent_t);
 template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int ubnd_threads(const Konst<R>&);
@@ -213,6 +214,8 @@ struct Handle : public xbg_handle {
     size_t slot_cap = 0;        // elements of St per slot
     std::vector<void*> allocs;
     cudaStream_t st = nullptr;
+    cudaStream_t side = nullptr;          // the boundary kernels' branch of the step graph
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     int per_step_launches = 0;
@@ -237,6 +240,9 @@ struct Handle : public xbg_handle {
         if (nx < 4 || ny < 4 || nt < 1 || nt > XBG_MAX_THETA) return XBG_ERR_ARG;
         size_t C = (size_t)nx * ny;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         std::memset(&S, 0, sizeof(S));
         S.nx = nx; S.ny = ny; S.nt = nt; S.C = (int)C;
         int rc;
@@ -248,7 +254,7 @@ struct Handle : public xbg_handle {
                 return rc;
             S.ee[k] = ee_buf[k]; S.rr[k] = rr_buf[k]; S.zsold[k] = zsold_buf[k];
         }
-        if ((rc = alloc(&S.edge, (size_t)4 * nx * nt)) || (rc = alloc(&S.St, (size_t)ny * nt))) return rc;
+        if ((rc = alloc(&S.St, (size_t)ny * nt))) return rc;
         // K
         std::memset(&K, 0, sizeof(K));
         K.nx = nx; K.ny = ny; K.nt = nt;
@@ -311,6 +317,9 @@ struct Handle : public xbg_handle {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
         for (void* p : allocs) cudaFree(p);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (st) cudaStreamDestroy(st);
     }
 
@@ -515,13 +524,25 @@ struct Handle : public xbg_handle {
         if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
     }
 
-    // one coupled step: the body of mainloopGPU (Wave_gpu.cu:620-757)
+    // one coupled step: the body of mainloopGPU (Wave_gpu.cu:620-757).  In
+    // the step graph the boundary kernels (St in time, ubnd1D) form a branch
+    // beside the dispersion kernel, which reads neither's outputs; the rows
+    // pass joins it.  A profiled step runs every kernel in order.
     int enqueue_step(Prof* pf = nullptr) {
         int n = 0;
         n += launch_step_begin(S, K, ser, nwave, st, pf);
-        if (K.swave == 1) n += launch_wavebnd(S, K, ser, st, pf, 0);
-        if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
-        if (K.swave == 1) n += launch_wave(S, K, st, pf);
+        if (K.swave == 1 && !pf) {
+            cudaEventRecord(ev_fork, st);
+            cudaStreamWaitEvent(side, ev_fork, 0);
+            n += launch_wavebnd(S, K, ser, side, nullptr, 0);
+            if (K.flow == 1) n += launch_ubnd(S, K, ser, side, nullptr);
+            cudaEventRecord(ev_join, side);
+            n += launch_wave(S, K, st, nullptr, ev_join);
+        } else {
+            if (K.swave == 1) n += launch_wavebnd(S, K, ser, st, pf, 0);
+            if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
+            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr);
+        }
         if (K.flow == 1) n += launch_flow(S, K, st, pf);
         if (P.sedtrans == 1) n += launch_sed(S, K, st, pf);
         if (K.means) n += launch_means(S, K, st, pf);
@@ -566,7 +587,7 @@ struct Handle : public xbg_handle {
             case 0: n = launch_step_begin(S, K, ser, nwave, st, nullptr); break;
             case 1: if (K.swave == 1) n = launch_wavebnd(S, K, ser, st, nullptr, 1); break;
             case 2: if (K.flow == 1) n = launch_ubnd(S, K, ser, st, nullptr); break;
-            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr); break;
+            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr); break;
             case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr); break;
             case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr); break;
             case 6: n = launch_means(S, K, st, nullptr); break;
@@ -659,6 +680,8 @@ struct Batch : public xbg_batch {
     std::vector<Dev<R>> hS;
     std::vector<cudaEvent_t> evs;
     cudaStream_t st = nullptr;
+    cudaStream_t side = nullptr;          // the boundary kernels' branch of the step graph
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
     int per_step = 0;
@@ -673,12 +696,18 @@ struct Batch : public xbg_batch {
         cudaFree(dS); cudaFree(dK); cudaFree(dA); cudaFree(dclk);
         for (int k = 0; k < BS_N; k++) cudaFree(ditems[k]);
         for (auto p : hs) delete p;
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (st) cudaStreamDestroy(st);
     }
 
     int setup(const xbg_params* ps, int ns, int prec) {
         n = ns;
         CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+        CK(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
         for (int s = 0; s < ns; s++) {
             const xbg_params& p = ps[s];
             if (s == 0) {
@@ -716,8 +745,6 @@ struct Batch : public xbg_batch {
             for (int by = 0; by < (ny - 2 + 7) / 8; by++)
                 for (int bx = 0; bx < (nx + 31) / 32; bx++) add(BS_WROWS, bx, by);
             for (int b = 0; b < (C + 255) / 256; b++) add(BS_LIN, b, 0);
-            for (int r = 0; r < 2; r++)
-                for (int b = 0; b < (nx + 127) / 128; b++) add(BS_EDGE, b, r);
             add(BS_ONE, 0, 0);
             for (int b = 0; b < (ny * nt + 255) / 256; b++) add(BS_BND, b, 0);
             for (int b = 0; b < hA[s].nflow; b++) add(BS_DT, b, 0);
@@ -732,7 +759,7 @@ struct Batch : public xbg_batch {
         int dev = 0, sms = 148;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const int per_sm[BS_N] = {8, 3, 8, 8, 2, 8, 8};   // resident-block targets per SM
+        const int per_sm[BS_N] = {8, 3, 8, 2, 8, 8};   // resident-block targets per SM
         for (int k = 0; k < BS_N; k++) {
             CK(cudaMalloc(&ditems[k], std::max<size_t>(1, it[k].size()) * sizeof(int2)));
             CK(cudaMemcpy(ditems[k], it[k].data(), it[k].size() * sizeof(int2), cudaMemcpyHostToDevice));
@@ -752,9 +779,18 @@ struct Batch : public xbg_batch {
         BatchTab<R> T = tab();
         int k = 0;
         k += launch_step_begin_batch(T, L, st, pf);
-        if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
-        if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
-        if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf);
+        if (swave == 1 && !pf) {   // the boundary kernels beside the dispersion kernel, as for one handle
+            cudaEventRecord(ev_fork, st);
+            cudaStreamWaitEvent(side, ev_fork, 0);
+            k += launch_wavebnd_batch(T, L, side, nullptr);
+            if (flow == 1) k += launch_ubnd_batch(T, L, side, nullptr);
+            cudaEventRecord(ev_join, side);
+            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join);
+        } else {
+            if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
+            if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
+            if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr);
+        }
         if (flow == 1) k += launch_flow_batch(T, L, st, pf);
         if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf);
         if (means) k += launch_means_batch(T, L, st, pf);

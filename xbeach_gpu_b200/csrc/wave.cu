@@ -12,26 +12,14 @@
 //                one bin ahead (three buffers, one barrier per bin); ctheta
 //                (propagtheta) is evaluated on the fly from per-cell slopes;
 //                the theta-face flux is computed once and carried to the
-//                next bin.  Emits the per-block WAVEDT minimum.
-//   k_wave_edge  rows 0 and ny-1, whose ee/rr are copies of rows 1 / ny-2
-//                (rollerlatbnd, wave_CPU.cpp:830-870) between the passes.
+//                next bin.  The threads of rows 1 and ny-2 then also
+//                finish rows 0 and ny-1, whose ee/rr are copies of theirs
+//                (rollerlatbnd, wave_CPU.cpp:830-870) around the
+//                dissipation.  Emits the per-block WAVEDT minimum.
 //   k_wave_force wavforce + twodimbnd(noix) + breakerdelay + twodimbnd(ust).
 #include "xbg_common.cuh"
 
 namespace xbg {
-
-// ---------------------------------------------------------------- helpers
-// (R)(1.5*(double)a - 0.5*(double)b): one rounding of the exact value, as the
-// double literals of xadvecupwind2CPU give (wave_CPU.cpp:426-453).
-template <class R> __device__ __forceinline__ R up2d(R a, R b) {
-    return DM<R>::fma((R)1.5, a, (R)-0.5 * b);
-}
-// 1.5f*a - 0.5f*b with two roundings (thetaadvecuw2hoCPU, wave_CPU.cpp:747-790).
-template <class R> __device__ __forceinline__ R up2f(R a, R b) {
-    R x = (R)1.5f * a;
-    R y = (R)0.5f * b;
-    return x - y;
-}
 
 // dispersion relation, wave_CPU.cpp:154-205 (golden-ratio relaxation)
 template <class R>
@@ -110,238 +98,6 @@ __device__ __forceinline__ R cth_eval(const CthCoef<R>& c, R cx, R sx) {
     return cmin(cmax(ctht, (R)(-0.25f * c.sg)), (R)(0.25f * c.sg));
 }
 
-// x/y second-order upwind fluxes of one theta plane, xadvecupwind2CPU /
-// yadvecupwind2CPU (wave_CPU.cpp:367-560).  q(-2..2) are the plane's values at
-// the clamped neighbours mminus2, mminus, i, pplus, pplus2.
-template <class R>
-__device__ __forceinline__ R adv2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin, R dxplus_i) {
-    R arrin, arrmin;
-    if (cf > (R)0.0f) {
-        arrin = up2d(qi, qm);
-        if (arrin < (R)0.0f) arrin = qi;
-        arrin = arrin * cf;
-    } else {
-        arrin = up2d(qp, qp2);
-        if (arrin < (R)0.0f) arrin = qp;
-        arrin = arrin * cf;
-    }
-    if (cfmin > (R)0.0f) {
-        arrmin = up2d(qm, qm2);
-        if (arrmin < (R)0.0f) arrmin = qm;
-        arrmin = arrmin * cfmin;
-    } else {
-        arrmin = up2d(qi, qp);
-        if (arrmin < (R)0.0f) arrmin = qi;
-        arrmin = arrmin * cfmin;
-    }
-    return (arrin - arrmin) * dxplus_i;
-}
-
-// Advected field of one cell: q_new[t] = q[t] - dt*(xadv + yadv + thetaadv).
-// loadq(ix, iy, t) returns the (transformed) plane value at a grid point.
-template <class R, int NMAX, class LoadQ>
-__device__ __forceinline__ void advect_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy,
-                                            const R* speed, const R* cthv, LoadQ loadq, R dtf,
-                                            R* out) {
-    const int nx = K.nx, ny = K.ny, nt = K.nt;
-    int i = ix + iy * nx;
-    int xm = mm(ix), xp = pp(ix, nx), xm2 = mm2(ix), xp2 = pp2(ix, nx);
-    int ym = mm(iy), yp = pp(iy, ny), ym2 = mm2(iy), yp2 = pp2(iy, ny);
-    R dxplus_i = (R)1.0f / K.dx;
-    R wci = K.wci * cmin(ld(S.f[HH] + i) / K.hwci, (R)1.0f);
-    R ccg = ld(speed + i);
-    R ccgxmin = ld(speed + xm + iy * nx), ccgxmax = ld(speed + xp + iy * nx);
-    R ccgymin = ld(speed + ix + ym * nx), ccgymax = ld(speed + ix + yp * nx);
-    const R* uu = S.f[UU]; const R* vv = S.f[VV];
-    R uui = ld(uu + i) * wci;
-    R uuixmin = ld(uu + xm + iy * nx) * wci;
-    R uuixmax = ld(uu + xp + iy * nx) * wci;
-    R vvi = wci * ld(vv + i);
-    R vviymin = wci * ld(vv + ix + ym * nx);
-    R vviymax = wci * ld(vv + ix + yp * nx);
-    R own[NMAX];
-#pragma unroll
-    for (int t = 0; t < NMAX; t++) own[t] = (t < nt) ? loadq(ix, iy, t) : (R)0;
-    R dth = K.dtheta;
-#pragma unroll
-    for (int t = 0; t < NMAX; t++) {
-        if (t < nt) {
-            R ct = K.cxsth[t], st = K.sxnth[t];
-            R cgx = (R)0.5f * (ccg * ct + uui + ccgxmax * ct + uuixmax);
-            R cgxmin = (R)0.5f * (ccg * ct + uui + ccgxmin * ct + uuixmin);
-            R xa = adv2(loadq(xm2, iy, t), loadq(xm, iy, t), own[t], loadq(xp, iy, t), loadq(xp2, iy, t),
-                        cgx, cgxmin, dxplus_i);
-            R cgy = (R)0.5f * (ccg * st + vvi + ccgymax * st + vviymax);
-            R cgymin = (R)0.5f * (ccg * st + vvi + ccgymin * st + vviymin);
-            R ya = adv2(loadq(ix, ym2, t), loadq(ix, ym, t), own[t], loadq(ix, yp, t), loadq(ix, yp2, t),
-                        cgy, cgymin, dxplus_i);
-            // thetaadvecuw2hoCPU (wave_CPU.cpp:706-806) with clamped bins
-            R ta = (R)0.0f;
-            if (nt > 1) {
-                const int tm = t > 0 ? t - 1 : 0;
-                const int tm2 = t > 1 ? t - 2 : 0;
-                const int t1 = (t + 1 < NMAX) ? t + 1 : t;
-                const int t2 = (t + 2 < NMAX) ? t + 2 : t1;
-                R e_p = (t + 1 < nt) ? own[t1] : own[t];
-                R e_p2 = (t + 2 < nt) ? own[t2] : e_p;
-                R c_p = (t + 1 < nt) ? cthv[t1] : cthv[t];
-                R cthetab = (R)0.5f * (cthv[t] + c_p);
-                R eupw;
-                if (cthetab > (R)0.0f) {
-                    eupw = up2f(own[t], own[tm]);
-                    if (eupw < (R)0.0f) eupw = own[t];
-                } else {
-                    eupw = up2f(e_p, e_p2);
-                    if (eupw < (R)0.0f) eupw = e_p;
-                }
-                R arrint = cthetab * eupw;
-                cthetab = (R)0.5f * (cthv[tm] + cthv[t]);
-                if (cthetab > (R)0.0f) {
-                    eupw = up2f(own[tm], own[tm2]);
-                    if (eupw < (R)0.0f) eupw = own[tm];
-                } else {
-                    eupw = up2f(own[t], e_p);
-                    if (eupw < (R)0.0f) eupw = own[t];
-                }
-                R arrmint = cthetab * eupw;
-                ta = (arrint - arrmint) / dth;
-                if (t == nt - 1) ta = ((R)0.0f - arrmint) / dth;
-                if (t == 0) ta = (arrint - (R)0.0f) / dth;
-            }
-            out[t] = own[t] - dtf * (xa + ya + ta);
-        } else {
-            out[t] = (R)0;
-        }
-    }
-}
-
-// Per-cell chain after advection: energy, energint, roelvink|baldock and
-// dissipation (wave_CPU.cpp:873-1092).  e (advected ee with the row copy
-// applied) and r (rr before dissipation) are updated in place.
-template <class R>
-struct CellOut { R E, H, D, R_, DR; };
-
-template <class R, int NMAX>
-__device__ __forceinline__ CellOut<R> chain_cell(const Dev<R>& S, const Konst<R>& K, int i, R sg, R dtf,
-                                                 R Trep, R* e, R* r) {
-    const int nt = K.nt;
-    R rho = K.rho, g = K.g, dth = K.dtheta;
-    R hh = ld(S.f[HH] + i);
-    CellOut<R> o;
-    // energyCPU
-#pragma unroll
-    for (int t = 0; t < NMAX; t++)
-        if (t < nt) e[t] = cmax(e[t], (R)0.0f);   // advected ee arrive in energy units
-    // energintCPU
-    R Etmp = (R)0.0f;
-#pragma unroll
-    for (int t = 0; t < NMAX; t++)
-        if (t < nt) Etmp = Etmp + e[t];
-    Etmp = Etmp * dth;
-    R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
-    R idiv = cmax((R)1.0f, DM<R>::pow(Htmp / (K.gammax * hh), (R)2.0f));
-#pragma unroll
-    for (int t = 0; t < NMAX; t++)
-        if (t < nt) e[t] = e[t] / idiv;
-    Htmp = cmin(Htmp, K.gammax * hh);
-    R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
-    R k = ld(S.f[WK] + i);
-    R fw = ld(S.f[FWM] + i);
-    R Dv;
-    if (K.breakmodel == 1) {
-        // roelvinkCPU (wave_CPU.cpp:927-985): double arithmetic as there
-        R fac = (R)(8.0 / (double)rho / (double)g);
-        R Ht = DM<R>::sqrt(Eint * fac);
-        R Qb = (R)(1.0 - ::exp(cmax(-1.0 * (double)DM<R>::pow((Ht / K.gammaa / hh), K.nexp), -100.0)));
-        Qb = cmin(Qb, (R)1.0f);
-        Dv = (R)((double)Qb * 2.0 * (double)K.alpha / (double)Trep * (double)Eint * (double)Ht / (double)hh);
-        R uorb = (R)(XBG_PI * (double)Ht / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
-        Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
-                                  (double)uorb * (double)uorb);
-    } else {
-        // baldockCPU (wave_CPU.cpp:987-1028)
-        R khh = k * hh;
-        R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
-        R Rr = Hb / cmax(Htmp, (R)0.00001f);
-        R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
-        Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
-        R uorb = (R)(XBG_PI * (double)Htmp / (double)(Trep * DM<R>::sinh(cmin(k * hh, (R)10.0f))));
-        Dv = (R)((double)Dv + (double)0.66666666f / XBG_PI * (double)rho * (double)fw * (double)uorb *
-                                  (double)uorb * (double)uorb);
-    }
-    // dissipationCPU (wave_CPU.cpp:1030-1092)
-    R wci = K.wci * cmin(hh / K.hwci, (R)1.0f);
-    R cc = ld(S.f[CC_] + i);
-    R uui = ld(S.f[UU] + i) * wci, vvi = ld(S.f[VV] + i) * wci;
-    R RR = (R)0.0f, drr = (R)0.0f;
-    R Emax = cmax(Eint, (R)0.0000001f);
-    bool wet = hh > K.eps;
-#pragma unroll
-    for (int t = 0; t < NMAX; t++) {
-        if (t < nt) {
-            R cx = cc * K.cxsth[t] + uui;
-            R cy = cc * K.sxnth[t] + vvi;
-            R eet = e[t];
-            R dd = eet * Dv / Emax;
-            R rrt;
-            if (wet) {
-                rrt = r[t];
-                R rrd = (R)2.0f * g * K.beta * rrt / DM<R>::sqrt(cx * cx + cy * cy);
-                eet = cmax(eet - dtf * dd, (R)0.0f);
-                rrt = cmax(rrt + dtf * (dd - rrd), (R)0.0f);
-                drr = drr + rrd;
-            } else {
-                eet = (R)0.0f; rrt = (R)0.0f; drr = (R)0.0f;
-            }
-            RR = RR + rrt;
-            e[t] = eet;
-            r[t] = rrt;
-        }
-    }
-    o.E = Eint; o.H = Htmp; o.D = Dv; o.R_ = RR * dth; o.DR = drr * dth;
-    return o;
-}
-
-// meandir + radstress (wave_CPU.cpp:1095-1162) of the final ee (e) and rr (r);
-// writes everything a cell owns at the end of the wave pass.
-template <class R, int NMAX>
-__device__ __forceinline__ void finish_cell(const Dev<R>& S, const Konst<R>& K, int i, const R* e,
-                                            const R* r, const CellOut<R>& o, R* een, R* rrn) {
-    const int nt = K.nt, C = S.C;
-    R rho = K.rho, g = K.g, dth = K.dtheta;
-    R sume = (R)0, sumethet = (R)0;
-    R txx = 0, txy = 0, tyy = 0, rxx = 0, rxy = 0, ryy = 0, sum2 = 0;
-#pragma unroll
-    for (int t = 0; t < NMAX; t++) {
-        if (t < nt) {
-            R et = e[t], rt = r[t];
-            R cx = K.cxsth[t], sx = K.sxnth[t];
-            sume = sume + et;
-            sumethet = sumethet + et * K.theta[t];
-            sum2 = sum2 + et;
-            txx = txx + (((R)1.0f + cx * cx) * et);
-            tyy = tyy + (((R)1.0f + sx * sx) * et);
-            txy = txy + (sx * cx * et);
-            rxx = rxx + ((cx * cx) * rt);
-            ryy = ryy + ((sx * sx) * rt);
-            rxy = rxy + (sx * cx * rt);
-            een[i + (size_t)t * C] = et;
-            rrn[i + (size_t)t * C] = rt;
-        }
-    }
-    sume = cmax(sume, (R)0.00001f);
-    S.f[THM][i] = (sumethet / (R)nt) / (sume / (R)nt);
-    S.f[E][i] = sume * dth;
-    S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
-    S.f[D][i] = o.D;
-    S.f[ROL][i] = o.R_;
-    S.f[DR][i] = o.DR;
-    R n = ld(S.f[CG] + i) / ld(S.f[CC_] + i);
-    S.tmp[T_SXX][i] = (n * txx - (R)0.5f * sum2) * dth + rxx * dth;
-    S.tmp[T_SYY][i] = (n * tyy - (R)0.5f * sum2) * dth + ryy * dth;
-    S.tmp[T_SXY][i] = n * txy * dth + rxy * dth;
-}
-
 template <class R>
 __device__ __forceinline__ void block_min_store(R v, R* dst) {
     // warp shuffle, then one value per warp through shared memory
@@ -356,23 +112,6 @@ __device__ __forceinline__ void block_min_store(R v, R* dst) {
         for (int o = 16; o > 0; o >>= 1) m = DM<R>::fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
         if (tid == 0) *dst = m;
     }
-}
-
-// ctheta of every bin of a cell and WAVEDT (Wave_kernel.cu:232-249):
-// min over theta of cfl*dtheta/|ctheta|.
-template <class R, int NMAX>
-__device__ __forceinline__ R ctheta_cell(const Konst<R>& K, const CthCoef<R>& cc, R* cthv) {
-    R mindt = (R)9999999.9f;
-#pragma unroll
-    for (int t = 0; t < NMAX; t++) {
-        if (t < K.nt) {
-            cthv[t] = cth_eval(cc, K.cxsth[t], K.sxnth[t]);
-            mindt = DM<R>::fmin(K.cfl * K.dtheta / DM<R>::fabs(cthv[t]), mindt);
-        } else {
-            cthv[t] = (R)0;
-        }
-    }
-    return mindt;
 }
 
 #define WT_X 32
@@ -396,20 +135,156 @@ __device__ __forceinline__ R upw(R a, R b) {   // 1.5a - 0.5b, first-order fallb
     R v = DM<R>::fma((R)1.5, a, (R)-0.5 * b);
     return v < (R)0 ? a : v;
 }
+// The upwind side is chosen first and one extrapolation evaluated (the same
+// value as evaluating both sides and selecting).
 template <class R>
 __device__ __forceinline__ R flux2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin) {
-    R arrin = (cf > (R)0 ? upw(qi, qm) : upw(qp, qp2)) * cf;
-    R arrmin = (cfmin > (R)0 ? upw(qm, qm2) : upw(qi, qp)) * cfmin;
+    const bool pin = cf > (R)0, pmin = cfmin > (R)0;
+    const R arrin = upw(pin ? qi : qp, pin ? qm : qp2) * cf;
+    const R arrmin = upw(pmin ? qm : qi, pmin ? qm2 : qp) * cfmin;
     return arrin - arrmin;
 }
 // theta-face flux between bins t and t+1 (the arrint of bin t, which is the
 // arrmint of bin t+1): e(t-1), e(t), e(t+1), e(t+2), ctheta(t), ctheta(t+1)
 template <class R>
 __device__ __forceinline__ R theta_face(R em, R e0, R ep, R ep2, R c0, R cp) {
-    R cb = (R)0.5f * (c0 + cp);
-    R u1 = (R)1.5f * e0 - (R)0.5f * em;   u1 = u1 < (R)0 ? e0 : u1;
-    R u2 = (R)1.5f * ep - (R)0.5f * ep2;  u2 = u2 < (R)0 ? ep : u2;
-    return cb * (cb > (R)0 ? u1 : u2);
+    const R cb = (R)0.5f * (c0 + cp);
+    const bool p = cb > (R)0;
+    const R a = p ? e0 : ep, b = p ? em : ep2;
+    R u = (R)1.5f * a - (R)0.5f * b;
+    u = u < (R)0 ? a : u;
+    return cb * u;
+}
+
+// Direction tables of the bins in shared memory: (cos, sin) and
+// (cos^2, sin^2, sin cos, theta), one vector load each.
+template <class R> struct alignas(2 * sizeof(R)) Dir2 { R c, s; };
+template <class R> struct alignas(4 * sizeof(R)) Dir4 { R c2, s2, cs, th; };
+
+// energint + roelvink|baldock (wave_CPU.cpp:873-1028) of one cell from the sum
+// over bins of its sanitised advected ee: 1/idiv, Dv and Dv / max(Eint, 1e-7).
+template <class R>
+__device__ __forceinline__ void wave_breaking(const Konst<R>& K, R esum, R hh, R k, R fw, R Trep, R& ridiv, R& Dv,
+                                              R& Dq) {
+    const R rho = K.rho, g = K.g;
+    const R Etmp = esum * K.dtheta;
+    R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
+    const R hr = Htmp / (K.gammax * hh);
+    const R idiv = DM<R>::fmax((R)1.0f, hr * hr);
+    ridiv = (R)1 / idiv;
+    Htmp = DM<R>::fmin(Htmp, K.gammax * hh);
+    const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
+    if (K.breakmodel == 1) {   // roelvinkCPU
+        R Ht = DM<R>::sqrt(Eint * (R)(8.0 / (double)rho / (double)g));
+        R x = Ht / K.gammaa / hh;
+        R Qb = (R)1 - DM<R>::exp(DM<R>::fmax(-DM<R>::pow(x, K.nexp), (R)-100));
+        Qb = DM<R>::fmin(Qb, (R)1.0f);
+        Dv = Qb * (R)2 * K.alpha / Trep * Eint * Ht / hh;
+        R uorb = (R)XBG_PI * Ht / (Trep * DM<R>::sinh(DM<R>::fmin(k * hh, (R)10.0f)));
+        Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
+    } else {                   // baldockCPU
+        R khh = k * hh;
+        R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
+        R Rr = Hb / DM<R>::fmax(Htmp, (R)0.00001f);
+        R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
+        Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
+        R uorb = (R)XBG_PI * Htmp / (Trep * DM<R>::sinh(DM<R>::fmin(k * hh, (R)10.0f)));
+        Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
+    }
+    Dq = Dv / DM<R>::fmax(Eint, (R)0.0000001f);
+}
+
+// Row 0 or ny-1 (iyE), the lateral copy of row iyS = 1 or ny-2
+// (rollerlatbnd, wave_CPU.cpp:830-870, around dissipationCPU): its advected
+// ee and rr are the source row's times the wet mask, breaking and roller
+// dissipation run with the edge cell's own depth and speeds, and after
+// dissipation its ee is again the source row's (final) ee times the mask.
+// Run by the thread of the source cell, which holds the advected bins in
+// sA / sR and has already written the source cell's final ee.  Returns the
+// edge cell's WAVEDT.
+template <class R, bool ROLLER, bool WCI>
+__device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iyE, int iyS,
+                                            const R* sA, const R* sR, const Dir2<R>* sCS2, const Dir4<R>* sMom,
+                                            R esum, R sg, R dtf, R Trep, const R* rro, R* een, R* rrn) {
+    const int nx = K.nx, nt = K.nt, C = S.C;
+    const int ie = ix + iyE * nx, is = ix + iyS * nx;
+    const R dth = K.dtheta, rho = K.rho, g = K.g;
+    const R hE = ld(S.f[HH] + ie);
+    const bool wet = hE > K.eps;
+    const R w = wet ? (R)1.0f : (R)0.0f;
+    // WAVEDT: cfl*dtheta over the largest |ctheta| of the edge cell's bins
+    const CthCoef<R> ce = cth_coef(S, K, ix, iyE, sg);
+    const R P = ce.s * ce.dhdx, Q = -(ce.s * ce.dhdy);
+    R cab = (R)0;
+    for (int t = 0; t < nt; t++) {
+        const Dir2<R> d = sCS2[t];
+        R c;
+        if (WCI) c = cth_eval(ce, d.c, d.s);
+        else c = cmin(cmax(DM<R>::fma(P, d.s, Q * d.c), (R)(-0.25f * ce.sg)), (R)(0.25f * ce.sg));
+        cab = DM<R>::fmax(cab, DM<R>::fabs(c));
+    }
+    const R dtw = DM<R>::fmin(K.cfl * dth / cab, (R)9999999.9f);
+    // sum of max(A * w, 0) over the bins: the source's sum, or 0 when dry
+    R ridiv, Dv, Dq;
+    wave_breaking(K, wet ? esum : (R)0, hE, ld(S.f[WK] + ie), ld(S.f[FWM] + ie), Trep, ridiv, Dv, Dq);
+    const R cE = ld(S.f[CC_] + ie);
+    const R twogb = (R)2.0f * g * K.beta;
+    R uE = (R)0, vE = (R)0;
+    if (WCI) {
+        const R wc = K.wci * cmin(hE / K.hwci, (R)1.0f);
+        uE = ld(S.f[UU] + ie) * wc;
+        vE = wc * ld(S.f[VV] + ie);
+    }
+    const R rcoef = twogb / cE;
+    const int tid = threadIdx.x + threadIdx.y * WT_X;
+    R RR = (R)0, drr = (R)0, rc = (R)0, rs = (R)0, rcs = (R)0;
+    for (int t = 0; t < nt; t++) {
+        const R eet = DM<R>::fmax(sA[t * 256 + tid] * w, (R)0.0f) * ridiv;
+        R rrt = ROLLER ? sR[t * 256 + tid] * w : ld(rro + ie + (size_t)t * C);
+        const R dd = eet * Dq;
+        R rrd;
+        if (WCI) {
+            const Dir2<R> d = sCS2[t];
+            const R cx = cE * d.c + uE, cy = cE * d.s + vE;
+            rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+        } else {
+            rrd = rrt * rcoef;
+        }
+        rrt = wet ? DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f) : (R)0;
+        drr = wet ? drr + rrd : (R)0;
+        RR = RR + rrt;
+        rrn[ie + (size_t)t * C] = rrt;
+        const Dir4<R> m = sMom[t];
+        rc = DM<R>::fma(m.c2, rrt, rc);
+        rs = DM<R>::fma(m.s2, rrt, rs);
+        rcs = DM<R>::fma(m.cs, rrt, rcs);
+    }
+    // the second copy of ee: the source cell's final bins (this thread's own
+    // stores, read back with ordinary loads)
+    R sume = (R)0, sumethet = (R)0, ec = (R)0, es = (R)0, ecs = (R)0;
+    for (int t = 0; t < nt; t++) {
+        const R eet = een[is + (size_t)t * C] * w;
+        een[ie + (size_t)t * C] = eet;
+        const Dir4<R> m = sMom[t];
+        sume = sume + eet;
+        sumethet = sumethet + eet * m.th;
+        ec = DM<R>::fma(m.c2, eet, ec);
+        es = DM<R>::fma(m.s2, eet, es);
+        ecs = DM<R>::fma(m.cs, eet, ecs);
+    }
+    const R sum2 = sume;
+    sume = DM<R>::fmax(sume, (R)0.00001f);
+    S.f[THM][ie] = sumethet / sume;
+    S.f[E][ie] = sume * dth;
+    S.f[H][ie] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
+    S.f[D][ie] = Dv;
+    S.f[ROL][ie] = RR * dth;
+    S.f[DR][ie] = drr * dth;
+    const R n = ld(S.f[CG] + ie) / cE;
+    S.tmp[T_SXX][ie] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
+    S.tmp[T_SYY][ie] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
+    S.tmp[T_SXY][ie] = n * ecs * dth + rcs * dth;
+    return dtw;
 }
 
 constexpr int WT_NB = 3;   // plane tile buffers: plane t+1 streams in while t is used
@@ -425,16 +300,12 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
     R* tR = tE + WT_NB * WT_N;            // [WT_NB][WT_N] plane tiles of rr
     R* sA = tR + WT_NB * WT_N;            // [nt][256] advected ee (energy units)
     R* sR = sA + (size_t)nt * 256;        // [nt][256] advected rr
-    R* sCos = sR + (size_t)nt * 256;      // [nt]
-    R* sSin = sCos + nt;                  // [nt]
-    R* sTh = sSin + nt;                   // [nt]
-    R* sC2 = sTh + nt;                    // [nt] cos^2, sin^2, sin cos of the bins
-    R* sS2 = sC2 + nt;
-    R* sCS = sS2 + nt;
+    Dir4<R>* sMom = reinterpret_cast<Dir4<R>*>(sR + (size_t)nt * 256);   // [nt]
+    Dir2<R>* sCS2 = reinterpret_cast<Dir2<R>*>(sMom + nt);               // [nt]
     if (tid < nt) {
         const R c = K.cxsth[tid], sn = K.sxnth[tid];
-        sCos[tid] = c; sSin[tid] = sn; sTh[tid] = K.theta[tid];
-        sC2[tid] = c * c; sS2[tid] = sn * sn; sCS[tid] = sn * c;
+        sCS2[tid] = Dir2<R>{c, sn};
+        sMom[tid] = Dir4<R>{c * c, sn * sn, sn * c, K.theta[tid]};
     }
     const int bx0 = bix * WT_X, by0 = 1 + biy * WT_Y;
     const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
@@ -511,8 +382,6 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         R v = own_bnd ? St[iy + t * ny] * taper : ld(eeo + i + (size_t)t * C);
         return DM<R>::fmax(v, (R)0);
     };
-    const bool edge_row = active && (iy == 1 || iy == ny - 2);
-    const int slot = (iy == 1) ? 0 : 1;
     issue(0);
     __syncthreads();   // theta tables
     if (active) {
@@ -540,8 +409,8 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         wr2 = ld(rro + i); wr1 = wr2;
         wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
         if (!WCI) { cthP = cc.s * cc.dhdx; cthQ = -(cc.s * cc.dhdy); }
-        c0 = cth(sCos[0], sSin[0]);
-        cpp = cth(sCos[cl(1)], sSin[cl(1)]);
+        c0 = cth(sCS2[0].c, sCS2[0].s);
+        cpp = cth(sCS2[cl(1)].c, sCS2[cl(1)].s);
     }
     // the cell's own bins ahead (window refill): plane min(t+3, nt-1)
     const R* wE = eeo + i + (size_t)min(3, nt - 1) * C;
@@ -549,8 +418,6 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
     const R* wS = St + iy + min(3, nt - 1) * ny;
     R* oA = sA + tid;
     R* oR = sR + tid;
-    R* oEdge = S.edge + ix + (size_t)slot * nt * nx;
-    const size_t edge_rr = (size_t)2 * nt * nx;
 #pragma unroll 1
     for (int t = 0; t < nt; t++) {
         const int b = t % WT_NB;
@@ -562,7 +429,8 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         if (active) {
             const R* qE = tE + b * WT_N + ctile;
             const R* qR = tR + b * WT_N + ctile;
-            const R ct = sCos[t], st = sSin[t];
+            const Dir2<R> d = sCS2[t];
+            const R ct = d.c, st = d.s;
             const bool last = t == nt - 1;
             cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
             R fx = flux2(qE[-2], qE[-1], we2, qE[1], qE[2], DM<R>::fma(ct, axp, bxp), DM<R>::fma(ct, axm, bxm));
@@ -586,18 +454,14 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
             *oA = A;
             *oR = Ar;
             oA += 256; oR += 256;
-            if (edge_row) {
-                oEdge[0] = A;
-                oEdge[edge_rr] = Ar;
-            }
-            oEdge += nx;
             Etmp = Etmp + DM<R>::fmax(A, (R)0);
             const int t2 = t + 2 < nt ? t + 2 : nt - 1;
             we1 = we2; we2 = we3; we3 = we4;
             we4 = DM<R>::fmax(own_bnd ? *wS * taper : ld(wE), (R)0);
             wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(wR);
             if (t + 4 <= nt - 1) { wE += C; wR += C; wS += ny; }
-            c0 = cpp; cpp = cth(sCos[t2], sSin[t2]);
+            const Dir2<R> d2 = sCS2[t2];
+            c0 = cpp; cpp = cth(d2.c, d2.s);
         }
     }
     R dtw = (R)3.0e38f;
@@ -608,37 +472,10 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         R* rrn = S.rr[par];
         const R Trep = (R)clk->Trep;
         const R rho = K.rho, g = K.g;
-        // energintCPU
-        Etmp = Etmp * dth;
-        R Htmp = DM<R>::sqrt(Etmp / (rho * g / (R)8.0f));
-        R hr = Htmp / (K.gammax * hh);
-        const R idiv = DM<R>::fmax((R)1.0f, hr * hr);
-        const R ridiv = (R)1 / idiv;
-        Htmp = DM<R>::fmin(Htmp, K.gammax * hh);
-        const R Eint = (rho * g * Htmp * Htmp) / (R)8.0f;
-        const R k = ld(S.f[WK] + i);
-        const R fw = ld(S.f[FWM] + i);
-        R Dv;
-        if (K.breakmodel == 1) {   // roelvinkCPU
-            R Ht = DM<R>::sqrt(Eint * (R)(8.0 / (double)rho / (double)g));
-            R x = Ht / K.gammaa / hh;
-            R Qb = (R)1 - DM<R>::exp(DM<R>::fmax(-DM<R>::pow(x, K.nexp), (R)-100));
-            Qb = DM<R>::fmin(Qb, (R)1.0f);
-            Dv = Qb * (R)2 * K.alpha / Trep * Eint * Ht / hh;
-            R uorb = (R)XBG_PI * Ht / (Trep * DM<R>::sinh(DM<R>::fmin(k * hh, (R)10.0f)));
-            Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
-        } else {                   // baldockCPU
-            R khh = k * hh;
-            R Hb = ((R)0.88f / k) * DM<R>::tanh(K.gammaa * khh / (R)0.88f);
-            R Rr = Hb / DM<R>::fmax(Htmp, (R)0.00001f);
-            R Qb = DM<R>::exp((R)-1.0f * Rr * Rr);
-            Dv = (R)0.25f * K.alpha * Qb * rho * ((R)1.0f / Trep) * g * (Hb * Hb + Htmp * Htmp);
-            R uorb = (R)XBG_PI * Htmp / (Trep * DM<R>::sinh(DM<R>::fmin(k * hh, (R)10.0f)));
-            Dv = Dv + (R)(0.66666666f / XBG_PI) * rho * fw * uorb * uorb * uorb;
-        }
+        R ridiv, Dv, Dq;
+        wave_breaking(K, Etmp, hh, ld(S.f[WK] + i), ld(S.f[FWM] + i), Trep, ridiv, Dv, Dq);
         // dissipationCPU, meandir, radstress
         const R cc_i = cci;
-        const R Dq = Dv / DM<R>::fmax(Eint, (R)0.0000001f);
         const R twogb = (R)2.0f * g * K.beta;
         const R rcoef = twogb / cc_i;   // without wave-current interaction |c (cos, sin)| = c
         const bool wet = hh > K.eps;
@@ -646,34 +483,42 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         R ec = 0, es = 0, ecs = 0, rc = 0, rs = 0, rcs = 0;   // sums of cos^2, sin^2, sin cos times e / r
         R* pe_n = een + i;
         R* pr_n = rrn + i;
+        if (wet) {
 #pragma unroll 2
-        for (int t = 0; t < nt; t++) {
-            R eet = DM<R>::fmax(sA[t * 256 + tid], (R)0.0f) * ridiv;
-            R rrt = sR[t * 256 + tid];
-            const R dd = eet * Dq;
-            R rrd;
-            if (WCI) {
-                const R cx = cc_i * sCos[t] + uui;
-                const R cy = cc_i * sSin[t] + vvi;
-                rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
-            } else {
-                rrd = rrt * rcoef;
+            for (int t = 0; t < nt; t++) {
+                R eet = DM<R>::fmax(sA[t * 256 + tid], (R)0.0f) * ridiv;
+                R rrt = sR[t * 256 + tid];
+                const R dd = eet * Dq;
+                R rrd;
+                if (WCI) {
+                    const Dir2<R> d = sCS2[t];
+                    const R cx = cc_i * d.c + uui;
+                    const R cy = cc_i * d.s + vvi;
+                    rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
+                } else {
+                    rrd = rrt * rcoef;
+                }
+                eet = DM<R>::fmax(eet - dtf * dd, (R)0.0f);
+                rrt = DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                drr = drr + rrd;
+                RR = RR + rrt;
+                pe_n[(size_t)t * C] = eet;
+                pr_n[(size_t)t * C] = rrt;
+                const Dir4<R> m = sMom[t];
+                sume = sume + eet;
+                sumethet = sumethet + eet * m.th;
+                ec = DM<R>::fma(m.c2, eet, ec);
+                es = DM<R>::fma(m.s2, eet, es);
+                ecs = DM<R>::fma(m.cs, eet, ecs);
+                rc = DM<R>::fma(m.c2, rrt, rc);
+                rs = DM<R>::fma(m.s2, rrt, rs);
+                rcs = DM<R>::fma(m.cs, rrt, rcs);
             }
-            eet = wet ? DM<R>::fmax(eet - dtf * dd, (R)0.0f) : (R)0;
-            rrt = wet ? DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f) : (R)0;
-            drr = wet ? drr + rrd : (R)0;
-            RR = RR + rrt;
-            pe_n[(size_t)t * C] = eet;
-            pr_n[(size_t)t * C] = rrt;
-            sume = sume + eet;
-            sumethet = sumethet + eet * sTh[t];
-            const R c2 = sC2[t], s2 = sS2[t], cs = sCS[t];
-            ec = DM<R>::fma(c2, eet, ec);
-            es = DM<R>::fma(s2, eet, es);
-            ecs = DM<R>::fma(cs, eet, ecs);
-            rc = DM<R>::fma(c2, rrt, rc);
-            rs = DM<R>::fma(s2, rrt, rs);
-            rcs = DM<R>::fma(cs, rrt, rcs);
+        } else {   // dry: ee, rr and every sum are zero
+            for (int t = 0; t < nt; t++) {
+                pe_n[(size_t)t * C] = (R)0;
+                pr_n[(size_t)t * C] = (R)0;
+            }
         }
         const R sum2 = sume;
         sume = DM<R>::fmax(sume, (R)0.00001f);
@@ -688,6 +533,14 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         S.tmp[T_SXX][i] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
         S.tmp[T_SYY][i] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
         S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
+        // the lateral rows 0 and ny-1, from rows 1 and ny-2
+        const R sg = (R)clk->sigm;
+        if (iy == 1)
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, WCI>(S, K, ix, 0, 1, sA, sR, sCS2, sMom, Etmp, sg, dtf,
+                                                                  Trep, rro, een, rrn));
+        if (iy == ny - 2)
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, WCI>(S, K, ix, ny - 1, ny - 2, sA, sR, sCS2, sMom, Etmp,
+                                                                  sg, dtf, Trep, rro, een, rrn));
     }
     block_min_store<R>(dtw, S.part_wave + bix + biy * ((K.nx + 31) / 32));
 }
@@ -729,60 +582,6 @@ void launch_wave_fast_batch(const BatchTab<R>& T, const BatchLaunch& L, int roll
 }
 template <class R>
 size_t wave_fast_smem(int nt) { return ((size_t)2 * WT_NB * WT_N + (size_t)2 * nt * 256 + 6 * nt) * sizeof(R); }
-
-template <class R, int NMAX>
-__device__ __forceinline__ void b_wave_edge(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
-    const Clock* clk = S.clk;
-    if (halted(clk)) return;
-    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
-    int ix = bix * blockDim.x + threadIdx.x;
-    int iy = (biy == 0) ? 0 : ny - 1;
-    R dtw = (R)3.0e38f;
-    if (ix < nx) {
-        int i = ix + iy * nx;
-        int src = (iy == 0) ? pp(0, ny) : mm(ny - 1);
-        int slot = (iy == 0) ? 0 : 1;
-        int par = clk->par;
-        const R* rro = S.rr[par ^ 1];
-        R* een = S.ee[par];
-        R* rrn = S.rr[par];
-        R sg = (R)clk->sigm;
-        R dtf = (R)clk->dt;
-        R Trep = (R)clk->Trep;
-        CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
-        R cthv[NMAX];
-        dtw = ctheta_cell<R, NMAX>(K, cc, cthv);
-        R w = ld(S.f[HH] + i) > K.eps ? (R)1.0f : (R)0.0f;
-        R e[NMAX], r[NMAX];
-#pragma unroll
-        for (int t = 0; t < NMAX; t++) {
-            if (t < nt) {
-                e[t] = S.edge[ix + (size_t)t * nx + (size_t)slot * nt * nx] * w;
-                r[t] = (K.roller == 1) ? S.edge[ix + (size_t)t * nx + (size_t)(slot + 2) * nt * nx] * w
-                                       : ld(rro + i + (size_t)t * C);
-            } else {
-                e[t] = (R)0; r[t] = (R)0;
-            }
-        }
-        CellOut<R> o = chain_cell<R, NMAX>(S, K, i, sg, dtf, Trep, e, r);
-        // second rollerlatbnd(ee) after dissipation: copy of the source row
-#pragma unroll
-        for (int t = 0; t < NMAX; t++)
-            if (t < nt) e[t] = een[ix + src * nx + (size_t)t * C] * w;
-        finish_cell<R, NMAX>(S, K, i, e, r, o, een, rrn);
-    }
-    block_min_store<R>(dtw, S.part_wave + ((K.nx + 31) / 32) * ((K.ny - 2 + 7) / 8) + bix + biy * ((K.nx + 127) / 128));
-}
-template <class R, int NMAX>
-__global__ void __launch_bounds__(128) k_wave_edge(Dev<R> S, Konst<R> K) {
-    b_wave_edge<R, NMAX>(S, K, blockIdx.x, blockIdx.y);
-}
-template <class R, int NMAX>
-__global__ void __launch_bounds__(128) kb_wave_edge(BatchTab<R> T, const int2* items, int n) {
-    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux&, int bx, int by) {
-        b_wave_edge<R, NMAX>(S, K, bx, by);
-    });
-}
 
 // wavforce (wave_CPU.cpp:1164-1238) at cell j, before the boundary copies.
 template <class R>
@@ -857,34 +656,22 @@ XBG_KERNELS(wave_force)
 // ---------------------------------------------------------------- launchers
 template <class R>
 int wave_parts(const Konst<R>& K) {
-    int gx = (K.nx + 31) / 32, gy = (K.ny - 2 + 7) / 8;
-    int ex = (K.nx + 127) / 128;
-    return gx * gy + ex * 2;
+    return ((K.nx + 31) / 32) * ((K.ny - 2 + 7) / 8);
 }
 
-template <class R, int NMAX>
-void launch_wave_main(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
-    dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
-    launch_wave_fast(S, K, g, b, wave_fast_smem<R>(K.nt), st);
-    PMARK(pf, "k_wave_fast");
-    dim3 be(128), ge((K.nx + 127) / 128, 2);
-    k_wave_edge<R, NMAX><<<ge, be, 0, st>>>(S, K);
-    PMARK(pf, "k_wave_edge");
-}
-
+// join: an event of a concurrent branch (the boundary kernels) that the
+// rows pass waits for after the dispersion kernel; null when sequential.
 template <class R>
-int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, cudaEvent_t join) {
     int n = 0;
     k_disp<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, K); n++;
     PMARK(pf, "k_disp");
-    if (K.nt <= 4) launch_wave_main<R, 4>(S, K, st, pf);
-    else if (K.nt <= 8) launch_wave_main<R, 8>(S, K, st, pf);
-    else if (K.nt <= 12) launch_wave_main<R, 12>(S, K, st, pf);
-    else if (K.nt <= 16) launch_wave_main<R, 16>(S, K, st, pf);
-    else if (K.nt <= 20) launch_wave_main<R, 20>(S, K, st, pf);
-    else if (K.nt <= 24) launch_wave_main<R, 24>(S, K, st, pf);
-    else launch_wave_main<R, 32>(S, K, st, pf);
-    n += 2;
+    if (join) cudaStreamWaitEvent(st, join, 0);
+    {
+        dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
+        launch_wave_fast(S, K, g, b, wave_fast_smem<R>(K.nt), st); n++;
+        PMARK(pf, "k_wave_fast");
+    }
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
     k_wave_force<R><<<g, b, 0, st>>>(S, K); n++;
     PMARK(pf, "k_wave_force");
@@ -893,33 +680,22 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
 
 // the wave kernels over every scenario of a batch (one ntheta and roller
 // setting for the whole batch)
-template <class R, int NMAX>
-void launch_wave_main_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
-                            Prof* pf) {
-    launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
-    PMARK(pf, "k_wave_fast");
-    kb_wave_edge<R, NMAX><<<L.grid[BS_EDGE], 128, 0, st>>>(T, L.items[BS_EDGE], L.n[BS_EDGE]);
-    PMARK(pf, "k_wave_edge");
-}
-
 template <class R>
 int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
-                      Prof* pf) {
+                      Prof* pf, cudaEvent_t join) {
     kb_disp<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
     PMARK(pf, "k_disp");
-    if (nt <= 4) launch_wave_main_batch<R, 4>(T, L, nt, roller, wci, st, pf);
-    else if (nt <= 8) launch_wave_main_batch<R, 8>(T, L, nt, roller, wci, st, pf);
-    else if (nt <= 12) launch_wave_main_batch<R, 12>(T, L, nt, roller, wci, st, pf);
-    else if (nt <= 16) launch_wave_main_batch<R, 16>(T, L, nt, roller, wci, st, pf);
-    else if (nt <= 20) launch_wave_main_batch<R, 20>(T, L, nt, roller, wci, st, pf);
-    else if (nt <= 24) launch_wave_main_batch<R, 24>(T, L, nt, roller, wci, st, pf);
-    else launch_wave_main_batch<R, 32>(T, L, nt, roller, wci, st, pf);
+    if (join) cudaStreamWaitEvent(st, join, 0);
+    launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
+    PMARK(pf, "k_wave_fast");
     kb_wave_force<R><<<L.grid[BS_TILE], dim3(32, 8), 0, st>>>(T, L.items[BS_TILE], L.n[BS_TILE]);
     PMARK(pf, "k_wave_force");
-    return 4;
+    return 3;
 }
-template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*);
-template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*);
+template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
+                                      cudaEvent_t);
+template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
+                                       cudaEvent_t);
 
 // One-time kernel attributes (dynamic shared memory above 48 KB for wide
 // theta sets in FP64).
@@ -939,8 +715,8 @@ int wave_prepare(const Konst<R>& K) {
 template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);
 
-template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
-template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
+template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, cudaEvent_t);
+template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, cudaEvent_t);
 template int wave_parts<float>(const Konst<float>&);
 template int wave_parts<double>(const Konst<double>&);
 

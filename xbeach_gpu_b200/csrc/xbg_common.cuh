@@ -97,7 +97,6 @@ struct Dev {
     R* umeanbnd;          // ny
     R* ee[2];             // two plane sets of nt*C
     R* rr[2];
-    R* edge;              // advected ee/rr of rows 1 and ny-2: 4*nx*nt
     R* St;                // interpolated offshore boundary, nt*ny
     R* stfile[2];         // boundary chunk slots: nrec*nt*ny
     R* qfile[2];          // nrec*4*ny
@@ -270,7 +269,6 @@ enum BatchShape {
     BS_TILE,    // 32 x 8 tiles over nx x ny
     BS_WROWS,   // 32 x 8 tiles over nx x rows 1..ny-2 (wave pass)
     BS_LIN,     // 256-cell runs of the C cells
-    BS_EDGE,    // 128-cell runs of rows 0 and ny-1
     BS_ONE,     // one block per scenario
     BS_BND,     // 256-value runs of the ny*ntheta boundary values
     BS_DT,      // the blocks of the dt reduction
