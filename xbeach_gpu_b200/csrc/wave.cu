@@ -9,7 +9,9 @@
 //                units), then energint, roelvink|baldock, dissipation,
 //                meandir, radstress.  Each bin's ee/rr plane tile (32 x 8
 //                cells + 2-cell halo) streams into shared memory by cp.async
-//                one bin ahead (three buffers, one barrier per bin); ctheta
+//                three bins ahead (five buffers, one barrier per bin), and
+//                the cell's own bins for the theta fluxes come from the
+//                resident tiles; ctheta
 //                (propagtheta) is evaluated on the fly from per-cell slopes;
 //                the theta-face flux is computed once and carried to the
 //                next bin.  The threads of rows 1 and ny-2 then also
@@ -287,7 +289,11 @@ __device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, 
     return dtw;
 }
 
-constexpr int WT_NB = 3;   // plane tile buffers: plane t+1 streams in while t is used
+// Plane tile buffers.  At bin t planes t, t+1 and t+2 are resident (the
+// stencil of plane t; the cell's own values of planes t+1 and t+2 for the
+// theta fluxes) and plane t+3 streams in; it goes into the buffer of plane
+// t-2, which every thread finished reading before the previous barrier.
+constexpr int WT_NB = 5;
 
 template <class R, bool ROLLER, bool WCI>
 __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
@@ -377,12 +383,10 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         const R ctht = DM<R>::fma(cthP, sx, cthQ * cx);
         return cmin(cmax(ctht, (R)(-0.25f * cc.sg)), (R)(0.25f * cc.sg));
     };
-    const bool own_bnd = ix == 0;
-    auto own_e = [&](int t) -> R {
-        R v = own_bnd ? St[iy + t * ny] * taper : ld(eeo + i + (size_t)t * C);
-        return DM<R>::fmax(v, (R)0);
-    };
+    // planes 0, 1, 2 (empty groups past the last plane)
     issue(0);
+    if (nt > 1) issue(1); else cp_async_commit();
+    if (nt > 2) issue(2); else cp_async_commit();
     __syncthreads();   // theta tables
     if (active) {
         i = ix + iy * nx;
@@ -405,30 +409,36 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         bxp = h * (uui + ld(uu + xp + iy * nx) * wci); bxm = h * (uui + ld(uu + xm + iy * nx) * wci);
         byp = h * (vvi + wci * ld(vv + ix + yp * nx)); bym = h * (vvi + wci * ld(vv + ix + ym * nx));
         auto cl = [&](int t) { return t < 0 ? 0 : (t >= nt ? nt - 1 : t); };
-        we2 = own_e(0); we1 = we2; we3 = own_e(cl(1)); we4 = own_e(cl(2));
-        wr2 = ld(rro + i); wr1 = wr2;
-        wr3 = ld(rro + i + (size_t)cl(1) * C); wr4 = ld(rro + i + (size_t)cl(2) * C);
         if (!WCI) { cthP = cc.s * cc.dhdx; cthQ = -(cc.s * cc.dhdy); }
         c0 = cth(sCS2[0].c, sCS2[0].s);
         cpp = cth(sCS2[cl(1)].c, sCS2[cl(1)].s);
     }
-    // the cell's own bins ahead (window refill): plane min(t+3, nt-1)
-    const R* wE = eeo + i + (size_t)min(3, nt - 1) * C;
-    const R* wR = rro + i + (size_t)min(3, nt - 1) * C;
-    const R* wS = St + iy + min(3, nt - 1) * ny;
+    cp_async_wait1();   // planes 0 and 1 have landed (this thread's copies)
+    fixup(0);
+    if (nt > 1) fixup(1);
     R* oA = sA + tid;
     R* oR = sR + tid;
+    const R* oldR = rro + i;   // without the roller pass rr is carried unchanged
 #pragma unroll 1
     for (int t = 0; t < nt; t++) {
         const int b = t % WT_NB;
-        if (t + 1 < nt) issue((t + 1) % WT_NB);
+        if (t + 3 < nt) issue((t + 3) % WT_NB);
         else cp_async_commit();
-        cp_async_wait1();   // plane t has landed (this thread's copies)
-        fixup(b);
-        __syncthreads();    // ... and every thread's; buffer (t+1)%3 was last read two planes ago
+        cp_async_wait1();   // plane t+2 has landed (this thread's copies)
+        if (t + 2 < nt) fixup((t + 2) % WT_NB);
+        __syncthreads();    // ... and every thread's
         if (active) {
             const R* qE = tE + b * WT_N + ctile;
             const R* qR = tR + b * WT_N + ctile;
+            // the cell's own bins t-1 .. t+2 (clamped to the last bin)
+            if (t == 0) {
+                const int b1 = (nt > 1 ? 1 : 0);
+                we2 = qE[0]; we1 = we2; we3 = tE[b1 * WT_N + ctile];
+                if (ROLLER) { wr2 = qR[0]; wr1 = wr2; wr3 = tR[b1 * WT_N + ctile]; }
+            }
+            const int b2 = (t + 2 < nt ? t + 2 : nt - 1) % WT_NB;
+            we4 = tE[b2 * WT_N + ctile];
+            if (ROLLER) wr4 = tR[b2 * WT_N + ctile];
             const Dir2<R> d = sCS2[t];
             const R ct = d.c, st = d.s;
             const bool last = t == nt - 1;
@@ -441,7 +451,8 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
             R ft = fup - fte;
             fte = fup;
             R A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
-            R Ar = wr2;
+            R Ar;
+            if (!ROLLER) Ar = ld(oldR + (size_t)t * C);
             if (ROLLER) {
                 R rx = flux2(qR[-2], qR[-1], wr2, qR[1], qR[2], DM<R>::fma(ct, rxp, bxp), DM<R>::fma(ct, rxm, bxm));
                 R ry = flux2(qR[-2 * WT_TX], qR[-WT_TX], wr2, qR[WT_TX], qR[2 * WT_TX], DM<R>::fma(st, ryp, byp),
@@ -457,9 +468,7 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
             Etmp = Etmp + DM<R>::fmax(A, (R)0);
             const int t2 = t + 2 < nt ? t + 2 : nt - 1;
             we1 = we2; we2 = we3; we3 = we4;
-            we4 = DM<R>::fmax(own_bnd ? *wS * taper : ld(wE), (R)0);
-            wr1 = wr2; wr2 = wr3; wr3 = wr4; wr4 = ld(wR);
-            if (t + 4 <= nt - 1) { wE += C; wR += C; wS += ny; }
+            wr1 = wr2; wr2 = wr3; wr3 = wr4;
             const Dir2<R> d2 = sCS2[t2];
             c0 = cpp; cpp = cth(d2.c, d2.s);
         }
