@@ -14,7 +14,9 @@
 //   k_flow_final wrkzs2Ocorr+zs2Ocorr, latbnd(zs), hsbnd, calcuvvu, uvlatbnd
 // (* = a per-step buffer).  viscovbnd (Flow_kernel.cu:1461) changes viscv only
 // at rows 0 and ny-2, whose eulervstep results vvlatbnd then overwrites, so it
-// has no effect on the state and is not evaluated.
+// has no effect on the state and is not evaluated.  Quotients by the grid
+// spacing are products with its reciprocal (within an ulp of the reference's
+// float division).
 #include "xbg_common.cuh"
 
 namespace xbg {
@@ -37,13 +39,13 @@ __device__ __forceinline__ R smago_cell(const Dev<R>& S, const Konst<R>& K, int 
     const int nx = K.nx, ny = K.ny;
     const R* uu = S.f[UU]; const R* vv = S.f[VV];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-    R dx = K.dx, nuh = K.nuh, nuhfac = K.nuhfac, rho = K.rho;
+    R dx = K.dx, rdx = K.rdx, nuh = K.nuh, nuhfac = K.nuhfac, rho = K.rho;
     R b = nuhfac * ld(S.f[HH] + i) * DM<R>::pow13(ld(S.f[DR] + i) / rho);
     if (K.usesmago == 1) {
-        R dudx = (ld(uu + i) - ld(uu + IDX(xm, iy))) / dx;
-        R dudy = (R)0.50f * (ld(uu + IDX(ix, yp)) - ld(uu + IDX(ix, ym)) + ld(uu + IDX(xm, yp)) - ld(uu + IDX(xm, ym))) / dx;
-        R dvdy = (ld(vv + i) - ld(vv + IDX(ix, ym))) / dx;
-        R dvdx = (R)0.50f * (ld(vv + IDX(xp, iy)) - ld(vv + IDX(xm, iy)) + ld(vv + IDX(xp, ym)) - ld(vv + IDX(xm, ym))) / dx;
+        R dudx = (ld(uu + i) - ld(uu + IDX(xm, iy))) * rdx;
+        R dudy = (R)0.50f * (ld(uu + IDX(ix, yp)) - ld(uu + IDX(ix, ym)) + ld(uu + IDX(xm, yp)) - ld(uu + IDX(xm, ym))) * rdx;
+        R dvdy = (ld(vv + i) - ld(vv + IDX(ix, ym))) * rdx;
+        R dvdx = (R)0.50f * (ld(vv + IDX(xp, iy)) - ld(vv + IDX(xm, iy)) + ld(vv + IDX(xp, ym)) - ld(vv + IDX(xm, ym))) * rdx;
         R tau = DM<R>::sqrt((R)2.0f * dudx * dudx + (R)2.0f * dvdy * dvdy + (dudy + dvdx) * (dudy + dvdx));
         return DM<R>::fmax(nuh * nuh * dx * dx * tau, b);
     }
@@ -79,26 +81,26 @@ __device__ R euler_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
     const R* hum = S.f[HUM]; const R* hvm = S.f[HVM]; const R* nuhg = S.tmp[T_NUH];
     const R* hh = S.f[HH];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-    R dx = K.dx, g = K.g, rho = K.rho;
+    R rdx = K.rdx, g = K.g, rho = K.rho;
     R uui = ld(uu + i);
     if (ld(S.wetu + i) != 1) return (R)0.0f;
     R humi = ld(hum + i);
     // wlevslopes, x
-    R dzsdx = (ld(S.f[ZS] + IDX(xp, iy)) - ld(S.f[ZS] + i)) / dx;
+    R dzsdx = (ld(S.f[ZS] + IDX(xp, iy)) - ld(S.f[ZS] + i)) * rdx;
     // ududx_adv
     R uur = ld(uu + IDX(xp, iy)), uul = ld(uu + IDX(xm, iy));
     R ududx = (R)0.0f;
     R qin = (R)0.5f * (ld(hu + i) * uui + ld(hu + IDX(xm, iy)) * uul);
     R du = uui - uul;
     if (qin > (R)0.0f) {
-        if (du > (R)0.5f) ududx = ududx + (R)0.5f * (uul + uui) * (uui - uul) / dx;
-        else ududx = ududx + qin / humi * (uui - uul) / dx;
+        if (du > (R)0.5f) ududx = ududx + (R)0.5f * (uul + uui) * (uui - uul) * rdx;
+        else ududx = ududx + qin / humi * (uui - uul) * rdx;
     }
     qin = (R)-0.5f * (ld(hu + i) * uui + ld(hu + IDX(xp, iy)) * uur);
     du = uur - uui;
     if (qin > (R)0.0f) {
-        if (du > (R)0.5f) ududx = ududx - (R)0.5f * (uur + uui) * (uui - uur) / dx;
-        else ududx = ududx + qin / humi * (uui - uur) / dx;
+        if (du > (R)0.5f) ududx = ududx - (R)0.5f * (uur + uui) * (uui - uur) * rdx;
+        else ududx = ududx + qin / humi * (uui - uur) * rdx;
     }
     // vdudy_adv
     R uut = ld(uu + IDX(ix, yp)), uub = ld(uu + IDX(ix, ym));
@@ -107,25 +109,25 @@ __device__ R euler_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
     qin = (R)0.5f * (vb * ld(hv + IDX(ix, ym)) + vbr * ld(hv + IDX(xp, ym)));
     R dv = vi - vb;
     if (qin > (R)0.0f) {
-        if (dv > (R)0.5f) vdudy = vdudy + (R)0.5f * (vb + vbr) * (uui - uub) / dx;
-        else vdudy = vdudy + qin / humi * (uui - uub) / dx;
+        if (dv > (R)0.5f) vdudy = vdudy + (R)0.5f * (vb + vbr) * (uui - uub) * rdx;
+        else vdudy = vdudy + qin / humi * (uui - uub) * rdx;
     }
     qin = (R)-0.5f * (vi * ld(hv + i) + vr * ld(hv + IDX(xp, iy)));
     dv = ld(vv + IDX(ix, yp)) - vi;
     if (qin > (R)0.0f) {
-        if (dv > (R)0.5f) vdudy = vdudy - (R)0.5f * (vi + vr) * (uui - uut) / dx;
-        else vdudy = vdudy + qin / humi * (uui - uut) / dx;
+        if (dv > (R)0.5f) vdudy = vdudy - (R)0.5f * (vi + vr) * (uui - uut) * rdx;
+        else vdudy = vdudy + qin / humi * (uui - uut) * rdx;
     }
     // viscou1 + viscou2
     R nuh1 = ld(nuhg + IDX(xp, iy)), nuh2 = ld(nuhg + i);
-    R dudx1 = nuh1 * ld(hh + IDX(xp, iy)) * (uur - uui) / dx;
-    R dudx2 = nuh2 * ld(hh + i) * (uui - uul) / dx;
-    R visc = ((R)1.0f / humi) * ((dudx1 - dudx2) / (dx));
+    R dudx1 = nuh1 * ld(hh + IDX(xp, iy)) * (uur - uui) * rdx;
+    R dudx2 = nuh2 * ld(hh + i) * (uui - uul) * rdx;
+    R visc = ((R)1.0f / humi) * ((dudx1 - dudx2) * rdx);
     nuh1 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xp, iy)) + ld(nuhg + IDX(xp, yp)) + ld(nuhg + IDX(ix, yp)));
     nuh2 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xp, iy)) + ld(nuhg + IDX(xp, ym)) + ld(nuhg + IDX(ix, ym)));
-    R dudy1 = nuh1 * (R)0.5f * (ld(hvm + i) + ld(hvm + IDX(xp, iy))) * (uut - uui) / dx;
-    R dudy2 = nuh2 * (R)0.5f * (ld(hvm + IDX(ix, ym)) + ld(hvm + IDX(xp, ym))) * (uui - uub) / dx;
-    visc = visc + ((R)1.0f / humi) * ((dudy1 - dudy2) / dx * (R)ld(S.wetu + IDX(ix, yp)) * (R)ld(S.wetu + IDX(ix, ym)));
+    R dudy1 = nuh1 * (R)0.5f * (ld(hvm + i) + ld(hvm + IDX(xp, iy))) * (uut - uui) * rdx;
+    R dudy2 = nuh2 * (R)0.5f * (ld(hvm + IDX(ix, ym)) + ld(hvm + IDX(xp, ym))) * (uui - uub) * rdx;
+    visc = visc + ((R)1.0f / humi) * ((dudy1 - dudy2) * rdx * (R)ld(S.wetu + IDX(ix, yp)) * (R)ld(S.wetu + IDX(ix, ym)));
     // eulerustep
     R hmin = (R)0.2;
     int sw = (wu > (R)0.0) - (wu < (R)0.0);
@@ -161,19 +163,19 @@ __device__ __forceinline__ R vdvdy_cell(const Dev<R>& S, const Konst<R>& K, int 
     R r = (R)0.0f;
     if (ix > 0 && iy > 0 && iy < ny - 2) {
         int i = IDX(ix, iy), ym = mm(iy), yp = pp(iy, ny);
-        R dx = K.dx, hvmi = ld(S.f[HVM] + i);
+        R rdx = K.rdx, hvmi = ld(S.f[HVM] + i);
         R vi = ld(vv + i), vb = ld(vv + IDX(ix, ym)), vt = ld(vv + IDX(ix, yp));
         R qin = (R)0.5f * (vi * ld(hv + i) + vb * ld(hv + IDX(ix, ym)));
         R dv = vi - vb;
         if (qin > (R)0.0f) {
-            if (dv > (R)0.5f) r = r + (R)0.5f * (vb - vi) * (vi - vb) / (dx);
-            else r = r + qin / hvmi * (vi - vb) / (dx);
+            if (dv > (R)0.5f) r = r + (R)0.5f * (vb - vi) * (vi - vb) * rdx;
+            else r = r + qin / hvmi * (vi - vb) * rdx;
         }
         qin = (R)-0.5f * (ld(hv + i) * vi + ld(hv + IDX(ix, yp)) * vt);
         dv = vt - vi;
         if (qin > (R)0.0f) {
-            if (dv > (R)0.5f) r = r - (R)0.5f * (vt + vi) * (vi - vt) / (dx);
-            else r = r + qin / hvmi * (vi - vt) / (dx);
+            if (dv > (R)0.5f) r = r - (R)0.5f * (vt + vi) * (vi - vt) * rdx;
+            else r = r + qin / hvmi * (vi - vt) * rdx;
         }
     }
     return r;
@@ -188,11 +190,11 @@ __device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
     const R* hum = S.f[HUM]; const R* hvm = S.f[HVM]; const R* nuhg = S.tmp[T_NUH];
     const R* hh = S.f[HH];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-    R dx = K.dx, g = K.g, rho = K.rho;
+    R rdx = K.rdx, g = K.g, rho = K.rho;
     R vvi = ld(vv + i);
     if (ld(S.wetv + i) != 1) return (R)0.0f;
     R hvmi = ld(hvm + i);
-    R dzsdy = (ld(S.f[ZS] + IDX(ix, yp)) - ld(S.f[ZS] + i)) / dx;
+    R dzsdy = (ld(S.f[ZS] + IDX(ix, yp)) - ld(S.f[ZS] + i)) * rdx;
     R vdvdy = vdvdy_cell(S, K, ix, iy);
     // udvdx_adv
     R ul = ld(uu + IDX(xm, iy)), ultl = ld(uu + IDX(xm, yp)), ui = ld(uu + i), ur = ld(uu + IDX(xp, iy));
@@ -201,26 +203,26 @@ __device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
     R qin = (R)(0.5 * (double)(ul * ld(hu + IDX(xm, iy)) + ultl * ld(hu + IDX(xm, yp))));
     R du = ui - ul;
     if (qin > (R)0.0f) {
-        if (du > (R)0.5f) udvdx = udvdx + (R)0.5f * (ul + ultl) * (vvi - vl) / (dx);
-        else udvdx = udvdx + qin / hvmi * (vvi - vl) / (dx);
+        if (du > (R)0.5f) udvdx = udvdx + (R)0.5f * (ul + ultl) * (vvi - vl) * rdx;
+        else udvdx = udvdx + qin / hvmi * (vvi - vl) * rdx;
     }
     qin = (R)(-0.5 * (double)(ui * ld(hu + i) + ld(uu + IDX(ix, yp)) * ld(hu + IDX(ix, yp))));
     du = ur - ui;
     if (qin > (R)0.0f) {
-        if (du > (R)0.5f) udvdx = udvdx - (R)0.5f * (ui + ur) * (vvi - vr) / (dx);
-        else udvdx = udvdx + qin / hvmi * (vvi - vr) / (dx);
+        if (du > (R)0.5f) udvdx = udvdx - (R)0.5f * (ui + ur) * (vvi - vr) * rdx;
+        else udvdx = udvdx + qin / hvmi * (vvi - vr) * rdx;
     }
     // viscov1 + viscov2
     R vt = ld(vv + IDX(ix, yp)), vb = ld(vv + IDX(ix, ym));
     R nuh1 = ld(nuhg + IDX(ix, yp)), nuh2 = ld(nuhg + i);
-    R dvdy1 = nuh1 * ld(hh + IDX(ix, yp)) * (vt - vvi) / dx;
-    R dvdy2 = nuh2 * ld(hh + i) * (vvi - vb) / dx;
-    R visc = ((R)1.0f / hvmi) * (dvdy1 - dvdy2) / dx * (R)ld(S.wetv + IDX(ix, yp)) * (R)ld(S.wetv + IDX(ix, ym));
+    R dvdy1 = nuh1 * ld(hh + IDX(ix, yp)) * (vt - vvi) * rdx;
+    R dvdy2 = nuh2 * ld(hh + i) * (vvi - vb) * rdx;
+    R visc = ((R)1.0f / hvmi) * (dvdy1 - dvdy2) * rdx * (R)ld(S.wetv + IDX(ix, yp)) * (R)ld(S.wetv + IDX(ix, ym));
     nuh1 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xp, iy)) + ld(nuhg + IDX(xp, yp)) + ld(nuhg + IDX(ix, yp)));
     nuh2 = (R)0.25f * (ld(nuhg + i) + ld(nuhg + IDX(xm, iy)) + ld(nuhg + IDX(xm, yp)) + ld(nuhg + IDX(ix, yp)));
-    R dvdx1 = nuh1 * (R)0.5f * (ld(hum + i) + ld(hum + IDX(ix, yp))) * (vr - vvi) / dx;
-    R dvdx2 = nuh2 * (R)0.5f * (ld(hum + IDX(xm, iy)) + ld(hum + IDX(xm, yp))) * (vvi - vl) / dx;
-    visc = visc + ((R)1.0f / hvmi) * ((dvdx1 - dvdx2) / (dx) * (R)ld(S.wetv + IDX(xp, iy)) * (R)ld(S.wetv + IDX(xm, iy)));
+    R dvdx1 = nuh1 * (R)0.5f * (ld(hum + i) + ld(hum + IDX(ix, yp))) * (vr - vvi) * rdx;
+    R dvdx2 = nuh2 * (R)0.5f * (ld(hum + IDX(xm, iy)) + ld(hum + IDX(xm, yp))) * (vvi - vl) * rdx;
+    visc = visc + ((R)1.0f / hvmi) * ((dvdx1 - dvdx2) * rdx * (R)ld(S.wetv + IDX(xp, iy)) * (R)ld(S.wetv + IDX(xm, iy)));
     R hmin = (R)0.2;
     int sw = (wv > (R)0.0) - (wv < (R)0.0);
     R urms = ld(S.f[URMS] + i), vmag = ld(S.f[VMAGEV] + i);
@@ -338,7 +340,7 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
     int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
-    R dtf = (R)clk->dt, dx = K.dx;
+    R dtf = (R)clk->dt, rdx = K.rdx;
     TileAt<R, FC_H> a{tile, (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H};
     R u = a(C_UU, 0, 0), v = a(C_VV, 0, 0);
     if (ix > 0 && iy > 0) {
@@ -349,14 +351,14 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
         R qw = (R)0.5f * (a(C_QX, 0, 0) + a(C_QX, -1, 0));
         R qn = (R)0.5f * (a(C_QY, 0, -1) + a(C_QY, 1, -1));
         R qs = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, -1, 0));
-        u = u - dtf / ld(S.f[HUM] + i) * ((qe * w1r - qw * w1i) / dx + (qs * w2i - qn * w2b) / dx);
+        u = u - dtf / ld(S.f[HUM] + i) * ((qe * w1r - qw * w1i) * rdx + (qs * w2i - qn * w2b) * rdx);
         // vv2Ocorr: wrk at i, xm and yp
         R v1i = sV1[c], v2i = sV2[c], v2l = sV2[c - 1], v1t = sV1[c + FT_TX];
         qe = (R)0.5f * (a(C_QX, 0, 1) + a(C_QX, 0, 0));
         qw = (R)0.5f * (a(C_QX, -1, 0) + a(C_QX, -1, 1));
         qn = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, 0, -1));
         qs = (R)0.5f * (a(C_QY, 0, 1) + a(C_QY, 0, 0));
-        v = v - dtf / ld(S.f[HVM] + i) * ((qe * v2i - qw * v2l) / dx + (qs * v1t - qn * v1i) / dx);
+        v = v - dtf / ld(S.f[HVM] + i) * ((qe * v2i - qw * v2l) * rdx + (qs * v1t - qn * v1i) * rdx);
     }
     S.f[UU][i] = u;
     S.f[VV][i] = v;
@@ -409,7 +411,7 @@ __device__ __forceinline__ void b_flow_cont(const Dev<R>& S, const Konst<R>& K, 
         int xm = mm(ix), ym = mm(iy);
         R qxl = ld(S.f[UU] + IDX(xm, iy)) * depth_u(S, K, xm, iy);
         R qyb = (ym == iy) ? qyi : ld(S.f[VV] + IDX(ix, ym)) * depth_v(S, K, ix, ym);
-        R dzdt = (qxl - qxi + qyb - qyi) / K.dx;
+        R dzdt = (qxl - qxi + qyb - qyi) * K.rdx;
         S.f[DZSDT][i] = dzdt;
         zs = zs + dzdt * dtf;
     }
@@ -459,7 +461,7 @@ __device__ R zs_corr_global(const Dev<R>& S, const Konst<R>& K, const R* zso, in
     if (ix > 0 && iy > 0) {
         wrk_z(at(ix - 1, iy), K, ix - 1, iy, w1l, t0);
         wrk_z(at(ix, iy - 1), K, ix, iy - 1, t1, w2b);
-        z = z - dtf * ((w1 - w1l) / K.dx + (w2 - w2b) / K.dx);
+        z = z - dtf * ((w1 - w1l) * K.rdx + (w2 - w2b) * K.rdx);
     }
     return z;
 }
@@ -532,7 +534,7 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
     TileAt<R, FC_H> as{tile, kc + (sy - iy) * G::TX};     // around (ix, sy)
     auto zcorr = [&](const TileAt<R, FC_H>& c, int r, int y) {
         R z = c(Z_ZS, 0, 0);
-        if (ix > 0 && y > 0) z = z - dtf * ((sW1[r] - sW1[r - 1]) / K.dx + (sW2[r] - sW2[r - FT_TX]) / K.dx);
+        if (ix > 0 && y > 0) z = z - dtf * ((sW1[r] - sW1[r - 1]) * K.rdx + (sW2[r] - sW2[r - FT_TX]) * K.rdx);
         return z;
     };
     R zf = zcorr(a, k, iy);
