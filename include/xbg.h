@@ -48,6 +48,7 @@ extern "C" {
 #define XBG_ERR_STATE     6  /* call out of order (e.g. no wave boundary set) */
 #define XBG_ERR_NOMEM     7  /* device allocation failed                      */
 #define XBG_ERR_BOUNDARY  8  /* time ran past the last uploaded boundary data */
+#define XBG_ERR_IO        9  /* a file could not be written (xbg_io.h)       */
 
 #define XBG_FP32 0
 #define XBG_FP64 1

@@ -1,0 +1,68 @@
+/*
+ * xbg_io.h -- output path of the B200-native XBeach_GPU step: the model's
+ * map output as a netCDF file, written without libnetcdf.
+ *
+ * The reference writes its map output with the netCDF-C library
+ * (writenetcdf.cpp:32-240): creatncfileUD creates the file with the
+ * dimensions xx (nx), yy (ny), theta (ntheta) and the unlimited time, and the
+ * coordinate variables time, xx, yy, theta; defncvar adds one float variable
+ * per requested output name, (time, yy, xx) for 2-D fields and
+ * (time, theta, yy, xx) for the directional ones, and writes the initial
+ * state as record 0; at every output time writenctimestep appends the time
+ * and writencvarstep the record of each variable (Wave_gpu.cu:819-832,
+ * 2943-2951).  The writer here produces the same dimensions, variables,
+ * types and record layout in the netCDF classic format (64-bit offset
+ * variant, "CDF\2"), encoded from the published format specification, so
+ * any netCDF reader opens it.  All values are 32-bit floats, as in the
+ * reference.
+ *
+ * Deviation, documented: the reference's theta axis is i*dtheta + 0.5*dtheta
+ * because the thetamin it passes (the global at Wave_gpu.cu:110) is never
+ * assigned; here the caller passes the model's thetamin, so the axis is the
+ * bin centres.
+ */
+#ifndef XBG_IO_H
+#define XBG_IO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "xbg.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct xbg_nc xbg_nc;
+
+/* creatncfileUD + defncvar (writenetcdf.cpp:32-174) for all variables at
+ * once.  names[k] / ndims[k] (3: time, yy, xx; 4: time, theta, yy, xx) for
+ * k < nvars, names unique and not one of time, xx, yy, theta.  xx[i] = i*dx,
+ * yy[j] = j*dx, theta[t] = t*dtheta + thetamin + dtheta/2 (floats).  An
+ * existing file is an error unless clobber is 1 (the reference opens with
+ * NC_NOCLOBBER).  No record is written yet.  XBG_ERR_IO on a file error. */
+int xbg_nc_create(const char* path, int clobber, int nx, int ny, double dx,
+                  int ntheta, double dtheta, double thetamin, int nvars,
+                  const char* const* names, const int* ndims, xbg_nc** out);
+/* writenctimestep + writencvarstep for every variable (writenetcdf.cpp:
+ * 176-240): appends one record, time (stored as float) and data[k] with
+ * nx*ny (ndims 3) or ntheta*nx*ny (ndims 4) floats in the model's layout
+ * (i = ix + iy*nx, theta-planes outermost), then updates the record count
+ * in the header, so the file is complete after every call. */
+int xbg_nc_write_record(xbg_nc* f, double time, const float* const* data);
+int xbg_nc_records(const xbg_nc* f, int64_t* nrec);
+int xbg_nc_close(xbg_nc* f);
+
+/* The asynchronous device-to-host copy of the output step (Wave_gpu.cu:
+ * 823-831, a synchronous cudaMemcpy per variable there): enqueues one copy
+ * per field on the handle's stream into host[k] (count of xbg_field_count
+ * values of the handle's element type; pinned memory makes the copies
+ * asynchronous) and returns without synchronising; xbg_sync (or any call
+ * that returns host data) completes them.  ee, rr and zsold are taken from
+ * the plane set current after the enqueued work. */
+int xbg_fetch_fields(xbg_handle* h, const int* fields, int n, void* const* host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -40,7 +40,7 @@ FILE_FLAGS = {"sed.cu": ["-use_fast_math"]}
 
 
 def _compile(src, force=False):
-    obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
+    obj = os.path.join(BUILD, os.path.splitext(os.path.basename(src))[0] + ".o")
     newest = max([os.path.getmtime(src), os.path.getmtime(__file__)] + [os.path.getmtime(h) for h in _headers()])
     if not force and os.path.exists(obj) and os.path.getmtime(obj) >= newest:
         return obj
@@ -53,7 +53,7 @@ def _compile(src, force=False):
 
 def build(force=False, verbose=True):
     os.makedirs(BUILD, exist_ok=True)
-    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, force), srcs))
     newest = max(os.path.getmtime(o) for o in objs)

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include "xbg_common.cuh"
 #include "../../include/xbg.h"
+#include "../../include/xbg_io.h"
 
 namespace xbg {
 template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t);
@@ -151,6 +152,7 @@ extern "C" const char* xbg_status_string(int s) {
         case XBG_ERR_STATE: return "call out of order";
         case XBG_ERR_NOMEM: return "out of device memory";
         case XBG_ERR_BOUNDARY: return "ran past the uploaded wave boundary";
+        case XBG_ERR_IO: return "file write failed";
     }
     return "unknown status";
 }
@@ -183,6 +185,7 @@ struct xbg_handle {
     virtual int profile(float* ms, const char** names, int* n) = 0;
     virtual int put_wave_records(int slot, int first, int n, const void* St, const void* q) = 0;
     virtual int set_forcing(const void* const* f0, const void* const* f1, double w, int rescale) = 0;
+    virtual int fetch(const int* fields, int n, void* const* dst) = 0;
 };
 
 struct xbg_batch {
@@ -324,11 +327,40 @@ struct Handle : public xbg_handle {
     }
 
     int host_cur_slot = 0;
+    int host_par = 0;           // plane set current as of the last clock read
+    bool clock_stale = true;    // a step that may flip the set was enqueued since
     int read_clock(Clock& c) {
         if (ext) CK(cudaStreamSynchronize(ext));
         CK(cudaStreamSynchronize(st));
         CK(cudaMemcpy(&c, clk, sizeof(c), cudaMemcpyDeviceToHost));
         host_cur_slot = c.cur_slot;
+        host_par = c.par;
+        clock_stale = false;
+        return XBG_OK;
+    }
+
+    // output fields to host memory, stream-ordered; synchronises only when the
+    // current plane set of ee/rr/zsold is not known on the host
+    int fetch(const int* fields, int n, void* const* dst) override {
+        if (n < 0 || (n > 0 && (!fields || !dst))) return XBG_ERR_ARG;
+        if (clock_stale || batch_owned) {
+            Clock c;
+            int rc = read_clock(c);
+            if (rc) return rc;
+        }
+        for (int k = 0; k < n; k++) {
+            const int f = fields[k];
+            if (!dst[k]) return XBG_ERR_ARG;
+            if (f == XBG_F_WETU || f == XBG_F_WETV) {
+                CK(cudaMemcpyAsync(dst[k], f == XBG_F_WETU ? S.wetu : S.wetv, (size_t)S.C * sizeof(int),
+                                   cudaMemcpyDeviceToHost, st));
+                continue;
+            }
+            size_t m;
+            R* d = field_ptr(f, &m, host_par);
+            if (!d) return XBG_ERR_ARG;
+            CK(cudaMemcpyAsync(dst[k], d, m * sizeof(R), cudaMemcpyDeviceToHost, st));
+        }
         return XBG_OK;
     }
 
@@ -582,6 +614,7 @@ struct Handle : public xbg_handle {
     }
 
     int piece(int which) override {
+        if (which == 0) clock_stale = true;
         int n = 0;
         switch (which) {
             case 0: n = launch_step_begin(S, K, ser, nwave, st, nullptr); break;
@@ -599,6 +632,7 @@ struct Handle : public xbg_handle {
     }
 
     int step(int nsteps) override {
+        clock_stale = true;
         if (!gexec) {
             CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
             per_step_launches = enqueue_step();
@@ -920,6 +954,9 @@ int xbg_output_done(xbg_handle* h) { return h ? h->output_done() : XBG_ERR_ARG; 
 int xbg_reset_means(xbg_handle* h) { return h ? h->reset_means() : XBG_ERR_ARG; }
 int xbg_set_time(xbg_handle* h, double t, double dt, double wdt) { return h ? h->set_time(t, dt, wdt) : XBG_ERR_ARG; }
 int xbg_sync(xbg_handle* h) { return h ? h->sync() : XBG_ERR_ARG; }
+int xbg_fetch_fields(xbg_handle* h, const int* fields, int n, void* const* host) {
+    return h ? h->fetch(fields, n, host) : XBG_ERR_ARG;
+}
 int xbg_launch_count(const xbg_handle* h, int64_t* n) { if (!h || !n) return XBG_ERR_ARG; *n = h->launches; return XBG_OK; }
 int xbg_get_stream(xbg_handle* h, void** s) { if (!h || !s) return XBG_ERR_ARG; *s = h->stream(); return XBG_OK; }
 int xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n) {
