@@ -48,7 +48,8 @@ extern "C" {
 #define XBG_ERR_STATE     6  /* call out of order (e.g. no wave boundary set) */
 #define XBG_ERR_NOMEM     7  /* device allocation failed                      */
 #define XBG_ERR_BOUNDARY  8  /* time ran past the last uploaded boundary data */
-#define XBG_ERR_IO        9  /* a file could not be written (xbg_io.h)       */
+#define XBG_ERR_IO        9  /* a file could not be opened or written        */
+#define XBG_ERR_FORMAT   10  /* an input file does not have the expected form */
 
 #define XBG_FP32 0
 #define XBG_FP64 1

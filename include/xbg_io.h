@@ -1,6 +1,7 @@
 /*
- * xbg_io.h -- output path of the B200-native XBeach_GPU step: the model's
- * map output as a netCDF file, written without libnetcdf.
+ * xbg_io.h -- host-side file IO around the B200-native XBeach_GPU step: the
+ * model's map output as a netCDF file (written without libnetcdf) and the
+ * reference's input files (bathymetry, sea level, wind, wave boundaries).
  *
  * The reference writes its map output with the netCDF-C library
  * (writenetcdf.cpp:32-240): creatncfileUD creates the file with the
@@ -61,6 +62,51 @@ int xbg_nc_close(xbg_nc* f);
  * that returns host data) completes them.  ee, rr and zsold are taken from
  * the plane set current after the enqueued work. */
 int xbg_fetch_fields(xbg_handle* h, const int* fields, int n, void* const* host);
+
+/* ---- input files (read_input.cpp) -------------------------------------
+ * The reference's file formats, read on the host.  Line-based files split
+ * each line on tabs, or on spaces when a line has fewer values than the
+ * format needs, or on commas (read_input.cpp:1476-1494); numbers parse like
+ * std::stod.  A malformed file is XBG_ERR_FORMAT (the reference exits), a
+ * file that does not open XBG_ERR_IO.  Angles in the files are degrees
+ * nautical; grdalpha (grid rotation) is in radians.                        */
+#define XBG_TAB_SEALEVEL 0  /* readWLfile (:259): time, wlev0, wlev1 (wlev1 =
+                               wlev0 without a third column); '#' lines skipped */
+#define XBG_TAB_WIND     1  /* readWNDfile (:332): time, spd, dir, theta, U, V
+                               with theta = 1.5 pi - grdalpha - dir pi/180 and
+                               (U, V) = spd (cos, sin) theta; '#' lines skipped */
+#define XBG_TAB_WAVECST  2  /* ReadCstBnd (:407): time, Hs, Tp, Dp, s with Dp
+                               = 1.5 pi - grdalpha - dir pi/180              */
+#define XBG_TAB_JONSWAP  3  /* ReadJSWPBnd (:468): time, Hs, Tp, Dp, s, gamma,
+                               plus a closing record at the last time + rtlength
+                               with the last record's values                  */
+/* Reads a table file of the given kind into out (row-major, *nrec records of
+ * *ncol doubles).  out = NULL: only *nrec and *ncol; cap: records out holds. */
+int xbg_read_table(const char* path, int kind, double grdalpha, double rtlength,
+                   double* out, int cap, int* nrec, int* ncol);
+/* readbathyHead (:1508): the first line of a .md bathymetry file, nx ny dx
+ * (unused) grdalpha [degrees, as written].                                 */
+int xbg_read_md_head(const char* path, int* nx, int* ny, double* dx,
+                     double* grdalpha_deg);
+/* readbathy (:1579): the .md grid, ny rows each led by its 1-based row number,
+ * into zb[ix + (row-1)*nx] as floats; the header must give nx and ny.       */
+int xbg_read_md(const char* path, int nx, int ny, float* zb);
+/* readXBbathy (:1608): an XBeach .dep grid, nx*ny floats row by row.        */
+int xbg_read_dep(const char* path, int nx, int ny, float* zb);
+/* readXbbndhead (:25): the first line of an XBeach reuse boundary list:
+ * hdr = thetamin, thetamax, dtheta [radians], dtbc, rtlength.              */
+int xbg_read_xbbnd_head(const char* path, double* hdr);
+/* readXbbndfile (:83): the list's entries (time, Trep) and a closing entry
+ * rtlength after the last.  time = Trep = NULL: only *nrec.                */
+int xbg_read_xbbnd_list(const char* path, double rtlength, double* time,
+                        double* Trep, int cap, int* nrec);
+/* readXbbndstep (:161): the records of entry `step`: its q file (4*ny*nrec
+ * doubles, qbnd layout) and E file (ntheta*ny*nrec doubles, St layout), with
+ * nrec = ceil(rtlength / dtbc), each value rounded to float as the
+ * reference stores it, and the entry's Trep (float-rounded).  Directly the
+ * St and qbnd of xbg_set_wave_boundary.                                    */
+int xbg_read_xbbnd_step(const char* path, int step, int ny, int ntheta, int nrec,
+                        double* q, double* St, double* Trep);
 
 #ifdef __cplusplus
 }

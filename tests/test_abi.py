@@ -54,5 +54,5 @@ def test_params_sanity_matches_python(lib):
 
 
 def test_status_strings(lib):
-    for s in range(10):
+    for s in range(11):
         assert lib.xbg_status_string(s)

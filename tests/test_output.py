@@ -83,3 +83,48 @@ def test_refuses_temporaries(tmp_path):
     with pytest.raises(ValueError, match="ctheta"):
         output.MapOutput(m, tmp_path / "x.nc", ["zs", "ctheta"])
     m.close()
+
+
+def test_model_from_input_files(tmp_path, monkeypatch):
+    """A model set up from the reference's input files (.md bathymetry,
+    sea-level and wind tables, an XBeach reuse boundary list) runs bit for
+    bit like the same model set up from the arrays the files hold."""
+    import math
+    from xbeach_gpu_b200 import inputs
+    monkeypatch.chdir(tmp_path)
+    p, zb, bnd = make_case("linear_beach", nx=96, ny=48, ntheta=10)
+    zb32 = zb.astype(np.float32).reshape(p.ny, p.nx)
+    with open("bathy.md", "w") as f:
+        f.write(f"{p.nx}\t{p.ny}\t{p.dx}\t0\t0\n")
+        for j in range(p.ny):
+            f.write(f"{j + 1}\t" + "\t".join(repr(float(v)) for v in zb32[j]) + "\n")
+    open("wl.txt", "w").write("0\t0.1\t0.2\n100000\t0.1\t0.2\n")
+    open("wind.txt", "w").write("# t spd dir\n0 5 270\n100000 5 270\n")
+    dtbc = p.dtbc
+    nrec = math.ceil(p.rtlength / dtbc)          # the records a reuse step holds
+    bnd["q"][:nrec].astype("<f8").tofile("q0.bin")
+    bnd["St"][:nrec].astype("<f8").tofile("E0.bin")
+    open("list.txt", "w").write(f"{math.degrees(p.thetamin)} {math.degrees(p.thetamax)} "
+                                f"{math.degrees(p.dtheta)} {dtbc} {p.rtlength}\n"
+                                f"0.0 {bnd['Trep']} q0.bin E0.bin\n")
+    a = Model(p, XBG_FP32)
+    nx, ny, dx, ga, zbf = inputs.read_md("bathy.md")
+    assert (nx, ny, dx) == (p.nx, p.ny, p.dx)
+    inputs.apply_series(a, inputs.read_sealevel("wl.txt"), inputs.read_wind("wind.txt", ga))
+    xb = inputs.XBeachReuse("list.txt")
+    assert xb.nrec == nrec
+    xb.apply(a, 0)
+    a.init_state(zbf, 0.1, 0.2)
+    b = Model(p, XBG_FP32)
+    th = 1.5 * 3.14159265 - 0.0 - 270 * 3.14159265 / 180
+    b.set_sealevel([0.0, 100000.0], [0.1, 0.1], [0.2, 0.2])
+    b.set_wind([0.0, 100000.0], [5 * math.cos(th)] * 2, [5 * math.sin(th)] * 2)
+    b.set_wave_boundary(0, bnd["St"][:nrec].astype(np.float32).astype(np.float64),
+                        bnd["q"][:nrec].astype(np.float32).astype(np.float64), t0=0.0, tend=p.rtlength,
+                        Trep=float(np.float32(bnd["Trep"])))
+    b.init_state(zb32, 0.1, 0.2)
+    a.advance(60)
+    b.advance(60)
+    for f in ("zs", "uu", "H", "ee", "zb"):
+        np.testing.assert_array_equal(a.get(f), b.get(f), err_msg=f)
+    a.close(); b.close()

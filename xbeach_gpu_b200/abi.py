@@ -18,7 +18,8 @@ XBG_ERR_BOUNDARY = 8
 STATUS_NAMES = {
     0: "ok", 1: "bad argument", 2: "CUDA error", 3: "model crashed (dt NaN/inf/0)",
     4: "initial dt too small", 5: "device wait timed out", 6: "call out of order",
-    7: "out of device memory", 8: "ran past the uploaded wave boundary", 9: "file write failed",
+    7: "out of device memory", 8: "ran past the uploaded wave boundary", 9: "file could not be opened or written",
+    10: "input file format error",
 }
 
 XBG_FP32 = 0

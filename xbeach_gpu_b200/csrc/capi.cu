@@ -152,7 +152,8 @@ extern "C" const char* xbg_status_string(int s) {
         case XBG_ERR_STATE: return "call out of order";
         case XBG_ERR_NOMEM: return "out of device memory";
         case XBG_ERR_BOUNDARY: return "ran past the uploaded wave boundary";
-        case XBG_ERR_IO: return "file write failed";
+        case XBG_ERR_IO: return "file could not be opened or written";
+        case XBG_ERR_FORMAT: return "input file format error";
     }
     return "unknown status";
 }
