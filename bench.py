@@ -32,7 +32,7 @@ B_ALGO = lambda nt: 4 * (77 + 4 * nt)   # algorithmic bytes per coupled cell-upd
 # capture and its command are summarised under profiles/).  Keyed by
 # (kernel, nx, ny, ntheta); other workloads report traffic null.
 NCU_TRAFFIC = {
-    ("k_wave_fast", 2048, 1024, 18): 361501952 + 334217216,
+    ("k_wave_fast", 2048, 1024, 18): 361049088 + 335545344,
 }
 
 
