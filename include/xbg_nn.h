@@ -33,6 +33,17 @@ int xbg_nn_gemm(const void* A, const void* B, const float* bias, void* C,
 /* ksplit > 1 (requires XBG_NN_ATOMIC): the K chunks are split over ksplit
  * CTAs per row tile, each adding its partial product into C.              */
 
+/* 3x3 convolution with zero padding as an implicit GEMM on the tensor cores:
+ * Y[p][n] = act(sum over tap, c of X[b, y+dy, x+dx, c] Wt[n][tap*cin + c]
+ * + bias[n]) for the B*H*W pixels p of the NHWC bf16 input X (channel
+ * stride ldx), n < N (16..256, a multiple of 16), tap = (dy+1)*3 + dx+1; the
+ * weights' columns 9*cin..Kp-1 are ignored (Kp a multiple of 64).  Same
+ * result as xbg_nn_im2col3x3 followed by xbg_nn_gemm, without the im2col
+ * matrix.  flags: XBG_NN_RELU, XBG_NN_OUT_BF16 (else fp32 Y).             */
+int xbg_nn_conv3x3(const void* X, const void* Wt, const float* bias, void* Y,
+                   int B, int H, int W, int cin, int ldx, int N, int Kp,
+                   int ldw, int ldy, int flags, int* err, void* stream);
+
 /* ---- layers around the GEMM (NHWC bf16 tensors, [pixels][channels], the
  * channel counts multiples of 8) ------------------------------------------ */
 /* col[p][tap*C + c] = x[b, y+dy, x+dx, c] (0 outside the image; tap = (dy+1)*3

@@ -213,8 +213,217 @@ int gemm_launch(const void* A, const void* B, const float* bias, void* C, int M,
     return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA;
 }
 
+// ------------------------------------------------------------------------
+// 3x3 convolution as an implicit GEMM: y[p][n] = act(sum over tap, c of
+// x[b, y+dy, x+dx, c] w[n][tap*cin + c] + bias[n]), the A operand (one row
+// per output pixel, K = tap*cin + c) gathered from the NHWC input straight
+// into the swizzled shared-memory tile, 16 bytes (8 channels of one tap) per
+// copy, zero outside the image and beyond tap 8.  Three cp.async stages: the
+// copies of chunk k+2 overlap the MMAs of chunk k; each stage is reused
+// after its MMAs' commit arrives.  Several CTAs per SM (small tiles, little
+// shared memory); the epilogue stores 8 channels per 16-byte write.
+constexpr int CSTAGES = 3;
+
+template <int BN>
+__global__ void __launch_bounds__(256, 2) k_conv_tc(const __nv_bfloat16* __restrict__ X,
+                                                    const __nv_bfloat16* __restrict__ Wt,
+                                                    const float* __restrict__ bias, void* Y, int Bn, int H, int W,
+                                                    int cin, int ldx, int N, int Kp, int ldw, int ldy, int flags,
+                                                    int* err) {
+    constexpr int A_BYTES = GM * GK * 2;
+    constexpr int B_BYTES = BN * GK * 2;
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long mbar[CSTAGES];
+    __shared__ unsigned tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int M = Bn * H * W;
+    const int m0 = blockIdx.x * GM;
+    const int nk = Kp / GK;
+    const unsigned base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - smem_u32(smem_raw));
+    // this thread's four A rows (pixels) and its 16-byte chunk within a row
+    const int cch = tid & 7;
+    int pb[4], py[4], px[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int m = m0 + (tid >> 3) + 32 * u;
+        if (m < M) {
+            px[u] = m % W;
+            const int t = m / W;
+            py[u] = t % H;
+            pb[u] = t / H;
+        } else {
+            pb[u] = -1; py[u] = 0; px[u] = 0;
+        }
+    }
+    auto load = [&](int kc, int s) {
+        const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+        const int k = kc * GK + cch * 8;
+        const int tap = k / cin, ch = k - tap * cin;
+        const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int r = (tid >> 3) + 32 * u;
+            const unsigned dst = sa + r * 128 + ((cch ^ (r & 7)) << 4);
+            const int sy = py[u] + dy, sx = px[u] + dx;
+            if (pb[u] >= 0 && tap < 9 && sy >= 0 && sy < H && sx >= 0 && sx < W)
+                cp16(dst, X + ((size_t)(pb[u] * H + sy) * W + sx) * ldx + ch);
+            else
+                *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
+        }
+        for (int q = tid; q < BN * 8; q += 256) {
+            const int r = q >> 3, c = q & 7;
+            const unsigned dst = sb + r * 128 + ((c ^ (r & 7)) << 4);
+            if (r < N) cp16(dst, Wt + (size_t)r * ldw + kc * GK + c * 8);
+            else *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
+        }
+    };
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < CSTAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_slot;
+    const uint32_t idesc = idesc_bf16(GM, BN);
+    bool ok = true;
+    int issued = 0;   // chunks whose MMAs were committed
+    // prologue: chunks 0 .. CSTAGES-2 in flight
+    for (int kc = 0; kc < CSTAGES - 1; kc++) {
+        if (kc < nk) load(kc, kc);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc % CSTAGES;
+        // refill the stage of chunk kc-1 with chunk kc+CSTAGES-1 once its MMAs are done
+        const int kn = kc + CSTAGES - 1;
+        if (kn < nk) {
+            if (kc >= 1) {
+                const bool w = mbar_wait(smem_u32(&mbar[(kc - 1) % CSTAGES]), ((kc - 1) / CSTAGES) & 1);
+                if (!__syncthreads_and(w)) { ok = false; break; }
+            }
+            load(kn, kn % CSTAGES);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(CSTAGES - 1) : "memory");   // chunk kc has landed
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+            const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
+#pragma unroll
+            for (int j = 0; j < GK / 16; j++) {
+                const unsigned acc = (kc > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da + (uint64_t)(2 * j)), "l"(db + (uint64_t)(2 * j)), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&mbar[s]))
+                         : "memory");
+        }
+        issued = kc + 1;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (ok && nk > 0) ok = mbar_wait(smem_u32(&mbar[(nk - 1) % CSTAGES]), ((nk - 1) / CSTAGES) & 1);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok && issued > 0)   // leaving early: let the committed MMAs finish (bounded) before TMEM is freed
+        mbar_wait(smem_u32(&mbar[(issued - 1) % CSTAGES]), ((issued - 1) / CSTAGES) & 1);
+    tc_fence_after();
+
+    if (ok) {   // warp w -> TMEM lanes 32*(w%4).., column half w/4; 8 channels per store
+        const int q = warp & 3, h = warp >> 2;
+        const int row = m0 + q * 32 + lane;
+        const int half = BN / 2;
+        for (int c0 = h * half; c0 < (h + 1) * half; c0 += 8) {
+            unsigned r[8];
+            const unsigned taddr = tmem + ((unsigned)(q * 32) << 16) + (unsigned)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (row < M && c0 < N) {
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    v[j] = (nk > 0 ? __uint_as_float(r[j]) : 0.0f) + (bias ? bias[c0 + j] : 0.0f);
+                    if (flags & XBG_NN_RELU) v[j] = fmaxf(v[j], 0.0f);
+                }
+                if (flags & XBG_NN_OUT_BF16) {
+                    __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) o[j] = __float2bfloat16(v[j]);
+                    *(uint4*)((__nv_bfloat16*)Y + (size_t)row * ldy + c0) = *(const uint4*)o;
+                } else {
+                    float* d = (float*)Y + (size_t)row * ldy + c0;
+                    *(float4*)d = make_float4(v[0], v[1], v[2], v[3]);
+                    *(float4*)(d + 4) = make_float4(v[4], v[5], v[6], v[7]);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, XBG_ERR_TIMEOUT);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
+template <int BN>
+int conv_launch(const void* X, const void* Wt, const float* bias, void* Y, int Bn, int H, int W, int cin, int ldx,
+                int N, int Kp, int ldw, int ldy, int flags, int* err, cudaStream_t st) {
+    constexpr int STAGE = GM * GK * 2 + BN * GK * 2;
+    const size_t smem = (size_t)CSTAGES * STAGE + 1024;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_conv_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return XBG_ERR_CUDA;
+        attr = true;
+    }
+    const long long M = (long long)Bn * H * W;
+    k_conv_tc<BN><<<(unsigned)((M + GM - 1) / GM), 256, smem, st>>>((const __nv_bfloat16*)X,
+                                                                     (const __nv_bfloat16*)Wt, bias, Y, Bn, H, W, cin,
+                                                                     ldx, N, Kp, ldw, ldy, flags, err);
+    return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA;
+}
+
 }  // namespace nn
 }  // namespace xbg
+
+extern "C" int xbg_nn_conv3x3(const void* X, const void* Wt, const float* bias, void* Y, int B, int H, int W,
+                              int cin, int ldx, int N, int Kp, int ldw, int ldy, int flags, int* err, void* stream) {
+    using namespace xbg::nn;
+    const long long M = (long long)B * H * W;
+    if (!X || !Wt || !Y || !err || B < 1 || H < 1 || W < 1 || M > 0x7fffffffLL || cin < 8 || (cin % 8) ||
+        (ldx % 8) || ldx < cin || Kp < 9 * cin || (Kp % GK) || ldw < Kp || (ldw % 8) || N < 16 || N > 256 ||
+        (N % 16) || ldy < N || (ldy % 8) || (flags & XBG_NN_ATOMIC))
+        return XBG_ERR_ARG;
+    if (((uintptr_t)X | (uintptr_t)Wt | (uintptr_t)Y) & 15) return XBG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (N) {
+        case 16: return conv_launch<16>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 32: return conv_launch<32>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 48: return conv_launch<48>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 64: return conv_launch<64>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 96: return conv_launch<96>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 128: return conv_launch<128>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 192: return conv_launch<192>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+        case 256: return conv_launch<256>(X, Wt, bias, Y, B, H, W, cin, ldx, N, Kp, ldw, ldy, flags, err, st);
+    }
+    return XBG_ERR_ARG;
+}
 
 extern "C" int xbg_nn_gemm(const void* A, const void* B, const float* bias, void* C, int M, int N, int K, int lda,
                            int ldb, int ldc, int flags, int ksplit, int* err, void* stream) {

@@ -21,6 +21,7 @@ def lib():
     L = load()
     vp, ip = C.c_void_p, C.c_int
     L.xbg_nn_gemm.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, ip, vp, vp]
+    L.xbg_nn_conv3x3.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, ip, ip, ip, vp, vp]
     _nn = L
     return L
 
@@ -47,6 +48,24 @@ def gemm(A, B, C_out, bias=None, relu=False, err=None, stream=None, ksplit=1):
                        flags, ksplit, _p(err), st)
     if rc != 0:
         raise RuntimeError(f"xbg_nn_gemm: status {rc}")
+    return err
+
+
+def conv3x3(x, w, y, B, H, W, cin, bias=None, relu=False, err=None, stream=None):
+    """y[P, N] = act(conv3x3(x) + bias) on the tensor cores without an im2col
+    matrix: x [P, ldx] bf16 NHWC (first cin channels used), w [N, Kp] bf16
+    with K = tap * cin + c, y f32 or bf16 [P, ldy]."""
+    import torch
+    L = lib()
+    N, Kp = w.shape
+    flags = (XBG_NN_RELU if relu else 0) | (XBG_NN_OUT_BF16 if y.dtype == torch.bfloat16 else 0)
+    if err is None:
+        err = torch.zeros(1, dtype=torch.int32, device=x.device)
+    st = None if stream is None else C.c_void_p(stream)
+    rc = L.xbg_nn_conv3x3(_p(x), _p(w), _p(bias), _p(y), B, H, W, cin, x.stride(0), N, Kp, w.stride(0),
+                          y.stride(0), flags, _p(err), st)
+    if rc != 0:
+        raise RuntimeError(f"xbg_nn_conv3x3: status {rc}")
     return err
 
 
@@ -150,8 +169,13 @@ class Conv3x3:
         L = lib()
         _ok(L.xbg_nn_transpose(_p(self.wb), _p(self.wt), self.Np, self.Kp, self.Kp, self.Nk, None), "transpose W")
 
-    def forward(self, x, y, B, H, W, S, out_f32=False):
-        """x [P, cin] bf16 -> y [P, cout] (bf16) or [P, Np] (f32 when out_f32)."""
+    def forward(self, x, y, B, H, W, S, out_f32=False, implicit=True):
+        """x [P, cin] bf16 -> y [P, cout] (bf16) or [P, Np] (f32 when out_f32).
+        implicit: the implicit-GEMM convolution kernel; else im2col + GEMM
+        (the same products in the same order)."""
+        if implicit:
+            conv3x3(x, self.wb, y, B, H, W, self.cin, bias=self.b, relu=self.relu, err=S.err)
+            return
         L = lib()
         P = B * H * W
         col = S.get("col", (P, self.Kp), x.dtype)
