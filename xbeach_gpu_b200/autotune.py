@@ -17,7 +17,7 @@ import os
 
 # tile shapes of xbg_batch_set_grid and the kernels that use them
 SHAPES = {
-    0: ("tile", {"k_wave_force", "k_flow_a", "k_flow_u", "k_flow_v", "k_flow_corr", "k_flow_cont",
+    0: ("tile", {"k_wave_force", "k_flow_a", "k_flow_u", "k_flow_v", "k_flow_corr",
                  "k_flow_final", "k_sed_a", "k_sed_b", "k_sed_c"}),
     1: ("wave_rows", {"k_wave_fast"}),
     2: ("lin", {"k_disp", "k_means"}),

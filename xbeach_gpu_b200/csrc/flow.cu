@@ -9,8 +9,8 @@
 //                latbnd(uu)                           -> uu*
 //   k_flow_v     wlevslopes(y), vdvdy_adv, udvdx_adv, viscov1+2, eulervstep,
 //                vvlatbnd                             -> vv*
-//   k_flow_corr  wrkuu2Ocorr+uu2Ocorr, wrkvv2Ocorr+vv2Ocorr -> uu, vv
-//   k_flow_cont  depthhu, depthhv, CalcQFlow, continuity -> hu hv qx qy zs* dzsdt
+//   k_flow_corr  wrkuu2Ocorr+uu2Ocorr, wrkvv2Ocorr+vv2Ocorr, then depthhu,
+//                depthhv, CalcQFlow, continuity      -> uu vv hu hv qx qy zs* dzsdt
 //   k_flow_final wrkzs2Ocorr+zs2Ocorr, latbnd(zs), hsbnd, calcuvvu, uvlatbnd
 // (* = a per-step buffer).  viscovbnd (Flow_kernel.cu:1461) changes viscv only
 // at rows 0 and ny-2, whose eulervstep results vvlatbnd then overwrites, so it
@@ -251,6 +251,19 @@ __device__ __forceinline__ void b_flow_v(const Dev<R>& S, const Konst<R>& K, con
 }
 XBG_KERNELS(flow_v)
 
+// depthhu / depthhv (Flow_kernel.cu:653-750) at a u (v) point from the levels
+// and beds of the cell and its right (upper) neighbour and the velocity there
+template <class R>
+__device__ __forceinline__ R depth_face(R zsi, R zsn, R zbi, R zbn, R u, R eps) {
+    const R b = DM<R>::fmax((R)-1.0f * zbi, (R)-1.0f * zbn);
+    const R ummn = (R)0.0f;
+    R h;
+    if (u > ummn) h = zsi - b;
+    else if (u < (R)-1.0f * ummn) h = zsn - b;
+    else h = DM<R>::fmax(DM<R>::fmax(zsi, zsn) - b, eps);
+    return DM<R>::fmax(h, (R)0.0f);
+}
+
 // Fields of the momentum-correction pass, in its shared-memory tile.
 enum { C_ZS, C_ZB, C_UU, C_VV, C_UO, C_VO, C_QX, C_QY, C_NF };
 
@@ -307,10 +320,13 @@ __device__ __forceinline__ void wrk_v(const A& a, const Konst<R>& K, int ix, int
     }
 }
 
-// uu2Ocorr + vv2Ocorr (Flow_kernel.cu:2210-2282).  The eight input fields of
-// the block's tile (halo 3) stream into shared memory first; the wrk values of
-// the tile cells and a one-cell ring (the left, right, lower and upper
-// neighbours the corrections read) are computed once from there.
+// uu2Ocorr + vv2Ocorr (Flow_kernel.cu:2210-2282), then depthhu/depthhv,
+// CalcQFlow and continuity (:653-750, 1917, 1626-1681).  The eight input
+// fields of the block's tile (halo 3) stream into shared memory first; the
+// wrk values of the tile cells and a one-cell ring (the left, right, lower and
+// upper neighbours the corrections read) are computed once from there.
+// Continuity needs the corrected velocities of the left and lower
+// neighbours, which each thread recomputes from the ring.
 constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT_TX * FT_TY;
 constexpr int FC_H = 3;
 
@@ -341,83 +357,71 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
     if (ix >= nx || iy >= ny) return;
     int i = IDX(ix, iy);
     R dtf = (R)clk->dt, rdx = K.rdx;
-    TileAt<R, FC_H> a{tile, (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H};
-    R u = a(C_UU, 0, 0), v = a(C_VV, 0, 0);
-    if (ix > 0 && iy > 0) {
-        const int c = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
-        // uu2Ocorr: wrk at i, xp and ym
-        R w1i = sU1[c], w2i = sU2[c], w1r = sU1[c + 1], w2b = sU2[c - FT_TX];
-        R qe = (R)0.5f * (a(C_QX, 1, 0) + a(C_QX, 0, 0));
-        R qw = (R)0.5f * (a(C_QX, 0, 0) + a(C_QX, -1, 0));
-        R qn = (R)0.5f * (a(C_QY, 0, -1) + a(C_QY, 1, -1));
-        R qs = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, -1, 0));
-        u = u - dtf / ld(S.f[HUM] + i) * ((qe * w1r - qw * w1i) * rdx + (qs * w2i - qn * w2b) * rdx);
-        // vv2Ocorr: wrk at i, xm and yp
-        R v1i = sV1[c], v2i = sV2[c], v2l = sV2[c - 1], v1t = sV1[c + FT_TX];
-        qe = (R)0.5f * (a(C_QX, 0, 1) + a(C_QX, 0, 0));
-        qw = (R)0.5f * (a(C_QX, -1, 0) + a(C_QX, -1, 1));
-        qn = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, 0, -1));
-        qs = (R)0.5f * (a(C_QY, 0, 1) + a(C_QY, 0, 0));
-        v = v - dtf / ld(S.f[HVM] + i) * ((qe * v2i - qw * v2l) * rdx + (qs * v1t - qn * v1i) * rdx);
-    }
+    const int kc = (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H;
+    const int c = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
+    // uu2Ocorr at the cell r (ring index) of tile slot k, grid cell (x, y), index j:
+    // wrk at the cell, its right and lower neighbours
+    auto ucorr = [&](int k, int r, int x, int y, int j) -> R {
+        TileAt<R, FC_H> a{tile, k};
+        R u = a(C_UU, 0, 0);
+        if (x > 0 && y > 0) {
+            R w1i = sU1[r], w2i = sU2[r], w1r = sU1[r + 1], w2b = sU2[r - FT_TX];
+            R qe = (R)0.5f * (a(C_QX, 1, 0) + a(C_QX, 0, 0));
+            R qw = (R)0.5f * (a(C_QX, 0, 0) + a(C_QX, -1, 0));
+            R qn = (R)0.5f * (a(C_QY, 0, -1) + a(C_QY, 1, -1));
+            R qs = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, -1, 0));
+            u = u - dtf / ld(S.f[HUM] + j) * ((qe * w1r - qw * w1i) * rdx + (qs * w2i - qn * w2b) * rdx);
+        }
+        return u;
+    };
+    // vv2Ocorr: wrk at the cell, its left and upper neighbours
+    auto vcorr = [&](int k, int r, int x, int y, int j) -> R {
+        TileAt<R, FC_H> a{tile, k};
+        R v = a(C_VV, 0, 0);
+        if (x > 0 && y > 0) {
+            R v1i = sV1[r], v2i = sV2[r], v2l = sV2[r - 1], v1t = sV1[r + FT_TX];
+            R qe = (R)0.5f * (a(C_QX, 0, 1) + a(C_QX, 0, 0));
+            R qw = (R)0.5f * (a(C_QX, -1, 0) + a(C_QX, -1, 1));
+            R qn = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, 0, -1));
+            R qs = (R)0.5f * (a(C_QY, 0, 1) + a(C_QY, 0, 0));
+            v = v - dtf / ld(S.f[HVM] + j) * ((qe * v2i - qw * v2l) * rdx + (qs * v1t - qn * v1i) * rdx);
+        }
+        return v;
+    };
+    const R u = ucorr(kc, c, ix, iy, i);
+    const R v = vcorr(kc, c, ix, iy, i);
     S.f[UU][i] = u;
     S.f[VV][i] = v;
+    // depthhu, depthhv, CalcQFlow (Flow_kernel.cu:653-750, 1917) and continuity
+    // (:1626-1681) with the corrected velocities: the left (lower) neighbour's
+    // are recomputed from the ring; the tile is clamped like pp()
+    TileAt<R, FC_H> a{tile, kc};
+    const R eps = K.eps;
+    const R hu = depth_face(a(C_ZS, 0, 0), a(C_ZS, 1, 0), a(C_ZB, 0, 0), a(C_ZB, 1, 0), u, eps);
+    const R hv = depth_face(a(C_ZS, 0, 0), a(C_ZS, 0, 1), a(C_ZB, 0, 0), a(C_ZB, 0, 1), v, eps);
+    const R qxi = u * hu, qyi = v * hv;
+    R zs = a(C_ZS, 0, 0);
+    R dzdt = (R)0;
+    if (ix > 0) {
+        const R ul = ucorr(kc - 1, c - 1, ix - 1, iy, i - 1);
+        const R qxl = ul * depth_face(a(C_ZS, -1, 0), a(C_ZS, 0, 0), a(C_ZB, -1, 0), a(C_ZB, 0, 0), ul, eps);
+        R qyb = qyi;
+        if (iy > 0) {
+            const R vb = vcorr(kc - G::TX, c - FT_TX, ix, iy - 1, i - nx);
+            qyb = vb * depth_face(a(C_ZS, 0, -1), a(C_ZS, 0, 0), a(C_ZB, 0, -1), a(C_ZB, 0, 0), vb, eps);
+        }
+        dzdt = (qxl - qxi + qyb - qyi) * rdx;
+        zs = zs + dzdt * dtf;
+    }
+    // the new fluxes go to per-step buffers: neighbouring blocks of this pass
+    // still read the previous step's qx, qy (k_flow_final stores the final ones)
+    S.f[HU][i] = hu; S.f[HV][i] = hv;
+    S.tmp[T_QX][i] = qxi; S.tmp[T_QY][i] = qyi;
+    if (ix > 0) S.f[DZSDT][i] = dzdt;
+    S.tmp[T_ZS][i] = zs;
 }
 XBG_KERNELS(flow_corr)
 
-// depthhu / depthhv (Flow_kernel.cu:653-750)
-template <class R>
-__device__ __forceinline__ R depth_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
-    const int nx = K.nx;
-    int i = IDX(ix, iy), j = IDX(pp(ix, nx), iy);
-    R zsi = ld(S.f[ZS] + i), zsr = ld(S.f[ZS] + j);
-    R b = DM<R>::fmax((R)-1.0f * ld(S.f[ZB] + i), (R)-1.0f * ld(S.f[ZB] + j));
-    R u = ld(S.f[UU] + i), h;
-    const R ummn = (R)0.0f;
-    if (u > ummn) h = zsi - b;
-    else if (u < (R)-1.0f * ummn) h = zsr - b;
-    else h = DM<R>::fmax(DM<R>::fmax(zsi, zsr) - b, K.eps);
-    return DM<R>::fmax(h, (R)0.0f);
-}
-template <class R>
-__device__ __forceinline__ R depth_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
-    const int nx = K.nx, ny = K.ny;
-    int i = IDX(ix, iy), j = IDX(ix, pp(iy, ny));
-    R zsi = ld(S.f[ZS] + i), zst = ld(S.f[ZS] + j);
-    R b = DM<R>::fmax((R)-1.0f * ld(S.f[ZB] + i), (R)-1.0f * ld(S.f[ZB] + j));
-    R v = ld(S.f[VV] + i), h;
-    const R ummn = (R)0.0f;
-    if (v > ummn) h = zsi - b;
-    else if (v < (R)-1 * ummn) h = zst - b;
-    else h = DM<R>::fmax(DM<R>::fmax(zsi, zst) - b, K.eps);
-    return DM<R>::fmax(h, (R)0.0f);
-}
-
-template <class R>
-__device__ __forceinline__ void b_flow_cont(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
-    const Clock* clk = S.clk;
-    if (halted(clk)) return;
-    const int nx = K.nx, ny = K.ny;
-    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
-    if (ix >= nx || iy >= ny) return;
-    int i = IDX(ix, iy);
-    R dtf = (R)clk->dt;
-    R hu = depth_u(S, K, ix, iy), hv = depth_v(S, K, ix, iy);
-    R qxi = ld(S.f[UU] + i) * hu, qyi = ld(S.f[VV] + i) * hv;   // CalcQFlow
-    S.f[HU][i] = hu; S.f[HV][i] = hv;
-    S.f[QX][i] = qxi; S.f[QY][i] = qyi;
-    R zs = ld(S.f[ZS] + i);
-    if (ix > 0) {   // continuity (Flow_kernel.cu:1626-1681)
-        int xm = mm(ix), ym = mm(iy);
-        R qxl = ld(S.f[UU] + IDX(xm, iy)) * depth_u(S, K, xm, iy);
-        R qyb = (ym == iy) ? qyi : ld(S.f[VV] + IDX(ix, ym)) * depth_v(S, K, ix, ym);
-        R dzdt = (qxl - qxi + qyb - qyi) * K.rdx;
-        S.f[DZSDT][i] = dzdt;
-        zs = zs + dzdt * dtf;
-    }
-    S.tmp[T_ZS][i] = zs;
-}
-XBG_KERNELS(flow_cont)
 
 // Fields of the final pass, in its shared-memory tile: the post-continuity
 // level, bed, previous step's level, corrected velocities, Stokes drift inputs.
@@ -538,7 +542,7 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
         return z;
     };
     R zf = zcorr(a, k, iy);
-    R qx = ld(S.f[QX] + i), qy = ld(S.f[QY] + i);
+    R qx = ld(S.tmp[T_QX] + i), qy = ld(S.tmp[T_QY] + i);
     R wu = (R)ld(S.wetu + IDX(ix, sy)), wv = (R)ld(S.wetv + IDX(ix, sy));
     if (sy != iy) {           // latbnd(zs)
         if (ks >= FT_TX) zf = zcorr(as, ks, sy);
@@ -546,10 +550,9 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
     }
     R o6[6];
     uvvu_cell(as, wu, wv, sS, sC, ks, o6);   // calcuvvu + uvlatbnd
-    if (ix > 0 && iy > 0) {   // zs2Ocorr flux update
-        S.f[QX][i] = qx + sW1[k];
-        S.f[QY][i] = qy + sW2[k];
-    }
+    // CalcQFlow's fluxes, with the zs2Ocorr update in the interior
+    S.f[QX][i] = (ix > 0 && iy > 0) ? qx + sW1[k] : qx;
+    S.f[QY][i] = (ix > 0 && iy > 0) ? qy + sW2[k] : qy;
     S.f[ZS][i] = zf;
     S.f[HH][i] = DM<R>::fmax(a(Z_ZB, 0, 0) + zf, K.eps);   // hsbnd
     S.f[UUOLD][i] = a(Z_UU, 0, 0);
@@ -571,13 +574,11 @@ int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
     PMARK(pf, "k_flow_v");
     k_flow_corr<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_flow_corr");
-    k_flow_cont<R><<<g, b, 0, st>>>(S, K);
-    PMARK(pf, "k_flow_cont");
     k_flow_final<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_flow_final");
-    return 6;
+    return 5;
 }
-// the six flow kernels over every scenario of a batch
+// the five flow kernels over every scenario of a batch
 template <class R>
 int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
     dim3 b(32, 8);
@@ -591,11 +592,9 @@ int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t s
     PMARK(pf, "k_flow_v");
     kb_flow_corr<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_flow_corr");
-    kb_flow_cont<R><<<g, b, 0, st>>>(T, it, n);
-    PMARK(pf, "k_flow_cont");
     kb_flow_final<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_flow_final");
-    return 6;
+    return 5;
 }
 template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*);
 template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*);

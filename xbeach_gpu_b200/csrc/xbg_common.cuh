@@ -84,7 +84,7 @@ enum Fld {
 // Per-step temporaries (never read across steps).
 enum Tmp {
     T_UU = 0, T_VV, T_ZS, T_NUH, T_SXX, T_SXY, T_SYY, T_CEQBG, T_TSG, T_UA, T_FACERO,
-    T_ERO, T_DEPO, T_ZB, T_STDEP, T_HH, NTMP
+    T_ERO, T_DEPO, T_ZB, T_STDEP, T_HH, T_QX, T_QY, NTMP
 };
 
 template <class R>
