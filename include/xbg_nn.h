@@ -44,6 +44,29 @@ int xbg_nn_conv3x3(const void* X, const void* Wt, const float* bias, void* Y,
                    int B, int H, int W, int cin, int ldx, int N, int Kp,
                    int ldw, int ldy, int flags, int* err, void* stream);
 
+/* Weight and bias gradient of xbg_nn_conv3x3 as an implicit GEMM over the
+ * pixels: gw[n][tap*cin + c] (+)= sum over p of dz[p][n] X[b, y+dy, x+dx, c]
+ * and, when gb is not NULL, gb[n] (+)= sum over p of dz[p][n], for n < N
+ * (16, 32, 48, 64, 96, 128, 192 or 256; dz bf16 [P][ldz], ldz >= N); adds
+ * when accumulate, else stores (columns 9*cin.. of gw untouched).  The
+ * pixels are split into ksplit ranges whose partial sums go to `work` (at
+ * least xbg_nn_conv3x3_wgrad_work(cin, N, ksplit) floats, 16-B aligned) and
+ * are added in a fixed order: the result does not depend on scheduling.
+ * gw f32 [N][ldw].                                                          */
+long long xbg_nn_conv3x3_wgrad_work(int cin, int N, int ksplit);
+int xbg_nn_conv3x3_wgrad(const void* X, const void* Dz, float* gw, float* gb,
+                         float* work, int B, int H, int W, int cin, int ldx,
+                         int N, int ldz, int ldw, int ksplit,
+                         int accumulate, int* err, void* stream);
+
+/* Weights of the input-gradient convolution: wf[c][tap*cd + n] =
+ * w[n][(8-tap)*cin + c] for c < cin, n < cd (w has at least cd rows, zero
+ * beyond the layer's outputs), columns 9*cd..ldf-1 zero.  With them
+ * xbg_nn_conv3x3 of dz (cd channels) gives dx = the gradient of the
+ * convolution's input.                                                      */
+int xbg_nn_conv3x3_flip(const void* w, int ldw, int cin, int cd, void* wf,
+                        int ldf, void* stream);
+
 /* ---- layers around the GEMM (NHWC bf16 tensors, [pixels][channels], the
  * channel counts multiples of 8) ------------------------------------------ */
 /* col[p][tap*C + c] = x[b, y+dy, x+dx, c] (0 outside the image; tap = (dy+1)*3
@@ -78,7 +101,8 @@ int xbg_nn_up2_bwd(const void* dy, void* dx, int B, int h, int w, int C,
 int xbg_nn_chan_copy(void* x, void* y, long long P, int C, int ldy, int c0,
                      int reverse, int accumulate, void* stream);
 /* mean squared error of pred[P][ldp] (f32) against tgt[P][nc] (f32):
- * *loss += mean, dpred[P][ldg] (bf16) = its gradient (0 in padding). */
+ * *loss += mean, dpred[P][ldg] (bf16, ldg a multiple of 8, 16-B aligned) =
+ * its gradient (0 in padding). */
 int xbg_nn_mse(const float* pred, const float* tgt, void* dpred, float* loss,
                int P, int nc, int ldp, int ldg, void* stream);
 /* Adam step `step` (1-based) on f32 master weights p with bf16 copy pb. */

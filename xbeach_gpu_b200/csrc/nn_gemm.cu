@@ -13,8 +13,9 @@
 // (row pitch 128 B, the 16-byte chunk index XOR the row within its 8-row
 // group, 1024-B aligned tiles), fence the async proxy and sync; one thread
 // issues four tcgen05.mma of 128 x BN x 16 (smem descriptors advanced by
-// 32 B) and commits them to the stage's mbarrier.  Two stages: the copy of
-// chunk k overlaps the MMAs of chunk k-1.  The epilogue waits for the last
+// 32 B) and commits them to the stage's mbarrier.  Three stages: the copies
+// of chunk k+2 are in flight while the MMAs of chunk k run; a stage is
+// refilled once the commit of its last MMAs has arrived.  The epilogue waits for the last
 // commit, reads the accumulators with tcgen05.ld (warp w reads TMEM lanes
 // 32*(w%4).. and half of the columns), adds the bias, applies ReLU and
 // stores.  Every mbarrier wait is bounded: on time-out the kernel records an
@@ -30,7 +31,7 @@ namespace nn {
 
 constexpr int GM = 128;          // rows of a CTA tile (TMEM lanes)
 constexpr int GK = 64;           // K chunk: 64 bf16 = one 128-B swizzle row
-constexpr int GSTAGES = 2;
+constexpr int GSTAGES = 3;
 constexpr unsigned WAIT_LIMIT = 1u << 22;   // try_wait polls before giving up
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -77,7 +78,7 @@ __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence:
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
 template <int BN>
-__global__ void __launch_bounds__(256, 1) k_gemm_tc(const __nv_bfloat16* __restrict__ A,
+__global__ void __launch_bounds__(256, 2) k_gemm_tc(const __nv_bfloat16* __restrict__ A,
                                                     const __nv_bfloat16* __restrict__ B,
                                                     const float* __restrict__ bias, void* C, int M, int N, int K,
                                                     int lda, int ldb, int ldc, int flags, int* err) {
@@ -114,13 +115,9 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __nv_bfloat16* __restr
     const uint32_t idesc = idesc_bf16(GM, BN);
     const int nk = max(0, ke - kb);
     bool ok = true;
-
-    for (int kc = 0; kc < nk; kc++) {
-        const int s = kc & 1;
-        if (kc >= GSTAGES) {   // the MMAs that read this stage are done (the block leaves together if not)
-            const bool w = mbar_wait(smem_u32(&mbar[s]), ((kc - GSTAGES) >> 1) & 1);
-            if (!__syncthreads_and(w)) { ok = false; break; }
-        }
+    int issued = 0;   // chunks whose MMAs were committed
+    // copy K chunk kc (of this CTA's range) into stage s
+    auto load = [&](int kc, int s) {
         const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
         const int k0 = (kb + kc) * GK;
         for (int q = tid; q < GM * 8; q += 256) {   // A: 128 rows x 8 chunks
@@ -136,11 +133,29 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __nv_bfloat16* __restr
             if (r < N) cp16(dst, B + (size_t)r * ldb + k0 + c * 8);
             else *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
         }
-        asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+    };
+    // pipeline as in k_conv_tc: copies of chunk kc+2 overlap the MMAs of chunk kc
+    for (int kc = 0; kc < GSTAGES - 1; kc++) {
+        if (kc < nk) load(kc, kc);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc % GSTAGES;
+        const int kn = kc + GSTAGES - 1;
+        if (kn < nk) {
+            if (kc >= 1) {   // the MMAs of chunk kc-1 read the stage chunk kn goes to
+                const bool w = mbar_wait(smem_u32(&mbar[(kc - 1) % GSTAGES]), ((kc - 1) / GSTAGES) & 1);
+                if (!__syncthreads_and(w)) { ok = false; break; }
+            }
+            load(kn, kn % GSTAGES);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(GSTAGES - 1) : "memory");   // chunk kc has landed
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
+            const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
             const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
 #pragma unroll
             for (int j = 0; j < GK / 16; j++) {
@@ -154,9 +169,13 @@ __global__ void __launch_bounds__(256, 1) k_gemm_tc(const __nv_bfloat16* __restr
                              smem_u32(&mbar[s]))
                          : "memory");
         }
+        issued = kc + 1;
     }
-    if (ok && nk > 0) ok = mbar_wait(smem_u32(&mbar[(nk - 1) & 1]), ((nk - 1) >> 1) & 1);
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (ok && nk > 0) ok = mbar_wait(smem_u32(&mbar[(nk - 1) % GSTAGES]), ((nk - 1) / GSTAGES) & 1);
     ok = __syncthreads_and(ok) != 0;   // the TMEM loads below are warp-collective
+    if (!ok && issued > 0)   // leaving early: let the committed MMAs finish (bounded) before TMEM is freed
+        mbar_wait(smem_u32(&mbar[(issued - 1) % GSTAGES]), ((issued - 1) / GSTAGES) & 1);
     tc_fence_after();
 
     if (ok) {   // epilogue: warp w -> lanes 32*(w%4).., column half w/4
@@ -399,6 +418,270 @@ int conv_launch(const void* X, const void* Wt, const float* bias, void* Y, int B
     return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA;
 }
 
+
+// ------------------------------------------------------------------------
+// Weight (and bias) gradient of the 3x3 convolution as an implicit GEMM over
+// the pixels:
+//
+//   D[k][n] = sum over pixels p of col[p][k] dz[p][n],
+//   col[p][tap*cin + c] = x[b, y+dy, x+dx, c] (0 outside the image),
+//   col[p][9*cin] = 1 (the bias row: D[9*cin][n] = sum_p dz[p][n]).
+//
+// M = k (128 rows of gw^T per CTA tile), N = n (BN, the layer's padded
+// output channels), K = pixels (64 per chunk).  Both operands are indexed
+// by pixel rows with the M or N index contiguous in global memory, so both
+// are staged "MN-major": a swizzle atom is 8 pixels x W elements (W = 64,
+// 32 or 16 with the 128-, 64- or 32-byte swizzle), atoms of one operand
+// laid out [MN atom][pixel group] so that a K step of 16 pixels advances
+// the descriptor by two atoms.  Each CTA reduces a contiguous range of
+// pixel chunks (gridDim.y ranges) into its own slice of `part`; a second
+// kernel adds the slices in a fixed order, so the result does not depend
+// on scheduling.
+__device__ __forceinline__ uint64_t mn_desc(unsigned saddr, unsigned lbo, unsigned sbo, unsigned layout) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;   // stride between atoms along M/N
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;   // stride between 8-pixel groups
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)layout << 61;
+    return d;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(256, 2) k_wgrad_tc(const __nv_bfloat16* __restrict__ X,
+                                                     const __nv_bfloat16* __restrict__ Dz, float* __restrict__ part,
+                                                     int Bn, int H, int W, int cin, int ldx, int ldz, int ldp,
+                                                     int bias_row, int* err) {
+    constexpr int A_BYTES = GM * GK * 2;   // 128 k x 64 pixels
+    constexpr int B_BYTES = BN * GK * 2;   // BN n x 64 pixels
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    // B operand atom: WB channels (a multiple of 16 dividing BN)
+    constexpr int WB = (BN % 64 == 0) ? 64 : ((BN % 32 == 0) ? 32 : 16);
+    constexpr int AB = WB * 2 * 8;                       // bytes of one atom
+    constexpr unsigned BMSK = WB == 64 ? 7u : (WB == 32 ? 3u : 1u);
+    constexpr unsigned BLAYOUT = WB == 64 ? 2u : (WB == 32 ? 4u : 6u);
+    constexpr int BCH = BN / 8;                          // 16-B pieces per pixel row of B
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long mbar[CSTAGES];
+    __shared__ unsigned tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int P = Bn * H * W;
+    const int Kc = 9 * cin;
+    const int m0 = blockIdx.x * GM;
+    const int nch = (P + GK - 1) / GK;
+    const int per = (nch + gridDim.y - 1) / gridDim.y;
+    const int kb = blockIdx.y * per, ke = min(nch, kb + per);
+    const int nk = max(0, ke - kb);
+    const unsigned base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - smem_u32(smem_raw));
+    // this thread's A piece: 8 consecutive k of one tap (fixed for the CTA)
+    const int c8 = tid & 15;
+    const int kcol = m0 + c8 * 8;
+    const int tap = kcol / cin, ch = kcol - tap * cin;
+    const int tdy = tap / 3 - 1, tdx = tap % 3 - 1;
+    const bool kval = kcol < Kc;
+    const bool kbias = bias_row && kcol == Kc;
+    const unsigned a_off = (unsigned)((c8 >> 3) * 8192);   // MN atom of the piece
+    // image coordinates of this thread's four A rows (pixels p0 + (tid>>4) + 16u
+    // of the next chunk to load), advanced by 64 pixels per loaded chunk
+    int ax[4], ay[4], ab[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int p = kb * GK + (tid >> 4) + 16 * u;
+        const int t = p / W;
+        ax[u] = p - t * W;
+        ab[u] = t / H;
+        ay[u] = t - ab[u] * H;
+    }
+
+    auto load = [&](int kc, int s) {   // called for kc = 0, 1, 2, ... in order
+        const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+        const int p0 = (kb + kc) * GK;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {   // A: 64 pixels x 16 pieces
+            const int r = (tid >> 4) + 16 * u;
+            const int p = p0 + r;
+            const unsigned dst = sa + a_off + (unsigned)((r >> 3) * 1024 + (r & 7) * 128 + (((c8 & 7) ^ (r & 7)) << 4));
+            const int sy = ay[u] + tdy, sx = ax[u] + tdx;
+            if (kval && p < P && sy >= 0 && sy < H && sx >= 0 && sx < W)
+                cp16(dst, X + ((size_t)(ab[u] * H + sy) * W + sx) * ldx + ch);
+            else
+                *(uint4*)(gbase + (dst - base)) = make_uint4((kbias && p < P) ? 0x3F80u : 0u, 0u, 0u, 0u);
+            ax[u] += GK;
+            while (ax[u] >= W) {
+                ax[u] -= W;
+                if (++ay[u] == H) { ay[u] = 0; ++ab[u]; }
+            }
+        }
+        for (int q = tid; q < GK * BCH; q += 256) {   // B: 64 pixels x BCH pieces
+            const int r = q / BCH, c = q - r * BCH;
+            const int p = p0 + r;
+            const unsigned lin = (unsigned)((c / (WB / 8)) * 8 * AB + (r >> 3) * AB + (r & 7) * (2 * WB) +
+                                            (c % (WB / 8)) * 16);
+            const unsigned dst = sb + (lin ^ (((lin >> 7) & BMSK) << 4));
+            if (p < P) cp16(dst, Dz + (size_t)p * ldz + c * 8);
+            else *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
+        }
+    };
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < CSTAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_slot;
+    const uint32_t idesc = idesc_bf16(GM, BN) | (1u << 15) | (1u << 16);   // A and B MN-major
+    bool ok = true;
+    int issued = 0;
+    for (int kc = 0; kc < CSTAGES - 1; kc++) {
+        if (kc < nk) load(kc, kc);
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc % CSTAGES;
+        const int kn = kc + CSTAGES - 1;
+        if (kn < nk) {
+            if (kc >= 1) {
+                const bool w = mbar_wait(smem_u32(&mbar[(kc - 1) % CSTAGES]), ((kc - 1) / CSTAGES) & 1);
+                if (!__syncthreads_and(w)) { ok = false; break; }
+            }
+            load(kn, kn % CSTAGES);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(CSTAGES - 1) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+#pragma unroll
+            for (int j = 0; j < GK / 16; j++) {   // 16 pixels = two 8-pixel groups per step
+                const uint64_t da = mn_desc(sa + j * 2048, 8192, 1024, 2);
+                const uint64_t db = mn_desc(sb + j * 2 * AB, 8 * AB, AB, BLAYOUT);
+                const unsigned acc = (kc > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&mbar[s]))
+                         : "memory");
+        }
+        issued = kc + 1;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (ok && nk > 0) ok = mbar_wait(smem_u32(&mbar[(nk - 1) % CSTAGES]), ((nk - 1) / CSTAGES) & 1);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok && issued > 0)
+        mbar_wait(smem_u32(&mbar[(issued - 1) % CSTAGES]), ((issued - 1) / CSTAGES) & 1);
+    tc_fence_after();
+
+    if (ok) {   // warp w -> TMEM lanes (k rows) 32*(w%4).., column half w/4; part[split][n][k]
+        const int q = warp & 3, h = warp >> 2;
+        const int row = m0 + q * 32 + lane;
+        const int half = BN / 2;
+        float* dst = part + (size_t)blockIdx.y * BN * ldp;
+        const int kmax = Kc + (bias_row ? 1 : 0);
+        for (int c0 = h * half; c0 < (h + 1) * half; c0 += 8) {
+            unsigned r[8];
+            const unsigned taddr = tmem + ((unsigned)(q * 32) << 16) + (unsigned)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (row < kmax) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) dst[(size_t)(c0 + j) * ldp + row] = nk > 0 ? __uint_as_float(r[j]) : 0.0f;
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, XBG_ERR_TIMEOUT);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
+// gw[n][k] (+)= sum over s of part[s][n][k] (k < Kc), gb[n] (+)= the bias
+// row.  Block (32, 8) covers 128 consecutive k of one n, four per thread
+// (16-B loads); thread row j adds slices j, j+8, j+16, ... into two
+// accumulators (alternating), then thread row 0 adds the sixteen partial sums
+// in a fixed order -- the same order whatever the scheduling.
+__global__ void k_wgrad_reduce(const float* __restrict__ part, float* __restrict__ gw, float* __restrict__ gb, int N,
+                               int Kc, int ldp, int ldw, int ks, int accumulate) {
+    __shared__ float4 red[8][33];
+    const int kmax = Kc + (gb ? 1 : 0);
+    const int k = (blockIdx.x * 32 + threadIdx.x) * 4, n = blockIdx.y, j = threadIdx.y;
+    float4 s0 = make_float4(0.f, 0.f, 0.f, 0.f), s1 = s0;
+    if (k < kmax) {
+        const float* src = part + (size_t)n * ldp + k;
+        const size_t step = (size_t)N * ldp;
+        int i = j;
+        for (; i + 8 < ks; i += 16) {
+            const float4 a = *(const float4*)(src + (size_t)i * step);
+            const float4 b = *(const float4*)(src + (size_t)(i + 8) * step);
+            s0.x += a.x; s0.y += a.y; s0.z += a.z; s0.w += a.w;
+            s1.x += b.x; s1.y += b.y; s1.z += b.z; s1.w += b.w;
+        }
+        if (i < ks) {
+            const float4 a = *(const float4*)(src + (size_t)i * step);
+            s0.x += a.x; s0.y += a.y; s0.z += a.z; s0.w += a.w;
+        }
+    }
+    red[j][threadIdx.x] = make_float4(s0.x + s1.x, s0.y + s1.y, s0.z + s1.z, s0.w + s1.w);
+    __syncthreads();
+    if (j != 0 || k >= kmax) return;
+    float4 t = red[0][threadIdx.x];
+#pragma unroll
+    for (int r = 1; r < 8; r++) {
+        const float4 v = red[r][threadIdx.x];
+        t.x += v.x; t.y += v.y; t.z += v.z; t.w += v.w;
+    }
+    const float tv[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+        const int kk = k + e;
+        if (kk >= kmax) break;
+        float* d = kk < Kc ? gw + (size_t)n * ldw + kk : gb + n;
+        *d = accumulate ? *d + tv[e] : tv[e];
+    }
+}
+
+template <int BN>
+int wgrad_launch(const void* X, const void* Dz, float* gw, float* gb, float* work, int Bn, int H, int W, int cin,
+                 int ldx, int ldz, int ldw, int ksplit, int accumulate, int* err, cudaStream_t st) {
+    constexpr int STAGE = GM * GK * 2 + BN * GK * 2;
+    const size_t smem = (size_t)CSTAGES * STAGE + 1024;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_wgrad_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return XBG_ERR_CUDA;
+        attr = true;
+    }
+    const int Kc = 9 * cin;
+    const int ldp = Kc + 8;
+    const int bias_row = gb ? 1 : 0;
+    dim3 grid((unsigned)((Kc + bias_row + GM - 1) / GM), (unsigned)ksplit);
+    k_wgrad_tc<BN><<<grid, 256, smem, st>>>((const __nv_bfloat16*)X, (const __nv_bfloat16*)Dz, work, Bn, H, W, cin,
+                                            ldx, ldz, ldp, bias_row, err);
+    if (cudaGetLastError() != cudaSuccess) return XBG_ERR_CUDA;
+    k_wgrad_reduce<<<dim3((unsigned)((Kc + bias_row + 127) / 128), BN), dim3(32, 8), 0, st>>>(work, gw, gb, BN, Kc,
+                                                                                             ldp, ldw, ksplit,
+                                                                                             accumulate);
+    return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA;
+}
+
 }  // namespace nn
 }  // namespace xbg
 
@@ -444,6 +727,34 @@ extern "C" int xbg_nn_gemm(const void* A, const void* B, const float* bias, void
         case 128: return gemm_launch<128>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
         case 192: return gemm_launch<192>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
         case 256: return gemm_launch<256>(A, B, bias, C, M, N, K, lda, ldb, ldc, flags, ksplit, err, st);
+    }
+    return XBG_ERR_ARG;
+}
+
+extern "C" long long xbg_nn_conv3x3_wgrad_work(int cin, int N, int ksplit) {
+    return (long long)ksplit * N * (9LL * cin + 8);
+}
+
+extern "C" int xbg_nn_conv3x3_wgrad(const void* X, const void* Dz, float* gw, float* gb, float* work, int B, int H,
+                                    int W, int cin, int ldx, int N, int ldz, int ldw, int ksplit, int accumulate,
+                                    int* err, void* stream) {
+    using namespace xbg::nn;
+    const long long P = (long long)B * H * W;
+    if (!X || !Dz || !gw || !work || !err || B < 1 || H < 1 || W < 1 || P > 0x7fffffffLL || cin < 8 || (cin % 8) ||
+        (ldx % 8) || ldx < cin || (ldz % 8) || ldz < N || ldw < 9 * cin || ksplit < 1 || ksplit > 65535 ||
+        9LL * cin + 8 > 0x7fffffffLL / 256)
+        return XBG_ERR_ARG;
+    if (((uintptr_t)X | (uintptr_t)Dz | (uintptr_t)work) & 15) return XBG_ERR_ARG;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (N) {
+        case 16: return wgrad_launch<16>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 32: return wgrad_launch<32>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 48: return wgrad_launch<48>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 64: return wgrad_launch<64>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 96: return wgrad_launch<96>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 128: return wgrad_launch<128>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 192: return wgrad_launch<192>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
+        case 256: return wgrad_launch<256>(X, Dz, gw, gb, work, B, H, W, cin, ldx, ldz, ldw, ksplit, accumulate, err, st);
     }
     return XBG_ERR_ARG;
 }

@@ -223,20 +223,30 @@ __global__ void k_chan_copy(bf* __restrict__ x, bf* __restrict__ y, long long P,
 // mean squared error over P pixels x nc channels of pred[P][ldp] (f32) and
 // target[P][nc] (f32); dpred[P][ldg] (bf16) = 2 (pred - target) / (P nc),
 // zero in the padding channels; loss[0] += sum of squares / (P nc)
+// one thread per pixel and 8-wide group of gradient columns (ldg % 8 == 0):
+// one 16-byte store of the bf16 gradient, the squared errors summed per
+// block and added to *loss once per block
 __global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ tgt, bf* __restrict__ dpred,
                       float* __restrict__ loss, int P, int nc, int ldp, int ldg, float scale) {
     __shared__ float red[TPB / 32];
-    long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
     float s = 0.0f;
-    if (idx < (long long)P * ldg) {
-        const int p = (int)(idx / ldg), c = (int)(idx % ldg);
-        float g = 0.0f;
-        if (c < nc) {
-            float d = pred[(size_t)p * ldp + c] - tgt[(size_t)p * nc + c];
-            s = d * d;
-            g = 2.0f * d * scale;
+    const int G = ldg / 8;
+    const int n = P * G;   // < 2^31 (checked by the host)
+    for (int idx = blockIdx.x * TPB + threadIdx.x; idx < n; idx += gridDim.x * TPB) {
+        const int p = idx / G, c0 = (idx - p * G) * 8;
+        __align__(16) bf g[8];
+#pragma unroll
+        for (int e = 0; e < 8; e++) {
+            const int c = c0 + e;
+            float v = 0.0f;
+            if (c < nc) {
+                const float d = pred[(size_t)p * ldp + c] - tgt[(size_t)p * nc + c];
+                s += d * d;
+                v = 2.0f * d * scale;
+            }
+            g[e] = __float2bfloat16(v);
         }
-        dpred[idx] = __float2bfloat16(g);
+        *(uint4*)(dpred + (size_t)p * ldg + c0) = *(const uint4*)g;
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
@@ -308,6 +318,19 @@ __global__ void k_copy_planes(const float* const* __restrict__ src, float* const
 
 using namespace xbg::nn;
 
+// wf[c][tap*cd + n] = w[n][(8-tap)*cin + c]; zero for k >= 9*cd
+__global__ void k_flip3x3(const bf* __restrict__ w, int ldw, int cin, int cd, bf* __restrict__ wf, int ldf) {
+    const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+    if (idx >= (long long)cin * ldf) return;
+    const int c = (int)(idx / ldf), k = (int)(idx - (long long)c * ldf);
+    bf v = __float2bfloat16(0.0f);
+    if (k < 9 * cd) {
+        const int tap = k / cd, n = k - tap * cd;
+        v = w[(size_t)n * ldw + (8 - tap) * cin + c];
+    }
+    wf[idx] = v;
+}
+
 #define NN_LAUNCH(n) if ((n) <= 0) return XBG_OK; cudaStream_t st_ = (cudaStream_t)stream
 #define NN_DONE return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA
 
@@ -326,6 +349,13 @@ int xbg_nn_col2im3x3(const void* dcol, void* dx, int B, int H, int W, int C, int
     long long n = (long long)B * H * W * (C / 8);
     NN_LAUNCH(n);
     k_col2im<<<blocks_for(n), TPB, 0, st_>>>((const bf*)dcol, (bf*)dx, B, H, W, C, Kp, accumulate);
+    NN_DONE;
+}
+int xbg_nn_conv3x3_flip(const void* w, int ldw, int cin, int cd, void* wf, int ldf, void* stream) {
+    if (!w || !wf || cin < 1 || cd < 1 || ldw < 9 * cin || ldf < 9 * cd) return XBG_ERR_ARG;
+    long long n = (long long)cin * ldf;
+    NN_LAUNCH(n);
+    k_flip3x3<<<blocks_for(n), TPB, 0, st_>>>((const bf*)w, ldw, cin, cd, (bf*)wf, ldf);
     NN_DONE;
 }
 int xbg_nn_transpose(const void* src, void* dst, int R, int Cc, int lds, int ldd, void* stream) {
@@ -386,10 +416,14 @@ int xbg_nn_chan_copy(void* x, void* y, long long P, int C, int ldy, int c0, int 
 }
 int xbg_nn_mse(const float* pred, const float* tgt, void* dpred, float* loss, int P, int nc, int ldp, int ldg,
                void* stream) {
-    if (!pred || !tgt || !dpred || !loss || P < 1 || nc < 1 || ldp < nc || ldg < nc) return XBG_ERR_ARG;
-    long long n = (long long)P * ldg;
+    if (!pred || !tgt || !dpred || !loss || P < 1 || nc < 1 || ldp < nc || ldg < nc || (ldg % 8) ||
+        ((uintptr_t)dpred & 15) || (long long)P * (ldg / 8) > 0x7fffffffLL - 1184LL * TPB)
+        return XBG_ERR_ARG;
+    long long n = (long long)P * (ldg / 8);
     NN_LAUNCH(n);
-    k_mse<<<blocks_for(n), TPB, 0, st_>>>(pred, tgt, (bf*)dpred, loss, P, nc, ldp, ldg, 1.0f / ((float)P * nc));
+    // grid-stride over a few blocks per SM: one atomic add of the loss per block
+    const unsigned nb = (unsigned)(blocks_for(n) < 1184 ? blocks_for(n) : 1184);
+    k_mse<<<nb, TPB, 0, st_>>>(pred, tgt, (bf*)dpred, loss, P, nc, ldp, ldg, 1.0f / ((float)P * nc));
     NN_DONE;
 }
 int xbg_nn_adam(float* p, void* pb, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,

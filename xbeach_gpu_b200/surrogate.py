@@ -22,6 +22,9 @@ def lib():
     vp, ip = C.c_void_p, C.c_int
     L.xbg_nn_gemm.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, ip, vp, vp]
     L.xbg_nn_conv3x3.argtypes = [vp, vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, ip, ip, ip, vp, vp]
+    L.xbg_nn_conv3x3_wgrad.argtypes = [vp, vp, vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, ip, ip, ip, vp, vp]
+    L.xbg_nn_conv3x3_wgrad_work.argtypes = [ip, ip, ip]
+    L.xbg_nn_conv3x3_wgrad_work.restype = C.c_longlong
     _nn = L
     return L
 
@@ -69,6 +72,31 @@ def conv3x3(x, w, y, B, H, W, cin, bias=None, relu=False, err=None, stream=None)
     return err
 
 
+def conv3x3_wgrad(x, dz, gw, gb, work, B, H, W, cin, ksplit, err, stream=None, accumulate=True):
+    """gw[n][tap*cin + c] (+)= sum_p dz[p][n] x[p + tap offset][c] and gb[n]
+    (+)= sum_p dz[p][n] (n < gw.shape[0]) on the tensor cores, without an
+    im2col matrix; `work` holds the ksplit partial sums (f32, at least
+    xbg_nn_conv3x3_wgrad_work elements), added in a fixed order."""
+    L = lib()
+    N = gw.shape[0]
+    need = L.xbg_nn_conv3x3_wgrad_work(cin, N, ksplit)
+    if work.numel() < need:
+        raise ValueError(f"wgrad work buffer {work.numel()} < {need}")
+    st = None if stream is None else C.c_void_p(stream)
+    rc = L.xbg_nn_conv3x3_wgrad(_p(x), _p(dz), _p(gw), _p(gb), _p(work), B, H, W, cin, x.stride(0), N,
+                                dz.stride(0), gw.stride(0), ksplit, 1 if accumulate else 0, _p(err), st)
+    if rc != 0:
+        raise RuntimeError(f"xbg_nn_conv3x3_wgrad: status {rc}")
+
+
+def wgrad_split(P, cin, N):
+    """Pixel ranges of the weight-gradient kernel: about four CTAs per SM
+    over the k tiles, at least eight 64-pixel chunks per range."""
+    tiles = (9 * cin + 1 + 127) // 128
+    chunks = (P + 63) // 64
+    return max(1, min(max(1, chunks // 8), (4 * 148 + tiles - 1) // tiles, 65535))
+
+
 # ---------------------------------------------------------------- network
 import math  # noqa: E402
 
@@ -95,6 +123,7 @@ def _bind_ops(L):
     L.xbg_nn_im2col3x3.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, vp]
     L.xbg_nn_col2im3x3.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, vp]
     L.xbg_nn_transpose.argtypes = [vp, vp, ip, ip, ip, ip, vp]
+    L.xbg_nn_conv3x3_flip.argtypes = [vp, ip, ip, ip, vp, ip, vp]
     L.xbg_nn_relu_bwd.argtypes = [vp, vp, vp, ll, vp]
     L.xbg_nn_bias_grad.argtypes = [vp, vp, ip, ip, ip, vp]
     L.xbg_nn_pool2.argtypes = [vp, vp, ip, ip, ip, ip, vp]
@@ -149,7 +178,9 @@ class Conv3x3:
         self.w = torch.from_numpy(w).to(dev)
         self.b = torch.zeros(self.Np, dtype=torch.float32, device=dev)
         self.wb = torch.empty(self.Np, self.Kp, dtype=torch.bfloat16, device=dev)
-        self.wt = torch.zeros(self.Kp, self.Nk, dtype=torch.bfloat16, device=dev)   # W^T, zero padded
+        self.wt = None                   # W^T (explicit backward only), built on first use
+        self.Kd = _r64(9 * self.Np)      # K of the input-gradient convolution (dz has Np channels)
+        self.wf = torch.zeros(cin, self.Kd, dtype=torch.bfloat16, device=dev)   # flipped weights
         self.gw = torch.zeros_like(self.w)
         self.gb = torch.zeros_like(self.b)
         self.mw, self.vw = torch.zeros_like(self.w), torch.zeros_like(self.w)
@@ -166,8 +197,14 @@ class Conv3x3:
         self.refresh_t()
 
     def refresh_t(self):
+        """Derived bf16 weights after an update: the flipped weights of the
+        input-gradient convolution (and W^T once the explicit backward has
+        been used)."""
         L = lib()
-        _ok(L.xbg_nn_transpose(_p(self.wb), _p(self.wt), self.Np, self.Kp, self.Kp, self.Nk, None), "transpose W")
+        _ok(L.xbg_nn_conv3x3_flip(_p(self.wb), self.Kp, self.cin, self.Np, _p(self.wf), self.Kd, None), "flip W")
+        if self.wt is not None:
+            _ok(L.xbg_nn_transpose(_p(self.wb), _p(self.wt), self.Np, self.Kp, self.Kp, self.Nk, None),
+                "transpose W")
 
     def forward(self, x, y, B, H, W, S, out_f32=False, implicit=True):
         """x [P, cin] bf16 -> y [P, cout] (bf16) or [P, Np] (f32 when out_f32).
@@ -182,11 +219,45 @@ class Conv3x3:
         _ok(L.xbg_nn_im2col3x3(_p(x), _p(col), B, H, W, self.cin, self.Kp, P, None), "im2col")
         gemm(col, self.wb, y, bias=self.b, relu=self.relu, err=S.err)
 
-    def backward(self, x, y, dy, dx, B, H, W, S, accumulate=False, need_dx=True):
-        """dy [P, cout] (bf16 gradient of the output, [P, Nk]-padded for the
-        head) -> dx [P, cin] (+)= input gradient; gw, gb accumulate."""
+    def backward(self, x, y, dy, dx, B, H, W, S, accumulate=False, need_dx=True, implicit=True,
+                 accumulate_grad=True):
+        """dy [P, cout] (bf16 gradient of the output; the head receives the
+        loss gradient [P, >= Np], zero beyond its outputs) -> dx [P, cin] =
+        the input gradient; gw, gb accumulate (are overwritten when
+        accumulate_grad is False, implicit only).  implicit: the weight gradient
+        and the input gradient as implicit GEMMs on the tensor cores (no
+        im2col matrix; deterministic); else im2col, transposes, split-K GEMMs
+        with atomic adds and col2im (dx += when accumulate)."""
+        if not implicit:
+            self._backward_explicit(x, y, dy, dx, B, H, W, S, accumulate, need_dx)
+            return
+        import torch
+        if accumulate:
+            raise ValueError("the implicit backward writes dx; accumulate needs implicit=False")
+        L = lib()
+        P = B * H * W
+        if self.relu:
+            t = S.get("dzc", (P, self.cout), torch.bfloat16)
+            _ok(L.xbg_nn_relu_bwd(_p(dy), _p(y), _p(t), P * self.cout, None), "relu_bwd")
+        else:
+            t = dy
+        ks = wgrad_split(P, self.cin, self.Np)
+        work = S.get("wgrad", (L.xbg_nn_conv3x3_wgrad_work(self.cin, self.Np, ks),), torch.float32)
+        conv3x3_wgrad(x, t, self.gw, self.gb, work, B, H, W, self.cin, ks, S.err, accumulate=accumulate_grad)
+        if not need_dx:
+            return
+        # dx = conv3x3(dz) with the flipped weights, in output-channel slices the kernel supports
+        n0 = 0
+        for nb in _nslices(self.cin):
+            conv3x3(t, self.wf[n0:n0 + nb], dx[:, n0:n0 + nb], B, H, W, self.Np, err=S.err)
+            n0 += nb
+
+    def _backward_explicit(self, x, y, dy, dx, B, H, W, S, accumulate, need_dx):
         import torch
         L = lib()
+        if self.wt is None:
+            self.wt = torch.zeros(self.Kp, self.Nk, dtype=torch.bfloat16, device=self.w.device)
+            self.refresh_t()
         P = B * H * W
         Mpad = (P + 127) // 128 * 128
         # ReLU mask; the input-gradient GEMM reduces over Nk (a multiple of 64)
@@ -228,6 +299,16 @@ class Conv3x3:
             gemm(dz, self.wt[n0:n0 + nb], dcol[:, n0:n0 + nb], err=S.err)
             n0 += nb
         _ok(L.xbg_nn_col2im3x3(_p(dcol), _p(dx), B, H, W, self.cin, self.Kp, 1 if accumulate else 0, None), "col2im")
+
+
+def _nslices(n):
+    """n (a multiple of 16) as output-channel slices of the supported widths."""
+    out = []
+    while n > 0:
+        nb = max(g for g in GEMM_N if g <= n)
+        out.append(nb)
+        n -= nb
+    return out
 
 
 def _c8(n):
@@ -273,6 +354,8 @@ class UNet:
         self.S.err = torch.zeros(1, dtype=torch.int32, device=dev)
         self.nstep = 0
         self.act = None
+        self.implicit_bwd = True          # False: im2col / transposes / split-K GEMMs (for comparison)
+        self._acc_grad = True
 
     # -- helpers
     def _new(self, P, C, dtype=None):
@@ -323,14 +406,21 @@ class UNet:
         return self._conv("head", d1, B, H, W, out_f32=True)
 
     def _bwd(self, name, dy, accumulate_into=None, need_dx=True):
+        acc = self._acc_grad
         x, y, B, H, W = self.act[name]
         l = self.L[name]
         dx = accumulate_into if accumulate_into is not None else (self._new(B * H * W, l.cin) if need_dx else None)
-        l.backward(x, y, dy, dx, B, H, W, self.S, accumulate=accumulate_into is not None, need_dx=need_dx)
+        l.backward(x, y, dy, dx, B, H, W, self.S, accumulate=accumulate_into is not None, need_dx=need_dx,
+                   implicit=self.implicit_bwd, accumulate_grad=acc)
         return dx
 
-    def backward(self, dout, B, H, W):
-        """dout [P, 64] bf16: gradient of the loss w.r.t. the head output."""
+    def backward(self, dout, B, H, W, accumulate_grad=True):
+        """dout [P, 64] bf16: gradient of the loss w.r.t. the head output.
+        The weight and bias gradients are added to gw, gb (stored over them
+        when accumulate_grad is False: implicit backward only)."""
+        if not accumulate_grad and not self.implicit_bwd:
+            raise ValueError("accumulate_grad=False needs the implicit backward")
+        self._acc_grad = accumulate_grad
         c1, c2, c3, c4 = self.c
         L = lib()
         H2, W2, H3, W3, H4, W4 = H // 2, W // 2, H // 4, W // 4, H // 8, W // 8
@@ -384,11 +474,13 @@ class UNet:
             l.refresh_t()
 
     def train_step(self, x, tgt, B, H, W, lr=1e-3):
-        """One Adam step on a batch; returns the loss (device scalar)."""
-        self.zero_grad()
+        """One Adam step on a batch; returns the loss (device scalar).  The
+        implicit backward stores the gradients, so nothing is zeroed first."""
+        if not self.implicit_bwd:
+            self.zero_grad()
         out = self.forward(x, B, H, W)
         loss, dout = self.loss_grad(out, tgt, B * H * W)
-        self.backward(dout, B, H, W)
+        self.backward(dout, B, H, W, accumulate_grad=not self.implicit_bwd)
         self.adam(lr)
         return loss
 
