@@ -151,3 +151,65 @@ def evaluate(net, norm, data):
         out[f] = dict(surrogate=rel_err(pred[..., c], data["y"][..., c]),
                       hold=rel_err(data["hold"][..., c], data["y"][..., c]))
     return out, pred
+
+
+def conv_flops(net, B, H, W):
+    """Useful FLOPs of one forward pass (the 3x3 convolutions, by level)."""
+    scale = {"e1": 1, "e2": 2, "e3": 4, "e4": 8, "d3": 4, "d2": 2, "d1": 1, "he": 1}
+    return sum(2 * (H // scale[n[:2]]) * (W // scale[n[:2]]) * B * l.cout * 9 * l.cin for n, l in net.L.items())
+
+
+def time_training(B, H, W, steps=10, warmup=3, base=32, implicit=True, seed=1):
+    """CUDA-event times of UNet.forward and UNet.train_step on a seeded random
+    batch of B crops of H x W: (forward ms, train ms, forward TFLOP/s, train
+    TFLOP/s); a training step does three times the forward's convolution
+    FLOPs (forward, input and weight gradients)."""
+    import torch
+    from .surrogate import UNet
+    net = UNet(seed=seed, base=base)
+    net.implicit_bwd = implicit
+    g = torch.Generator(device="cuda").manual_seed(seed + 2)
+    x = torch.randn(B * H * W, IN_CH, device="cuda", generator=g).bfloat16()
+    tgt = torch.randn(B * H * W, OUT_CH, device="cuda", generator=g)
+    for _ in range(warmup):
+        net.train_step(x, tgt, B, H, W)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    for _ in range(steps):
+        net.forward(x, B, H, W)
+    ev[1].record()
+    for _ in range(steps):
+        net.train_step(x, tgt, B, H, W)
+    ev[2].record()
+    torch.cuda.synchronize()
+    net.check()
+    fw = ev[0].elapsed_time(ev[1]) / steps
+    tr = ev[1].elapsed_time(ev[2]) / steps
+    fl = conv_flops(net, B, H, W)
+    return fw, tr, fl / fw / 1e9, 3 * fl / tr / 1e9
+
+
+def main(argv=None):
+    """python -m xbeach_gpu_b200.surrogate_train time B H W [--steps S]
+    [--warmup W] [--base C] [--explicit]: times the surrogate's forward pass
+    and training step (the workload of the training profiles)."""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m xbeach_gpu_b200.surrogate_train")
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("time", help="time forward and training step on random crops")
+    t.add_argument("B", type=int)
+    t.add_argument("H", type=int)
+    t.add_argument("W", type=int)
+    t.add_argument("--steps", type=int, default=10)
+    t.add_argument("--warmup", type=int, default=3)
+    t.add_argument("--base", type=int, default=32)
+    t.add_argument("--explicit", action="store_true", help="im2col / split-K GEMM backward")
+    a = ap.parse_args(argv)
+    fw, tr, tf_fw, tf_tr = time_training(a.B, a.H, a.W, a.steps, a.warmup, a.base, not a.explicit)
+    print(f"{'explicit' if a.explicit else 'implicit'} backward, B={a.B} H={a.H} W={a.W} base={a.base}: "
+          f"forward {fw:.3f} ms ({tf_fw:.1f} TFLOP/s), training step {tr:.3f} ms ({tf_tr:.1f} TFLOP/s)")
+
+
+if __name__ == "__main__":
+    main()
