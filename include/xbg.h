@@ -211,6 +211,15 @@ int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,
  * xbg_flow_step in place of xbg_wave_step.                                   */
 int  xbg_set_wave_forcing(xbg_handle* h, const void* const* f0,
                           const void* const* f1, double w, int rescale);
+/* No counterpart in the reference.  k coupled steps in which the forcing
+ * replaces the wave sub-step: step j = 1..k runs the dt pass, ubnd1D,
+ * xbg_set_wave_forcing(f0, f1, j/k, rescale = (j == k)), flow, sediment and
+ * means -- the same kernels in the same order as those calls made one by one
+ * -- replayed from one CUDA graph captured on the first call for this
+ * (f0, f1, k).  Enqueued on the handle's stream; the planes must stay valid
+ * while it runs.                                                             */
+int  xbg_forcing_steps(xbg_handle* h, const void* const* f0,
+                       const void* const* f1, int k);
 
 /* ---- batches of scenarios ------------------------------------------------
  * No counterpart in the reference (it runs one grid per process).  A batch

@@ -133,6 +133,42 @@ def test_training_is_deterministic():
         assert e < 2e-2 and cos > 0.9998, (name, e, cos)
 
 
+def test_forcing_steps_graph_matches_the_calls():
+    """xbg_forcing_steps (k forced steps replayed from one CUDA graph) leaves
+    the model bit for bit where the same sequence of C-ABI calls made one by
+    one leaves it -- dt pass, ubnd1D, forcing at j/k (rescaled at j = k),
+    flow, sediment, means -- over two segments (the second a graph replay)."""
+    import numpy as np
+    import torch
+    from xbeach_gpu_b200.surrogate_train import OUT_FIELDS, beach_model
+    k = 5
+    a, _ = beach_model(2.2, seed=3, nx=192, ny=96, warm=30)
+    b, _ = beach_model(2.2, seed=3, nx=192, ny=96, warm=30)
+    P = 192 * 96
+    f0 = torch.empty(6, P, device="cuda")
+    for c, f in enumerate(OUT_FIELDS):
+        f0[c] = torch.from_numpy(a.get(f)).cuda()
+    f1 = f0 * torch.tensor([1.08, 1.04, 0.9, 1.1, 0.95, 1.05], device="cuda")[:, None]
+    p0 = [f0[c].data_ptr() for c in range(6)]
+    p1 = [f1[c].data_ptr() for c in range(6)]
+    torch.cuda.synchronize()
+    for _ in range(2):
+        for j in range(1, k + 1):
+            a.compute_dt()
+            a.flow_boundary()
+            a.set_wave_forcing(p0, p1, j / k, rescale=(j == k))
+            a.flow_step()
+            a.sediment_step()
+            a.accumulate_means()
+        b.forcing_steps(p0, p1, k)
+    a.sync()
+    b.sync()
+    assert a.time()[:3] == b.time()[:3]
+    for f in ("zs", "uu", "vv", "hh", "zb", "qx", "qy", "E", "H", "DR", "Fx", "Fy", "C", "ee", "rr", "zsmean",
+              "Hmean"):
+        assert np.array_equal(a.get(f), b.get(f)), f
+
+
 @pytest.fixture(scope="module")
 def trained():
     """A small surrogate trained on plain runs (256 x 128 barred beaches, two

@@ -186,6 +186,7 @@ struct xbg_handle {
     virtual int profile(float* ms, const char** names, int* n) = 0;
     virtual int put_wave_records(int slot, int first, int n, const void* St, const void* q) = 0;
     virtual int set_forcing(const void* const* f0, const void* const* f1, double w, int rescale) = 0;
+    virtual int forcing_steps(const void* const* f0, const void* const* f1, int k) = 0;
     virtual int fetch(const int* fields, int n, void* const* dst) = 0;
 };
 
@@ -222,6 +223,11 @@ struct Handle : public xbg_handle {
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
+    // graph of a forced segment (xbg_forcing_steps) and what it was captured for
+    cudaGraphExec_t seg_exec = nullptr;
+    cudaGraph_t seg_graph = nullptr;
+    const void* seg_key[13] = {};
+    int seg_launches = 0;
     int per_step_launches = 0;
     int nwave = 0;
     cudaError_t last_err = cudaSuccess;
@@ -320,6 +326,8 @@ struct Handle : public xbg_handle {
         if (st) cudaStreamSynchronize(st);
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
+        if (seg_exec) cudaGraphExecDestroy(seg_exec);
+        if (seg_graph) cudaGraphDestroy(seg_graph);
         for (void* p : allocs) cudaFree(p);
         if (ev_fork) cudaEventDestroy(ev_fork);
         if (ev_join) cudaEventDestroy(ev_join);
@@ -555,6 +563,9 @@ struct Handle : public xbg_handle {
     void drop_graph() {
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
         if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+        if (seg_exec) { cudaGraphExecDestroy(seg_exec); seg_exec = nullptr; }
+        if (seg_graph) { cudaGraphDestroy(seg_graph); seg_graph = nullptr; }
+        seg_key[12] = nullptr;
     }
 
     // one coupled step: the body of mainloopGPU (Wave_gpu.cu:620-757).  In
@@ -696,6 +707,48 @@ struct Handle : public xbg_handle {
     }
     int put_wave_records(int slot, int first, int n, const void* St, const void* q) override {
         return put_records(slot, first, n, St, q);
+    }
+    // k coupled steps whose wave sub-step is the forcing f0 + (j/k)(f1 - f0)
+    // (the rescale at j = k): per step the dt/clock pass, ubnd1D, the forcing,
+    // flow, sediment and means -- the sequence a caller gets from
+    // xbg_compute_dt, xbg_flow_boundary, xbg_set_wave_forcing, xbg_flow_step,
+    // xbg_sediment_step, xbg_accumulate_means, captured once per (f0, f1, k)
+    // as one graph and replayed.
+    int forcing_steps(const void* const* f0, const void* const* f1, int k) override {
+        Forcing6<R> a, b;
+        for (int c = 0; c < 6; c++) {
+            if (!f0[c] || !f1[c]) return XBG_ERR_ARG;
+            a.p[c] = (const R*)f0[c];
+            b.p[c] = (const R*)f1[c];
+        }
+        bool same = seg_exec && seg_key[12] == (const void*)(intptr_t)k;
+        for (int c = 0; c < 6 && same; c++) same = seg_key[c] == f0[c] && seg_key[6 + c] == f1[c];
+        if (!same) {
+            if (seg_exec) { cudaGraphExecDestroy(seg_exec); seg_exec = nullptr; }
+            if (seg_graph) { cudaGraphDestroy(seg_graph); seg_graph = nullptr; }
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int n = 0;
+            for (int j = 1; j <= k; j++) {
+                n += launch_step_begin(S, K, ser, nwave, st, nullptr);
+                if (K.flow == 1) n += launch_ubnd(S, K, ser, st, nullptr);
+                k_set_forcing<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, ee_buf[0], ee_buf[1], rr_buf[0], rr_buf[1],
+                                                                    a, b, (R)((double)j / k), j == k ? 1 : 0);
+                n++;
+                if (K.flow == 1) n += launch_flow(S, K, st, nullptr);
+                if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr);
+                n += launch_means(S, K, st, nullptr);
+            }
+            cudaError_t e = cudaStreamEndCapture(st, &seg_graph);
+            if (e != cudaSuccess) { last_err = e; return XBG_ERR_CUDA; }
+            CK(cudaGraphInstantiate(&seg_exec, seg_graph, 0));
+            for (int c = 0; c < 6; c++) { seg_key[c] = f0[c]; seg_key[6 + c] = f1[c]; }
+            seg_key[12] = (const void*)(intptr_t)k;
+            seg_launches = n;
+        }
+        clock_stale = true;
+        CK(cudaGraphLaunch(seg_exec, st));
+        launches += seg_launches;
+        return XBG_OK;
     }
 };
 
@@ -970,6 +1023,9 @@ int xbg_put_wave_records(xbg_handle* h, int slot, int first, int n, const void* 
 int xbg_mass(xbg_handle* h, double* w, double* s, double* b) { return h ? h->mass(w, s, b) : XBG_ERR_ARG; }
 int xbg_set_wave_forcing(xbg_handle* h, const void* const* f0, const void* const* f1, double w, int rescale) {
     return (h && f0 && f1) ? h->set_forcing(f0, f1, w, rescale) : XBG_ERR_ARG;
+}
+int xbg_forcing_steps(xbg_handle* h, const void* const* f0, const void* const* f1, int k) {
+    return (h && f0 && f1 && k >= 1 && k <= 100000) ? h->forcing_steps(f0, f1, k) : XBG_ERR_ARG;
 }
 
 int xbg_batch_create(const xbg_params* p, int n, int precision, xbg_batch** out) {

@@ -31,7 +31,7 @@ EXPORTS = [
     "xbg_flow_dt_noalloc",
     "xbg_batch_create", "xbg_batch_destroy", "xbg_batch_scenario", "xbg_batch_advance", "xbg_batch_status",
     "xbg_batch_sync", "xbg_batch_get_stream", "xbg_batch_profile_step", "xbg_batch_set_grid",
-    "xbg_batch_launch_count", "xbg_set_wave_forcing",
+    "xbg_batch_launch_count", "xbg_set_wave_forcing", "xbg_forcing_steps",
 ]
 
 
@@ -75,6 +75,7 @@ def load():
     L.xbg_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
     L.xbg_flow_dt_noalloc.argtypes = [ip, vp, ip, ip, C.c_double, C.c_double, vp, vp]
     L.xbg_set_wave_forcing.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, ip]
+    L.xbg_forcing_steps.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), ip]
     L.xbg_batch_create.argtypes = [C.POINTER(Params), ip, ip, C.POINTER(vp)]
     L.xbg_batch_destroy.argtypes = [vp]
     L.xbg_batch_scenario.argtypes = [vp, ip, C.POINTER(vp)]
@@ -218,6 +219,14 @@ class Model:
         a = (C.c_void_p * 6)(*[C.c_void_p(int(x)) for x in f0])
         b = (C.c_void_p * 6)(*[C.c_void_p(int(x)) for x in f1])
         _check(self.L.xbg_set_wave_forcing(self.h, a, b, float(w), 1 if rescale else 0), "set_wave_forcing")
+
+    def forcing_steps(self, f0, f1, k):
+        """k coupled steps with the wave sub-step replaced by the forcing
+        f0 + (j/k)(f1 - f0), rescaled at j = k (one CUDA graph per (f0, f1, k));
+        f0, f1: six device plane pointers (ints) each."""
+        a = (C.c_void_p * 6)(*[C.c_void_p(int(x)) for x in f0])
+        b = (C.c_void_p * 6)(*[C.c_void_p(int(x)) for x in f1])
+        _check(self.L.xbg_forcing_steps(self.h, a, b, int(k)), "forcing_steps")
 
     def profile_step(self):
         """One non-graph step with an event after every kernel: [(name, ms)]."""

@@ -11,6 +11,12 @@ runs k full plain steps (wave solver included) from the current state and
 compares their H with the network's prediction for the same k steps; when the
 relative L2 error exceeds `threshold` the run falls back to the plain method
 for good.  Flow, sediment, dt and boundaries are the plain kernels throughout.
+
+The k forced steps of a segment run as one CUDA graph (xbg_forcing_steps).
+The network's kernels run on the default stream and the model's on its own;
+CUDA events order the two (the network reads the model's state after the
+model's last step, the forced steps read the prediction after the network),
+so a segment needs no host synchronisation.
 """
 import numpy as np
 
@@ -43,41 +49,48 @@ class SurrogateRun:
         self.xi = torch.from_numpy((1.0 / norm.xs).astype(np.float32)).to(dev)
         self.ym = torch.from_numpy(norm.ym.astype(np.float32)).to(dev)
         self.ys = torch.from_numpy(norm.ys.astype(np.float32)).to(dev)
+        self.f0_ptrs = [self.f0[c].data_ptr() for c in range(OUT_CH)]
+        self.f1_ptrs = [self.f1[c].data_ptr() for c in range(OUT_CH)]
+        self._ms = torch.cuda.ExternalStream(model.stream())
+        self._ev_m = torch.cuda.Event()
+        self._ev_n = torch.cuda.Event()
         self.fallback = False
         self.steps = 0
         self.judged = []          # (step, relative H error of the prediction)
         self.surrogate_steps = 0
 
-    def _predict(self):
-        """f1 <- the network's wave fields k steps after the model's state."""
+    def _nn_after_model(self):
+        """The default stream (network kernels) waits for the model's stream."""
         import torch
+        self._ev_m.record(self._ms)
+        torch.cuda.default_stream().wait_event(self._ev_m)
+
+    def _model_after_nn(self):
+        """The model's stream waits for the default stream."""
+        import torch
+        self._ev_n.record(torch.cuda.default_stream())
+        self._ms.wait_event(self._ev_n)
+
+    def _predict(self):
+        """f1 <- the network's wave fields k steps after the model's state
+        (enqueued on the default stream after the model's work)."""
         L = lib()
-        self.m.sync()
+        self._nn_after_model()
         _ok(L.xbg_nn_encode(_p(self.enc), IN_CH, _p(self.xm), _p(self.xi), _p(self.x), self.P, None), "encode")
         out = self.net.forward(self.x, 1, self.ny, self.nx)
         _ok(L.xbg_nn_decode(_p(out), out.shape[1], _p(self.wave), _p(self.ym), _p(self.ys), _p(self.f1p), OUT_CH,
                             self.P, None), "decode")
-        torch.cuda.synchronize()
 
     def _surrogate_segment(self):
-        import torch
         self._predict()
         _ok(lib().xbg_nn_copy_planes(_p(self.wave), _p(self.f0p), OUT_CH, self.P, None), "copy planes")
-        torch.cuda.synchronize()
-        f0 = [self.f0[c].data_ptr() for c in range(OUT_CH)]
-        f1 = [self.f1[c].data_ptr() for c in range(OUT_CH)]
-        m = self.m
-        for j in range(1, self.k + 1):
-            m.compute_dt()
-            m.flow_boundary()
-            m.set_wave_forcing(f0, f1, j / self.k, rescale=(j == self.k))
-            m.flow_step()
-            m.sediment_step()
-            m.accumulate_means()
+        self._model_after_nn()
+        self.m.forcing_steps(self.f0_ptrs, self.f1_ptrs, self.k)
         self.surrogate_steps += self.k
 
     def _judge_segment(self):
         self._predict()
+        self._model_after_nn()     # the plain steps change the fields the network read
         self.m.advance(self.k)
         H = self.m.get("H").astype(np.float64)
         Hp = self.f1[OUT_FIELDS.index("H")].double().cpu().numpy()
