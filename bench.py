@@ -50,6 +50,8 @@ def parse():
                          "ragged ensemble (256 scenarios, one launch per kernel for all)")
     ap.add_argument("--scenarios", type=int, default=256)
     ap.add_argument("--no-autotune", action="store_true", help="ensemble: keep the default persistent grids")
+    ap.add_argument("--surrogate-base", type=int, default=32, choices=[16, 32],
+                    help="surrogate: channels of the U-Net's first level")
     return ap.parse_args()
 
 
@@ -345,7 +347,7 @@ def run_surrogate(args, rank, world, local):
     test_d = st.collect(nx=512, ny=256, seeds=(7,), Hs_list=(2.0,), warm=300, every=15, count=6, k=10)
     t_collect = time.perf_counter() - t0
     norm = st.Normalizer(train_d)
-    net = UNet(seed=0, base=32)
+    net = UNet(seed=0, base=args.surrogate_base)
     steps = max(200, args.steps * 3)
     t0 = time.perf_counter()
     hist = st.train(net, train_d, norm, steps=steps, batch=16, crop=128, lr=5e-4, log_every=max(1, steps // 6))
@@ -413,7 +415,8 @@ def run_surrogate(args, rank, world, local):
         "data": "synthetic (plain-run snapshots of seeded barred beaches)",
         "config": {"workload": "surrogate-assisted coupled step, 1024x512 barred beach, k=10, judge every 50 "
                                "(value: judge without a bar, 80% surrogate steps)",
-                   "train_crops": "16 x 128 x 128", "net": "U-Net 4 levels, 32 base channels, 3x3"},
+                   "train_crops": "16 x 128 x 128",
+                   "net": f"U-Net 4 levels, {args.surrogate_base} base channels, 3x3"},
         "plain_value": cells * nsteps / t_plain,
         "speedup_vs_plain": t_plain / t_sur,
         "unjudged_final_rel_err_vs_plain": final_free,

@@ -67,6 +67,14 @@ int xbg_nn_conv3x3_wgrad(const void* X, const void* Dz, float* gw, float* gb,
 int xbg_nn_conv3x3_flip(const void* w, int ldw, int cin, int cd, void* wf,
                         int ldf, void* stream);
 
+/* Training crops: dst[b] = the crop x crop window of image idx[3b] of src
+ * ([images][ny][nx] pixels of bytes_per_px bytes, a multiple of 4) whose
+ * first row and column are idx[3b+1], idx[3b+2] (a DEVICE int array; the
+ * caller keeps the windows inside the images).                             */
+int xbg_nn_gather_crops(const void* src, void* dst, const int* idx, int B,
+                        int ny, int nx, int crop, int bytes_per_px,
+                        void* stream);
+
 /* ---- layers around the GEMM (NHWC bf16 tensors, [pixels][channels], the
  * channel counts multiples of 8) ------------------------------------------ */
 /* col[p][tap*C + c] = x[b, y+dy, x+dx, c] (0 outside the image; tap = (dy+1)*3

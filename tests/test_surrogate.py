@@ -133,6 +133,31 @@ def test_training_is_deterministic():
         assert e < 2e-2 and cos > 0.9998, (name, e, cos)
 
 
+def test_training_crops_match_host_crops():
+    """The crops cut on the GPU from the resident normalised training set are
+    bit for bit the crops normalised on the host (same positions)."""
+    import numpy as np
+    import torch
+    from xbeach_gpu_b200 import surrogate_train as st
+    from xbeach_gpu_b200.surrogate import IN_CH, OUT_CH
+    rng = np.random.default_rng(4)
+    S, ny, nx = 3, 40, 56
+    data = dict(x=rng.standard_normal((S, ny, nx, IN_CH)).astype(np.float32) * 3 + 1,
+                y=rng.standard_normal((S, ny, nx, OUT_CH)).astype(np.float32),
+                hold=rng.standard_normal((S, ny, nx, OUT_CH)).astype(np.float32))
+    norm = st.Normalizer(data)
+    B, crop = 5, 24
+    xt, yt = next(st.batches(data, norm, B, crop, np.random.default_rng(9)))
+    r = np.random.default_rng(9)
+    s, y0, x0 = r.integers(0, S, B), r.integers(0, ny - crop + 1, B), r.integers(0, nx - crop + 1, B)
+    xb = np.stack([data["x"][s[i], y0[i]:y0[i] + crop, x0[i]:x0[i] + crop] for i in range(B)])
+    yb = np.stack([data["y"][s[i], y0[i]:y0[i] + crop, x0[i]:x0[i] + crop] -
+                   data["hold"][s[i], y0[i]:y0[i] + crop, x0[i]:x0[i] + crop] for i in range(B)])
+    xr = torch.from_numpy(norm.x(xb).reshape(-1, IN_CH).astype(np.float32)).cuda().bfloat16()
+    yr = torch.from_numpy(norm.y(yb).reshape(-1, OUT_CH).astype(np.float32)).cuda()
+    assert torch.equal(xt, xr) and torch.equal(yt, yr)
+
+
 def test_forcing_steps_graph_matches_the_calls():
     """xbg_forcing_steps (k forced steps replayed from one CUDA graph) leaves
     the model bit for bit where the same sequence of C-ABI calls made one by

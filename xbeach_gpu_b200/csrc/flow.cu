@@ -518,10 +518,11 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
         TileAt<R, FC_H> a{tile, k};
         R w1, w2;
         wrk_z(a, K, gx, gy, w1, w2);
-        R us = a(Z_UST, 0, 0), tm = a(Z_THM, 0, 0);
+        R us = a(Z_UST, 0, 0), tm = a(Z_THM, 0, 0), sn, cs;
+        DM<R>::sincos(tm, &sn, &cs);   // one range reduction for both
         sW1[e] = w1; sW2[e] = w2;
-        sS[e] = us * DM<R>::sin(tm);
-        sC[e] = us * DM<R>::cos(tm);
+        sS[e] = us * sn;
+        sC[e] = us * cs;
     }
     __syncthreads();
     int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;

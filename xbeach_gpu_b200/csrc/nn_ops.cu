@@ -331,6 +331,22 @@ __global__ void k_flip3x3(const bf* __restrict__ w, int ldw, int cin, int cd, bf
     wf[idx] = v;
 }
 
+// dst[b][r][q] = src[s_b][y_b + r][x_b + q] for crop x crop pixels of `wpp`
+// 4-byte words each (idx: s, y, x per crop); one thread per word
+__global__ void k_gather_crops(const unsigned* __restrict__ src, unsigned* __restrict__ dst,
+                               const int* __restrict__ idx, int ny, int nx, int crop, int wpp, long long n) {
+    const long long t = (long long)blockIdx.x * TPB + threadIdx.x;
+    if (t >= n) return;
+    const long long row = (long long)crop * wpp;        // words of one crop row
+    const long long per = row * crop;                   // words of one crop
+    const int b = (int)(t / per);
+    const long long r = t - (long long)b * per;
+    const int y = (int)(r / row);
+    const long long w = r - (long long)y * row;
+    const int s = idx[3 * b], y0 = idx[3 * b + 1], x0 = idx[3 * b + 2];
+    dst[t] = src[(((long long)s * ny + y0 + y) * nx + x0) * wpp + w];
+}
+
 #define NN_LAUNCH(n) if ((n) <= 0) return XBG_OK; cudaStream_t st_ = (cudaStream_t)stream
 #define NN_DONE return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA
 
@@ -356,6 +372,17 @@ int xbg_nn_conv3x3_flip(const void* w, int ldw, int cin, int cd, void* wf, int l
     long long n = (long long)cin * ldf;
     NN_LAUNCH(n);
     k_flip3x3<<<blocks_for(n), TPB, 0, st_>>>((const bf*)w, ldw, cin, cd, (bf*)wf, ldf);
+    NN_DONE;
+}
+int xbg_nn_gather_crops(const void* src, void* dst, const int* idx, int B, int ny, int nx, int crop,
+                        int bytes_per_px, void* stream) {
+    if (!src || !dst || !idx || B < 1 || crop < 1 || crop > ny || crop > nx || bytes_per_px < 4 ||
+        (bytes_per_px % 4) || (((uintptr_t)src | (uintptr_t)dst) & 3))
+        return XBG_ERR_ARG;
+    const long long n = (long long)B * crop * crop * (bytes_per_px / 4);
+    NN_LAUNCH(n);
+    k_gather_crops<<<blocks_for(n), TPB, 0, st_>>>((const unsigned*)src, (unsigned*)dst, idx, ny, nx, crop,
+                                                   bytes_per_px / 4, n);
     NN_DONE;
 }
 int xbg_nn_transpose(const void* src, void* dst, int R, int Cc, int lds, int ldd, void* stream) {

@@ -36,6 +36,7 @@ template <> struct DM<float> {
     static __device__ __forceinline__ float log10(float x) { return log10f(x); }
     static __device__ __forceinline__ float cos(float x) { return cosf(x); }
     static __device__ __forceinline__ float sin(float x) { return sinf(x); }
+    static __device__ __forceinline__ void sincos(float x, float* s, float* c) { sincosf(x, s, c); }
     static __device__ __forceinline__ float fabs(float x) { return fabsf(x); }
     static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
     static __device__ __forceinline__ float fmax(float a, float b) { return fmaxf(a, b); }
@@ -54,6 +55,7 @@ template <> struct DM<double> {
     static __device__ __forceinline__ double log10(double x) { return ::log10(x); }
     static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
     static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
+    static __device__ __forceinline__ void sincos(double x, double* s, double* c) { ::sincos(x, s, c); }
     static __device__ __forceinline__ double fabs(double x) { return ::fabs(x); }
     static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
     static __device__ __forceinline__ double fmax(double a, double b) { return ::fmax(a, b); }

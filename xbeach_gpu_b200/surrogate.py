@@ -124,6 +124,7 @@ def _bind_ops(L):
     L.xbg_nn_col2im3x3.argtypes = [vp, vp, ip, ip, ip, ip, ip, ip, vp]
     L.xbg_nn_transpose.argtypes = [vp, vp, ip, ip, ip, ip, vp]
     L.xbg_nn_conv3x3_flip.argtypes = [vp, ip, ip, ip, vp, ip, vp]
+    L.xbg_nn_gather_crops.argtypes = [vp, vp, vp, ip, ip, ip, ip, ip, vp]
     L.xbg_nn_relu_bwd.argtypes = [vp, vp, vp, ll, vp]
     L.xbg_nn_bias_grad.argtypes = [vp, vp, ip, ip, ip, vp]
     L.xbg_nn_pool2.argtypes = [vp, vp, ip, ip, ip, ip, vp]

@@ -92,20 +92,39 @@ class Normalizer:
         return a * self.ys + self.ym
 
 
-def batches(data, norm, batch, crop, rng):
-    """An endless stream of (x [B*crop*crop, 8] bf16, y [B*crop*crop, 6] f32)
-    CUDA tensors of random crops."""
+def device_data(data, norm):
+    """The normalised training set resident on the GPU: inputs bf16 [S, ny,
+    nx, IN_CH] and targets (the normalised k-step changes) f32 [S, ny, nx,
+    OUT_CH], built once per (data, norm)."""
     import torch
+    c = data.get("_device")
+    if c is None or c[0] is not norm:
+        x = torch.from_numpy(np.ascontiguousarray(norm.x(data["x"]), dtype=np.float32)).cuda().bfloat16()
+        y = torch.from_numpy(np.ascontiguousarray(norm.y(data["y"] - data["hold"]), dtype=np.float32)).cuda()
+        c = data["_device"] = (norm, x, y)
+    return c[1], c[2]
+
+
+def batches(data, norm, batch, crop, rng):
+    """An endless stream of (x [B*crop*crop, IN_CH] bf16, y [B*crop*crop, 6]
+    f32) CUDA tensors of random crops, cut on the GPU from the resident
+    normalised training set (xbg_nn_gather_crops); the crop positions come
+    from rng."""
+    import torch
+    from .surrogate import _bind_ops, _ok, _p, lib
+    L = lib()
+    _bind_ops(L)
     S, ny, nx, _ = data["x"].shape
+    X, Y = device_data(data, norm)
     while True:
         s = rng.integers(0, S, batch)
         y0 = rng.integers(0, ny - crop + 1, batch)
         x0 = rng.integers(0, nx - crop + 1, batch)
-        xb = np.stack([data["x"][s[i], y0[i]:y0[i] + crop, x0[i]:x0[i] + crop] for i in range(batch)])
-        yb = np.stack([data["y"][s[i], y0[i]:y0[i] + crop, x0[i]:x0[i] + crop] -
-                       data["hold"][s[i], y0[i]:y0[i] + crop, x0[i]:x0[i] + crop] for i in range(batch)])
-        xt = torch.from_numpy(norm.x(xb).reshape(-1, IN_CH).astype(np.float32)).cuda().bfloat16()
-        yt = torch.from_numpy(norm.y(yb).reshape(-1, OUT_CH).astype(np.float32)).cuda()
+        idx = torch.from_numpy(np.stack([s, y0, x0], 1).astype(np.int32).ravel()).cuda()
+        xt = torch.empty(batch * crop * crop, IN_CH, dtype=torch.bfloat16, device="cuda")
+        yt = torch.empty(batch * crop * crop, OUT_CH, dtype=torch.float32, device="cuda")
+        _ok(L.xbg_nn_gather_crops(_p(X), _p(xt), _p(idx), batch, ny, nx, crop, IN_CH * 2, None), "crops x")
+        _ok(L.xbg_nn_gather_crops(_p(Y), _p(yt), _p(idx), batch, ny, nx, crop, OUT_CH * 4, None), "crops y")
         yield xt, yt
 
 
