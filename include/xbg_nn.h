@@ -52,7 +52,9 @@ int xbg_nn_conv3x3(const void* X, const void* Wt, const float* bias, void* Y,
  * pixels are split into ksplit ranges whose partial sums go to `work` (at
  * least xbg_nn_conv3x3_wgrad_work(cin, N, ksplit) floats, 16-B aligned) and
  * are added in a fixed order: the result does not depend on scheduling.
- * gw f32 [N][ldw].                                                          */
+ * X: the convolution's NHWC bf16 input (B*H*W pixels, channel stride ldx,
+ * cin a multiple of 8, 16-B aligned); gw f32 [N][ldw], ldw >= 9*cin; *err
+ * receives XBG_ERR_TIMEOUT if a bounded tensor-core wait ran out.          */
 long long xbg_nn_conv3x3_wgrad_work(int cin, int N, int ksplit);
 int xbg_nn_conv3x3_wgrad(const void* X, const void* Dz, float* gw, float* gb,
                          float* work, int B, int H, int W, int cin, int ldx,
