@@ -130,6 +130,10 @@ int  xbg_set_field(xbg_handle* h, int field, const void* host, size_t count);
 int  xbg_get_field(xbg_handle* h, int field, void* host, size_t count);
 /* Zero-copy access: the device pointer of a field (owned by the handle). */
 int  xbg_field_device_ptr(xbg_handle* h, int field, void** dptr, size_t* count);
+/* ee (wave energy per bin) is non-negative in memory: xbg_set_field clips
+ * negative values to 0 (the reference's sanity step, Wave_kernel.cu:324,
+ * applied when the state is set); values written through the device
+ * pointer must be >= 0.                                                     */
 
 /* ---- boundaries ----------------------------------------------------------
  * Wave boundary data of one chunk: St[nrec][ntheta][ny] (Stfile layout
@@ -195,6 +199,16 @@ int  xbg_get_stream(xbg_handle* h, void** stream);
  * kernel; returns each kernel's duration [ms] and name.  *n: in = capacity,
  * out = kernels run.                                                      */
 int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
+/* Kernel variants of a phase, for comparison and tuning.  Phase
+ * XBG_PHASE_WAVE (the fused wave rows pass): variant 1 moves its plane tiles
+ * with the tensor memory accelerator (box copies issued by one thread per
+ * block; used when wave-current interaction is off and nx is a multiple of
+ * 4, the default where it applies), variant 0 copies them with every thread
+ * (cp.async).  Both give the same results bit for bit.  Setting a variant
+ * that does not apply is XBG_ERR_ARG; get reports the one in use.         */
+#define XBG_PHASE_WAVE 0
+int  xbg_set_kernel_variant(xbg_handle* h, int phase, int variant);
+int  xbg_get_kernel_variant(xbg_handle* h, int phase, int* variant);
 /* Device-side water and sediment ledgers (sum zs*dx^2, sum (C*h) dx^2,
  * sum zb dx^2) in double, computed on the device.                         */
 int  xbg_mass(xbg_handle* h, double* water, double* sediment_susp,

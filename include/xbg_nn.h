@@ -20,6 +20,12 @@ extern "C" {
 #define XBG_NN_OUT_BF16  2   /* epilogue: store bf16 (else f32) */
 #define XBG_NN_ATOMIC    4   /* epilogue: atomically add into f32 C (split-K
                                 partials; no bias or activation)          */
+#define XBG_NN_CHECK_TIMEOUT 8  /* xbg_nn_gemm only: check of the time-out
+                                exit.  Every CTA waits, with a short limit,
+                                on a barrier that nothing completes, then
+                                leaves as a stalled pipeline does: no MMA
+                                issued, C untouched, tensor memory freed,
+                                *err = XBG_ERR_TIMEOUT.                    */
 
 /* C[M x N] = act(A[M x K] . B[N x K]^T + bias[N]); A, B bf16 row-major (K
  * contiguous, leading dimensions lda/ldb in elements, multiples of 8, 16-B

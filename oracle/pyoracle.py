@@ -26,11 +26,14 @@ _lib = None
 _ref = None
 
 
-def build(ref=True):
-    """Compile the checkers (gcc); the reference part only if its sources exist."""
+def build(ref=True, ref_dir=None):
+    """Compile the checkers (gcc).  The reference part is compiled in place
+    from ref_dir (default: $XBG_REFERENCE) when that checkout exists; without
+    one the prebuilt oracle/_ref libraries are used as they are."""
     subprocess.run(["make", "-s", "-C", HERE, "_build/libxbg_oracle.so"], check=True)
-    if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref_dir = ref_dir or os.environ.get("XBG_REFERENCE")
+    if ref and ref_dir:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_dir}"], check=True)
 
 
 def lib():

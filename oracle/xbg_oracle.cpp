@@ -297,7 +297,12 @@ struct Oracle : public xbgo {
             if ((double)v < mn) mn = v;
         }
         double ndt = (T)mn * 0.5;
-        if (ndt == 0.0 || std::isinf(ndt) || std::isnan(ndt)) {
+        /* the CUDA path's dt pass also checks the state itself: a non-finite
+         * hh or zs anywhere is the same "model crashed" status */
+        const T* zs = f(XBG_F_ZS);
+        for (int i = 0; i < C; i++)
+            if (!std::isfinite((double)hh[i]) || !std::isfinite((double)zs[i])) ndt = -1.0;
+        if (!(ndt > 0.0) || std::isinf(ndt)) {
             status = XBG_ERR_NAN; return status;       /* :642-647 */
         }
         if (P.swave == 1 && totaltime > 0.0) {         /* WAVEDT :651-672 */

@@ -1,0 +1,180 @@
+"""Parity on the benchmarked workloads, not only on small grids.
+
+* The large single domain as it is benchmarked: the barred beach at
+  2048 x 1024, 18 bins over -90..90 deg (bins whose cos is ~0 at the lateral
+  limits), morfac 10.  The CUDA model steps a few whole steps; its state is
+  copied into the FP32 oracle, and one coupled step then runs phase by phase
+  on both (wave boundary, wave, flow boundary, flow, sediment, means) and is
+  compared at the per-step FP32 bar after every phase.
+* The same beach on a 256 x 128 grid for 200 whole steps against the FP64
+  error oracle, with the rule of the full-run test: the CUDA FP32 result is
+  within 3x the distance of the oracle's own FP32 result from the FP64 one,
+  per field and in the max and L2 norms.  The CUDA-FP32 vs oracle-FP32
+  distance is reported beside the 1e-3 full-run figure.
+* Eight batched scenarios drawn from the ensemble's own ranges (nx 128-1024,
+  ny 64-512, 12 bins) against the oracle run one by one: FP32 after one
+  step at the per-step bar, FP64 after 10 steps at 1e-8.
+
+Tolerances: TOL32 = 1e-5 relative (max|a-b| / max|b|) per phase; wet flags
+exact; FP64 1e-8 after 10 whole steps.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle
+from helpers import FLOW_OUT, FLOWBND_OUT, MEANS_OUT, SED_OUT, WAVE_OUT, rel_err
+from xbeach_gpu_b200.abi import FIELD_NAMES, XBG_FP32, XBG_FP64
+from xbeach_gpu_b200.model import Batch, Model
+from xbeach_gpu_b200.scenarios import make_case, make_ensemble
+
+pytestmark = pytest.mark.gpu
+
+TOL32 = 1e-5
+FULL_FIELDS = ["H", "zs", "uu", "vv", "zb"]
+
+
+def report(name, payload):
+    """Append a result line to $XBG_REPORT_DIR/parity.jsonl when set."""
+    d = os.environ.get("XBG_REPORT_DIR")
+    print(name, payload)
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "parity.jsonl"), "a") as f:
+            f.write(json.dumps({"test": name, **payload}) + "\n")
+
+
+def _setup(h, p, zb, bnd):
+    h.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    h.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    h.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    h.init_state(zb, 0.0, 0.0)
+
+
+def _cmp(a, b, names, tol, what):
+    bad, errs = [], {}
+    for n in names:
+        x, y = a.get(n), b.get(n)
+        if n in ("wetu", "wetv"):
+            nd = int(np.count_nonzero(x != y))
+            errs[n] = nd
+            if nd:
+                bad.append((n, f"{nd} flags differ"))
+            continue
+        e = rel_err(x, y)
+        errs[n] = e
+        if not e <= tol:
+            bad.append((n, e))
+    assert not bad, f"{what}: {bad}"
+    return errs
+
+
+def test_barred_beach_2048x1024_phases_vs_oracle():
+    p, zb, bnd = make_case("barred_beach")
+    assert (p.nx, p.ny, p.ntheta) == (2048, 1024, 18)
+    m = Model(p, XBG_FP32)
+    _setup(m, p, zb, bnd)
+    m.advance(4)
+    t, dt, n, _, rc = m.time()
+    assert rc == 0 and n == 4
+    o = pyoracle.Oracle(p, XBG_FP32)
+    o.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    o.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    o.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    for name in FIELD_NAMES:
+        o.set(name, m.get(name))
+    for h in (m, o):
+        h.set_time(t + dt, dt, dt)
+    worst = {}
+    for tag, call, names in (("wave", "wave_step", WAVE_OUT), ("flowbnd", "flow_boundary", FLOWBND_OUT),
+                             ("flow", "flow_step", FLOW_OUT), ("sediment", "sediment_step", SED_OUT),
+                             ("means", "accumulate_means", MEANS_OUT)):
+        if tag == "wave":
+            m.wave_boundary()
+            o.call("wave_boundary")
+        getattr(m, call)()
+        o.call(call)
+        errs = _cmp(m, o, names, TOL32, f"barred beach 2048x1024 {tag}")
+        worst[tag] = max((v for k, v in errs.items() if k not in ("wetu", "wetv")), default=0.0)
+    report("barred_beach_2048x1024_phases", {"t": t + dt, "dt": dt, "worst_rel_err_per_phase": worst, "tol": TOL32})
+
+
+def _run(h, nsteps, chunk=50):
+    done = 0
+    while done < nsteps:
+        k = min(chunk, nsteps - done)
+        h.advance(k)
+        done += k
+    t, dt, n, _, rc = h.time()
+    assert rc == 0 and n == nsteps
+    return t, {f: h.get(f).astype(np.float64) for f in FULL_FIELDS}
+
+
+def _l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def test_barred_beach_256x128_200_steps_vs_fp64_oracle():
+    """200 whole steps of the barred beach on a 256 x 128 crop (18 bins over
+    +-90 deg, morfac 10, sediment from t = 0): CUDA FP32 against the FP64
+    oracle within 3x the oracle's own FP32-vs-FP64 distance (+1e-6)."""
+    p, zb, bnd = make_case("barred_beach", nx=256, ny=128)
+    res = {}
+    for name, cls, prec in (("gpu32", Model, XBG_FP32), ("o32", pyoracle.Oracle, XBG_FP32),
+                            ("o64", pyoracle.Oracle, XBG_FP64)):
+        h = cls(p, prec)
+        _setup(h, p, zb, bnd)
+        res[name] = _run(h, 200)
+    t32, g = res["gpu32"]
+    _, o32 = res["o32"]
+    t64, o64 = res["o64"]
+    assert abs(t32 - t64) <= 1e-3 * t64
+    bad, table = {}, {}
+    for f in FULL_FIELDS:
+        row = {}
+        for nm, norm in (("max", rel_err), ("l2", _l2)):
+            ref, got = norm(o32[f], o64[f]), norm(g[f], o64[f])
+            row[nm] = {"cuda32_vs_o64": got, "o32_vs_o64": ref, "cuda32_vs_o32": norm(g[f], o32[f])}
+            if not got <= 3.0 * ref + 1e-6:
+                bad[(f, nm)] = (got, ref)
+        table[f] = row
+    report("barred_beach_256x128_200_steps", {"t_end": t32, "fields": table, "full_run_bar": 1e-3})
+    assert not bad, bad
+
+
+def _ens_cases():
+    # eight scenarios from the ensemble's ranges (nx 128..1024, ny 64..512, N = 12)
+    return make_ensemble(8, seed=2024, dtbc=5.0)
+
+
+@pytest.mark.parametrize("precision,nsteps,tol", [(XBG_FP32, 1, TOL32), (XBG_FP64, 10, 1e-8)])
+def test_batch_ensemble_ranges_vs_oracle(precision, nsteps, tol):
+    sc = _ens_cases()
+    assert all(128 <= p.nx <= 1024 and 64 <= p.ny <= 512 and p.ntheta == 12 for p, _, _ in sc)
+    b = Batch([p for p, _, _ in sc], precision)
+    for s, (p, zb, bnd) in enumerate(sc):
+        _setup(b.scenario(s), p, zb, bnd)
+    b.advance(nsteps)
+    st = b.status()
+    assert list(st["status"]) == [0] * len(sc) and list(st["nstep"]) == [nsteps] * len(sc)
+    worst = {}
+    for s, (p, zb, bnd) in enumerate(sc):
+        o = pyoracle.Oracle(p, precision)
+        _setup(o, p, zb, bnd)
+        o.advance(nsteps)
+        to, dto, no, _, rco = o.time()
+        assert rco == 0 and no == nsteps
+        assert abs(st["t"][s] - to) <= 1e-6 * max(1.0, to) and abs(st["dt"][s] - dto) <= 1e-5 * dto
+        m = b.scenario(s)
+        errs = {}
+        for f in ["H", "E", "zs", "uu", "vv", "hh", "zb", "C", "ee", "rr", "Fx", "Fy", "DR", "ueu", "qx"]:
+            errs[f] = rel_err(m.get(f), o.get(f))
+        worst[f"{p.nx}x{p.ny}"] = max(errs.values())
+        bad = {f: e for f, e in errs.items() if not e <= tol}
+        assert not bad, (s, p.nx, p.ny, bad)
+        del o
+    report(f"batch_ensemble_ranges_{'fp32' if precision == XBG_FP32 else 'fp64'}",
+           {"nsteps": nsteps, "worst_rel_err": worst, "tol": tol})
+    b.close()

@@ -1,0 +1,90 @@
+"""The wave rows pass has two implementations of the same arithmetic: plane
+tiles moved by the tensor memory accelerator (one box copy per bin, issued by
+one thread; the default where it applies) and plane tiles copied by every
+thread (cp.async).  They must give the same state bit for bit over whole
+coupled steps, on grids whose tiles are partial in x and in y, at the
+offshore and lateral edges, for few bins (fewer than the four tile buffers),
+with and without the roller, in FP32 and FP64."""
+import numpy as np
+import pytest
+
+from xbeach_gpu_b200.abi import XBG_FP32, XBG_FP64, XBG_PHASE_WAVE
+from xbeach_gpu_b200.model import Model, XbgError
+from xbeach_gpu_b200.scenarios import make_case
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ["ee", "rr", "H", "E", "D", "DR", "R", "thetamean", "Fx", "Fy", "urms", "ust", "zs", "uu", "vv", "zb",
+          "C", "hh"]
+
+CASES = {
+    "barred_256x128_n18": dict(case="barred_beach", nx=256, ny=128, nt=None, kw={}),
+    "linear_200x100_n10": dict(case="linear_beach", nx=200, ny=100, nt=10, kw={}),
+    "linear_68x37_n7": dict(case="linear_beach", nx=68, ny=37, nt=7, kw={}),
+    "linear_96x12_n3": dict(case="linear_beach", nx=96, ny=12, nt=3, kw={}),
+    "linear_64x9_n1": dict(case="linear_beach", nx=64, ny=9, nt=1, kw={}),
+    "barred_160x72_noroller": dict(case="barred_beach", nx=160, ny=72, nt=None, kw=dict(roller=0)),
+    "linear_100x50_baldock": dict(case="linear_beach", nx=100, ny=50, nt=10, kw=dict(breakmodel=2)),
+}
+
+
+def _model(c, precision, variant):
+    p, zb, bnd = make_case(c["case"], nx=c["nx"], ny=c["ny"], ntheta=c["nt"])
+    for k, v in c["kw"].items():
+        setattr(p, k, v)
+    m = Model(p, precision)
+    m.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.init_state(zb, 0.0, 0.0)
+    m.set_variant(XBG_PHASE_WAVE, variant)
+    return m
+
+
+@pytest.mark.parametrize("precision", [XBG_FP32, XBG_FP64])
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_tma_tiles_equal_thread_copied_tiles(name, precision):
+    c = CASES[name]
+    runs = []
+    for variant in (0, 1):
+        m = _model(c, precision, variant)
+        assert m.variant(XBG_PHASE_WAVE) == variant
+        m.advance(25)
+        m.advance(15)
+        t, dt, n, _, rc = m.time()
+        assert rc == 0 and n == 40
+        runs.append((t, dt, {f: m.get(f).copy() for f in FIELDS}))
+        m.close()
+    assert runs[0][:2] == runs[1][:2]
+    for f in FIELDS:
+        assert np.array_equal(runs[0][2][f], runs[1][2][f]), f
+
+
+def test_tma_variant_applies_only_where_it_can():
+    """nx not a multiple of 4 (row pitch of a tensor map) or wave-current
+    interaction on: the thread-copied tiles, and asking for the TMA ones is
+    refused."""
+    for nx, kw in ((45, {}), (64, dict(wci=1.0, hwci=0.5))):
+        p, zb, bnd = make_case("linear_beach", nx=nx, ny=32, ntheta=6)
+        for k, v in kw.items():
+            setattr(p, k, v)
+        m = Model(p)
+        assert m.variant(XBG_PHASE_WAVE) == 0
+        with pytest.raises(XbgError):
+            m.set_variant(XBG_PHASE_WAVE, 1)
+        m.close()
+    p, zb, bnd = make_case("linear_beach", nx=64, ny=32, ntheta=6)
+    m = Model(p)
+    assert m.variant(XBG_PHASE_WAVE) == 1
+    m.close()
+
+
+def test_negative_energy_is_clipped_when_set():
+    """The wave pass relies on ee >= 0 in memory (its sanity step); a caller
+    that sets negative values gets them clipped, as that step would."""
+    p, zb, bnd = make_case("linear_beach", nx=64, ny=32, ntheta=6)
+    m = Model(p)
+    ee = np.linspace(-5.0, 5.0, p.nx * p.ny * p.ntheta).astype(np.float32)
+    m.set("ee", ee)
+    assert np.array_equal(m.get("ee"), np.maximum(ee, 0.0))
+    m.close()

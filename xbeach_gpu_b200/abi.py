@@ -25,6 +25,8 @@ STATUS_NAMES = {
 XBG_FP32 = 0
 XBG_FP64 = 1
 
+XBG_PHASE_WAVE = 0   # xbg_set_kernel_variant phases
+
 XBG_FLAG_OUTPUT_DUE = 1
 XBG_FLAG_ENDED = 2
 XBG_FLAG_NEED_BOUNDARY = 4

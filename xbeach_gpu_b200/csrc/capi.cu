@@ -15,7 +15,8 @@
 #include "../../include/xbg_io.h"
 
 namespace xbg {
-template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t);
+template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t, const WaveMaps*);
+template <class R> int wave_maps_make(const Dev<R>&, const Konst<R>&, WaveMaps*);
 template <class R> int wave_parts(const Konst<R>&);
 template <class R> int wave_prepare(const Konst<R>&);
 template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
@@ -188,6 +189,8 @@ struct xbg_handle {
     virtual int set_forcing(const void* const* f0, const void* const* f1, double w, int rescale) = 0;
     virtual int forcing_steps(const void* const* f0, const void* const* f1, int k) = 0;
     virtual int fetch(const int* fields, int n, void* const* dst) = 0;
+    virtual int set_variant(int phase, int variant) = 0;
+    virtual int get_variant(int phase, int* variant) = 0;
 };
 
 struct xbg_batch {
@@ -232,6 +235,12 @@ struct Handle : public xbg_handle {
     int nwave = 0;
     cudaError_t last_err = cudaSuccess;
     double* mass_buf = nullptr;
+    // wave rows pass: TMA tiles (variant 1, when its maps could be made and
+    // wave-current interaction is off) or thread-copied tiles (variant 0)
+    WaveMaps maps;
+    bool maps_ok = false;
+    int wave_variant = 1;
+    const WaveMaps* wave_maps() const { return (maps_ok && wave_variant == 1) ? &maps : nullptr; }
 
     template <class T> int alloc(T** p, size_t n) {
         void* q = nullptr;
@@ -302,6 +311,7 @@ struct Handle : public xbg_handle {
             K.sxnth[i] = (R)std::sin(K.theta[i]);
         }
         if (wave_prepare(K)) return XBG_ERR_CUDA;
+        maps_ok = K.wci == (R)0 && wave_maps_make(S, K, &maps) == 0;
         // reductions and clock
         int nflow = step_begin_blocks(K);
         nwave = wave_parts(K);
@@ -408,6 +418,13 @@ struct Handle : public xbg_handle {
         size_t m;
         R* d = field_ptr(f, &m, c.par);
         if (!d || m != n) return XBG_ERR_ARG;
+        std::vector<R> clipped;
+        if (f == XBG_F_EE) {   // wave energy is kept non-negative in memory (the sanity step of the wave pass)
+            const R* src = (const R*)p;
+            clipped.resize(n);
+            for (size_t j = 0; j < n; j++) clipped[j] = src[j] > (R)0 ? src[j] : (R)0;
+            p = clipped.data();
+        }
         CK(cudaMemcpy(d, p, n * sizeof(R), cudaMemcpyHostToDevice));
         // double-buffered fields: both sets, so a piece-wise step (without
         // compute_dt flipping the set) reads what was set
@@ -581,11 +598,11 @@ struct Handle : public xbg_handle {
             n += launch_wavebnd(S, K, ser, side, nullptr, 0);
             if (K.flow == 1) n += launch_ubnd(S, K, ser, side, nullptr);
             cudaEventRecord(ev_join, side);
-            n += launch_wave(S, K, st, nullptr, ev_join);
+            n += launch_wave(S, K, st, nullptr, ev_join, wave_maps());
         } else {
             if (K.swave == 1) n += launch_wavebnd(S, K, ser, st, pf, 0);
             if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
-            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr);
+            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps());
         }
         if (K.flow == 1) n += launch_flow(S, K, st, pf);
         if (P.sedtrans == 1) n += launch_sed(S, K, st, pf);
@@ -632,7 +649,7 @@ struct Handle : public xbg_handle {
             case 0: n = launch_step_begin(S, K, ser, nwave, st, nullptr); break;
             case 1: if (K.swave == 1) n = launch_wavebnd(S, K, ser, st, nullptr, 1); break;
             case 2: if (K.flow == 1) n = launch_ubnd(S, K, ser, st, nullptr); break;
-            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr); break;
+            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps()); break;
             case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr); break;
             case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr); break;
             case 6: n = launch_means(S, K, st, nullptr); break;
@@ -703,6 +720,21 @@ struct Handle : public xbg_handle {
                                                             rescale);
         launches++;
         CK(cudaGetLastError());
+        return XBG_OK;
+    }
+    int set_variant(int phase, int variant) override {
+        if (phase != XBG_PHASE_WAVE || variant < 0 || variant > 1) return XBG_ERR_ARG;
+        if (variant == 1 && !maps_ok) return XBG_ERR_ARG;
+        if (variant != wave_variant) {
+            CK(cudaStreamSynchronize(st));
+            wave_variant = variant;
+            drop_graph();
+        }
+        return XBG_OK;
+    }
+    int get_variant(int phase, int* variant) override {
+        if (phase != XBG_PHASE_WAVE || !variant) return XBG_ERR_ARG;
+        *variant = wave_maps() ? 1 : 0;
         return XBG_OK;
     }
     int put_wave_records(int slot, int first, int n, const void* St, const void* q) override {
@@ -1013,6 +1045,12 @@ int xbg_fetch_fields(xbg_handle* h, const int* fields, int n, void* const* host)
 }
 int xbg_launch_count(const xbg_handle* h, int64_t* n) { if (!h || !n) return XBG_ERR_ARG; *n = h->launches; return XBG_OK; }
 int xbg_get_stream(xbg_handle* h, void** s) { if (!h || !s) return XBG_ERR_ARG; *s = h->stream(); return XBG_OK; }
+int xbg_set_kernel_variant(xbg_handle* h, int phase, int variant) {
+    return h ? h->set_variant(phase, variant) : XBG_ERR_ARG;
+}
+int xbg_get_kernel_variant(xbg_handle* h, int phase, int* variant) {
+    return h ? h->get_variant(phase, variant) : XBG_ERR_ARG;
+}
 int xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n) {
     if (!h || !ms || !n) return XBG_ERR_ARG;
     return h->profile(ms, names, n);

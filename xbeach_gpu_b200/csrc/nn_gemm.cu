@@ -33,6 +33,7 @@ constexpr int GM = 128;          // rows of a CTA tile (TMEM lanes)
 constexpr int GK = 64;           // K chunk: 64 bf16 = one 128-B swizzle row
 constexpr int GSTAGES = 3;
 constexpr unsigned WAIT_LIMIT = 1u << 22;   // try_wait polls before giving up
+constexpr unsigned CHECK_WAIT_LIMIT = 4096; // polls of the time-out check (XBG_NN_CHECK_TIMEOUT)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -61,8 +62,8 @@ __device__ __forceinline__ void mbar_init(unsigned a, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(a), "r"(count));
 }
 // bounded wait for the phase with the given parity; false on time-out
-__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity) {
-    for (unsigned it = 0; it < WAIT_LIMIT; it++) {
+__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity, unsigned limit = WAIT_LIMIT) {
+    for (unsigned it = 0; it < limit; it++) {
         unsigned ok;
         asm volatile(
             "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tc(const __nv_bfloat16* __restr
     constexpr int STAGE = A_BYTES + B_BYTES;   // multiple of 1024
     constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
     extern __shared__ unsigned char smem_raw[];
-    __shared__ __align__(8) unsigned long long mbar[GSTAGES];
+    __shared__ __align__(8) unsigned long long mbar[GSTAGES + 1];   // + the time-out check's barrier
     __shared__ unsigned tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m0 = blockIdx.x * GM;
@@ -105,7 +106,7 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tc(const __nv_bfloat16* __restr
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
     }
     if (tid == 0) {
-        for (int s = 0; s < GSTAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
+        for (int s = 0; s <= GSTAGES; s++) mbar_init(smem_u32(&mbar[s]), 1);
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     tc_fence_before();
@@ -113,8 +114,14 @@ __global__ void __launch_bounds__(256, 2) k_gemm_tc(const __nv_bfloat16* __restr
     tc_fence_after();
     const unsigned tmem = tmem_slot;
     const uint32_t idesc = idesc_bf16(GM, BN);
-    const int nk = max(0, ke - kb);
     bool ok = true;
+    if (flags & XBG_NN_CHECK_TIMEOUT) {
+        // check of the time-out exit: a short bounded wait on a barrier that
+        // nothing arrives on runs out, and the CTA leaves the way a stalled
+        // pipeline does (nothing issued, error recorded, tensor memory freed)
+        ok = __syncthreads_and(mbar_wait(smem_u32(&mbar[GSTAGES]), 0, CHECK_WAIT_LIMIT)) != 0;
+    }
+    const int nk = ok ? max(0, ke - kb) : 0;
     int issued = 0;   // chunks whose MMAs were committed
     // copy K chunk kc (of this CTA's range) into stage s
     auto load = [&](int kc, int s) {

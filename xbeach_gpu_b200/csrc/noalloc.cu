@@ -2,6 +2,9 @@
 // (the FLOWDT minimum that k_step_begin reduces) for caller-owned device
 // arrays, without allocating any device memory.
 //
+// The result is the FLOWDT part of xbg_compute_dt bit for bit (same maximum
+// depth, same single square root, same rounding).
+//
 // Who needs it: a host code that couples this model into its own solver and
 // has handed the whole device to its own pool allocator (an ocean or
 // atmosphere coupler, an ML framework's caching allocator) may not allocate
@@ -24,8 +27,10 @@
 //     before each launch; the per-block minima need no clearing (each launch
 //     writes every slot it later reads).
 //   * the first call on a device (the current device) looks up the device
-//     address of the array (cudaGetSymbolAddress) and keeps it; make that
-//     first call before any stream capture on that device.
+//     address of the array (cudaGetSymbolAddress) and keeps it for the life
+//     of the process; make that first call before any stream capture on that
+//     device.  After cudaDeviceReset the kept address is stale: reload the
+//     library (a new process) before calling it again.
 #include <mutex>
 
 #include "xbg_common.cuh"
@@ -44,12 +49,20 @@ constexpr int NA_MAX_DEVICES = 64;
 static_assert(XBG_NOALLOC_SCRATCH_BYTES >= 256 + 8 * XBG_NOALLOC_MAX_BLOCKS, "scratch too small");
 
 std::mutex na_mu;
+
+// max of two block depth maxima, where -1 marks a block that saw a
+// non-finite depth and must win
+template <class R>
+__device__ __forceinline__ R na_max(R a, R b) { return (a < (R)0 || b < (R)0) ? (R)-1 : DM<R>::fmax(a, b); }
 void* na_addr[NA_MAX_DEVICES] = {};
 
-// Same per-cell limit and reduction as k_step_begin's FLOWDT part
-// (Wave_kernel.cu:161, Wave_gpu.cu:620-640): cfl*dx/sqrt(g*hh), block
-// minima, and the last block to finish reduces them; no block waits on
-// another.  Writes 0.5 * the minimum (the dt candidate of the step).
+// Same limit and reduction as k_step_begin's FLOWDT part (Wave_kernel.cu:161,
+// Wave_gpu.cu:620-640): cfl*dx/sqrt(g*hh) falls as hh grows, so the minimum
+// over cells is the limit at the deepest cell; each block reduces the maximum
+// depth, the last block to finish reduces the block maxima and takes one
+// square root.  No block waits on another.  Writes 0.5 * the minimum (the dt
+// candidate of the step), 3.0e38 * 0.5 when no depth is positive, and NaN
+// when any depth is NaN or infinite.
 template <class R>
 __global__ void __launch_bounds__(NA_THREADS) k_flow_dt_noalloc(const R* __restrict__ hh, int n, R cfl, R dx,
                                                                  unsigned char* scratch, R* out) {
@@ -58,15 +71,19 @@ __global__ void __launch_bounds__(NA_THREADS) k_flow_dt_noalloc(const R* __restr
     __shared__ R red[NA_THREADS / 32];
     __shared__ int last;
     int tid = threadIdx.x;
-    R m = (R)3.0e38f;
-    for (int i = blockIdx.x * NA_THREADS + tid; i < n; i += gridDim.x * NA_THREADS)
-        m = DM<R>::fmin(m, cfl * dx / (DM<R>::sqrt((R)9.81f * ld(hh + i))));
-    for (int o = 16; o > 0; o >>= 1) m = DM<R>::fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((tid & 31) == 0) red[tid >> 5] = m;
+    R hmax = (R)0, probe = (R)0;   // probe: sum of hh * 0, zero only if every depth is finite
+    for (int i = blockIdx.x * NA_THREADS + tid; i < n; i += gridDim.x * NA_THREADS) {
+        const R h = ld(hh + i);
+        hmax = DM<R>::fmax(hmax, h);
+        probe = probe + h * (R)0;
+    }
+    if (!(probe == (R)0)) hmax = (R)-1;   // marks the block; carried by the max below as NaN
+    for (int o = 16; o > 0; o >>= 1) hmax = na_max(hmax, __shfl_xor_sync(0xffffffffu, hmax, o));
+    if ((tid & 31) == 0) red[tid >> 5] = hmax;
     __syncthreads();
     if (tid == 0) {
         R b = red[0];
-        for (int w = 1; w < NA_THREADS / 32; w++) b = DM<R>::fmin(b, red[w]);
+        for (int w = 1; w < NA_THREADS / 32; w++) b = na_max(b, red[w]);
         part[blockIdx.x] = b;
         __threadfence();
         last = (atomicAdd(counter, 1u) == gridDim.x - 1);
@@ -74,14 +91,17 @@ __global__ void __launch_bounds__(NA_THREADS) k_flow_dt_noalloc(const R* __restr
     __syncthreads();
     if (!last) return;
     __threadfence();
-    R mf = (R)3.0e38f;
-    for (int j = tid; j < (int)gridDim.x; j += NA_THREADS) mf = DM<R>::fmin(mf, ((volatile R*)part)[j]);
-    for (int o = 16; o > 0; o >>= 1) mf = DM<R>::fmin(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+    R hm = (R)0;
+    for (int j = tid; j < (int)gridDim.x; j += NA_THREADS) hm = na_max(hm, ((volatile R*)part)[j]);
+    for (int o = 16; o > 0; o >>= 1) hm = na_max(hm, __shfl_xor_sync(0xffffffffu, hm, o));
     __syncthreads();
-    if ((tid & 31) == 0) red[tid >> 5] = mf;
+    if ((tid & 31) == 0) red[tid >> 5] = hm;
     __syncthreads();
     if (tid == 0) {
-        for (int w = 0; w < NA_THREADS / 32; w++) mf = DM<R>::fmin(mf, red[w]);
+        for (int w = 0; w < NA_THREADS / 32; w++) hm = na_max(hm, red[w]);
+        R mf = (R)3.0e38f;
+        if (hm < (R)0) mf = (R)NAN;   // a block saw a non-finite depth
+        else if (hm > (R)0) mf = cfl * dx / (DM<R>::sqrt((R)9.81f * hm));
         *out = (R)0.5 * mf;
         *counter = 0;
     }

@@ -12,8 +12,11 @@
 //                 No block waits on another: the last block is found with an
 //                 atomic counter.  A halted step (end time, pending output,
 //                 error) sets clk->halt and every later kernel of the step
-//                 returns at once.
-//   k_ubnd        ubnd1D / ubnd1Dnowaves (Flow_kernel.cu:167-242, 332-408) in
+//                 returns at once.  The same pass checks that hh and zs
+//                 are finite everywhere; a NaN or inf sets XBG_ERR_NAN,
+//                 which halts this and every later step of the handle
+//                 (the reference exits on a NaN dt, Wave_gpu.cu:642-647).
+//   k_ubnd       ubnd1D / ubnd1Dnowaves (Flow_kernel.cu:167-242, 332-408) in
 //                 one block: the column mean of the pre-kernel uu, then the
 //                 ix = 0 column.
 //   k_means       addavg_var x6 + max_var (Wave_gpu.cu:731-757).
@@ -45,7 +48,9 @@ __device__ void finalize_scalar(const Dev<R>& S, const Konst<R>& K, const Series
     c.nstep_total++;
     R wd = (R)c.dt;                                  // wdt = dt, Wave_gpu.cu:622
     double ndt = (double)mflow * 0.5;
-    if (ndt == 0.0 || isinf(ndt) || isnan(ndt)) { c.status = XBG_ERR_NAN; return; }
+    // 0, inf or NaN (the reference's "Model crashed!", Wave_gpu.cu:642-647),
+    // or negative: a block of the dt pass saw a non-finite hh or zs
+    if (!(ndt > 0.0) || isinf(ndt)) { c.status = XBG_ERR_NAN; return; }
     if (K.swave == 1 && c.totaltime > 0.0) {
         double dtwave = (double)mwave * 0.5;
         ndt = cmin(ndt, dtwave);
@@ -75,16 +80,28 @@ __device__ __forceinline__ void b_step_begin(const Dev<R>& S, const Konst<R>& K,
     R m = (R)3.0e38f;
     {   // FLOWDT: min of hh first (4 loads in flight per thread), one sqrt per thread
         const R* hh = S.f[HH];
+        const R* zs = S.f[ZS];
         const int stride = nb * blockDim.x;
         R hmax = (R)0;
+        // health check of the state: a NaN or infinite depth or water level
+        // anywhere (the sum of every value read is finite only if each is)
+        R probe = (R)0;
         int i = bi * blockDim.x + tid;
         for (; i + 3 * stride < S.C; i += 4 * stride) {
             R a = ld(hh + i), b = ld(hh + i + stride), c = ld(hh + i + 2 * stride), d = ld(hh + i + 3 * stride);
+            R za = ld(zs + i), zb = ld(zs + i + stride), zc = ld(zs + i + 2 * stride), zd = ld(zs + i + 3 * stride);
             hmax = DM<R>::fmax(hmax, DM<R>::fmax(DM<R>::fmax(a, b), DM<R>::fmax(c, d)));
+            probe = probe + (((a + b) + (c + d)) * (R)0 + ((za + zb) + (zc + zd)) * (R)0);
         }
-        for (; i < S.C; i += stride) hmax = DM<R>::fmax(hmax, ld(hh + i));
+        for (; i < S.C; i += stride) {
+            hmax = DM<R>::fmax(hmax, ld(hh + i));
+            probe = probe + (ld(hh + i) * (R)0 + ld(zs + i) * (R)0);
+        }
         // cfl*dx/sqrt(g*hh) decreases with hh, so its minimum is at the deepest cell
         if (hmax > (R)0) m = K.cfl * K.dx / (DM<R>::sqrt((R)9.81f * hmax));
+        // a non-finite value makes this block's minimum negative, which the
+        // min reductions carry to the clock pass (no valid limit is negative)
+        if (!(probe == (R)0)) m = (R)-1;
     }
     // this block's share of the wave kernel's per-block WAVEDT minima
     R mwv = (R)3.0e38f;

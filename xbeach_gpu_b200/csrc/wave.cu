@@ -20,6 +20,7 @@
 //                dissipation.  Emits the per-block WAVEDT minimum.
 //   k_wave_force wavforce + twodimbnd(noix) + breakerdelay + twodimbnd(ust).
 #include "xbg_common.cuh"
+#include "../../include/xbg.h"
 
 namespace xbg {
 
@@ -196,20 +197,31 @@ __device__ __forceinline__ void wave_breaking(const Konst<R>& K, R esum, R hh, R
     Dq = Dv / DM<R>::fmax(Eint, (R)0.0000001f);
 }
 
+// dissipationCPU's wave-energy part of one bin (wave_CPU.cpp:1258-1295): the
+// sanitised advected energy a scaled by 1/idiv, its dissipation dd = e Dq,
+// and the new energy max(e - dt dd, 0).  One definition for every kernel
+// that forms it, so they round alike.
+template <class R>
+__device__ __forceinline__ R diss_ee(R a, R ridiv, R Dq, R dtf, R& dd) {
+    const R eet = DM<R>::fmax(a, (R)0.0f) * ridiv;
+    dd = eet * Dq;
+    return DM<R>::fmax(eet - dtf * dd, (R)0.0f);
+}
+
 // Row 0 or ny-1 (iyE), the lateral copy of row iyS = 1 or ny-2
 // (rollerlatbnd, wave_CPU.cpp:830-870, around dissipationCPU): its advected
 // ee and rr are the source row's times the wet mask, breaking and roller
 // dissipation run with the edge cell's own depth and speeds, and after
 // dissipation its ee is again the source row's (final) ee times the mask.
 // Run by the thread of the source cell, which holds the advected bins in
-// sA / sR and has already written the source cell's final ee.  Returns the
-// edge cell's WAVEDT.
-template <class R, bool ROLLER, bool WCI>
-__device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iyE, int iyS,
-                                            const R* sA, const R* sR, const Dir2<R>* sCS2, const Dir4<R>* sMom,
-                                            R esum, R sg, R dtf, R Trep, const R* rro, R* een, R* rrn) {
+// sA / sR; src_final(t) gives the source cell's final ee of bin t.  Returns
+// the edge cell's WAVEDT.
+template <class R, bool ROLLER, bool WCI, class SrcFinal>
+__device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iyE, const R* sA,
+                                            const R* sR, const Dir2<R>* sCS2, const Dir4<R>* sMom, R esum, R sg,
+                                            R dtf, R Trep, const R* rro, R* een, R* rrn, SrcFinal&& src_final) {
     const int nx = K.nx, nt = K.nt, C = S.C;
-    const int ie = ix + iyE * nx, is = ix + iyS * nx;
+    const int ie = ix + iyE * nx;
     const R dth = K.dtheta, rho = K.rho, g = K.g;
     const R hE = ld(S.f[HH] + ie);
     const bool wet = hE > K.eps;
@@ -261,11 +273,10 @@ __device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, 
         rs = DM<R>::fma(m.s2, rrt, rs);
         rcs = DM<R>::fma(m.cs, rrt, rcs);
     }
-    // the second copy of ee: the source cell's final bins (this thread's own
-    // stores, read back with ordinary loads)
+    // the second copy of ee: the source cell's final bins
     R sume = (R)0, sumethet = (R)0, ec = (R)0, es = (R)0, ecs = (R)0;
     for (int t = 0; t < nt; t++) {
-        const R eet = een[is + (size_t)t * C] * w;
+        const R eet = src_final(t) * w;
         een[ie + (size_t)t * C] = eet;
         const Dir4<R> m = sMom[t];
         sume = sume + eet;
@@ -495,9 +506,9 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         if (wet) {
 #pragma unroll 2
             for (int t = 0; t < nt; t++) {
-                R eet = DM<R>::fmax(sA[t * 256 + tid], (R)0.0f) * ridiv;
+                R dd;
+                R eet = diss_ee(sA[t * 256 + tid], ridiv, Dq, dtf, dd);
                 R rrt = sR[t * 256 + tid];
-                const R dd = eet * Dq;
                 R rrd;
                 if (WCI) {
                     const Dir2<R> d = sCS2[t];
@@ -507,7 +518,6 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
                 } else {
                     rrd = rrt * rcoef;
                 }
-                eet = DM<R>::fmax(eet - dtf * dd, (R)0.0f);
                 rrt = DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f);
                 drr = drr + rrd;
                 RR = RR + rrt;
@@ -544,12 +554,14 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
         // the lateral rows 0 and ny-1, from rows 1 and ny-2
         const R sg = (R)clk->sigm;
+        // the source cell's final bins: this thread's own stores, read back
+        auto own = [&](int t) { return een[i + (size_t)t * C]; };
         if (iy == 1)
-            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, WCI>(S, K, ix, 0, 1, sA, sR, sCS2, sMom, Etmp, sg, dtf,
-                                                                  Trep, rro, een, rrn));
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, WCI>(S, K, ix, 0, sA, sR, sCS2, sMom, Etmp, sg, dtf, Trep,
+                                                                  rro, een, rrn, own));
         if (iy == ny - 2)
-            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, WCI>(S, K, ix, ny - 1, ny - 2, sA, sR, sCS2, sMom, Etmp,
-                                                                  sg, dtf, Trep, rro, een, rrn));
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, WCI>(S, K, ix, ny - 1, sA, sR, sCS2, sMom, Etmp, sg, dtf,
+                                                                  Trep, rro, een, rrn, own));
     }
     block_min_store<R>(dtw, S.part_wave + bix + biy * ((K.nx + 31) / 32));
 }
@@ -591,6 +603,367 @@ void launch_wave_fast_batch(const BatchTab<R>& T, const BatchLaunch& L, int roll
 }
 template <class R>
 size_t wave_fast_smem(int nt) { return ((size_t)2 * WT_NB * WT_N + (size_t)2 * nt * 256 + 6 * nt) * sizeof(R); }
+
+// ------------------------------------------------------------------------
+// Rows pass with tensor-memory-accelerator (TMA) tiles: the same arithmetic
+// as b_wave_fast (identical results), with the data movement moved off the
+// threads.
+//  - One elected thread loads each bin's ee and rr plane tile with one 2-D
+//    box copy (cp.async.bulk.tensor, no multicast) into one of four
+//    buffers, completion counted on the buffer's mbarrier; the box starts
+//    4 columns left of the block (the 16-byte rule on x) and 2 rows below,
+//    40 x 12 cells.  Cells outside the grid arrive as zeros; blocks at the
+//    grid's edges rewrite those (and the offshore column, St * taper) with
+//    the clamped values the reference reads through mm()/pp().
+//  - ee in memory is never negative (every writer stores max(., 0), and
+//    xbg_set_field clips what a caller sets), so the tile needs no sanity
+//    pass.
+//  - The new bins go to shared memory (in place of the advected ones) and
+//    leave in two 3-D box stores (all bins of the block's 32 x 8 cells); the
+//    store map ends at row ny-2, so rows 0 and ny-1 (rollerlatbnd copies,
+//    written by the row 1 / ny-2 threads) are never touched by it.
+//  - Every wait on an mbarrier is bounded; a block that gives up records
+//    XBG_ERR_TIMEOUT in the clock, halts the step, waits (bounded) for its
+//    copies in flight and leaves.
+// Used for wave-current interaction off and nx a multiple of 4 (the row
+// pitch of a tensor map is a multiple of 16 bytes); else b_wave_fast.
+constexpr int TM_X = 40, TM_Y = 12, TM_N = TM_X * TM_Y, TM_NB = 4;
+constexpr unsigned TM_WAIT_LIMIT = 1u << 20;   // mbarrier polls before a block gives up (copies land in microseconds)
+
+__device__ __forceinline__ unsigned su32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void tm_mbar_init(unsigned a) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ void tm_expect(unsigned a, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool tm_wait(unsigned a, unsigned parity) {
+    for (unsigned it = 0; it < TM_WAIT_LIMIT; it++) {
+        unsigned ok;
+        asm volatile(
+            "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(a), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void tm_load3(unsigned dst, const CUtensorMap* m, int x, int y, int z, unsigned mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+        "[%5];\n" ::"r"(dst),
+        "l"((unsigned long long)m), "r"(x), "r"(y), "r"(z), "r"(mbar)
+        : "memory");
+}
+__device__ __forceinline__ void tm_store3(const CUtensorMap* m, int x, int y, int z, unsigned src) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];\n" ::"l"(
+                     (unsigned long long)m),
+                 "r"(x), "r"(y), "r"(z), "r"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void tm_fence_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+template <class R>
+size_t wave_tma_smem(int nt) {
+    return 128 + ((size_t)2 * TM_NB * TM_N + (size_t)2 * nt * 256 + 6 * nt) * sizeof(R);
+}
+
+template <class R, bool ROLLER>
+__device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, const WaveMaps& M, const int bix,
+                                           const int biy) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long mbar[TM_NB];
+    Clock* clk = S.clk;
+    if (halted(clk)) return;
+    const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
+    const int tid = threadIdx.x + threadIdx.y * WT_X;
+    const unsigned base = (su32(smem_raw) + 127u) & ~127u;
+    R* tE = reinterpret_cast<R*>(smem_raw + (base - su32(smem_raw)));   // [TM_NB][TM_N] plane tiles of ee
+    R* tR = tE + TM_NB * TM_N;                                          // [TM_NB][TM_N] plane tiles of rr
+    R* sA = tR + TM_NB * TM_N;           // [nt][256] advected ee (energy units), then the new ee
+    R* sR = sA + (size_t)nt * 256;       // [nt][256] advected rr, then the new rr
+    Dir4<R>* sMom = reinterpret_cast<Dir4<R>*>(sR + (size_t)nt * 256);
+    Dir2<R>* sCS2 = reinterpret_cast<Dir2<R>*>(sMom + nt);
+    if (tid < nt) {
+        const R c = K.cxsth[tid], sn = K.sxnth[tid];
+        sCS2[tid] = Dir2<R>{c, sn};
+        sMom[tid] = Dir4<R>{c * c, sn * sn, sn * c, K.theta[tid]};
+    }
+    const int bx0 = bix * WT_X, by0 = 1 + biy * WT_Y;
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool active = ix < nx && iy <= ny - 2;
+    const int par = clk->par;
+    const CUtensorMap* mE = &M.ld_e[par ^ 1];
+    const CUtensorMap* mR = &M.ld_r[par ^ 1];
+    const R* rro = S.rr[par ^ 1];
+    const R dtf = (R)clk->dt;
+    const R taper = (R)cmin((double)(R)clk->totaltime / 100.0, 1.0);
+    const R dth = K.dtheta;
+    const R rdth = (R)1 / dth;
+    const R rdx = (R)1 / K.dx;
+    constexpr unsigned TBYTES = (ROLLER ? 2u : 1u) * TM_N * sizeof(R);
+    if (tid == 0) {
+        for (int b = 0; b < TM_NB; b++) tm_mbar_init(su32(&mbar[b]));
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        tm_fence_async();
+    }
+    __syncthreads();   // barriers initialised, theta tables written
+    int issued = 0;             // planes issued so far (elected thread)
+    auto issue = [&](int p) {   // elected thread: plane p into buffer p % 4
+        issued = p + 1;
+        const int b = p & (TM_NB - 1);
+        const unsigned mb = su32(&mbar[b]);
+        tm_expect(mb, TBYTES);
+        tm_load3(su32(tE + b * TM_N), mE, bx0 - 4, by0 - 2, p, mb);
+        if (ROLLER) tm_load3(su32(tR + b * TM_N), mR, bx0 - 4, by0 - 2, p, mb);
+    };
+    if (tid == 0)
+        for (int p = 0; p < nt && p < TM_NB; p++) issue(p);
+    auto wait_plane = [&](int p) { return tm_wait(su32(&mbar[p & (TM_NB - 1)]), (unsigned)(p >> 2) & 1u); };
+    // blocks whose box reaches outside the grid or over the offshore column
+    const bool edge = bx0 == 0 || bx0 + 35 > nx - 1 || by0 - 2 < 0 || by0 + 9 > ny - 1;
+    // the clamped values of the box's out-of-grid cells, and St * taper on
+    // column 0 (ee only): every rewritten cell reads an in-grid cell of
+    // column >= 1 of the same box, which no thread rewrites
+    auto fixup = [&](int p) {
+        R* dE = tE + (p & (TM_NB - 1)) * TM_N;
+        R* dR = tR + (p & (TM_NB - 1)) * TM_N;
+        for (int e = tid; e < TM_N; e += 256) {
+            const int gx = bx0 - 4 + e % TM_X, gy = by0 - 2 + e / TM_X;
+            const int cx = min(max(gx, 0), nx - 1), cy = min(max(gy, 0), ny - 1);
+            const bool in = cx == gx && cy == gy;
+            const int src = (cx - (bx0 - 4)) + (cy - (by0 - 2)) * TM_X;
+            if (!(in && gx != 0)) dE[e] = cx == 0 ? DM<R>::fmax(S.St[cy + p * ny] * taper, (R)0) : dE[src];
+            if (ROLLER && !in) dR[e] = dR[src];
+        }
+        tm_fence_async();   // these writes before the buffer's next box copy
+    };
+    const int ctile = (iy - by0 + 2) * TM_X + (ix - bx0 + 4);
+    int i = 0;
+    R hh = 0;
+    R axp = 0, axm = 0, ayp = 0, aym = 0, rxp = 0, rxm = 0, ryp = 0, rym = 0, cgi = 0, cci = 0;
+    CthCoef<R> cc{};
+    R we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;
+    R c0 = 0, cpp = 0, Etmp = 0, cabs = 0, fte = 0, ftr = 0;
+    R cthP = 0, cthQ = 0;
+    auto cth = [&](R cx, R sx) -> R {
+        const R ctht = DM<R>::fma(cthP, sx, cthQ * cx);
+        return cmin(cmax(ctht, (R)(-0.25f * cc.sg)), (R)(0.25f * cc.sg));
+    };
+    if (active) {
+        i = ix + iy * nx;
+        const int xm = mm(ix), xp = pp(ix, nx);
+        const int ym = mm(iy), yp = pp(iy, ny);
+        hh = ld(S.f[HH] + i);
+        cc = cth_coef(S, K, ix, iy, (R)clk->sigm);
+        const R* cgp = S.f[CG];
+        const R* cp = S.f[CC_];
+        cgi = ld(cgp + i); cci = ld(cp + i);
+        const R h = (R)0.5f;
+        // face speeds: without wave-current interaction the current terms of
+        // the face speed are exactly zero
+        axp = h * (cgi + ld(cgp + xp + iy * nx)); axm = h * (cgi + ld(cgp + xm + iy * nx));
+        ayp = h * (cgi + ld(cgp + ix + yp * nx)); aym = h * (cgi + ld(cgp + ix + ym * nx));
+        rxp = h * (cci + ld(cp + xp + iy * nx)); rxm = h * (cci + ld(cp + xm + iy * nx));
+        ryp = h * (cci + ld(cp + ix + yp * nx)); rym = h * (cci + ld(cp + ix + ym * nx));
+        cthP = cc.s * cc.dhdx; cthQ = -(cc.s * cc.dhdy);
+        c0 = cth(sCS2[0].c, sCS2[0].s);
+        const int t1 = nt > 1 ? 1 : 0;
+        cpp = cth(sCS2[t1].c, sCS2[t1].s);
+    }
+    bool ok = wait_plane(0) && (nt < 2 || wait_plane(1));
+    if (edge) {
+        fixup(0);
+        if (nt > 1) fixup(1);
+    }
+    R* oA = sA + tid;
+    R* oR = sR + tid;
+    const R* oldR = rro + i;   // without the roller pass rr is carried unchanged
+    bool failed = false;
+#pragma unroll 1
+    for (int t = 0; t < nt; t++) {
+        const int b = t & (TM_NB - 1);
+        if (t + 2 < nt) {
+            ok = ok && wait_plane(t + 2);
+            if (edge) fixup(t + 2);
+        }
+        if (__syncthreads_or(!ok)) { failed = true; break; }   // fixups visible; plane t-1 read by all
+        if (tid == 0 && t >= 1 && t + 3 < nt) issue(t + 3);    // into plane t-1's buffer
+        if (active) {
+            const R* qE = tE + b * TM_N + ctile;
+            const R* qR = tR + b * TM_N + ctile;
+            if (t == 0) {
+                const int b1 = (nt > 1 ? 1 : 0);
+                we2 = qE[0]; we1 = we2; we3 = tE[b1 * TM_N + ctile];
+                if (ROLLER) { wr2 = qR[0]; wr1 = wr2; wr3 = tR[b1 * TM_N + ctile]; }
+            }
+            const int b2 = (t + 2 < nt ? t + 2 : nt - 1) & (TM_NB - 1);
+            we4 = tE[b2 * TM_N + ctile];
+            if (ROLLER) wr4 = tR[b2 * TM_N + ctile];
+            const Dir2<R> d = sCS2[t];
+            const R ct = d.c, st = d.s;
+            const bool last = t == nt - 1;
+            cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
+            R fx = flux2(qE[-2], qE[-1], we2, qE[1], qE[2], ct * axp, ct * axm);
+            R fy = flux2(qE[-2 * TM_X], qE[-TM_X], we2, qE[TM_X], qE[2 * TM_X], st * ayp, st * aym);
+            R fup = last ? (R)0 : theta_face(we1, we2, we3, we4, c0, cpp);
+            R ft = fup - fte;
+            fte = fup;
+            R A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
+            R Ar;
+            if (!ROLLER) Ar = ld(oldR + (size_t)t * C);
+            if (ROLLER) {
+                R rx = flux2(qR[-2], qR[-1], wr2, qR[1], qR[2], ct * rxp, ct * rxm);
+                R ry = flux2(qR[-2 * TM_X], qR[-TM_X], wr2, qR[TM_X], qR[2 * TM_X], st * ryp, st * rym);
+                R rup = last ? (R)0 : theta_face(wr1, wr2, wr3, wr4, c0, cpp);
+                R rt = rup - ftr;
+                ftr = rup;
+                Ar = wr2 - dtf * ((rx + ry) * rdx + rt * rdth);
+            }
+            *oA = A;
+            *oR = Ar;
+            oA += 256; oR += 256;
+            Etmp = Etmp + DM<R>::fmax(A, (R)0);
+            const int t2 = t + 2 < nt ? t + 2 : nt - 1;
+            we1 = we2; we2 = we3; we3 = we4;
+            wr1 = wr2; wr2 = wr3; wr3 = wr4;
+            const Dir2<R> d2 = sCS2[t2];
+            c0 = cpp; cpp = cth(d2.c, d2.s);
+        }
+    }
+    if (failed) {   // a copy never completed: record, halt, let the copies in flight land (bounded), leave
+        if (tid == 0) {
+            atomicExch(&clk->status, XBG_ERR_TIMEOUT);
+            atomicExch(&clk->halt, 1);
+            for (int p = issued - TM_NB < 0 ? 0 : issued - TM_NB; p < issued; p++)
+                wait_plane(p);   // the last plane issued into each buffer
+        }
+        __syncthreads();
+        return;
+    }
+    R dtw = (R)3.0e38f;
+    if (active) {
+        dtw = DM<R>::fmin(K.cfl * dth / cabs, (R)9999999.9f);   // WAVEDT (Wave_kernel.cu:232-249)
+        R* een = S.ee[par];
+        R* rrn = S.rr[par];
+        const R Trep = (R)clk->Trep;
+        const R rho = K.rho, g = K.g;
+        R ridiv, Dv, Dq;
+        wave_breaking(K, Etmp, hh, ld(S.f[WK] + i), ld(S.f[FWM] + i), Trep, ridiv, Dv, Dq);
+        const R cc_i = cci;
+        const R twogb = (R)2.0f * g * K.beta;
+        const R rcoef = twogb / cc_i;
+        const bool wet = hh > K.eps;
+        // the lateral rows 0 and ny-1 first, while sA / sR still hold the
+        // advected bins; the source cell's new ee is formed as below
+        const R sg = (R)clk->sigm;
+        auto fin = [&](int t) {
+            R dd;
+            return wet ? diss_ee(sA[t * 256 + tid], ridiv, Dq, dtf, dd) : (R)0;
+        };
+        if (iy == 1)
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, false>(S, K, ix, 0, sA, sR, sCS2, sMom, Etmp, sg, dtf,
+                                                                   Trep, rro, een, rrn, fin));
+        if (iy == ny - 2)
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, false>(S, K, ix, ny - 1, sA, sR, sCS2, sMom, Etmp, sg,
+                                                                   dtf, Trep, rro, een, rrn, fin));
+        R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
+        R ec = 0, es = 0, ecs = 0, rc = 0, rs = 0, rcs = 0;
+        R* pA = sA + tid;
+        R* pR = sR + tid;
+        if (wet) {
+#pragma unroll 2
+            for (int t = 0; t < nt; t++) {
+                R dd;
+                const R eet = diss_ee(pA[t * 256], ridiv, Dq, dtf, dd);
+                R rrt = pR[t * 256];
+                const R rrd = rrt * rcoef;
+                rrt = DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                drr = drr + rrd;
+                RR = RR + rrt;
+                pA[t * 256] = eet;
+                pR[t * 256] = rrt;
+                const Dir4<R> m = sMom[t];
+                sume = sume + eet;
+                sumethet = sumethet + eet * m.th;
+                ec = DM<R>::fma(m.c2, eet, ec);
+                es = DM<R>::fma(m.s2, eet, es);
+                ecs = DM<R>::fma(m.cs, eet, ecs);
+                rc = DM<R>::fma(m.c2, rrt, rc);
+                rs = DM<R>::fma(m.s2, rrt, rs);
+                rcs = DM<R>::fma(m.cs, rrt, rcs);
+            }
+        } else {
+            for (int t = 0; t < nt; t++) {
+                pA[t * 256] = (R)0;
+                pR[t * 256] = (R)0;
+            }
+        }
+        const R sum2 = sume;
+        sume = DM<R>::fmax(sume, (R)0.00001f);
+        S.f[THM][i] = sumethet / sume;
+        S.f[E][i] = sume * dth;
+        S.f[H][i] = DM<R>::sqrt(sume * dth / (rho * g / (R)8));
+        S.f[D][i] = Dv;
+        S.f[ROL][i] = RR * dth;
+        S.f[DR][i] = drr * dth;
+        const R n = cgi / cc_i;
+        S.tmp[T_SXX][i] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
+        S.tmp[T_SYY][i] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
+        S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
+    }
+    // the block's new bins of rows 1..ny-2 in two box stores
+    tm_fence_async();
+    __syncthreads();
+    if (tid == 0) {
+        tm_store3(&M.st_e[par], bx0, by0, 0, su32(sA));
+        tm_store3(&M.st_r[par], bx0, by0, 0, su32(sR));
+        asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+    }
+    block_min_store<R>(dtw, S.part_wave + bix + biy * ((K.nx + 31) / 32));
+    if (tid == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");   // shared memory read out
+}
+template <class R, bool ROLLER>
+__global__ void __launch_bounds__(256, 3) k_wave_tma(Dev<R> S, Konst<R> K, const __grid_constant__ WaveMaps M) {
+    b_wave_tma<R, ROLLER>(S, K, M, blockIdx.x, blockIdx.y);
+}
+
+// Tensor maps of the TMA rows pass: ee and rr of both plane sets as 3-D
+// arrays [nt][ny][nx]; loads in 40 x 12 x 1 boxes, stores in 32 x 8 x nt
+// boxes over rows 0..ny-2 (the map ends before row ny-1).  Encoded with the
+// driver's cuTensorMapEncodeTiled (fetched through the runtime).
+template <class R>
+int wave_maps_make(const Dev<R>& S, const Konst<R>& K, WaveMaps* M) {
+    if (K.nx % 4 != 0 || K.nt > 256) return 1;
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (!enc) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return 1;
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const CUtensorMapDataType dt = sizeof(R) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+    const cuuint64_t es = sizeof(R);
+    const cuuint32_t one[3] = {1, 1, 1};
+    auto make = [&](CUtensorMap* m, const R* base, int rows, cuuint32_t bx, cuuint32_t by, cuuint32_t bz) {
+        const cuuint64_t dims[3] = {(cuuint64_t)K.nx, (cuuint64_t)rows, (cuuint64_t)K.nt};
+        const cuuint64_t strides[2] = {(cuuint64_t)K.nx * es, (cuuint64_t)K.nx * K.ny * es};
+        const cuuint32_t box[3] = {bx, by, bz};
+        return enc(m, dt, 3, (void*)base, dims, strides, box, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    };
+    for (int k = 0; k < 2; k++) {
+        if (make(&M->ld_e[k], S.ee[k], K.ny, TM_X, TM_Y, 1) != CUDA_SUCCESS ||
+            make(&M->ld_r[k], S.rr[k], K.ny, TM_X, TM_Y, 1) != CUDA_SUCCESS ||
+            make(&M->st_e[k], S.ee[k], K.ny - 1, WT_X, WT_Y, (cuuint32_t)K.nt) != CUDA_SUCCESS ||
+            make(&M->st_r[k], S.rr[k], K.ny - 1, WT_X, WT_Y, (cuuint32_t)K.nt) != CUDA_SUCCESS)
+            return 1;
+    }
+    return 0;
+}
 
 // wavforce (wave_CPU.cpp:1164-1238) at cell j, before the boundary copies.
 template <class R>
@@ -670,16 +1043,27 @@ int wave_parts(const Konst<R>& K) {
 
 // join: an event of a concurrent branch (the boundary kernels) that the
 // rows pass waits for after the dispersion kernel; null when sequential.
+// maps: the tensor maps of the TMA rows pass, or null for the thread-copied
+// tiles (b_wave_fast); the TMA pass has no wave-current interaction variant.
 template <class R>
-int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, cudaEvent_t join) {
+int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, cudaEvent_t join,
+                const WaveMaps* maps) {
     int n = 0;
     k_disp<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, K); n++;
     PMARK(pf, "k_disp");
     if (join) cudaStreamWaitEvent(st, join, 0);
     {
         dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
-        launch_wave_fast(S, K, g, b, wave_fast_smem<R>(K.nt), st); n++;
-        PMARK(pf, "k_wave_fast");
+        if (maps && K.wci == (R)0) {
+            const size_t smem = wave_tma_smem<R>(K.nt);
+            if (K.roller == 1) k_wave_tma<R, true><<<g, b, smem, st>>>(S, K, *maps);
+            else k_wave_tma<R, false><<<g, b, smem, st>>>(S, K, *maps);
+            n++;
+            PMARK(pf, "k_wave_tma");
+        } else {
+            launch_wave_fast(S, K, g, b, wave_fast_smem<R>(K.nt), st); n++;
+            PMARK(pf, "k_wave_fast");
+        }
     }
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
     k_wave_force<R><<<g, b, 0, st>>>(S, K); n++;
@@ -711,7 +1095,11 @@ template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunc
 template <class R>
 int wave_prepare(const Konst<R>& K) {
     const int smem = (int)wave_fast_smem<R>(K.nt);
+    const int smem_tma = (int)wave_tma_smem<R>(K.nt);
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (cudaFuncSetAttribute(k_wave_tma<R, true>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(k_wave_tma<R, false>, a, smem_tma) != cudaSuccess)
+        return 1;
     cudaError_t e[8] = {
         cudaFuncSetAttribute(k_wave_fast<R, true, true>, a, smem), cudaFuncSetAttribute(k_wave_fast<R, true, false>, a, smem),
         cudaFuncSetAttribute(k_wave_fast<R, false, true>, a, smem), cudaFuncSetAttribute(k_wave_fast<R, false, false>, a, smem),
@@ -724,8 +1112,12 @@ int wave_prepare(const Konst<R>& K) {
 template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);
 
-template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, cudaEvent_t);
-template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, cudaEvent_t);
+template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, cudaEvent_t,
+                                const WaveMaps*);
+template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, cudaEvent_t,
+                                 const WaveMaps*);
+template int wave_maps_make<float>(const Dev<float>&, const Konst<float>&, WaveMaps*);
+template int wave_maps_make<double>(const Dev<double>&, const Konst<double>&, WaveMaps*);
 template int wave_parts<float>(const Konst<float>&);
 template int wave_parts<double>(const Konst<double>&);
 

@@ -9,6 +9,8 @@
 // CUDA graph can replay any number of steps without pointer swaps.
 #pragma once
 #include <cstdint>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #define XBG_PI 3.14159265          /* the reference's `pi` macro (double) */
@@ -159,6 +161,13 @@ struct Konst {
     double endtime, outputtimestep, sedstart, dtbc, eps_d;
     int sedtrans;
     R cxsth[XBG_MAX_THETA], sxnth[XBG_MAX_THETA], theta[XBG_MAX_THETA];
+};
+
+// Tensor maps of the wave rows pass (TMA variant): ee and rr of both plane
+// sets, box loads of one bin's plane tile and box stores of all bins of a
+// block's cells.  Passed to the kernel as a __grid_constant__ parameter.
+struct WaveMaps {
+    CUtensorMap ld_e[2], ld_r[2], st_e[2], st_r[2];
 };
 
 // Per-kernel timing of a non-graph step (xbg_profile_step): an event after

@@ -28,7 +28,7 @@ EXPORTS = [
     "xbg_sediment_step", "xbg_accumulate_means", "xbg_step", "xbg_advance", "xbg_get_time",
     "xbg_output_done", "xbg_reset_means", "xbg_set_time", "xbg_sync", "xbg_launch_count",
     "xbg_mass", "xbg_put_wave_records", "xbg_get_stream", "xbg_profile_step",
-    "xbg_flow_dt_noalloc",
+    "xbg_flow_dt_noalloc", "xbg_set_kernel_variant", "xbg_get_kernel_variant",
     "xbg_batch_create", "xbg_batch_destroy", "xbg_batch_scenario", "xbg_batch_advance", "xbg_batch_status",
     "xbg_batch_sync", "xbg_batch_get_stream", "xbg_batch_profile_step", "xbg_batch_set_grid",
     "xbg_batch_launch_count", "xbg_set_wave_forcing", "xbg_forcing_steps",
@@ -74,6 +74,8 @@ def load():
     L.xbg_get_stream.argtypes = [vp, C.POINTER(vp)]
     L.xbg_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
     L.xbg_flow_dt_noalloc.argtypes = [ip, vp, ip, ip, C.c_double, C.c_double, vp, vp]
+    L.xbg_set_kernel_variant.argtypes = [vp, ip, ip]
+    L.xbg_get_kernel_variant.argtypes = [vp, ip, C.POINTER(ip)]
     L.xbg_set_wave_forcing.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.c_double, ip]
     L.xbg_forcing_steps.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), ip]
     L.xbg_batch_create.argtypes = [C.POINTER(Params), ip, ip, C.POINTER(vp)]
@@ -236,6 +238,15 @@ class Model:
         n = C.c_int(cap)
         _check(self.L.xbg_profile_step(self.h, ms, names, C.byref(n)), "profile_step")
         return [(names[k].decode(), float(ms[k])) for k in range(n.value)]
+
+    def set_variant(self, phase, variant):
+        """Kernel variant of a phase (XBG_PHASE_WAVE: 1 TMA tiles, 0 thread-copied)."""
+        _check(self.L.xbg_set_kernel_variant(self.h, phase, variant), "set_kernel_variant")
+
+    def variant(self, phase):
+        v = C.c_int()
+        _check(self.L.xbg_get_kernel_variant(self.h, phase, C.byref(v)), "get_kernel_variant")
+        return v.value
 
     def mass(self):
         w, s, b = C.c_double(), C.c_double(), C.c_double()

@@ -9,6 +9,7 @@ from .model import load
 XBG_NN_RELU = 1
 XBG_NN_OUT_BF16 = 2
 XBG_NN_ATOMIC = 4
+XBG_NN_CHECK_TIMEOUT = 8   # check of the GEMM's time-out exit (include/xbg_nn.h)
 
 _nn = None
 
