@@ -33,6 +33,7 @@ B_ALGO = lambda nt: 4 * (77 + 4 * nt)   # algorithmic bytes per coupled cell-upd
 # (kernel, nx, ny, ntheta); other workloads report traffic null.
 NCU_TRAFFIC = {
     ("k_wave_fast", 2048, 1024, 18): 361049088 + 335545344,
+    ("k_wave_tma", 2048, 1024, 18): 344964352 + 332152576,
 }
 
 
@@ -74,6 +75,75 @@ def peaks():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+class NvmlClockSampler:
+    """SM clock, its maximum, power and the clock-event (throttle) reasons
+    read through NVML (the library nvidia-smi reports from) every 2 ms on a
+    background thread, so that even a timed region of a few tens of
+    milliseconds holds several samples; stop() keeps those inside
+    [mark_start(), mark_end()]."""
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
+
+    def __init__(self, local):
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        h = None
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(local).uuid)
+            h = pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(local)
+        self.h = h
+        self.rows = []
+        self.t0 = self.t1 = None
+        self.run = False
+
+    def start(self):
+        self.run = True
+        self.th = threading.Thread(target=self._loop, daemon=True)
+        self.th.start()
+
+    def _loop(self):
+        nv, h = self.nv, self.h
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while self.run:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.rows.append((time.time(), sm, mx, rs, pw))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+
+    def stop(self):
+        self.run = False
+        self.th.join(timeout=2)
+        inside = [r for r in self.rows if self.t0 is not None and self.t0 <= r[0] <= self.t1]
+        if not inside:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+        reasons = sorted({n for r in inside for n, bit in self.REASONS if r[3] & bit})
+        return {"sm_mhz": float(np.median([r[1] for r in inside])), "sm_max_mhz": float(max(r[2] for r in inside)),
+                "reasons": reasons, "samples": len(inside), "window_s": round(self.t1 - self.t0, 4),
+                "power_w_max": float(max(r[4] for r in inside)), "source": "nvml, 2 ms"}
+
+
+def clock_sampler(local):
+    """NVML sampler where the library loads, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(local)
+    except Exception:
+        return ClockSampler(local)
 
 
 class ClockSampler:
@@ -277,7 +347,7 @@ def run_ensemble(args, rank, world, local):
         tuned = tune(b, reps=2)
     stream = torch.cuda.ExternalStream(b.stream())
     W, K = max(3, args.warmup), args.steps
-    sampler = ClockSampler(local)
+    sampler = clock_sampler(local)
     sampler.start()
     b.advance(W)
     b.sync()
@@ -305,7 +375,7 @@ def run_ensemble(args, rank, world, local):
     peak, peak_kind = peaks()
     dom = max(kern, key=kern.get)
     roof = None
-    if dom == "k_wave_fast":
+    if dom in ("k_wave_fast", "k_wave_tma"):
         achieved = 4 * (4 * nt + 16) * wrows / (kern[dom] / 1e3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
@@ -473,15 +543,19 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
+    from xbeach_gpu_b200.abi import XBG_FLAG_ENDED, XBG_FLAG_OUTPUT_DUE
     p, m, bnd = setup_model(args.nx, args.ny, seed=rank)
     C = p.nx * p.ny
     stream = torch.cuda.ExternalStream(m.stream())
     W = max(3, args.warmup)
     K = args.steps
-    sampler = ClockSampler(local)
+    sampler = clock_sampler(local)
     sampler.start()
     m.advance(W)
     m.sync()
+    _, _, nstep0, flags0, rc0 = m.time()
+    if rc0 != 0 or nstep0 != W or flags0 & (XBG_FLAG_OUTPUT_DUE | XBG_FLAG_ENDED):
+        raise RuntimeError(f"warm-up did not run W steps (status {rc0}, steps {nstep0}, flags {flags0})")
     launches0 = m.launches()
     if dist:
         dist.barrier()
@@ -501,6 +575,10 @@ def main():
     t_end, dt_end, nstep, flags, rc = m.time()
     if rc != 0:
         raise RuntimeError(f"device status {rc} after the timed steps")
+    # every timed replay ran a whole step: the device clock advanced by K steps
+    # and no end-of-run or output stop was reached inside the region
+    if nstep != nstep0 + K or flags & (XBG_FLAG_OUTPUT_DUE | XBG_FLAG_ENDED):
+        raise RuntimeError(f"timed region ran {nstep - nstep0} of {K} steps (flags {flags})")
     launches = m.launches() - launches0
     # per-kernel times of full steps (events between launches), for the roofline
     prof = {}
@@ -536,8 +614,9 @@ def main():
     # dominant kernel: the fused wave-action kernel
     dom = max(kern, key=kern.get)
     nt = p.ntheta
-    algo_dom = {"k_wave_fast": 4 * (4 * nt + 16)}.get(dom, None)
-    rows = p.ny - 2 if dom == "k_wave_fast" else p.ny
+    wave_rows = ("k_wave_fast", "k_wave_tma")
+    algo_dom = 4 * (4 * nt + 16) if dom in wave_rows else None
+    rows = p.ny - 2 if dom in wave_rows else p.ny
     roof = None
     if algo_dom:
         achieved = algo_dom * p.nx * rows / (kern[dom] / 1e3) / 1e9

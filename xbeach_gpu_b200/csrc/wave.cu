@@ -19,6 +19,8 @@
 //                (rollerlatbnd, wave_CPU.cpp:830-870) around the
 //                dissipation.  Emits the per-block WAVEDT minimum.
 //   k_wave_force wavforce + twodimbnd(noix) + breakerdelay + twodimbnd(ust).
+#include <type_traits>
+
 #include "xbg_common.cuh"
 #include "../../include/xbg.h"
 
@@ -146,6 +148,25 @@ __device__ __forceinline__ R flux2(R qm2, R qm, R qi, R qp, R qp2, R cf, R cfmin
     const R arrin = upw(pin ? qi : qp, pin ? qm : qp2) * cf;
     const R arrmin = upw(pmin ? qm : qi, pmin ? qm2 : qp) * cfmin;
     return arrin - arrmin;
+}
+// The same flux when the sign of the face speeds is known for the whole bin:
+// the speeds cg and c are positive, so without wave-current interaction the
+// face speed 0.5 (cg_i + cg_j) cos(theta) has the sign of cos(theta) (of
+// sin(theta) for y), and a zero speed gives a zero flux on either side.  Only
+// the two upwind taps at stride s are read.
+template <class R, bool POS>
+__device__ __forceinline__ R flux2s(const R* q, int s, R qi, R cf, R cfmin) {
+    if (POS) {
+        const R qm = q[-s], qm2 = q[-2 * s];
+        const R arrin = upw(qi, qm) * cf;
+        const R arrmin = upw(qm, qm2) * cfmin;
+        return arrin - arrmin;
+    } else {
+        const R qp = q[s], qp2 = q[2 * s];
+        const R arrin = upw(qp, qp2) * cf;
+        const R arrmin = upw(qi, qp) * cfmin;
+        return arrin - arrmin;
+    }
 }
 // theta-face flux between bins t and t+1 (the arrint of bin t, which is the
 // arrmint of bin t+1): e(t-1), e(t), e(t+1), e(t+2), ctheta(t), ctheta(t+1)
@@ -805,8 +826,25 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
             const R ct = d.c, st = d.s;
             const bool last = t == nt - 1;
             cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
-            R fx = flux2(qE[-2], qE[-1], we2, qE[1], qE[2], ct * axp, ct * axm);
-            R fy = flux2(qE[-2 * TM_X], qE[-TM_X], we2, qE[TM_X], qE[2 * TM_X], st * ayp, st * aym);
+            // x and y fluxes with the upwind side of the bin (the sign of
+            // cos and sin is the same for every cell of the bin)
+            R fx, fy, rx = 0, ry = 0;
+            auto xy = [&](auto px, auto py) {
+                constexpr bool PX = decltype(px)::value, PY = decltype(py)::value;
+                fx = flux2s<R, PX>(qE, 1, we2, ct * axp, ct * axm);
+                fy = flux2s<R, PY>(qE, TM_X, we2, st * ayp, st * aym);
+                if (ROLLER) {
+                    rx = flux2s<R, PX>(qR, 1, wr2, ct * rxp, ct * rxm);
+                    ry = flux2s<R, PY>(qR, TM_X, wr2, st * ryp, st * rym);
+                }
+            };
+            using T_ = std::true_type;
+            using F_ = std::false_type;
+            if (ct > (R)0) {
+                if (st > (R)0) xy(T_{}, T_{}); else xy(T_{}, F_{});
+            } else {
+                if (st > (R)0) xy(F_{}, T_{}); else xy(F_{}, F_{});
+            }
             R fup = last ? (R)0 : theta_face(we1, we2, we3, we4, c0, cpp);
             R ft = fup - fte;
             fte = fup;
@@ -814,8 +852,6 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
             R Ar;
             if (!ROLLER) Ar = ld(oldR + (size_t)t * C);
             if (ROLLER) {
-                R rx = flux2(qR[-2], qR[-1], wr2, qR[1], qR[2], ct * rxp, ct * rxm);
-                R ry = flux2(qR[-2 * TM_X], qR[-TM_X], wr2, qR[TM_X], qR[2 * TM_X], st * ryp, st * rym);
                 R rup = last ? (R)0 : theta_face(wr1, wr2, wr3, wr4, c0, cpp);
                 R rt = rup - ftr;
                 ftr = rup;
@@ -924,8 +960,12 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
     block_min_store<R>(dtw, S.part_wave + bix + biy * ((K.nx + 31) / 32));
     if (tid == 0) asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");   // shared memory read out
 }
+// FP32: 64 registers, four blocks (32 warps) per SM, which hides the pass's
+// dependent-arithmetic latency better than three (-15 % at 2048 x 1024);
+// FP64 (the error-oracle build) keeps room for its wider registers.
 template <class R, bool ROLLER>
-__global__ void __launch_bounds__(256, 3) k_wave_tma(Dev<R> S, Konst<R> K, const __grid_constant__ WaveMaps M) {
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
+    k_wave_tma(Dev<R> S, Konst<R> K, const __grid_constant__ WaveMaps M) {
     b_wave_tma<R, ROLLER>(S, K, M, blockIdx.x, blockIdx.y);
 }
 
