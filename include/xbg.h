@@ -181,6 +181,8 @@ int  xbg_get_time(xbg_handle* h, double* totaltime, double* dt, int64_t* nstep,
 #define XBG_FLAG_OUTPUT_DUE   1   /* nextoutputtime reached               */
 #define XBG_FLAG_ENDED        2   /* totaltime >= endtime                 */
 #define XBG_FLAG_NEED_BOUNDARY 4  /* next wave-boundary chunk consumed    */
+#define XBG_FLAG_FALLBACK     8   /* batch scenario left surrogate forcing
+                                     for the plain wave solver for good    */
 /* Output bookkeeping of mainloopGPU (Wave_gpu.cu:784-930): divide the means
  * by the step count, advance nextoutputtime; xbg_reset_means clears them. */
 int  xbg_output_done(xbg_handle* h);
@@ -270,6 +272,40 @@ int  xbg_batch_profile_step(xbg_batch* b, float* ms, const char** names,
  * values, 5: dt reduction); used by the autotuner. */
 int  xbg_batch_set_grid(xbg_batch* b, int shape, int blocks);
 int  xbg_batch_launch_count(xbg_batch* b, int64_t* count);
+/* As xbg_set_kernel_variant, for every scenario of a batch (the TMA rows
+ * pass needs every scenario eligible).  Used by the autotuner.             */
+int  xbg_batch_set_kernel_variant(xbg_batch* b, int phase, int variant);
+int  xbg_batch_get_kernel_variant(xbg_batch* b, int phase, int* variant);
+
+/* ---- surrogate-assisted batches --------------------------------------
+ * No counterpart in the reference (its wave sub-stepping, nwstp of
+ * Wave_gpu.cu:77 and wavebndOLD of Wavestep.cu:386, was removed).  Each
+ * scenario's wave sub-step is either the plain wave solver or a forcing
+ * given from outside (the surrogate's predictions), per scenario:       */
+#define XBG_WAVE_PLAIN    0   /* the wave solver runs                      */
+#define XBG_WAVE_FORCED   1   /* E, H, D, DR, Fx, Fy come from the forcing */
+#define XBG_WAVE_FALLBACK 2   /* plain, and XBG_FLAG_FALLBACK is set (the
+                                 scenario failed its judge)                */
+/* Stream-ordered on the batch's stream.  FORCED needs forcing planes.      */
+int  xbg_batch_set_wave_mode(xbg_batch* b, int s, int mode);
+/* Scenario s's forcing: six device planes each of f0 (the fields at the
+ * segment start) and f1 (the fields predicted at its end), in the order
+ * E, H, D, DR, Fx, Fy, element type of the batch, nx*ny values each.     */
+int  xbg_batch_set_forcing(xbg_batch* b, int s, const void* const* f0,
+                           const void* const* f1);
+/* k coupled steps of every scenario (one CUDA graph per k, replayed): a
+ * scenario in FORCED mode takes the wave sub-step of step j from
+ * f0 + (j/k)(f1 - f0) (E, H, D, DR clipped at 0), and at j = k its wave
+ * action and roller energy are rescaled per cell to the forced E and DR, so
+ * that the wave solver can take over; the others run the wave solver.  Dt,
+ * boundaries, flow, sediment and means are the plain kernels throughout.
+ * Does not synchronise.                                                    */
+int  xbg_batch_forced_segment(xbg_batch* b, int k);
+/* The judge: per scenario, the relative L2 distance ||pred - f|| / ||f||
+ * of a prediction plane from the model's 2-D field f (XBG_F_*); pred: n
+ * device plane pointers (NULL: scenario skipped, err = -1).  Synchronises. */
+int  xbg_batch_rel_err(xbg_batch* b, int field, const void* const* pred,
+                       double* err);
 
 /* ---- no-allocation entry point ------------------------------------------
  * No counterpart in the reference.  For callers that may not allocate

@@ -134,6 +134,23 @@ int xbg_nn_copy_planes(const float* const* src, float* const* dst, int nc,
  * a zero plane).                                                           */
 int xbg_nn_encode(const float* const* planes, int nc, const float* mean,
                   const float* inv_std, void* x, long long P, void* stream);
+/* xbg_nn_encode for nimg images of different sizes padded to one Hp x Wp
+ * batch ([nimg][Hp][Wp][nc] bf16): image b has dims[2b] x dims[2b+1]
+ * (<= Wp x Hp) pixels and planes planes[b*nc + c]; a NULL plane is the
+ * constant cval[b*nc + c] (or 0 when cval is NULL); pixels beyond the image
+ * repeat its last column and row.  planes, dims, cval: DEVICE arrays.      */
+int xbg_nn_encode_batch(const float* const* planes, int nc, const int* dims,
+                        const float* cval, const float* mean,
+                        const float* inv_std, void* x, int nimg, int Hp,
+                        int Wp, void* stream);
+/* xbg_nn_decode for such a batch: out [nimg][Hp][Wp][ldo] f32; hold, dst
+ * and (optional, may be NULL) dst0 are DEVICE arrays of nimg*nc plane
+ * pointers; dst0 receives a copy of hold.  Only each image's own pixels
+ * are written.                                                             */
+int xbg_nn_decode_batch(const float* out, int ldo, const float* const* hold,
+                        const float* ym, const float* ys, float* const* dst,
+                        float* const* dst0, const int* dims, int nc, int nimg,
+                        int Hp, int Wp, void* stream);
 /* network output to model planes: dst[c][p] = hold[c][p] + out[p][c] *
  * ys[c] + ym[c]; hold and dst are DEVICE arrays of nc f32 plane pointers. */
 int xbg_nn_decode(const float* out, int ldo, const float* const* hold,

@@ -77,25 +77,35 @@ def test_batch_scenarios_end_on_their_own():
 
 
 def test_batch_grid_choice_does_not_change_results(tmp_path):
-    """The autotuner's knob (persistent blocks per tile shape) only changes
-    which block runs which tile: two batches with different block counts end
+    """The autotuner's knobs (persistent blocks per tile shape, the wave rows
+    variant) only change which block runs which tile and how the tiles are
+    moved: batches with different block counts and either wave variant end
     bit for bit the same."""
     from xbeach_gpu_b200.autotune import tune
     sc = _cases(4, 21)
+    from xbeach_gpu_b200.abi import XBG_PHASE_WAVE
     runs = []
-    for variant in ("default", "tuned"):
+    for variant in ("default", "tuned", "thread_tiles"):
         b = Batch([p for p, _, _ in sc], XBG_FP32)
         for s, (p, zb, bnd) in enumerate(sc):
             _setup(b.scenario(s), p, zb, bnd)
         if variant == "tuned":
             for shape, blocks in ((0, 7), (1, 3), (2, 5), (5, 2)):
                 b.set_grid(shape, blocks)
+        if variant == "thread_tiles":
+            assert b.variant(XBG_PHASE_WAVE) == 1
+            b.set_variant(XBG_PHASE_WAVE, 0)
+            assert b.variant(XBG_PHASE_WAVE) == 0
         b.advance(25)
         runs.append({s: {f: b.scenario(s).get(f).copy() for f in ("zs", "uu", "H", "ee")} for s in range(len(sc))})
         if variant == "tuned":
             choice = tune(b, cache=str(tmp_path / "tune.json"), reps=1)
-            assert set(choice) == {0, 1, 2, 5} and all(v >= 1 for v in choice.values())
+            assert {0, 1, 2, 5} <= set(choice) and all(choice[k] >= 1 for k in (0, 1, 2, 5))
+            assert choice["wave_variant"] in (0, 1) and b.variant(XBG_PHASE_WAVE) == choice["wave_variant"]
+            again = tune(b, cache=str(tmp_path / "tune.json"), reps=1)   # from the cache
+            assert again == choice
         b.close()
     for s in runs[0]:
         for f in runs[0][s]:
             assert np.array_equal(runs[0][s][f], runs[1][s][f]), (s, f)
+            assert np.array_equal(runs[0][s][f], runs[2][s][f]), (s, f)

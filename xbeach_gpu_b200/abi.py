@@ -30,6 +30,11 @@ XBG_PHASE_WAVE = 0   # xbg_set_kernel_variant phases
 XBG_FLAG_OUTPUT_DUE = 1
 XBG_FLAG_ENDED = 2
 XBG_FLAG_NEED_BOUNDARY = 4
+XBG_FLAG_FALLBACK = 8
+
+XBG_WAVE_PLAIN = 0      # xbg_batch_set_wave_mode
+XBG_WAVE_FORCED = 1
+XBG_WAVE_FALLBACK = 2
 
 FIELD_NAMES = [
     "zb", "zs", "hh", "uu", "vv",

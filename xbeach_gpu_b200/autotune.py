@@ -3,26 +3,36 @@
 The batched kernels are persistent: each launch runs a chosen number of
 blocks that walk contiguous runs of the (scenario, tile) work list of its
 tile shape.  The best number depends on the kernel's occupancy, the number of
-work items and how ragged the scenarios are, so it is measured: for each
-shape, every candidate block count is timed with CUDA events around each
-kernel of a batched step (xbg_batch_profile_step), the fastest is kept, and
-the choice is cached in a JSON file keyed by (shape, scenarios, cells,
-ntheta, precision, GPU name) so a later batch of the same make-up reuses it.
+work items and how ragged the scenarios are, and for the wave rows pass it
+also depends on which implementation runs (TMA plane tiles or thread-copied
+tiles: they trade per-item latency for per-cell instructions differently).
+So both are measured: for each phase, every (kernel variant, block count)
+candidate is timed with CUDA events around each kernel of a batched step
+(xbg_batch_profile_step), the fastest is kept, and the choice is cached in a
+JSON file keyed by (phase, scenario grids, ntheta, precision, GPU name) so a
+later batch of the same make-up reuses it.  The tile shape itself (32 x 8
+cells) is fixed at compile time.
 
     from xbeach_gpu_b200.autotune import tune
-    choice = tune(batch)          # applies and returns {shape: blocks}
+    choice = tune(batch)   # applies and returns {shape: blocks, "wave_variant": v}
 """
+import hashlib
 import json
 import os
 
-# tile shapes of xbg_batch_set_grid and the kernels that use them
-SHAPES = {
-    0: ("tile", {"k_wave_force", "k_flow_a", "k_flow_u", "k_flow_v", "k_flow_corr",
-                 "k_flow_final", "k_sed_a", "k_sed_b", "k_sed_c"}),
-    1: ("wave_rows", {"k_wave_fast"}),
-    2: ("lin", {"k_disp", "k_means"}),
-    5: ("dt", {"k_step_begin"}),
+from .abi import XBG_PHASE_WAVE
+from .model import XbgError
+
+# phases: the tile shape of xbg_batch_set_grid they launch with, the kernels
+# timed, and the kernel variants searched (None: the phase has one)
+PHASES = {
+    "tile": (0, {"k_wave_force", "k_flow_a", "k_flow_u", "k_flow_v", "k_flow_corr", "k_flow_final", "k_sed_a",
+                 "k_sed_b", "k_sed_c"}, (None,)),
+    "wave_rows": (1, {"k_wave_fast", "k_wave_tma"}, (1, 0)),
+    "lin": (2, {"k_disp", "k_means"}, (None,)),
+    "dt": (5, {"k_step_begin"}, (None,)),
 }
+SHAPES = {sh: (label, kern) for label, (sh, kern, _) in PHASES.items()}
 FACTORS = (1, 2, 3, 4, 6, 8, 12, 16)
 
 
@@ -58,34 +68,57 @@ def _time_shape(batch, kernels, reps):
     return ts[len(ts) // 2]
 
 
+def make_up(batch):
+    """The batch's make-up in the cache key: scenario grids, ntheta, precision."""
+    grids = sorted((m.p.nx, m.p.ny) for m in batch.models)
+    h = hashlib.sha1(json.dumps(grids).encode()).hexdigest()[:12]
+    prec = "f32" if batch.models[0].dtype.itemsize == 4 else "f64"
+    return f"{batch.n}|{h}|{batch.models[0].p.ntheta}|{prec}"
+
+
 def tune(batch, cache=None, reps=3, shapes=None, use_cache=True):
-    """Measure and apply the persistent block count of each tile shape of
-    `batch` (a model.Batch).  Returns {shape: blocks}.  The simulation state
+    """Measure and apply, per phase of `batch` (a model.Batch), the kernel
+    variant and the persistent block count.  Returns {shape: blocks} and,
+    under "wave_variant", the wave rows variant in use.  The simulation state
     advances by the profiled steps."""
     name, sms = _gpu()
-    cells = sum(m.p.nx * m.p.ny for m in batch.models)
-    nt = batch.models[0].p.ntheta
-    prec = "f32" if batch.models[0].dtype.itemsize == 4 else "f64"
+    key0 = f"{make_up(batch)}|{name}"
     path = _cache_path(cache)
     db = _load(path) if use_cache else {}
     choice = {}
-    for shape in (shapes or SHAPES):
-        label, kernels = SHAPES[shape]
-        key = f"{label}|{batch.n}|{cells}|{nt}|{prec}|{name}"
+    for label, (shape, kernels, variants) in PHASES.items():
+        if shapes is not None and shape not in shapes:
+            continue
+        key = f"{label}|{key0}"
         if key in db:
-            choice[shape] = int(db[key])
-            batch.set_grid(shape, choice[shape])
+            v, g = db[key]
+            if v is not None:
+                batch.set_variant(XBG_PHASE_WAVE, v)
+            batch.set_grid(shape, g)
+            choice[shape] = g
+            if v is not None:
+                choice["wave_variant"] = v
             continue
         best = None
-        for f in FACTORS:
-            g = sms * f
-            batch.set_grid(shape, g)
-            t = _time_shape(batch, kernels, reps)
-            if best is None or t < best[1]:
-                best = (g, t)
-        choice[shape] = best[0]
-        batch.set_grid(shape, best[0])
-        db[key] = best[0]
+        for v in variants:
+            if v is not None:
+                try:
+                    batch.set_variant(XBG_PHASE_WAVE, v)
+                except XbgError:   # not available for this batch
+                    continue
+            for f in FACTORS:
+                g = sms * f
+                batch.set_grid(shape, g)
+                t = _time_shape(batch, kernels, reps)
+                if best is None or t < best[2]:
+                    best = (v, g, t)
+        v, g, _ = best
+        if v is not None:
+            batch.set_variant(XBG_PHASE_WAVE, v)
+            choice["wave_variant"] = v
+        batch.set_grid(shape, g)
+        choice[shape] = g
+        db[key] = [v, g]
     if use_cache:
         try:
             os.makedirs(os.path.dirname(path), exist_ok=True)

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <cstdio>
+#include <map>
 #include <vector>
 #include <algorithm>
 #include "xbg_common.cuh"
@@ -31,7 +32,7 @@ template <class R> int launch_wavebnd_batch(const BatchTab<R>&, const BatchLaunc
 template <class R> int launch_ubnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_means_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                         cudaEvent_t);
+                                         cudaEvent_t, const WaveMaps*);
 template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int ubnd_threads(const Konst<R>&);
@@ -59,17 +60,15 @@ template <class R>
 struct Forcing6 { const R* p[6]; };
 
 template <class R>
-__global__ void k_set_forcing(Dev<R> S, R* ee0, R* ee1, R* rr0, R* rr1, Forcing6<R> f0, Forcing6<R> f1, R w,
-                              int rescale) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.C) return;
+__device__ __forceinline__ void set_forcing_cell(const Dev<R>& S, R* ee0, R* ee1, R* rr0, R* rr1,
+                                                 const R* const* f0, const R* const* f1, R w, int rescale, int i) {
     R v[6];
 #pragma unroll
-    for (int c = 0; c < 6; c++) v[c] = f0.p[c][i] + w * (f1.p[c][i] - f0.p[c][i]);
+    for (int c = 0; c < 6; c++) v[c] = f0[c][i] + w * (f1[c][i] - f0[c][i]);
 #pragma unroll
     for (int c = 0; c < 4; c++) v[c] = v[c] > (R)0 ? v[c] : (R)0;
     if (rescale) {   // ee, rr still hold the state of f0 (the segment start)
-        const R Eo = f0.p[0][i], DRo = f0.p[3][i];
+        const R Eo = f0[0][i], DRo = f0[3][i];
         const R re = Eo > (R)1e-12 ? v[0] / Eo : (R)1;
         const R rr = DRo > (R)1e-12 ? v[3] / DRo : (R)1;
         for (int t = 0; t < S.nt; t++) {
@@ -80,6 +79,65 @@ __global__ void k_set_forcing(Dev<R> S, R* ee0, R* ee1, R* rr0, R* rr1, Forcing6
         S.f[ROL][i] *= rr;
     }
     S.f[E][i] = v[0]; S.f[H][i] = v[1]; S.f[D][i] = v[2]; S.f[DR][i] = v[3]; S.f[FX][i] = v[4]; S.f[FY][i] = v[5];
+}
+template <class R>
+__global__ void k_set_forcing(Dev<R> S, R* ee0, R* ee1, R* rr0, R* rr1, Forcing6<R> f0, Forcing6<R> f1, R w,
+                              int rescale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.C) return;
+    set_forcing_cell(S, ee0, ee1, rr0, rr1, f0.p, f1.p, w, rescale, i);
+}
+
+// The forcing planes of each scenario of a batch (xbg_batch_set_forcing).
+template <class R>
+struct ForcingPair { const R* f0[6]; const R* f1[6]; };
+
+// The forcing of every scenario in forced mode, one 256-cell run per item;
+// scenarios in plain mode (their wave solver ran this step) are left alone.
+template <class R>
+__global__ void __launch_bounds__(256) kb_set_forcing(BatchTab<R> T, const ForcingPair<R>* fp, R w, int rescale,
+                                                      const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>&, const BatchAux& A, int bx, int) {
+        if (halted(S.clk) || *((volatile const int*)&S.clk->forced) == 0) return;
+        const int i = bx * 256 + threadIdx.x;
+        if (i >= S.C) return;
+        const ForcingPair<R>& f = fp[A.scen];
+        set_forcing_cell(S, S.ee[0], S.ee[1], S.rr[0], S.rr[1], f.f0, f.f1, w, rescale, i);
+    });
+}
+
+// Per scenario sum((pred - field)^2) and sum(field^2) (FP64 accumulators,
+// one pair per scenario); scenarios without a prediction are skipped.
+template <class R>
+struct ErrPair { const R* field; const R* pred; };
+template <class R>
+__global__ void __launch_bounds__(256) kb_rel_err(BatchTab<R> T, const ErrPair<R>* ep, double* acc,
+                                                  const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>&, const BatchAux& A, int bx, int) {
+        const ErrPair<R> e = ep[A.scen];
+        if (!e.pred) return;
+        const int i = bx * 256 + threadIdx.x;
+        double d2 = 0.0, f2 = 0.0;
+        if (i < S.C) {
+            const double f = (double)e.field[i], d = (double)e.pred[i] - f;
+            d2 = d * d;
+            f2 = f * f;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            f2 += __shfl_xor_sync(0xffffffffu, f2, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(acc + 2 * A.scen, d2);
+            atomicAdd(acc + 2 * A.scen + 1, f2);
+        }
+    });
+}
+
+// wave mode of one clock: forced (1) or plain (0); fallback also marks it
+__global__ void k_set_wave_mode(Clock* c, int forced, int fallback) {
+    c->forced = forced;
+    if (fallback) c->flags |= XBG_FLAG_FALLBACK;
 }
 
 // Copy every scenario's device clock of a batch into one array.
@@ -204,6 +262,12 @@ struct xbg_batch {
     virtual int profile(float* ms, const char** names, int* n) = 0;
     virtual int set_grid(int shape, int blocks) = 0;
     virtual int64_t launches() = 0;
+    virtual int set_variant(int phase, int variant) = 0;
+    virtual int get_variant(int phase, int* variant) = 0;
+    virtual int set_wave_mode(int s, int mode) = 0;
+    virtual int set_forcing(int s, const void* const* f0, const void* const* f1) = 0;
+    virtual int forced_segment(int k) = 0;
+    virtual int rel_err(int field, const void* const* pred, double* err) = 0;
 };
 
 namespace {
@@ -808,12 +872,28 @@ struct Batch : public xbg_batch {
     int64_t nlaunch = 0;
     cudaError_t last_err = cudaSuccess;
     int nt = 0, swave = 0, flow = 0, sedtrans = 0, roller = 0, means = 0, wci = 0;   // wci: any scenario with wave-current interaction
+    WaveMaps* dmaps = nullptr;            // the scenarios' tensor maps (TMA rows pass), if every scenario has them
+    int wave_variant = 1;                 // 1: TMA rows pass (when dmaps), 0: thread-copied tiles
+    const WaveMaps* wave_maps() const { return wave_variant == 1 ? dmaps : nullptr; }
+    // surrogate-assisted stepping: forcing planes per scenario, graphs of
+    // forced segments by length, judge accumulators
+    std::vector<ForcingPair<R>> hfp;
+    ForcingPair<R>* dfp = nullptr;
+    std::vector<ErrPair<R>> hep;
+    ErrPair<R>* dep = nullptr;
+    double* dacc = nullptr;
+    std::map<int, cudaGraphExec_t> seg_exec;
+    std::map<int, cudaGraph_t> seg_graph;
+    std::map<int, int> seg_n;
 
     ~Batch() override {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
         for (auto e : evs) cudaEventDestroy(e);
-        cudaFree(dS); cudaFree(dK); cudaFree(dA); cudaFree(dclk);
+        for (auto& kv : seg_exec) cudaGraphExecDestroy(kv.second);
+        for (auto& kv : seg_graph) cudaGraphDestroy(kv.second);
+        cudaFree(dS); cudaFree(dK); cudaFree(dA); cudaFree(dclk); cudaFree(dmaps);
+        cudaFree(dfp); cudaFree(dep); cudaFree(dacc);
         for (int k = 0; k < BS_N; k++) cudaFree(ditems[k]);
         for (auto p : hs) delete p;
         if (ev_fork) cudaEventDestroy(ev_fork);
@@ -858,7 +938,7 @@ struct Batch : public xbg_batch {
             hA[s].nflow = std::min((C + 255) / 256, 32);   // within the handle's 2 * step_begin_blocks partials
             hA[s].nwave = H.nwave;
             hA[s].ubnd_threads = ubnd_threads(H.K);
-            hA[s].pad = 0;
+            hA[s].scen = s;
             auto add = [&](int sh, int bx, int by) { it[sh].push_back(make_int2(s, bx | (by << 16))); };
             for (int by = 0; by < (ny + 7) / 8; by++)
                 for (int bx = 0; bx < (nx + 31) / 32; bx++) add(BS_TILE, bx, by);
@@ -868,6 +948,14 @@ struct Batch : public xbg_batch {
             add(BS_ONE, 0, 0);
             for (int b = 0; b < (ny * nt + 255) / 256; b++) add(BS_BND, b, 0);
             for (int b = 0; b < hA[s].nflow; b++) add(BS_DT, b, 0);
+        }
+        bool all_maps = true;
+        for (int s = 0; s < ns; s++) all_maps = all_maps && hs[s]->maps_ok;
+        if (all_maps) {
+            std::vector<WaveMaps> hm(ns);
+            for (int s = 0; s < ns; s++) hm[s] = hs[s]->maps;
+            CK(cudaMalloc(&dmaps, ns * sizeof(WaveMaps)));
+            CK(cudaMemcpy(dmaps, hm.data(), ns * sizeof(WaveMaps), cudaMemcpyHostToDevice));
         }
         CK(cudaMalloc(&dS, ns * sizeof(Dev<R>)));
         CK(cudaMalloc(&dK, ns * sizeof(Konst<R>)));
@@ -879,7 +967,7 @@ struct Batch : public xbg_batch {
         int dev = 0, sms = 148;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const int per_sm[BS_N] = {8, 3, 8, 2, 8, 8};   // resident-block targets per SM
+        const int per_sm[BS_N] = {8, dmaps ? 4 : 3, 8, 2, 8, 8};   // resident-block targets per SM
         for (int k = 0; k < BS_N; k++) {
             CK(cudaMalloc(&ditems[k], std::max<size_t>(1, it[k].size()) * sizeof(int2)));
             CK(cudaMemcpy(ditems[k], it[k].data(), it[k].size() * sizeof(int2), cudaMemcpyHostToDevice));
@@ -889,14 +977,20 @@ struct Batch : public xbg_batch {
         }
         evs.resize(ns);
         for (int s = 0; s < ns; s++) CK(cudaEventCreateWithFlags(&evs[s], cudaEventDisableTiming));
+        hfp.assign(ns, ForcingPair<R>{});
+        hep.assign(ns, ErrPair<R>{});
+        CK(cudaMalloc(&dfp, ns * sizeof(ForcingPair<R>)));
+        CK(cudaMemset(dfp, 0, ns * sizeof(ForcingPair<R>)));
+        CK(cudaMalloc(&dep, ns * sizeof(ErrPair<R>)));
+        CK(cudaMalloc(&dacc, 2 * ns * sizeof(double)));
         for (auto* hp : hs) CK(cudaStreamSynchronize(hp->st));
         return XBG_OK;
     }
 
     BatchTab<R> tab() const { return BatchTab<R>{dS, dK, dA}; }
 
-    int enqueue(Prof* pf) {
-        BatchTab<R> T = tab();
+    // dt/clock pass, boundaries and the wave solver of one batched step
+    int enqueue_waves(const BatchTab<R>& T, Prof* pf) {
         int k = 0;
         k += launch_step_begin_batch(T, L, st, pf);
         if (swave == 1 && !pf) {   // the boundary kernels beside the dispersion kernel, as for one handle
@@ -905,16 +999,26 @@ struct Batch : public xbg_batch {
             k += launch_wavebnd_batch(T, L, side, nullptr);
             if (flow == 1) k += launch_ubnd_batch(T, L, side, nullptr);
             cudaEventRecord(ev_join, side);
-            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join);
+            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join, wave_maps());
         } else {
             if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
             if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
-            if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr);
+            if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr, wave_maps());
         }
+        return k;
+    }
+    // flow, sediment and means of one batched step
+    int enqueue_rest(const BatchTab<R>& T, Prof* pf) {
+        int k = 0;
         if (flow == 1) k += launch_flow_batch(T, L, st, pf);
         if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf);
         if (means) k += launch_means_batch(T, L, st, pf);
         return k;
+    }
+    int enqueue(Prof* pf) {
+        BatchTab<R> T = tab();
+        int k = enqueue_waves(T, pf);
+        return k + enqueue_rest(T, pf);
     }
 
     // order the batch after the scenarios' own streams and refresh the
@@ -964,11 +1068,106 @@ struct Batch : public xbg_batch {
     void* stream() override { return (void*)st; }
     int64_t launches() override { return nlaunch; }
 
+    void drop_segments() {
+        for (auto& kv : seg_exec) cudaGraphExecDestroy(kv.second);
+        for (auto& kv : seg_graph) cudaGraphDestroy(kv.second);
+        seg_exec.clear(); seg_graph.clear(); seg_n.clear();
+    }
     int set_grid(int shape, int blocks) override {
         if (shape < 0 || shape >= BS_N || blocks < 1) return XBG_ERR_ARG;
         L.grid[shape] = std::min(blocks, std::max(1, L.n[shape]));
         if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
         if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+        drop_segments();
+        return XBG_OK;
+    }
+
+    int set_variant(int phase, int variant) override {
+        if (phase != XBG_PHASE_WAVE || variant < 0 || variant > 1 || (variant == 1 && !dmaps)) return XBG_ERR_ARG;
+        if (variant != wave_variant) {
+            CK(cudaStreamSynchronize(st));
+            wave_variant = variant;
+            if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+            if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
+            drop_segments();
+        }
+        return XBG_OK;
+    }
+    int get_variant(int phase, int* variant) override {
+        if (phase != XBG_PHASE_WAVE || !variant) return XBG_ERR_ARG;
+        *variant = wave_maps() ? 1 : 0;
+        return XBG_OK;
+    }
+    int set_wave_mode(int s, int mode) override {
+        if (s < 0 || s >= n || mode < XBG_WAVE_PLAIN || mode > XBG_WAVE_FALLBACK) return XBG_ERR_ARG;
+        if (mode == XBG_WAVE_FORCED && !hfp[s].f0[0]) return XBG_ERR_STATE;   // no forcing planes yet
+        k_set_wave_mode<<<1, 1, 0, st>>>(hs[s]->clk, mode == XBG_WAVE_FORCED ? 1 : 0, mode == XBG_WAVE_FALLBACK);
+        nlaunch++;
+        CK(cudaGetLastError());
+        return XBG_OK;
+    }
+    int set_forcing(int s, const void* const* f0, const void* const* f1) override {
+        if (s < 0 || s >= n || !f0 || !f1) return XBG_ERR_ARG;
+        ForcingPair<R> fp;
+        for (int c = 0; c < 6; c++) {
+            if (!f0[c] || !f1[c]) return XBG_ERR_ARG;
+            fp.f0[c] = (const R*)f0[c];
+            fp.f1[c] = (const R*)f1[c];
+        }
+        hfp[s] = fp;
+        CK(cudaMemcpyAsync(dfp + s, &hfp[s], sizeof(fp), cudaMemcpyHostToDevice, st));
+        return XBG_OK;
+    }
+    // k coupled steps of every scenario: scenarios in forced mode take the
+    // wave sub-step of step j from f0 + (j/k)(f1 - f0) (rescaled at j = k),
+    // the others run the wave solver; one CUDA graph per k, replayed
+    int forced_segment(int k) override {
+        if (k < 1 || k > 100000) return XBG_ERR_ARG;
+        int rc = prepare();
+        if (rc) return rc;
+        if (!seg_exec.count(k)) {
+            BatchTab<R> T = tab();
+            CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int cnt = 0;
+            for (int j = 1; j <= k; j++) {
+                cnt += enqueue_waves(T, nullptr);
+                kb_set_forcing<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, dfp, (R)((double)j / k), j == k ? 1 : 0,
+                                                                   L.items[BS_LIN], L.n[BS_LIN]);
+                cnt++;
+                cnt += enqueue_rest(T, nullptr);
+            }
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (e != cudaSuccess) { last_err = e; return XBG_ERR_CUDA; }
+            cudaGraphExec_t x = nullptr;
+            CK(cudaGraphInstantiate(&x, g, 0));
+            seg_graph[k] = g; seg_exec[k] = x; seg_n[k] = cnt;
+        }
+        CK(cudaGraphLaunch(seg_exec[k], st));
+        nlaunch += seg_n[k];
+        return XBG_OK;
+    }
+    int rel_err(int field, const void* const* pred, double* err) override {
+        if (!pred || !err) return XBG_ERR_ARG;
+        int rc = prepare();
+        if (rc) return rc;
+        for (int s = 0; s < n; s++) {
+            size_t m = 0;
+            const R* f = hs[s]->field_ptr(field, &m, 0);
+            if (!f || m != (size_t)hs[s]->S.C || field == XBG_F_EE || field == XBG_F_RR || field == XBG_F_ZSOLD)
+                return XBG_ERR_ARG;
+            hep[s] = ErrPair<R>{f, (const R*)pred[s]};
+        }
+        CK(cudaMemcpyAsync(dep, hep.data(), n * sizeof(ErrPair<R>), cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(dacc, 0, 2 * n * sizeof(double), st));
+        kb_rel_err<R><<<L.grid[BS_LIN], 256, 0, st>>>(tab(), dep, dacc, L.items[BS_LIN], L.n[BS_LIN]);
+        nlaunch++;
+        CK(cudaGetLastError());
+        std::vector<double> h(2 * n);
+        CK(cudaMemcpyAsync(h.data(), dacc, 2 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        for (int s = 0; s < n; s++)
+            err[s] = pred[s] ? std::sqrt(h[2 * s]) / std::max(std::sqrt(h[2 * s + 1]), 1e-30) : -1.0;
         return XBG_OK;
     }
 
@@ -1093,6 +1292,20 @@ int xbg_batch_get_stream(xbg_batch* b, void** s) { if (!b || !s) return XBG_ERR_
 int xbg_batch_profile_step(xbg_batch* b, float* ms, const char** names, int* n) {
     if (!b || !ms || !n) return XBG_ERR_ARG;
     return b->profile(ms, names, n);
+}
+int xbg_batch_set_kernel_variant(xbg_batch* b, int phase, int variant) {
+    return b ? b->set_variant(phase, variant) : XBG_ERR_ARG;
+}
+int xbg_batch_get_kernel_variant(xbg_batch* b, int phase, int* variant) {
+    return b ? b->get_variant(phase, variant) : XBG_ERR_ARG;
+}
+int xbg_batch_set_wave_mode(xbg_batch* b, int s, int mode) { return b ? b->set_wave_mode(s, mode) : XBG_ERR_ARG; }
+int xbg_batch_set_forcing(xbg_batch* b, int s, const void* const* f0, const void* const* f1) {
+    return b ? b->set_forcing(s, f0, f1) : XBG_ERR_ARG;
+}
+int xbg_batch_forced_segment(xbg_batch* b, int k) { return b ? b->forced_segment(k) : XBG_ERR_ARG; }
+int xbg_batch_rel_err(xbg_batch* b, int field, const void* const* pred, double* err) {
+    return b ? b->rel_err(field, pred, err) : XBG_ERR_ARG;
 }
 int xbg_batch_set_grid(xbg_batch* b, int shape, int blocks) { return b ? b->set_grid(shape, blocks) : XBG_ERR_ARG; }
 int xbg_batch_launch_count(xbg_batch* b, int64_t* n) { if (!b || !n) return XBG_ERR_ARG; *n = b->launches(); return XBG_OK; }

@@ -303,6 +303,57 @@ __global__ void k_decode(const float* __restrict__ out, int ldo, const float* co
     dst[c][p] = hold[c][p] + out[p * ldo + c] * ys[c] + ym[c];
 }
 
+// Network input of several images of different sizes padded to one Hp x Wp:
+// image b (nx = dims[2b], ny = dims[2b+1] <= Hp, Wp) from its planes
+// planes[b*nc + c] (a NULL plane is the constant cval[b*nc + c], or 0);
+// pixels beyond the image repeat its last column / row.
+__global__ void k_encode_batch(const float* const* __restrict__ planes, int nc, const int* __restrict__ dims,
+                               const float* __restrict__ cval, const float* __restrict__ mean,
+                               const float* __restrict__ inv_std, bf* __restrict__ x, int nimg, int Hp, int Wp) {
+    const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+    const long long total = (long long)nimg * Hp * Wp * nc;
+    if (idx >= total) return;
+    const int c = (int)(idx % nc);
+    const long long pix = idx / nc;
+    const int xw = (int)(pix % Wp);
+    const long long r = pix / Wp;
+    const int yh = (int)(r % Hp);
+    const int b = (int)(r / Hp);
+    const int nx = dims[2 * b], ny = dims[2 * b + 1];
+    const float* pl = planes[(long long)b * nc + c];
+    const int xs = min(xw, nx - 1), ys = min(yh, ny - 1);
+    float v = 0.0f;
+    if (pl) v = (pl[xs + (long long)ys * nx] - mean[c]) * inv_std[c];
+    else if (cval) v = (cval[(long long)b * nc + c] - mean[c]) * inv_std[c];
+    x[idx] = __float2bfloat16(v);
+}
+
+// Network output of a padded batch back to each image's planes:
+// dst[b*nc + c][p] = hold[b*nc + c][p] + out[b][y][x][c] * ys[c] + ym[c]
+// for the image's own pixels, and dst0[b*nc + c][p] = hold[...][p] when dst0
+// is given (the fields the prediction starts from, kept).
+__global__ void k_decode_batch(const float* __restrict__ out, int ldo, const float* const* __restrict__ hold,
+                               const float* __restrict__ ym, const float* __restrict__ ysd,
+                               float* const* __restrict__ dst, float* const* __restrict__ dst0,
+                               const int* __restrict__ dims, int nc, int nimg, int Hp, int Wp) {
+    const long long idx = (long long)blockIdx.x * TPB + threadIdx.x;
+    const long long total = (long long)nimg * Hp * Wp * nc;
+    if (idx >= total) return;
+    const int c = (int)(idx % nc);
+    const long long pix = idx / nc;
+    const int xw = (int)(pix % Wp);
+    const long long r = pix / Wp;
+    const int yh = (int)(r % Hp);
+    const int b = (int)(r / Hp);
+    const int nx = dims[2 * b], ny = dims[2 * b + 1];
+    if (xw >= nx || yh >= ny) return;
+    const long long p = xw + (long long)yh * nx;
+    const long long k = (long long)b * nc + c;
+    const float h = hold[k][p];
+    dst[k][p] = h + out[pix * ldo + c] * ysd[c] + ym[c];
+    if (dst0) dst0[k][p] = h;
+}
+
 // dst[c][p] = src[c][p] (device arrays of nc plane pointers)
 __global__ void k_copy_planes(const float* const* __restrict__ src, float* const* __restrict__ dst, int nc,
                               long long P) {
@@ -473,6 +524,24 @@ int xbg_nn_decode(const float* out, int ldo, const float* const* hold, const flo
     if (!out || !hold || !ym || !ys || !dst || nc < 1 || ldo < nc || P < 1) return XBG_ERR_ARG;
     NN_LAUNCH(P * nc);
     k_decode<<<blocks_for(P * nc), TPB, 0, st_>>>(out, ldo, hold, ym, ys, dst, nc, P);
+    NN_DONE;
+}
+int xbg_nn_encode_batch(const float* const* planes, int nc, const int* dims, const float* cval, const float* mean,
+                        const float* inv_std, void* x, int nimg, int Hp, int Wp, void* stream) {
+    if (!planes || !dims || !mean || !inv_std || !x || nc < 1 || nimg < 1 || Hp < 1 || Wp < 1) return XBG_ERR_ARG;
+    const long long n = (long long)nimg * Hp * Wp * nc;
+    NN_LAUNCH(n);
+    k_encode_batch<<<blocks_for(n), TPB, 0, st_>>>(planes, nc, dims, cval, mean, inv_std, (bf*)x, nimg, Hp, Wp);
+    NN_DONE;
+}
+int xbg_nn_decode_batch(const float* out, int ldo, const float* const* hold, const float* ym, const float* ys,
+                        float* const* dst, float* const* dst0, const int* dims, int nc, int nimg, int Hp, int Wp,
+                        void* stream) {
+    if (!out || !hold || !ym || !ys || !dst || !dims || nc < 1 || ldo < nc || nimg < 1 || Hp < 1 || Wp < 1)
+        return XBG_ERR_ARG;
+    const long long n = (long long)nimg * Hp * Wp * nc;
+    NN_LAUNCH(n);
+    k_decode_batch<<<blocks_for(n), TPB, 0, st_>>>(out, ldo, hold, ym, ys, dst, dst0, dims, nc, nimg, Hp, Wp);
     NN_DONE;
 }
 int xbg_nn_copy_planes(const float* const* src, float* const* dst, int nc, long long P, void* stream) {

@@ -58,7 +58,7 @@ __device__ void disp_cell(const Konst<R>& K, R sg, R h, R& k_, R& c_, R& cg_) {
 
 template <class R>
 __device__ __forceinline__ void b_disp(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
-    if (halted(S.clk)) return;
+    if (wave_off(S.clk)) return;
     int i = bix * blockDim.x + threadIdx.x;
     if (i >= S.C) return;
     R sg = (R)S.clk->sigm;
@@ -331,7 +331,7 @@ template <class R, bool ROLLER, bool WCI>
 __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    if (wave_off(clk)) return;
     const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
     const int tid = threadIdx.x + threadIdx.y * WT_X;
     R* tE = (R*)smem_raw;                 // [WT_NB][WT_N] plane tiles of ee
@@ -696,7 +696,7 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long mbar[TM_NB];
     Clock* clk = S.clk;
-    if (halted(clk)) return;
+    if (wave_off(clk)) return;
     const int nx = K.nx, ny = K.ny, nt = K.nt, C = S.C;
     const int tid = threadIdx.x + threadIdx.y * WT_X;
     const unsigned base = (su32(smem_raw) + 127u) & ~127u;
@@ -968,6 +968,15 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
     k_wave_tma(Dev<R> S, Konst<R> K, const __grid_constant__ WaveMaps M) {
     b_wave_tma<R, ROLLER>(S, K, M, blockIdx.x, blockIdx.y);
 }
+// every scenario of a batch: its tensor maps from a device array (written
+// by the host before the first launch), one per scenario
+template <class R, bool ROLLER>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
+    kb_wave_tma(BatchTab<R> T, const WaveMaps* __restrict__ maps, const int2* items, int n) {
+    batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux& A, int bx, int by) {
+        b_wave_tma<R, ROLLER>(S, K, maps[A.scen], bx, by);
+    });
+}
 
 // Tensor maps of the TMA rows pass: ee and rr of both plane sets as 3-D
 // arrays [nt][ny][nx]; loads in 40 x 12 x 1 boxes, stores in 32 x 8 x nt
@@ -1040,7 +1049,7 @@ __device__ __forceinline__ void breaker_raw(const Dev<R>& S, const Konst<R>& K, 
 template <class R>
 __device__ __forceinline__ void b_wave_force(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    if (wave_off(clk)) return;
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x;
     int iy = biy * blockDim.y + threadIdx.y;
@@ -1113,22 +1122,33 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, c
 
 // the wave kernels over every scenario of a batch (one ntheta and roller
 // setting for the whole batch)
+// maps: the scenarios' tensor maps (device array) for the TMA rows pass, or
+// null for the thread-copied tiles
 template <class R>
 int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
-                      Prof* pf, cudaEvent_t join) {
+                      Prof* pf, cudaEvent_t join, const WaveMaps* maps) {
     kb_disp<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
     PMARK(pf, "k_disp");
     if (join) cudaStreamWaitEvent(st, join, 0);
-    launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
-    PMARK(pf, "k_wave_fast");
+    if (maps && !wci) {
+        const int g = L.grid[BS_WROWS], n = L.n[BS_WROWS];
+        const int2* it = L.items[BS_WROWS];
+        const size_t smem = wave_tma_smem<R>(nt);
+        if (roller == 1) kb_wave_tma<R, true><<<g, dim3(32, 8), smem, st>>>(T, maps, it, n);
+        else kb_wave_tma<R, false><<<g, dim3(32, 8), smem, st>>>(T, maps, it, n);
+        PMARK(pf, "k_wave_tma");
+    } else {
+        launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
+        PMARK(pf, "k_wave_fast");
+    }
     kb_wave_force<R><<<L.grid[BS_TILE], dim3(32, 8), 0, st>>>(T, L.items[BS_TILE], L.n[BS_TILE]);
     PMARK(pf, "k_wave_force");
     return 3;
 }
 template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                      cudaEvent_t);
+                                      cudaEvent_t, const WaveMaps*);
 template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                       cudaEvent_t);
+                                       cudaEvent_t, const WaveMaps*);
 
 // One-time kernel attributes (dynamic shared memory above 48 KB for wide
 // theta sets in FP64).
@@ -1138,7 +1158,9 @@ int wave_prepare(const Konst<R>& K) {
     const int smem_tma = (int)wave_tma_smem<R>(K.nt);
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
     if (cudaFuncSetAttribute(k_wave_tma<R, true>, a, smem_tma) != cudaSuccess ||
-        cudaFuncSetAttribute(k_wave_tma<R, false>, a, smem_tma) != cudaSuccess)
+        cudaFuncSetAttribute(k_wave_tma<R, false>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(kb_wave_tma<R, true>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(kb_wave_tma<R, false>, a, smem_tma) != cudaSuccess)
         return 1;
     cudaError_t e[8] = {
         cudaFuncSetAttribute(k_wave_fast<R, true, true>, a, smem), cudaFuncSetAttribute(k_wave_fast<R, true, false>, a, smem),

@@ -136,7 +136,7 @@ struct Clock {
     int SLstep, WNDstep, nsl, nwnd;
     double zsbndi, zsbndn, windu, windv;
     int n_wave_parts;          // number of valid WAVEDT partials (0 = none)
-    int pad;
+    int forced;                // 1: the wave sub-step comes from a forcing (surrogate), the wave kernels skip
 };
 #define XBG_MAX_SERIES 4096
 struct Series {
@@ -265,7 +265,7 @@ struct BatchAux {
     int nflow;          // blocks of the dt reduction
     int nwave;          // WAVEDT partials
     int ubnd_threads;   // logical thread count of the ubnd block
-    int pad;
+    int scen;           // the scenario's index in the batch
 };
 
 template <class R>
@@ -335,6 +335,10 @@ __device__ __forceinline__ void batch_items(const BatchTab<R>& T, const int2* it
 // Early exit of a kernel in a step that the device clock has halted.
 __device__ __forceinline__ bool halted(const Clock* c) {
     return *((volatile const int*)&c->halt) != 0;
+}
+// ... and of the wave solver's kernels while a forcing replaces them.
+__device__ __forceinline__ bool wave_off(const Clock* c) {
+    return halted(c) || *((volatile const int*)&c->forced) != 0;
 }
 
 }  // namespace xbg

@@ -32,6 +32,8 @@ EXPORTS = [
     "xbg_batch_create", "xbg_batch_destroy", "xbg_batch_scenario", "xbg_batch_advance", "xbg_batch_status",
     "xbg_batch_sync", "xbg_batch_get_stream", "xbg_batch_profile_step", "xbg_batch_set_grid",
     "xbg_batch_launch_count", "xbg_set_wave_forcing", "xbg_forcing_steps",
+    "xbg_batch_set_kernel_variant", "xbg_batch_get_kernel_variant",
+    "xbg_batch_set_wave_mode", "xbg_batch_set_forcing", "xbg_batch_forced_segment", "xbg_batch_rel_err",
 ]
 
 
@@ -88,6 +90,12 @@ def load():
     L.xbg_batch_profile_step.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_char_p), C.POINTER(ip)]
     L.xbg_batch_set_grid.argtypes = [vp, ip, ip]
     L.xbg_batch_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
+    L.xbg_batch_set_wave_mode.argtypes = [vp, ip, ip]
+    L.xbg_batch_set_kernel_variant.argtypes = [vp, ip, ip]
+    L.xbg_batch_get_kernel_variant.argtypes = [vp, ip, C.POINTER(ip)]
+    L.xbg_batch_set_forcing.argtypes = [vp, ip, C.POINTER(vp), C.POINTER(vp)]
+    L.xbg_batch_forced_segment.argtypes = [vp, ip]
+    L.xbg_batch_rel_err.argtypes = [vp, ip, C.POINTER(vp), vp]
     _lib = L
     return L
 
@@ -300,6 +308,35 @@ class Batch:
         n = C.c_int64()
         _check(self.L.xbg_batch_launch_count(self.b, C.byref(n)), "xbg_batch_launch_count")
         return n.value
+
+    def set_variant(self, phase, variant):
+        _check(self.L.xbg_batch_set_kernel_variant(self.b, phase, variant), "xbg_batch_set_kernel_variant")
+
+    def variant(self, phase):
+        v = C.c_int()
+        _check(self.L.xbg_batch_get_kernel_variant(self.b, phase, C.byref(v)), "xbg_batch_get_kernel_variant")
+        return v.value
+
+    def set_wave_mode(self, s, mode):
+        """XBG_WAVE_PLAIN / XBG_WAVE_FORCED / XBG_WAVE_FALLBACK for scenario s."""
+        _check(self.L.xbg_batch_set_wave_mode(self.b, s, mode), "xbg_batch_set_wave_mode")
+
+    def set_forcing(self, s, f0, f1):
+        """Scenario s's forcing planes (six device pointers each, E H D DR Fx Fy)."""
+        a = (C.c_void_p * 6)(*[C.c_void_p(int(x)) for x in f0])
+        b = (C.c_void_p * 6)(*[C.c_void_p(int(x)) for x in f1])
+        _check(self.L.xbg_batch_set_forcing(self.b, s, a, b), "xbg_batch_set_forcing")
+
+    def forced_segment(self, k):
+        """k steps; forced scenarios take their wave sub-step from the forcing."""
+        _check(self.L.xbg_batch_forced_segment(self.b, int(k)), "xbg_batch_forced_segment")
+
+    def rel_err(self, field, preds):
+        """Per scenario ||pred - field|| / ||field|| (preds: device pointers or None)."""
+        arr = (C.c_void_p * self.n)(*[C.c_void_p(int(x)) if x else None for x in preds])
+        out = np.zeros(self.n)
+        _check(self.L.xbg_batch_rel_err(self.b, FIELD[field], arr, _ptr(out)), "xbg_batch_rel_err")
+        return out
 
     def profile_step(self):
         cap = 64

@@ -24,6 +24,12 @@ Cases
                  a Gaussian bar with probability 0.5, Hm0 on [0.5, 4] m, Tp on
                  [6, 14] s, mean direction on [-30, 30] deg, D50 on
                  [0.15, 0.4] mm, 1800 s, boundary seed = seed + k.
+  storm          (iter_storm_ensemble) the surrogate-assisted ensemble: n
+                 scenarios drawn as the ensemble's with nx on [256, 1024] and
+                 ny on [128, 512], morfac 10, each under a 6 h storm whose Hm0
+                 ramps linearly 1 -> 5 -> 1 m and Tp 8 -> 14 -> 8 s; model
+                 time 0 is storm time t_start, and the boundary chunk covers
+                 the next rtlength seconds.
 The wave boundary is a seeded wave-group series on the bins: a cos^2s
 directional spreading of the JONSWAP energy Hm0^2 rho g / 16 (as GenCstWave,
 makjonswap.cpp:24-70, spreads it) modulated in time by a sum of random-phase
@@ -203,4 +209,42 @@ def iter_ensemble(n, seed=0, nx_range=(128, 1024), ny_range=(64, 512), step=32, 
             continue
         St, q = wave_group_boundary(p, nrec, Hs, Tp, mdir, seed=seed + 1 + k, dtbc=dtbc)
         bnd = dict(St=St, q=q, t0=0.0, tend=p.rtlength, Trep=Tp / 1.1, Hs=Hs, Tp=Tp)
+        yield p, zb, bnd
+
+
+STORM_S = 6 * 3600.0
+
+
+def storm_hs_tp(tau):
+    """Hm0 and Tp of the 6 h storm at storm time tau [s]: linear 1 -> 5 -> 1 m
+    and 8 -> 14 -> 8 s, peaking at 3 h."""
+    r = 1.0 - abs(2.0 * np.clip(tau, 0.0, STORM_S) / STORM_S - 1.0)
+    return 1.0 + 4.0 * r, 8.0 + 6.0 * r
+
+
+def iter_storm_ensemble(n, seed=0, nx_range=(256, 1024), ny_range=(128, 512), step=32, dx=4.0, ntheta=12,
+                        t_start=7200.0, rtlength=3600.0, dtbc=5.0, boundary=True):
+    """The storm scenarios one at a time: (params, zb, boundary) as
+    iter_ensemble gives them, morfac 10, with the boundary chunk of storm
+    times [t_start, t_start + rtlength): St scaled per record by Hm0(t)^2
+    (the wave energy) and q by Hm0(t) from a unit-height group series, Trep
+    from Tp at the chunk's middle; boundary["storm"] maps model time to
+    (Hm0, Tp)."""
+    base = iter_ensemble(n, seed, nx_range=nx_range, ny_range=ny_range, step=step, dx=dx, ntheta=ntheta,
+                         endtime=rtlength, dtbc=dtbc, boundary=False)
+    rng = np.random.default_rng(seed + 7777)
+    for k, (p, zb, _) in enumerate(base):
+        p.morfac = 10.0
+        mdir = rng.uniform(-30.0, 30.0) * PI / 180
+        if not boundary:
+            yield p, zb, None
+            continue
+        nrec = int(math.ceil(p.rtlength / p.dtbc)) + 1
+        hs_mid, tp_mid = storm_hs_tp(t_start + 0.5 * rtlength)
+        St, q = wave_group_boundary(p, nrec, 1.0, tp_mid, mdir, seed=seed + 1 + k, dtbc=p.dtbc)
+        hs_t = storm_hs_tp(t_start + np.arange(nrec) * p.dtbc)[0]
+        St = St * (hs_t ** 2)[:, None, None]
+        q = q * hs_t[:, None, None]
+        bnd = dict(St=St, q=q, t0=0.0, tend=p.rtlength, Trep=tp_mid / 1.1, Hs=hs_mid, Tp=tp_mid,
+                   storm=lambda t, t0=t_start: storm_hs_tp(t0 + t))
         yield p, zb, bnd

@@ -139,6 +139,8 @@ def _bind_ops(L):
     L.xbg_nn_encode.argtypes = [vp, ip, vp, vp, vp, ll, vp]
     L.xbg_nn_decode.argtypes = [vp, ip, vp, vp, vp, vp, ip, ll, vp]
     L.xbg_nn_copy_planes.argtypes = [vp, vp, ip, ll, vp]
+    L.xbg_nn_encode_batch.argtypes = [vp, ip, vp, vp, vp, vp, vp, ip, ip, ip, vp]
+    L.xbg_nn_decode_batch.argtypes = [vp, ip, vp, vp, vp, vp, vp, vp, ip, ip, ip, ip, vp]
 
 
 def _ok(rc, what):

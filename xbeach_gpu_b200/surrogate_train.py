@@ -71,6 +71,107 @@ def collect(nx=512, ny=256, seeds=(0, 1), Hs_list=(1.5, 2.5), warm=300, every=20
     return dict(x=np.stack(xs), y=np.stack(ys), hold=np.stack(hs))
 
 
+def collect_batch(scen, warm=200, every=20, count=6, k=10, crop=160, crops_per=4, seed=0):
+    """Snapshot pairs from a plain batched run of (params, zb, boundary)
+    scenarios (the storm ensemble: boundary["storm"] gives Hm0, Tp at model
+    time t): at each snapshot, crops_per windows of crop x crop cells per
+    scenario around its shoreline (x from 55 % to 85 % of the cross-shore
+    extent) of the inputs and held wave fields at t, and of the wave fields
+    at t + k in the same windows.  Returns dict(x, y, hold) as collect()."""
+    from .model import Batch
+    b = Batch([p for p, _, _ in scen])
+    for s, (p, zb, bnd) in enumerate(scen):
+        m = b.scenario(s)
+        m.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+        m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        m.init_state(zb, 0.0, 0.0)
+    b.advance(warm)
+    rng = np.random.default_rng(seed)
+    xs, ys, hs = [], [], []
+    for _ in range(count):
+        t = b.status()["t"]
+        wins = []
+        for s, (p, zb, bnd) in enumerate(scen):
+            m = b.scenario(s)
+            hs_, tp_ = bnd["storm"](float(t[s]))
+            fin = np.stack([m.get(f).reshape(p.ny, p.nx) for f in IN_FIELDS] +
+                           [np.full((p.ny, p.nx), hs_, np.float32), np.full((p.ny, p.nx), tp_, np.float32)], -1)
+            hold = np.stack([m.get(f).reshape(p.ny, p.nx) for f in OUT_FIELDS], -1)
+            z = np.zeros((p.ny, p.nx, IN_CH - len(IN_FIELDS) - 2 - OUT_CH), np.float32)
+            x = np.concatenate([fin, hold, z], -1).astype(np.float32)
+            for _c in range(crops_per):
+                lo = max(0, int(0.55 * p.nx) - crop // 2)
+                hi = max(lo, min(p.nx - crop, int(0.85 * p.nx) - crop // 2))
+                x0 = int(rng.integers(lo, hi + 1))
+                y0 = int(rng.integers(0, p.ny - crop + 1))
+                wins.append((s, y0, x0))
+                xs.append(x[y0:y0 + crop, x0:x0 + crop])
+                hs.append(hold[y0:y0 + crop, x0:x0 + crop].astype(np.float32))
+        b.advance(k)
+        cache = {}
+        for s, y0, x0 in wins:
+            p = scen[s][0]
+            if s not in cache:
+                m = b.scenario(s)
+                cache[s] = np.stack([m.get(f).reshape(p.ny, p.nx) for f in OUT_FIELDS], -1)
+            ys.append(cache[s][y0:y0 + crop, x0:x0 + crop].astype(np.float32))
+        b.advance(max(0, every - k))
+    b.close()
+    return dict(x=np.stack(xs), y=np.stack(ys), hold=np.stack(hs))
+
+
+class CropRecorder:
+    """Training pairs from the states a surrogate-assisted batch actually
+    visits (push-forward data): around each judge segment of a
+    BatchSurrogateRun, crops_per windows per scenario of the inputs and held
+    fields before the segment's k plain steps and of the wave fields after
+    them (windows around the shoreline as in collect_batch)."""
+
+    def __init__(self, batch, scen, crop=96, crops_per=2, seed=0):
+        self.b, self.scen, self.crop, self.crops_per = batch, scen, crop, crops_per
+        self.rng = np.random.default_rng(seed)
+        self.xs, self.ys, self.hs = [], [], []
+        self.wins = []
+
+    def before(self, t):
+        crop = self.crop
+        self.wins = []
+        for s, (p, zb, bnd) in enumerate(self.scen):
+            m = self.b.scenario(s)
+            hs_, tp_ = bnd["storm"](t)
+            fin = np.stack([m.get(f).reshape(p.ny, p.nx) for f in IN_FIELDS] +
+                           [np.full((p.ny, p.nx), hs_, np.float32), np.full((p.ny, p.nx), tp_, np.float32)], -1)
+            hold = np.stack([m.get(f).reshape(p.ny, p.nx) for f in OUT_FIELDS], -1)
+            z = np.zeros((p.ny, p.nx, IN_CH - len(IN_FIELDS) - 2 - OUT_CH), np.float32)
+            x = np.concatenate([fin, hold, z], -1).astype(np.float32)
+            for _c in range(self.crops_per):
+                lo = max(0, int(0.55 * p.nx) - crop // 2)
+                hi = max(lo, min(p.nx - crop, int(0.85 * p.nx) - crop // 2))
+                x0 = int(self.rng.integers(lo, hi + 1))
+                y0 = int(self.rng.integers(0, p.ny - crop + 1))
+                self.wins.append((s, y0, x0))
+                self.xs.append(x[y0:y0 + crop, x0:x0 + crop])
+                self.hs.append(hold[y0:y0 + crop, x0:x0 + crop].astype(np.float32))
+
+    def after(self):
+        crop, cache = self.crop, {}
+        for s, y0, x0 in self.wins:
+            p = self.scen[s][0]
+            if s not in cache:
+                m = self.b.scenario(s)
+                cache[s] = np.stack([m.get(f).reshape(p.ny, p.nx) for f in OUT_FIELDS], -1)
+            self.ys.append(cache[s][y0:y0 + crop, x0:x0 + crop].astype(np.float32))
+
+    def data(self):
+        return dict(x=np.stack(self.xs), y=np.stack(self.ys), hold=np.stack(self.hs))
+
+
+def merge(*ds):
+    """One training set from several of the same crop size."""
+    return {k: np.concatenate([d[k] for d in ds]) for k in ("x", "y", "hold")}
+
+
 class Normalizer:
     """Per-channel mean and standard deviation of the inputs and of the
     k-step changes of the wave fields (the targets)."""
