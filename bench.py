@@ -46,9 +46,14 @@ def parse():
     ap.add_argument("--nx", type=int, default=2048)
     ap.add_argument("--ny", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="large", choices=["large", "ensemble", "surrogate"],
+    ap.add_argument("--workload", default="large", choices=["large", "ensemble", "surrogate", "storm"],
                     help="large: the 2048x1024 single domain (the headline line); ensemble: the batched "
-                         "ragged ensemble (256 scenarios, one launch per kernel for all)")
+                         "ragged ensemble (256 scenarios, one launch per kernel for all); storm: the "
+                         "surrogate-assisted storm ensemble (512 scenarios) beside its plain run")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="large: leave out the ensemble and storm-ensemble keys of the line")
+    ap.add_argument("--storm-scenarios", type=int, default=512)
+    ap.add_argument("--storm-steps", type=int, default=100)
     ap.add_argument("--scenarios", type=int, default=256)
     ap.add_argument("--no-autotune", action="store_true", help="ensemble: keep the default persistent grids")
     ap.add_argument("--surrogate-base", type=int, default=32, choices=[16, 32],
@@ -501,6 +506,122 @@ def run_surrogate(args, rank, world, local):
     }
 
 
+def _storm_batch(sc, warm):
+    from xbeach_gpu_b200.model import Batch
+    b = Batch([p for p, _, _ in sc])
+    for s, (p, zb, bnd) in enumerate(sc):
+        m = b.scenario(s)
+        m.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+        m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+        m.init_state(zb, 0.0, 0.0)
+    b.advance(warm)
+    b.sync()
+    return b
+
+
+def run_storm(args, local):
+    """The surrogate-assisted storm ensemble: n scenarios (nx 256..1024, ny
+    128..512, 12 bins, morfac 10, the 6 h storm from storm time 2 h) stepped
+    plain and surrogate-assisted (network trained here on snapshots of other
+    storm scenarios; judge every 50 steps; 2 % bar, and without a bar) from
+    the same state; cell-updates/s of each, final H and zb against the plain
+    run, fallback rate, inference tensor throughput and the Amdahl bound of
+    replacing the wave sub-step (the wave kernels' share of a plain step)."""
+    import torch
+    from xbeach_gpu_b200 import surrogate_train as st
+    from xbeach_gpu_b200.scenarios import iter_storm_ensemble
+    from xbeach_gpu_b200.surrogate import UNet
+    from xbeach_gpu_b200.surrogate_couple import BatchSurrogateRun
+    torch.cuda.set_device(local)
+    t_all = time.perf_counter()
+    train_sc = list(iter_storm_ensemble(16, seed=100, nx_range=(128, 256), ny_range=(96, 160)))
+    data = st.collect_batch(train_sc, warm=150, every=12, count=16, k=10, crop=96, crops_per=4, seed=1)
+    norm = st.Normalizer(data)
+    net = UNet(seed=0, base=32)
+    t0 = time.perf_counter()
+    st.train(net, data, norm, steps=2000, batch=16, crop=96, lr=5e-4, log_every=500)
+    t_train = time.perf_counter() - t0
+    sc = list(iter_storm_ensemble(args.storm_scenarios, seed=7, rtlength=600.0))
+    params = [p for p, _, _ in sc]
+    cells = sum(p.nx * p.ny for p in params)
+    K, warm = args.storm_steps, 200   # the wave field established over the domains before the comparison
+    storm = lambda s, t: sc[s][2]["storm"](t)   # noqa: E731
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"scenarios": len(sc), "cells": cells, "steps": K, "k": 10, "judge_every": 50, "train_s": t_train,
+           "train_crops": int(data["x"].shape[0])}
+    finals = {}
+    for mode in ("plain", "2pct", "nobar"):
+        b = _storm_batch(sc, warm)
+        if mode == "plain":   # (the default persistent grids in all three runs)
+            prof = {}
+            for _ in range(2):
+                for name, t in b.profile_step():
+                    prof.setdefault(name, []).append(t)
+            kern = {k: float(np.mean(v)) for k, v in prof.items()}
+            wave = sum(v for k, v in kern.items() if k in ("k_disp", "k_wave_tma", "k_wave_fast", "k_wave_force",
+                                                               "k_wavebnd"))
+            out["wave_share"] = wave / sum(kern.values())
+            out["amdahl_bound"] = 1.0 / (1.0 - out["wave_share"])
+            b.sync()
+            stream = torch.cuda.ExternalStream(b.stream())
+            e0.record(stream)
+            b.advance(K)
+            e1.record(stream)
+            e1.synchronize()
+        else:
+            b.advance(2)   # the plain run's two profiled steps: all three start from the same step
+            thr = 0.02 if mode == "2pct" else float("inf")
+            run = BatchSurrogateRun(b, params, net, norm, storm, k=10, judge_every=50, threshold=thr, hp=64, wp=128)
+            torch.cuda.synchronize()
+            e0.record()
+            run.advance(K)
+            torch.cuda.synchronize()
+            e1.record()
+            e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        stt = b.status()
+        if (stt["status"] != 0).any():
+            raise RuntimeError(f"storm ensemble ({mode}): a scenario reported an error")
+        finals[mode] = [{f: b.scenario(s).get(f).astype(np.float64) for f in ("H", "zb")} for s in range(len(sc))]
+        out[f"{mode}_value"] = cells * K / (ms / 1e3)
+        if mode != "plain":
+            out[f"{mode}_fallback_rate"] = float(run.fallback.mean())
+            out[f"{mode}_judged_median"] = [[j, float(np.median(e[e >= 0])) if (e >= 0).any() else None]
+                                            for j, e in run.judged]
+        b.close()
+    for mode in ("2pct", "nobar"):
+        out[f"{mode}_speedup_vs_plain"] = out[f"{mode}_value"] / out["plain_value"]
+        for f in ("H", "zb"):
+            errs = [np.linalg.norm(a[f] - r[f]) / max(np.linalg.norm(r[f]), 1e-30)
+                    for a, r in zip(finals[mode], finals["plain"])]
+            out[f"{mode}_final_rel_err_{f}"] = {"median": float(np.median(errs)), "max": float(np.max(errs))}
+    # inference on one 1024 x 512 domain: tensor throughput of the network
+    fwd_px = sum(2.0 * 9 * l.cin * l.cout / {"e1": 1, "d1": 1, "he": 1, "e2": 4, "d2": 4, "e3": 16, "d3": 16,
+                                               "e4": 64}[n[:2]] for n, l in net.L.items())
+    xi = torch.zeros(512 * 1024, 16, dtype=torch.bfloat16, device="cuda")
+    for _ in range(3):
+        net.forward(xi, 1, 512, 1024)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(10):
+        net.forward(xi, 1, 512, 1024)
+    e1.record()
+    e1.synchronize()
+    infer_ms = e0.elapsed_time(e1) / 10
+    tflops = fwd_px * 512 * 1024 / (infer_ms / 1e3) / 1e12
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak_tc, kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        peak_tc, kind = 1590.0, "fallback"
+    out["infer_1024x512"] = {"ms": infer_ms, "achieved_tflops": tflops, "peak_tflops": peak_tc, "peak_kind": kind,
+                             "frac": tflops / peak_tc, "bound": "tensor"}
+    net.check()
+    out["wall_s"] = time.perf_counter() - t_all
+    return out
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -527,6 +648,16 @@ def main():
         out = run_surrogate(args, rank, world, local) if rank == 0 else None
         if out is not None:
             print(json.dumps(out), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    if args.workload == "storm":
+        out = run_storm(args, local) if rank == 0 else None
+        if out is not None:
+            print(json.dumps({"metric": "coupled cell-updates/s", "value": out["2pct_value"],
+                              "unit": "cell-updates/s", "impl": "surrogate-ensemble", "n_gpus": 1,
+                              "higher_is_better": True, "storm": out}), flush=True)
         if dist:
             dist.barrier()
             dist.destroy_process_group()
@@ -604,7 +735,7 @@ def main():
     _, _, _, _, rc = m.time()
     e2e_s = time.perf_counter() - t0
     h2d = recs.numel() * 4 + qrec.numel() * 4
-    d2h = 232   # the device clock struct read by xbg_get_time
+    d2h = 240   # the device clock struct read by xbg_get_time (sizeof(Clock))
     # max over ranks
     if dist:
         (ms, e2e_s), _ = over_ranks(dist, [ms, e2e_s], [C], "cuda")
@@ -647,9 +778,26 @@ def main():
             out["cpu_baseline"] = cpu_baseline_port(p.nx, p.ny)
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"unavailable": str(e)}
+    m.close()
+    if world == 1 and not args.no_extras:
+        # the batched half of the metric, measured in the same run: the plain
+        # ragged ensemble (256 scenarios) and the surrogate-assisted storm
+        # ensemble (512 scenarios) beside its own plain run
+        try:
+            ea = argparse.Namespace(scenarios=256, steps=min(K, 20), warmup=3, no_autotune=False)
+            e = run_ensemble(ea, 0, 1, local)
+            out["ensemble"] = {k: e[k] for k in ("value", "ms_per_step", "steps", "roofline", "roofline_step",
+                                                  "gpu_launches", "clocks", "autotuned_blocks")}
+            out["ensemble"]["workload"] = e["config"]["workload"]
+            out["ensemble"]["cells"] = e["config"]["cells"]
+        except Exception as ex:
+            out["ensemble"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
+        try:
+            out["storm_ensemble"] = run_storm(args, local)
+        except Exception as ex:
+            out["storm_ensemble"] = {"unavailable": f"{type(ex).__name__}: {ex}"}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    m.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()

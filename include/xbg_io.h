@@ -108,6 +108,14 @@ int xbg_read_xbbnd_list(const char* path, double rtlength, double* time,
 int xbg_read_xbbnd_step(const char* path, int step, int ny, int ntheta, int nrec,
                         double* q, double* St, double* Trep);
 
+/* ReadSPECBnd (:534): a SWAN spectrum boundary list, one record per line
+ * (time [s], spectrum file name), plus a closing record rtlength after the
+ * last with the same file.  Names go NUL-terminated into rows of name_len
+ * bytes of `names` (cap rows); a longer name is XBG_ERR_FORMAT.  time =
+ * names = NULL: only *nrec.                                                */
+int xbg_read_spec_list(const char* path, double rtlength, double* time,
+                       char* names, int name_len, int cap, int* nrec);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,12 @@ int xbg_nn_conv3x3(const void* X, const void* Wt, const float* bias, void* Y,
                    int B, int H, int W, int cin, int ldx, int N, int Kp,
                    int ldw, int ldy, int flags, int* err, void* stream);
 
+/* Input movement of xbg_nn_conv3x3 where the shape tiles (128-pixel tiles of
+ * whole rows or of 128-pixel row pieces, channel counts a multiple of 16):
+ * on (1, the default) the tensor memory accelerator copies each tap's input
+ * box into shared memory; off (0) every thread gathers 16-byte pieces.  The
+ * results are identical; the switch exists for comparison.                */
+int xbg_nn_conv_set_tma(int on);
 /* Weight and bias gradient of xbg_nn_conv3x3 as an implicit GEMM over the
  * pixels: gw[n][tap*cin + c] (+)= sum over p of dz[p][n] X[b, y+dy, x+dx, c]
  * and, when gb is not NULL, gb[n] (+)= sum over p of dz[p][n], for n < N

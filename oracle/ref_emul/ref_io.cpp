@@ -22,6 +22,7 @@ std::vector<Wavebndparam> ReadCstBnd(XBGPUParam XParam);
 std::vector<Wavebndparam> ReadJSWPBnd(XBGPUParam XParam);
 XBGPUParam readXbbndhead(XBGPUParam Param);
 std::vector<Wavebndparam> readXbbndfile(XBGPUParam Param);
+std::vector<Wavebndparam> ReadSPECBnd(XBGPUParam XParam);
 void readbathyHead(std::string filename, int& nx, int& ny, double& dx, double& grdalpha);
 extern "C" void readbathy(std::string filename, float*& zb);
 extern "C" void readXBbathy(std::string filename, int nx, int ny, float*& zb);
@@ -96,6 +97,20 @@ void ref_io_xbstep(const char* path, double rtlength, double dtbc, int nx, int n
     float tr = 0.0f;
     readXbbndstep(P, v, step, tr, q, St);
     *Trep = tr;
+}
+
+// ReadSPECBnd's records: times and file names (rows of name_len bytes)
+int ref_io_speclist(const char* path, double rtlength, double* time, char* names, int name_len, int cap) {
+    XBGPUParam P;
+    P.wavebndfile = path;
+    P.rtlength = rtlength;
+    std::vector<Wavebndparam> v = ReadSPECBnd(P);
+    for (int k = 0; k < (int)v.size() && k < cap; k++) {
+        time[k] = v[k].time;
+        std::memset(names + (size_t)k * name_len, 0, name_len);
+        std::strncpy(names + (size_t)k * name_len, v[k].Swanfile.c_str(), name_len - 1);
+    }
+    return (int)v.size();
 }
 
 }  // extern "C"

@@ -32,6 +32,7 @@ def ref():
     L.ref_io_xbhead.argtypes = [C.c_char_p, dp]
     L.ref_io_xblist.argtypes = [C.c_char_p, C.c_double, dp, dp, ip]
     L.ref_io_xbstep.argtypes = [C.c_char_p, C.c_double, C.c_double, ip, ip, ip, ip, dp, dp, dp]
+    L.ref_io_speclist.argtypes = [C.c_char_p, C.c_double, dp, C.c_char_p, ip, ip]
     return L
 
 
@@ -152,6 +153,28 @@ def test_xbeach_reuse_boundary(ref, tmp_path, monkeypatch):
         assert trep == trw.value
 
 
+@pytest.mark.parametrize("sep", ["\t", " ", ","])
+def test_swan_spectrum_list(ref, tmp_path, sep):
+    """ReadSPECBnd's list (time, spectrum file) with each separator, blank
+    lines, and the closing record, as the reference reads it."""
+    rng = np.random.default_rng(len(sep))
+    lines = []
+    for k in range(7):
+        lines.append(f"{k * 1800.0 + rng.uniform(0, 5):.6g}{sep}spec_{k:03d}_{rng.integers(1000)}.sp2")
+        if k == 3:
+            lines.append("")
+    f = tmp_path / "specs.txt"
+    f.write_text("\n".join(lines) + "\n")
+    t, names = inputs.read_spec_list(f, 3600.0)
+    wt = np.empty(16)
+    wn = C.create_string_buffer(16 * 256)
+    n = ref.ref_io_speclist(str(f).encode(), 3600.0, _dp(wt), wn, 256, 16)
+    assert n == len(t) == 8
+    np.testing.assert_array_equal(t, wt[:n])
+    assert names == [wn.raw[k * 256:(k + 1) * 256].split(b"\0", 1)[0].decode() for k in range(n)]
+    assert names[-1] == names[-2] and t[-1] == t[-2] + 3600.0
+
+
 def test_malformed_files(tmp_path):
     from xbeach_gpu_b200.model import XbgError
     f = tmp_path / "bad.txt"
@@ -163,6 +186,9 @@ def test_malformed_files(tmp_path):
         inputs.read_wind(f)
     with pytest.raises(XbgError, match="opened"):
         inputs.read_sealevel(tmp_path / "missing.txt")
+    f.write_text("0.0\n")                          # a spectrum list line without its file
+    with pytest.raises(XbgError, match="format"):
+        inputs.read_spec_list(f, 3600.0)
     f.write_text("3\t2\t1.0\t0\t0\n1 1 2 3\n2 1 2\n")   # short last row
     with pytest.raises(XbgError, match="format"):
         inputs.read_md(f)

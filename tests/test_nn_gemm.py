@@ -207,3 +207,41 @@ def test_wgrad_refuses_bad_layouts():
     gw = torch.zeros(24, 192, device="cuda")
     with pytest.raises(RuntimeError):
         sg.conv3x3_wgrad(x, dz, gw, None, work, 1, 8, 8, 16, 1, err)
+
+
+TMA_CONV = [(2, 32, 128, 32, 32), (1, 64, 256, 16, 32), (4, 16, 64, 64, 64), (1, 8, 32, 96, 32),
+            (2, 16, 16, 384, 128), (1, 16, 256, 48, 16), (2, 16, 8, 192, 64)]
+
+
+@pytest.mark.parametrize("B,H,W,cin,N", TMA_CONV)
+def test_conv3x3_tma_input_equals_gathered_input(B, H, W, cin, N):
+    """Shapes that tile into 128-pixel row boxes take the tensor-memory-
+    accelerator input path; its result equals the thread-gathered path (and
+    so im2col + GEMM) bit for bit, including the zero padding at the image
+    edges, between images of a batch and in the K padding."""
+    import torch
+    from xbeach_gpu_b200 import surrogate as sg
+    L = sg.lib()
+    g = torch.Generator(device="cuda").manual_seed(B * 977 + H * 31 + W * 7 + cin + N)
+    P = B * H * W
+    Kp = (9 * cin + 63) // 64 * 64
+    ldx = cin + 8
+    x = torch.randn(P, ldx, device="cuda", generator=g).bfloat16()
+    w = torch.zeros(N, Kp, device="cuda", dtype=torch.bfloat16)
+    w[:, :9 * cin] = (torch.randn(N, 9 * cin, device="cuda", generator=g) / (3 * cin ** 0.5)).bfloat16()
+    bias = torch.randn(N, device="cuda", generator=g)
+    ys = []
+    for on in (1, 0):
+        assert L.xbg_nn_conv_set_tma(on) == 0
+        y = torch.empty(P, N, device="cuda", dtype=torch.bfloat16)
+        err = sg.conv3x3(x, w, y, B, H, W, cin, bias=bias, relu=True)
+        torch.cuda.synchronize()
+        assert int(err.item()) == 0
+        ys.append(y)
+    L.xbg_nn_conv_set_tma(1)
+    assert torch.equal(ys[0], ys[1])
+    import torch.nn.functional as F
+    wt = w[:, :9 * cin].float().view(N, 9, cin).permute(0, 2, 1).reshape(N, cin, 3, 3)
+    xi = x[:, :cin].float().view(B, H, W, cin).permute(0, 3, 1, 2)
+    ref = torch.relu(F.conv2d(xi, wt, bias, padding=1)).permute(0, 2, 3, 1).reshape(P, N)
+    assert torch.allclose(ys[0].float(), ref, rtol=2e-2, atol=2e-2 * ref.abs().max().item())

@@ -267,3 +267,25 @@ def test_judge_falls_back_to_the_plain_method(trained):
     assert run.fallback and run.judged[0][1] > 0.02 and run.surrogate_steps == 0
     for f in ("H", "zs", "uu", "zb", "ee"):
         assert np.array_equal(b.get(f), a.get(f)), f
+
+
+def test_device_set_matches_host_collection():
+    """The device-resident training set (config 4's stated size runs through
+    it) holds the same snapshot pairs as the host collection of the same
+    runs, bit for bit, and its crops feed the training step."""
+    import torch
+    from xbeach_gpu_b200 import surrogate_train as st
+    from xbeach_gpu_b200.surrogate import UNet
+    kw = dict(nx=256, ny=128, seeds=(0,), Hs_list=(2.0,), warm=40, every=20, count=2, k=10)
+    host = st.collect(**kw)
+    ds = st.DeviceSet(pairs=24, crop=64, **kw)
+    raw = ds.raw.cpu().numpy()
+    S, ny, nx = ds.S, ds.ny, ds.nx
+    assert S == host["x"].shape[0] == 2
+    x = np.moveaxis(raw[:, :16].reshape(S, 16, ny, nx), 1, -1)
+    y = np.moveaxis(raw[:, 16:].reshape(S, 6, ny, nx), 1, -1)
+    assert np.array_equal(x, host["x"]) and np.array_equal(y, host["y"])
+    net = UNet(seed=0, base=16)
+    hist = st.train_set(net, ds, epochs=2, batch=8, lr=1e-3, log_every=1)
+    assert len(hist) >= 6 and all(np.isfinite(v) for _, v in hist)
+    torch.cuda.synchronize()

@@ -20,6 +20,8 @@
 // 32*(w%4).. and half of the columns), adds the bias, applies ReLU and
 // stores.  Every mbarrier wait is bounded: on time-out the kernel records an
 // error code and leaves (the host reads it).
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cstdint>
 
@@ -407,6 +409,262 @@ __global__ void __launch_bounds__(256, 2) k_conv_tc(const __nv_bfloat16* __restr
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
 }
 
+// ------------------------------------------------------------------------
+// The same convolution with the A operand moved by the tensor memory
+// accelerator.  A CTA's 128 output pixels are R whole image rows of Wt
+// pixels (Wt = W when W divides 128, else 128 pixels of one row), so for
+// one tap the 128 input pixels it needs are one box [R][Wt] of the NHWC
+// input shifted by (dy, dx); pixels outside the image arrive as zeros (the
+// padding).  Each 64-wide K chunk is 64/WC boxes of WC channels (a tap's
+// channel run, WC = 32, or 16 for 16-channel inputs), written by the copy
+// engine in the WC*2-byte swizzled K-major layout the MMA reads, on the
+// stage's "full" mbarrier; one elected thread issues them.  The weights
+// (B) keep the cp.async copies.  Taps beyond the ninth (K padding) are
+// zero-filled by the threads.  No multicast; the map covers this GPU's
+// memory only.
+template <int WC>
+__host__ __device__ constexpr uint32_t sw_layout() { return WC == 32 ? 4u : 6u; }   // SWIZZLE_64B / SWIZZLE_32B
+
+template <int WC>
+__device__ __forceinline__ uint64_t swk_desc(unsigned saddr) {   // K-major, rows of WC*2 bytes
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                          // LBO (unused with swizzling)
+    d |= (uint64_t)((8 * WC * 2) >> 4) << 32;        // SBO: 8 rows
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)sw_layout<WC>() << 61;
+    return d;
+}
+
+template <int BN, int WC>
+__global__ void __launch_bounds__(256, 2) k_conv_tma(const __grid_constant__ CUtensorMap xmap,
+                                                     const __nv_bfloat16* __restrict__ Wt,
+                                                     const float* __restrict__ bias, void* Y, int Bn, int H, int W,
+                                                     int cin, int N, int Kp, int ldw, int ldy, int flags, int* err) {
+    constexpr int NSUB = GK / WC;                 // boxes per K chunk
+    constexpr int SUB_BYTES = GM * WC * 2;        // one box: 128 rows of WC channels
+    constexpr int A_BYTES = GM * GK * 2;
+    constexpr int B_BYTES = BN * GK * 2;
+    constexpr int STAGE = A_BYTES + B_BYTES;
+    constexpr int TCOLS = BN <= 32 ? 32 : (BN <= 64 ? 64 : (BN <= 128 ? 128 : 256));
+    extern __shared__ unsigned char smem_raw[];
+    __shared__ __align__(8) unsigned long long mbar[CSTAGES];    // MMAs of a stage done
+    __shared__ __align__(8) unsigned long long full[CSTAGES];    // A boxes of a stage landed
+    __shared__ unsigned tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int M = Bn * H * W;
+    const int m0 = blockIdx.x * GM;
+    const int nk = Kp / GK;
+    const unsigned base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    unsigned char* gbase = smem_raw + (base - smem_u32(smem_raw));
+    // the tile's first pixel
+    const int HW = H * W;
+    const int tb = m0 / HW, rem = m0 - tb * HW;
+    const int ty0 = rem / W, tx0 = rem - ty0 * W;
+    auto load = [&](int kc, int s) {   // all threads: zero boxes, weights; thread 0: the A boxes
+        const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+        int nbox = 0;
+#pragma unroll
+        for (int u = 0; u < NSUB; u++) {
+            const int k0 = kc * GK + u * WC;
+            if (k0 / cin >= 9) {   // K padding: zeros
+                for (int q = tid; q < SUB_BYTES / 16; q += 256)
+                    *(uint4*)(gbase + (sa + u * SUB_BYTES - base) + q * 16) = make_uint4(0, 0, 0, 0);
+            } else {
+                nbox++;
+            }
+        }
+        if (tid == 0) {
+            const unsigned fb = smem_u32(&full[s]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb),
+                         "r"((unsigned)(nbox * SUB_BYTES))
+                         : "memory");
+#pragma unroll
+            for (int u = 0; u < NSUB; u++) {
+                const int k0 = kc * GK + u * WC;
+                const int tap = k0 / cin;
+                if (tap >= 9) continue;
+                const int c0 = k0 - tap * cin;
+                const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+                asm volatile(
+                    "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, "
+                    "%3, %4, %5}], [%6];\n" ::"r"(sa + u * SUB_BYTES),
+                    "l"((unsigned long long)&xmap), "r"(c0), "r"(tx0 + dx), "r"(ty0 + dy), "r"(tb), "r"(fb)
+                    : "memory");
+            }
+        }
+        for (int q = tid; q < BN * 8; q += 256) {
+            const int r = q >> 3, c = q & 7;
+            const unsigned dst = sb + r * 128 + ((c ^ (r & 7)) << 4);
+            if (r < N) cp16(dst, Wt + (size_t)r * ldw + kc * GK + c * 8);
+            else *(uint4*)(gbase + (dst - base)) = make_uint4(0, 0, 0, 0);
+        }
+    };
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_slot)),
+                     "r"(TCOLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+    }
+    if (tid == 0) {
+        for (int s = 0; s < CSTAGES; s++) {
+            mbar_init(smem_u32(&mbar[s]), 1);
+            mbar_init(smem_u32(&full[s]), 1);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const unsigned tmem = tmem_slot;
+    const uint32_t idesc = idesc_bf16(GM, BN);
+    bool ok = true;
+    int issued = 0;   // chunks whose MMAs were committed
+    int loaded = 0;   // chunks whose boxes were issued
+    for (int kc = 0; kc < CSTAGES - 1; kc++) {
+        if (kc < nk) { load(kc, kc); loaded = kc + 1; }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    }
+    for (int kc = 0; kc < nk; kc++) {
+        const int s = kc % CSTAGES;
+        const int kn = kc + CSTAGES - 1;
+        if (kn < nk) {
+            if (kc >= 1) {   // the stage of chunk kc-1 is free once its MMAs are done
+                const bool w = mbar_wait(smem_u32(&mbar[(kc - 1) % CSTAGES]), ((kc - 1) / CSTAGES) & 1);
+                if (!__syncthreads_and(w)) { ok = false; break; }
+            }
+            load(kn, kn % CSTAGES);
+            loaded = kn + 1;
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(CSTAGES - 1) : "memory");   // chunk kc's weights
+        const bool landed = mbar_wait(smem_u32(&full[s]), (kc / CSTAGES) & 1);      // chunk kc's boxes
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if (!__syncthreads_and(landed)) { ok = false; break; }
+        if (tid == 0) {
+            tc_fence_after();
+            const unsigned sa = base + s * STAGE, sb = sa + A_BYTES;
+            const uint64_t db = sw128_desc(sb);
+#pragma unroll
+            for (int j = 0; j < GK / 16; j++) {
+                const int u = (j * 16) / WC;                        // the box of this K step
+                const unsigned off = (unsigned)((j * 16) % WC) * 2;  // bytes into its rows
+                const uint64_t da = swk_desc<WC>(sa + u * SUB_BYTES + off);
+                const unsigned acc = (kc > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+                    "l"(da), "l"(db + (uint64_t)(2 * j)), "r"(idesc), "r"(acc));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&mbar[s]))
+                         : "memory");
+        }
+        issued = kc + 1;
+    }
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    if (ok && nk > 0) ok = mbar_wait(smem_u32(&mbar[(nk - 1) % CSTAGES]), ((nk - 1) / CSTAGES) & 1);
+    ok = __syncthreads_and(ok) != 0;
+    if (!ok) {   // leaving early: committed MMAs and issued box copies finish (bounded) before TMEM / smem go
+        if (issued > 0) mbar_wait(smem_u32(&mbar[(issued - 1) % CSTAGES]), ((issued - 1) / CSTAGES) & 1);
+        if (tid == 0)
+            for (int c = loaded - CSTAGES < issued ? issued : loaded - CSTAGES; c < loaded; c++)
+                mbar_wait(smem_u32(&full[c % CSTAGES]), (c / CSTAGES) & 1);
+        __syncthreads();
+    }
+    tc_fence_after();
+
+    if (ok) {   // epilogue as k_conv_tc
+        const int q = warp & 3, h = warp >> 2;
+        const int row = m0 + q * 32 + lane;
+        const int half = BN / 2;
+        for (int c0 = h * half; c0 < (h + 1) * half; c0 += 8) {
+            unsigned r[8];
+            const unsigned taddr = tmem + ((unsigned)(q * 32) << 16) + (unsigned)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+            if (row < M && c0 < N) {
+                float v[8];
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    v[j] = (nk > 0 ? __uint_as_float(r[j]) : 0.0f) + (bias ? bias[c0 + j] : 0.0f);
+                    if (flags & XBG_NN_RELU) v[j] = fmaxf(v[j], 0.0f);
+                }
+                if (flags & XBG_NN_OUT_BF16) {
+                    __align__(16) __nv_bfloat16 o[8];
+#pragma unroll
+                    for (int j = 0; j < 8; j++) o[j] = __float2bfloat16(v[j]);
+                    *(uint4*)((__nv_bfloat16*)Y + (size_t)row * ldy + c0) = *(const uint4*)o;
+                } else {
+                    float* d = (float*)Y + (size_t)row * ldy + c0;
+                    *(float4*)d = make_float4(v[0], v[1], v[2], v[3]);
+                    *(float4*)(d + 4) = make_float4(v[4], v[5], v[6], v[7]);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicExch(err, XBG_ERR_TIMEOUT);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
+}
+
+// The tensor map of an NHWC bf16 input for k_conv_tma: dims (ldx, W, H, B),
+// box (WC, Wt, R, 1) with the WC*2-byte swizzle; false when the shape does
+// not tile (W neither a multiple nor a divisor of 128, H not a multiple of R,
+// channel counts not multiples of WC, strides not 16-byte multiples).
+template <int WC>
+bool conv_map(const void* X, int B, int H, int W, int cin, int ldx, CUtensorMap* m) {
+    static PFN_cuTensorMapEncodeTiled_v12000 enc = nullptr;
+    if (cin % WC || ldx % 8) return false;
+    const int Wt = W >= GM ? GM : W;
+    if (W >= GM ? (W % GM) : (GM % W)) return false;
+    const int R = GM / Wt;
+    if (H % R) return false;
+    if (!enc) {
+        cudaDriverEntryPointQueryResult q;
+        void* fn = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+    }
+    const cuuint64_t dims[4] = {(cuuint64_t)ldx, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+    const cuuint64_t strides[3] = {(cuuint64_t)ldx * 2, (cuuint64_t)W * ldx * 2, (cuuint64_t)H * W * ldx * 2};
+    const cuuint32_t box[4] = {(cuuint32_t)WC, (cuuint32_t)Wt, (cuuint32_t)R, 1};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(X), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, WC == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_32B,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int BN, int WC>
+int conv_tma_launch(const CUtensorMap& m, const void* Wt, const float* bias, void* Y, int Bn, int H, int W, int cin,
+                    int N, int Kp, int ldw, int ldy, int flags, int* err, cudaStream_t st) {
+    constexpr int STAGE = GM * GK * 2 + BN * GK * 2;
+    const size_t smem = (size_t)CSTAGES * STAGE + 1024;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_conv_tma<BN, WC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return XBG_ERR_CUDA;
+        attr = true;
+    }
+    const long long M = (long long)Bn * H * W;
+    k_conv_tma<BN, WC><<<(unsigned)((M + GM - 1) / GM), 256, smem, st>>>(m, (const __nv_bfloat16*)Wt, bias, Y, Bn,
+                                                                          H, W, cin, N, Kp, ldw, ldy, flags, err);
+    return cudaGetLastError() == cudaSuccess ? XBG_OK : XBG_ERR_CUDA;
+}
+
+// whether xbg_nn_conv3x3 moves its input with box copies (test switch of the
+// thread-gathered path, xbg_nn_conv_set_tma)
+static int g_conv_tma = 1;
+
 template <int BN>
 int conv_launch(const void* X, const void* Wt, const float* bias, void* Y, int Bn, int H, int W, int cin, int ldx,
                 int N, int Kp, int ldw, int ldy, int flags, int* err, cudaStream_t st) {
@@ -419,6 +677,13 @@ int conv_launch(const void* X, const void* Wt, const float* bias, void* Y, int B
         attr = true;
     }
     const long long M = (long long)Bn * H * W;
+    if (g_conv_tma && M % GM == 0) {   // box copies of the input when the shape tiles
+        CUtensorMap m;
+        if (cin % 32 == 0 && conv_map<32>(X, Bn, H, W, cin, ldx, &m))
+            return conv_tma_launch<BN, 32>(m, Wt, bias, Y, Bn, H, W, cin, N, Kp, ldw, ldy, flags, err, st);
+        if (cin % 32 != 0 && conv_map<16>(X, Bn, H, W, cin, ldx, &m))
+            return conv_tma_launch<BN, 16>(m, Wt, bias, Y, Bn, H, W, cin, N, Kp, ldw, ldy, flags, err, st);
+    }
     k_conv_tc<BN><<<(unsigned)((M + GM - 1) / GM), 256, smem, st>>>((const __nv_bfloat16*)X,
                                                                      (const __nv_bfloat16*)Wt, bias, Y, Bn, H, W, cin,
                                                                      ldx, N, Kp, ldw, ldy, flags, err);
@@ -691,6 +956,11 @@ int wgrad_launch(const void* X, const void* Dz, float* gw, float* gb, float* wor
 
 }  // namespace nn
 }  // namespace xbg
+
+extern "C" int xbg_nn_conv_set_tma(int on) {
+    xbg::nn::g_conv_tma = on ? 1 : 0;
+    return XBG_OK;
+}
 
 extern "C" int xbg_nn_conv3x3(const void* X, const void* Wt, const float* bias, void* Y, int B, int H, int W,
                               int cin, int ldx, int N, int Kp, int ldw, int ldy, int flags, int* err, void* stream) {

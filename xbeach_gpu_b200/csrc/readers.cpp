@@ -271,3 +271,40 @@ extern "C" int xbg_read_xbbnd_step(const char* path, int step, int ny, int nthet
     *Trep = (double)(float)tr[step];
     return XBG_OK;
 }
+
+// ReadSPECBnd (read_input.cpp:534-593): a list of (time, SWAN spectrum file)
+// records, tab / space / comma separated, blank lines skipped, and the
+// closing record rtlength after the last (same file).  Names are copied
+// NUL-terminated into rows of name_len bytes; a name that does not fit is a
+// format error.
+extern "C" int xbg_read_spec_list(const char* path, double rtlength, double* time, char* names, int name_len,
+                                  int cap, int* nrec) {
+    if (!path || !nrec) return XBG_ERR_ARG;
+    std::ifstream fs(path);
+    if (fs.fail()) return XBG_ERR_IO;
+    std::vector<double> tm;
+    std::vector<std::string> nm;
+    std::string line;
+    std::vector<std::string> t;
+    while (std::getline(fs, line)) {
+        if (line.empty()) continue;
+        if (!tokens(line, 2, t)) return XBG_ERR_FORMAT;
+        double v;
+        if (!num(t[0], v)) return XBG_ERR_FORMAT;
+        tm.push_back(v);
+        nm.push_back(t[1]);
+    }
+    if (tm.empty()) return XBG_ERR_FORMAT;
+    tm.push_back(tm.back() + rtlength);   // the closing record
+    nm.push_back(nm.back());
+    *nrec = (int)tm.size();
+    if (!time && !names) return XBG_OK;
+    if (cap < *nrec || !time || !names || name_len < 2) return XBG_ERR_ARG;
+    for (int k = 0; k < *nrec; k++) {
+        if ((int)nm[k].size() >= name_len) return XBG_ERR_FORMAT;
+        time[k] = tm[k];
+        std::memset(names + (size_t)k * name_len, 0, name_len);
+        std::memcpy(names + (size_t)k * name_len, nm[k].data(), nm[k].size());
+    }
+    return XBG_OK;
+}

@@ -8,6 +8,7 @@
 // device clock flips `par` reads set par^1 and writes set par, so a captured
 // CUDA graph can replay any number of steps without pointer swaps.
 #pragma once
+#include <cstddef>
 #include <cstdint>
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -118,6 +119,7 @@ struct Clock {
     float wdt;                 // previous dt, a float in the reference (Wave_gpu.cu:78)
     int par;                   // which ee/rr plane set holds the current state
     int halt;                  // 1: the rest of this step is skipped
+    int forced;                // 1: the wave sub-step comes from a forcing (surrogate), the wave kernels skip
     int flags;                 // XBG_FLAG_*
     int status;                // XBG_OK or XBG_ERR_*
     int do_sed;                // sedimentstep runs this step
@@ -136,8 +138,9 @@ struct Clock {
     int SLstep, WNDstep, nsl, nwnd;
     double zsbndi, zsbndn, windu, windv;
     int n_wave_parts;          // number of valid WAVEDT partials (0 = none)
-    int forced;                // 1: the wave sub-step comes from a forcing (surrogate), the wave kernels skip
 };
+static_assert(offsetof(Clock, forced) == offsetof(Clock, halt) + sizeof(int) && offsetof(Clock, halt) % 8 == 0,
+              "halt and forced form one aligned 8-byte word (read together by wave_off)");
 #define XBG_MAX_SERIES 4096
 struct Series {
     double slt[XBG_MAX_SERIES], sla[XBG_MAX_SERIES], slb[XBG_MAX_SERIES];
@@ -336,9 +339,10 @@ __device__ __forceinline__ void batch_items(const BatchTab<R>& T, const int2* it
 __device__ __forceinline__ bool halted(const Clock* c) {
     return *((volatile const int*)&c->halt) != 0;
 }
-// ... and of the wave solver's kernels while a forcing replaces them.
+// ... and of the wave solver's kernels while a forcing replaces them (halt
+// and forced in one load).
 __device__ __forceinline__ bool wave_off(const Clock* c) {
-    return halted(c) || *((volatile const int*)&c->forced) != 0;
+    return *((volatile const unsigned long long*)&c->halt) != 0ull;
 }
 
 }  // namespace xbg

@@ -33,6 +33,7 @@ def _lib():
         L.xbg_read_xbbnd_head.argtypes = [C.c_char_p, dp]
         L.xbg_read_xbbnd_list.argtypes = [C.c_char_p, C.c_double, dp, dp, ip, C.POINTER(ip)]
         L.xbg_read_xbbnd_step.argtypes = [C.c_char_p, ip, ip, ip, ip, dp, dp, dp]
+        L.xbg_read_spec_list.argtypes = [C.c_char_p, C.c_double, dp, C.c_char_p, ip, ip, C.POINTER(ip)]
         _bound = True
     return L
 
@@ -123,3 +124,19 @@ def apply_series(model, sealevel=None, wind=None):
         model.set_sealevel(sealevel[:, 0], sealevel[:, 1], sealevel[:, 2])
     if wind is not None:
         model.set_wind(wind[:, 0], wind[:, 4], wind[:, 5])
+
+
+def read_spec_list(path, rtlength, name_len=1024):
+    """ReadSPECBnd (read_input.cpp:534): the SWAN spectrum boundary list as
+    (times [n], file names [n]) with the closing record rtlength after the
+    last."""
+    L = _lib()
+    n = C.c_int()
+    _check(L.xbg_read_spec_list(str(path).encode(), rtlength, None, None, 0, 0, C.byref(n)), f"read {path}")
+    t = np.empty(n.value)
+    buf = C.create_string_buffer(n.value * name_len)
+    _check(L.xbg_read_spec_list(str(path).encode(), rtlength, _dp(t), buf, name_len, n.value, C.byref(n)),
+           f"read {path}")
+    raw = buf.raw
+    names = [raw[k * name_len:(k + 1) * name_len].split(b"\0", 1)[0].decode() for k in range(n.value)]
+    return t, names

@@ -223,28 +223,31 @@ def storm_hs_tp(tau):
 
 
 def iter_storm_ensemble(n, seed=0, nx_range=(256, 1024), ny_range=(128, 512), step=32, dx=4.0, ntheta=12,
-                        t_start=7200.0, rtlength=3600.0, dtbc=5.0, boundary=True):
+                        t_start=7200.0, rtlength=3600.0, dtbc=5.0, boundary=True, t_start_range=None):
     """The storm scenarios one at a time: (params, zb, boundary) as
     iter_ensemble gives them, morfac 10, with the boundary chunk of storm
     times [t_start, t_start + rtlength): St scaled per record by Hm0(t)^2
     (the wave energy) and q by Hm0(t) from a unit-height group series, Trep
     from Tp at the chunk's middle; boundary["storm"] maps model time to
-    (Hm0, Tp)."""
+    (Hm0, Tp).  t_start_range = (a, b): each scenario starts at its own
+    storm time drawn uniformly from [a, b] (training sets that span the
+    storm)."""
     base = iter_ensemble(n, seed, nx_range=nx_range, ny_range=ny_range, step=step, dx=dx, ntheta=ntheta,
                          endtime=rtlength, dtbc=dtbc, boundary=False)
     rng = np.random.default_rng(seed + 7777)
     for k, (p, zb, _) in enumerate(base):
         p.morfac = 10.0
         mdir = rng.uniform(-30.0, 30.0) * PI / 180
+        ts = t_start if t_start_range is None else float(rng.uniform(*t_start_range))
         if not boundary:
             yield p, zb, None
             continue
         nrec = int(math.ceil(p.rtlength / p.dtbc)) + 1
-        hs_mid, tp_mid = storm_hs_tp(t_start + 0.5 * rtlength)
+        hs_mid, tp_mid = storm_hs_tp(ts + 0.5 * rtlength)
         St, q = wave_group_boundary(p, nrec, 1.0, tp_mid, mdir, seed=seed + 1 + k, dtbc=p.dtbc)
-        hs_t = storm_hs_tp(t_start + np.arange(nrec) * p.dtbc)[0]
+        hs_t = storm_hs_tp(ts + np.arange(nrec) * p.dtbc)[0]
         St = St * (hs_t ** 2)[:, None, None]
         q = q * hs_t[:, None, None]
         bnd = dict(St=St, q=q, t0=0.0, tend=p.rtlength, Trep=tp_mid / 1.1, Hs=hs_mid, Tp=tp_mid,
-                   storm=lambda t, t0=t_start: storm_hs_tp(t0 + t))
+                   storm=lambda t, t0=ts: storm_hs_tp(t0 + t))
         yield p, zb, bnd

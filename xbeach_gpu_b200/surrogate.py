@@ -26,6 +26,7 @@ def lib():
     L.xbg_nn_conv3x3_wgrad.argtypes = [vp, vp, vp, vp, vp, ip, ip, ip, ip, ip, ip, ip, ip, ip, ip, vp, vp]
     L.xbg_nn_conv3x3_wgrad_work.argtypes = [ip, ip, ip]
     L.xbg_nn_conv3x3_wgrad_work.restype = C.c_longlong
+    L.xbg_nn_conv_set_tma.argtypes = [ip]
     _nn = L
     return L
 

@@ -183,6 +183,12 @@ class Normalizer:
         self.ym = d.mean(0)
         self.ys = d.std(0) + 1e-6
 
+    @classmethod
+    def from_stats(cls, xm, xs, ym, ys):
+        n = cls.__new__(cls)
+        n.xm, n.xs, n.ym, n.ys = xm, xs, ym, ys
+        return n
+
     def x(self, a):
         return (a - self.xm) / self.xs
 
@@ -273,6 +279,160 @@ def evaluate(net, norm, data):
     return out, pred
 
 
+class DeviceSet:
+    """The surrogate's training set kept on the GPU at its stated size:
+    snapshot pairs of config-2-style runs (barred beaches at full domain
+    size), copied from the model planes on the device after each snapshot
+    (xbg_nn_copy_planes; nothing crosses to the host), then normalised into
+    one bf16 channel-last input tensor [S, ny, nx, IN_CH] (xbg_nn_encode)
+    and one f32 target tensor [S, ny, nx, 6] of the normalised k-step
+    changes.  The dataset is `pairs` crops of crop x crop cells drawn once
+    from the snapshot pairs (seeded); epochs walk it in shuffled batches,
+    cut on the device (xbg_nn_gather_crops)."""
+
+    def __init__(self, nx=1024, ny=512, seeds=tuple(range(8)), Hs_list=(1.5, 2.5, 3.5), warm=300, every=20,
+                 count=20, k=10, pairs=20000, crop=256, seed=0):
+        import torch
+        from .abi import XBG_FP32
+        from .model import Model
+        from .scenarios import make_case, wave_group_boundary
+        from .surrogate import _bind_ops, _ok, _p, lib
+        L = lib()
+        _bind_ops(L)
+        P = nx * ny
+        runs = [(sd, hs) for sd in seeds for hs in Hs_list]
+        S = len(runs) * count
+        raw = torch.empty(S, IN_CH + OUT_CH, P, dtype=torch.float32, device="cuda")   # inputs, then y at t + k
+        raw[:, len(IN_FIELDS):len(IN_FIELDS) + 2].zero_()
+        raw[:, IN_CH - (IN_CH - len(IN_FIELDS) - 2 - OUT_CH):IN_CH].zero_()
+        j = 0
+        for sd, hs in runs:
+            p, zb, bnd = make_case("barred_beach", seed=sd, nx=nx, ny=ny)
+            St, q = wave_group_boundary(p, bnd["St"].shape[0], hs, bnd["Tp"], 10 * np.pi / 180, seed=sd + 1)
+            m = Model(p, XBG_FP32)
+            m.set_wave_boundary(0, St, q, t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+            m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+            m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+            m.init_state(zb, 0.0, 0.0)
+            m.advance(warm)
+            src_in = [m.device_ptr(f)[0] for f in IN_FIELDS]
+            src_out = [m.device_ptr(f)[0] for f in OUT_FIELDS]
+            for _ in range(count):
+                m.sync()
+                row = raw[j]
+                dst = [row[c].data_ptr() for c in range(len(IN_FIELDS))] + \
+                      [row[len(IN_FIELDS) + 2 + c].data_ptr() for c in range(OUT_CH)]
+                src = torch.tensor(src_in + src_out, dtype=torch.int64, device="cuda")
+                dstt = torch.tensor(dst, dtype=torch.int64, device="cuda")
+                _ok(L.xbg_nn_copy_planes(_p(src), _p(dstt), len(dst), P, None), "copy planes")
+                row[len(IN_FIELDS)].fill_(float(hs))
+                row[len(IN_FIELDS) + 1].fill_(float(bnd["Tp"]))
+                torch.cuda.synchronize()
+                m.advance(k)
+                m.sync()
+                srcy = torch.tensor(src_out, dtype=torch.int64, device="cuda")
+                dsty = torch.tensor([row[IN_CH + c].data_ptr() for c in range(OUT_CH)], dtype=torch.int64,
+                                    device="cuda")
+                _ok(L.xbg_nn_copy_planes(_p(srcy), _p(dsty), OUT_CH, P, None), "copy planes")
+                torch.cuda.synchronize()
+                m.advance(max(0, every - k))
+                j += 1
+            m.close()
+        hold = raw[:, len(IN_FIELDS) + 2:len(IN_FIELDS) + 2 + OUT_CH]
+        dy = raw[:, IN_CH:] - hold
+        xm = raw[:, :IN_CH].mean(dim=(0, 2)).double().cpu().numpy()
+        xs = raw[:, :IN_CH].std(dim=(0, 2)).double().cpu().numpy() + 1e-6
+        ym = dy.mean(dim=(0, 2)).double().cpu().numpy()
+        ys = dy.std(dim=(0, 2)).double().cpu().numpy() + 1e-6
+        self.norm = Normalizer.from_stats(xm, xs, ym, ys)
+        # inputs: normalised bf16, channel-last, by the library's encoder
+        self.X = torch.empty(S, ny, nx, IN_CH, dtype=torch.bfloat16, device="cuda")
+        mean = torch.from_numpy(xm.astype(np.float32)).cuda()
+        istd = torch.from_numpy((1.0 / xs).astype(np.float32)).cuda()
+        for t in range(S):
+            planes = torch.tensor([raw[t, c].data_ptr() for c in range(IN_CH)], dtype=torch.int64, device="cuda")
+            _ok(L.xbg_nn_encode(_p(planes), IN_CH, _p(mean), _p(istd), _p(self.X[t]), P, None), "encode")
+        # targets: normalised changes, channel-last f32 (data loading, on the device)
+        self.Y = ((dy - torch.from_numpy(ym.astype(np.float32)).cuda()[None, :, None]) /
+                  torch.from_numpy(ys.astype(np.float32)).cuda()[None, :, None]).permute(0, 2, 1).contiguous()
+        self.Y = self.Y.view(S, ny, nx, OUT_CH)
+        self.hold_raw = raw[:, len(IN_FIELDS) + 2:len(IN_FIELDS) + 2 + OUT_CH]
+        self.y_raw = raw[:, IN_CH:]
+        self.raw = raw
+        self.S, self.ny, self.nx, self.crop, self.k = S, ny, nx, crop, k
+        rng = np.random.default_rng(seed)
+        self.pairs = np.stack([rng.integers(0, S, pairs), rng.integers(0, ny - crop + 1, pairs),
+                               rng.integers(0, nx - crop + 1, pairs)], 1).astype(np.int32)
+
+    def epoch(self, batch, rng):
+        """Batches (x [B*crop*crop, IN_CH] bf16, y [B*crop*crop, 6] f32) over
+        the dataset's crops in a shuffled order (the last partial batch left
+        out)."""
+        import torch
+        from .surrogate import _ok, _p, lib
+        L = lib()
+        order = rng.permutation(len(self.pairs))
+        c = self.crop
+        xt = torch.empty(batch * c * c, IN_CH, dtype=torch.bfloat16, device="cuda")
+        yt = torch.empty(batch * c * c, OUT_CH, dtype=torch.float32, device="cuda")
+        for b0 in range(0, len(order) - batch + 1, batch):
+            idx = torch.from_numpy(self.pairs[order[b0:b0 + batch]].ravel()).cuda()
+            _ok(L.xbg_nn_gather_crops(_p(self.X), _p(xt), _p(idx), batch, self.ny, self.nx, c, IN_CH * 2, None),
+                "crops x")
+            _ok(L.xbg_nn_gather_crops(_p(self.Y), _p(yt), _p(idx), batch, self.ny, self.nx, c, OUT_CH * 4, None),
+                "crops y")
+            yield xt, yt
+
+
+def train_set(net, ds, epochs=3, batch=64, lr=1e-3, seed=0, log_every=100):
+    """Adam over `epochs` passes of a DeviceSet; returns the loss history."""
+    rng = np.random.default_rng(seed)
+    hist, k = [], 0
+    for _e in range(epochs):
+        for xt, yt in ds.epoch(batch, rng):
+            loss = net.train_step(xt, yt, batch, ds.crop, ds.crop, lr=lr)
+            k += 1
+            if k % log_every == 0:
+                hist.append((k, float(loss.item())))
+    hist.append((k, float(loss.item())))
+    net.check()
+    return hist
+
+
+def evaluate_fp64(net, norm, nx=1024, ny=512, seed=11, Hs=2.2, warm=300, k=10, count=3, every=20):
+    """Full-domain inference on a held-out beach against the plain wave
+    solver of the FP64 build: from each of `count` states of the FP64 run
+    (its inputs rounded to float for the network), the prediction k steps on
+    and the held fields, both against the FP64 plain result; relative L2
+    errors per output field, worst over the states."""
+    from .abi import XBG_FP64
+    from .model import Model
+    from .scenarios import make_case, wave_group_boundary
+    p, zb, bnd = make_case("barred_beach", seed=seed, nx=nx, ny=ny)
+    St, q = wave_group_boundary(p, bnd["St"].shape[0], Hs, bnd["Tp"], 10 * np.pi / 180, seed=seed + 1)
+    m = Model(p, XBG_FP64)
+    m.set_wave_boundary(0, St, q, t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
+    m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
+    m.init_state(zb, 0.0, 0.0)
+    m.advance(warm)
+    out = {f: dict(surrogate=0.0, hold=0.0) for f in OUT_FIELDS}
+    for _ in range(count):
+        h = np.stack([m.get(f).reshape(ny, nx) for f in OUT_FIELDS], -1)
+        z = np.zeros((ny, nx, IN_CH - len(IN_FIELDS) - 2 - OUT_CH))
+        x = np.concatenate([np.stack([m.get(f).reshape(ny, nx) for f in IN_FIELDS] +
+                                     [np.full((ny, nx), Hs), np.full((ny, nx), bnd["Tp"])], -1), h, z], -1)
+        pred = predict(net, norm, x[None].astype(np.float32), h[None].astype(np.float32))[0].astype(np.float64)
+        m.advance(k)
+        y = np.stack([m.get(f).reshape(ny, nx) for f in OUT_FIELDS], -1)
+        for c, f in enumerate(OUT_FIELDS):
+            out[f]["surrogate"] = max(out[f]["surrogate"], rel_err(pred[..., c], y[..., c]))
+            out[f]["hold"] = max(out[f]["hold"], rel_err(h[..., c], y[..., c]))
+        m.advance(max(0, every - k))
+    m.close()
+    return out
+
+
 def conv_flops(net, B, H, W):
     """Useful FLOPs of one forward pass (the 3x3 convolutions, by level)."""
     scale = {"e1": 1, "e2": 2, "e3": 4, "e4": 8, "d3": 4, "d2": 2, "d1": 1, "he": 1}
@@ -325,10 +485,42 @@ def main(argv=None):
     t.add_argument("--warmup", type=int, default=3)
     t.add_argument("--base", type=int, default=32)
     t.add_argument("--explicit", action="store_true", help="im2col / split-K GEMM backward")
+    c = sub.add_parser("config4", help="train at the stated size (20,000 pairs of 256x256 crops, batch 64) "
+                                        "and check inference against the FP64 build")
+    c.add_argument("--pairs", type=int, default=20000)
+    c.add_argument("--batch", type=int, default=64)
+    c.add_argument("--crop", type=int, default=256)
+    c.add_argument("--epochs", type=int, default=3)
+    c.add_argument("--lr", type=float, default=1e-3)
+    c.add_argument("--base", type=int, default=32)
+    c.add_argument("--runs-seeds", type=int, default=8)
+    c.add_argument("--count", type=int, default=20)
     a = ap.parse_args(argv)
-    fw, tr, tf_fw, tf_tr = time_training(a.B, a.H, a.W, a.steps, a.warmup, a.base, not a.explicit)
-    print(f"{'explicit' if a.explicit else 'implicit'} backward, B={a.B} H={a.H} W={a.W} base={a.base}: "
-          f"forward {fw:.3f} ms ({tf_fw:.1f} TFLOP/s), training step {tr:.3f} ms ({tf_tr:.1f} TFLOP/s)")
+    if a.cmd == "time":
+        fw, tr, tf_fw, tf_tr = time_training(a.B, a.H, a.W, a.steps, a.warmup, a.base, not a.explicit)
+        print(f"{'explicit' if a.explicit else 'implicit'} backward, B={a.B} H={a.H} W={a.W} base={a.base}: "
+              f"forward {fw:.3f} ms ({tf_fw:.1f} TFLOP/s), training step {tr:.3f} ms ({tf_tr:.1f} TFLOP/s)")
+        return
+    import json
+    import time
+    import torch
+    from .surrogate import UNet
+    t0 = time.perf_counter()
+    ds = DeviceSet(seeds=tuple(range(a.runs_seeds)), count=a.count, pairs=a.pairs, crop=a.crop)
+    t_collect = time.perf_counter() - t0
+    net = UNet(seed=0, base=a.base)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = train_set(net, ds, epochs=a.epochs, batch=a.batch, lr=a.lr)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    steps = hist[-1][0]
+    flops = 3 * conv_flops(net, a.batch, a.crop, a.crop) * steps
+    ev = evaluate_fp64(net, ds.norm)
+    print(json.dumps({"snapshot_pairs_full_domain": ds.S, "crop_pairs": len(ds.pairs), "crop": a.crop,
+                      "batch": a.batch, "epochs": a.epochs, "steps": steps, "collect_s": t_collect,
+                      "train_s": t_train, "train_tflops": flops / t_train / 1e12, "loss": hist,
+                      "fp64_check_rel_l2": ev}))
 
 
 if __name__ == "__main__":
