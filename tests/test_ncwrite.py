@@ -22,7 +22,8 @@ def test_io_header_symbols_exported():
     syms = sorted(set(re.findall(r"\b(xbg_[a-z0-9_]+)\s*\(", txt)))
     assert set(syms) == {"xbg_nc_create", "xbg_nc_write_record", "xbg_nc_records", "xbg_nc_close",
                          "xbg_fetch_fields", "xbg_read_table", "xbg_read_md_head", "xbg_read_md",
-                         "xbg_read_dep", "xbg_read_xbbnd_head", "xbg_read_xbbnd_list", "xbg_read_xbbnd_step"}
+                         "xbg_read_dep", "xbg_read_xbbnd_head", "xbg_read_xbbnd_list", "xbg_read_xbbnd_step",
+                         "xbg_read_spec_list"}
     assert all(hasattr(L, s) for s in syms)
 
 
