@@ -506,20 +506,6 @@ def run_surrogate(args, rank, world, local):
     }
 
 
-def _storm_batch(sc, warm):
-    from xbeach_gpu_b200.model import Batch
-    b = Batch([p for p, _, _ in sc])
-    for s, (p, zb, bnd) in enumerate(sc):
-        m = b.scenario(s)
-        m.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
-        m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
-        m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
-        m.init_state(zb, 0.0, 0.0)
-    b.advance(warm)
-    b.sync()
-    return b
-
-
 def run_storm(args, local):
     """The surrogate-assisted storm ensemble: n scenarios (nx 256..1024, ny
     128..512, 12 bins, morfac 10, the 6 h storm from storm time 2 h) stepped
@@ -552,7 +538,7 @@ def run_storm(args, local):
            "train_crops": int(data["x"].shape[0])}
     finals = {}
     for mode in ("plain", "2pct", "nobar"):
-        b = _storm_batch(sc, warm)
+        b = st.storm_batch(sc, warm)
         if mode == "plain":   # (the default persistent grids in all three runs)
             prof = {}
             for _ in range(2):

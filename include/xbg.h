@@ -202,13 +202,17 @@ int  xbg_get_stream(xbg_handle* h, void** stream);
  * out = kernels run.                                                      */
 int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
 /* Kernel variants of a phase, for comparison and tuning.  Phase
- * XBG_PHASE_WAVE (the fused wave rows pass): variant 1 moves its plane tiles
- * with the tensor memory accelerator (box copies issued by one thread per
- * block; used when wave-current interaction is off and nx is a multiple of
- * 4, the default where it applies), variant 0 copies them with every thread
- * (cp.async).  Both give the same results bit for bit.  Setting a variant
- * that does not apply is XBG_ERR_ARG; get reports the one in use.         */
+ * XBG_PHASE_WAVE (the fused wave rows pass): variants 1 and 2 move its plane
+ * tiles with the tensor memory accelerator (box copies issued by one thread
+ * per block; available when wave-current interaction is off and nx is a
+ * multiple of 4) with one or two cells per thread, variant 0 copies them
+ * with every thread (cp.async).  Phase XBG_PHASE_FLOW: variant 1 runs
+ * eulerustep and eulervstep as one pass (uu* of the block's tile and its
+ * ring in shared memory), variant 0 as two.  All variants of a phase give
+ * the same results bit for bit.  Setting a variant that does not apply is
+ * XBG_ERR_ARG; get reports the one in use.                                */
 #define XBG_PHASE_WAVE 0
+#define XBG_PHASE_FLOW 1
 int  xbg_set_kernel_variant(xbg_handle* h, int phase, int variant);
 int  xbg_get_kernel_variant(xbg_handle* h, int phase, int* variant);
 /* Device-side water and sediment ledgers (sum zs*dx^2, sum (C*h) dx^2,

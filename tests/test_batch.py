@@ -78,14 +78,14 @@ def test_batch_scenarios_end_on_their_own():
 
 def test_batch_grid_choice_does_not_change_results(tmp_path):
     """The autotuner's knobs (persistent blocks per tile shape, the wave rows
-    variant) only change which block runs which tile and how the tiles are
-    moved: batches with different block counts and either wave variant end
-    bit for bit the same."""
+    variant, the flow pass split) only change which block runs which tile,
+    how the tiles are moved and where the passes cut: batches with different
+    block counts and any of the variants end bit for bit the same."""
     from xbeach_gpu_b200.autotune import tune
     sc = _cases(4, 21)
-    from xbeach_gpu_b200.abi import XBG_PHASE_WAVE
+    from xbeach_gpu_b200.abi import XBG_PHASE_FLOW, XBG_PHASE_WAVE
     runs = []
-    for variant in ("default", "tuned", "thread_tiles"):
+    for variant in ("default", "tuned", "thread_tiles", "two_cells", "split_flow"):
         b = Batch([p for p, _, _ in sc], XBG_FP32)
         for s, (p, zb, bnd) in enumerate(sc):
             _setup(b.scenario(s), p, zb, bnd)
@@ -96,16 +96,23 @@ def test_batch_grid_choice_does_not_change_results(tmp_path):
             assert b.variant(XBG_PHASE_WAVE) == 1
             b.set_variant(XBG_PHASE_WAVE, 0)
             assert b.variant(XBG_PHASE_WAVE) == 0
+        if variant == "two_cells":
+            b.set_variant(XBG_PHASE_WAVE, 2)
+            assert b.variant(XBG_PHASE_WAVE) == 2
+        if variant == "split_flow":
+            b.set_variant(XBG_PHASE_FLOW, 0)
+            assert b.variant(XBG_PHASE_FLOW) == 0
         b.advance(25)
         runs.append({s: {f: b.scenario(s).get(f).copy() for f in ("zs", "uu", "H", "ee")} for s in range(len(sc))})
         if variant == "tuned":
             choice = tune(b, cache=str(tmp_path / "tune.json"), reps=1)
             assert {0, 1, 2, 5} <= set(choice) and all(choice[k] >= 1 for k in (0, 1, 2, 5))
-            assert choice["wave_variant"] in (0, 1) and b.variant(XBG_PHASE_WAVE) == choice["wave_variant"]
+            assert choice["wave_variant"] in (0, 1, 2) and b.variant(XBG_PHASE_WAVE) == choice["wave_variant"]
+            assert choice["flow_variant"] in (0, 1) and b.variant(XBG_PHASE_FLOW) == choice["flow_variant"]
             again = tune(b, cache=str(tmp_path / "tune.json"), reps=1)   # from the cache
             assert again == choice
         b.close()
     for s in runs[0]:
         for f in runs[0][s]:
-            assert np.array_equal(runs[0][s][f], runs[1][s][f]), (s, f)
-            assert np.array_equal(runs[0][s][f], runs[2][s][f]), (s, f)
+            for r in runs[1:]:
+                assert np.array_equal(runs[0][s][f], r[s][f]), (s, f)

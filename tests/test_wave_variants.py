@@ -1,14 +1,16 @@
-"""The wave rows pass has two implementations of the same arithmetic: plane
-tiles moved by the tensor memory accelerator (one box copy per bin, issued by
-one thread; the default where it applies) and plane tiles copied by every
-thread (cp.async).  They must give the same state bit for bit over whole
-coupled steps, on grids whose tiles are partial in x and in y, at the
+"""Kernel variants of the same arithmetic.  The wave rows pass has three:
+plane tiles moved by the tensor memory accelerator (one box copy per bin,
+issued by one thread; the default where it applies) with one or with two
+cells per thread, and plane tiles copied by every thread (cp.async).  The
+flow step's momentum updates run as one pass (uu* of the tile and its ring
+in shared memory) or as two.  Each must give the same state bit for bit over
+whole coupled steps, on grids whose tiles are partial in x and in y, at the
 offshore and lateral edges, for few bins (fewer than the four tile buffers),
 with and without the roller, in FP32 and FP64."""
 import numpy as np
 import pytest
 
-from xbeach_gpu_b200.abi import XBG_FP32, XBG_FP64, XBG_PHASE_WAVE
+from xbeach_gpu_b200.abi import XBG_FP32, XBG_FP64, XBG_PHASE_FLOW, XBG_PHASE_WAVE
 from xbeach_gpu_b200.model import Model, XbgError
 from xbeach_gpu_b200.scenarios import make_case
 
@@ -28,7 +30,7 @@ CASES = {
 }
 
 
-def _model(c, precision, variant):
+def _model(c, precision, variant, phase=XBG_PHASE_WAVE):
     p, zb, bnd = make_case(c["case"], nx=c["nx"], ny=c["ny"], ntheta=c["nt"])
     for k, v in c["kw"].items():
         setattr(p, k, v)
@@ -37,7 +39,7 @@ def _model(c, precision, variant):
     m.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
     m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
     m.init_state(zb, 0.0, 0.0)
-    m.set_variant(XBG_PHASE_WAVE, variant)
+    m.set_variant(phase, variant)
     return m
 
 
@@ -46,9 +48,35 @@ def _model(c, precision, variant):
 def test_tma_tiles_equal_thread_copied_tiles(name, precision):
     c = CASES[name]
     runs = []
-    for variant in (0, 1):
+    for variant in (0, 1, 2):
         m = _model(c, precision, variant)
         assert m.variant(XBG_PHASE_WAVE) == variant
+        m.advance(25)
+        m.advance(15)
+        t, dt, n, _, rc = m.time()
+        assert rc == 0 and n == 40
+        runs.append((t, dt, {f: m.get(f).copy() for f in FIELDS}))
+        m.close()
+    for r in runs[1:]:
+        assert runs[0][:2] == r[:2]
+        for f in FIELDS:
+            assert np.array_equal(runs[0][2][f], r[2][f]), f
+
+
+# grids whose ny - 2 is a multiple of the tile height put row ny - 3 (the
+# vvlatbnd source of row ny - 2) outside the fused pass's shared rows
+FLOW_CASES = dict(CASES, linear_70x42_n4=dict(case="linear_beach", nx=70, ny=42, nt=4, kw={}),
+                  barred_96x34_n18=dict(case="barred_beach", nx=96, ny=34, nt=None, kw={}))
+
+
+@pytest.mark.parametrize("precision", [XBG_FP32, XBG_FP64])
+@pytest.mark.parametrize("name", sorted(FLOW_CASES))
+def test_fused_momentum_pass_equals_two_passes(name, precision):
+    c = FLOW_CASES[name]
+    runs = []
+    for variant in (0, 1):
+        m = _model(c, precision, variant, XBG_PHASE_FLOW)
+        assert m.variant(XBG_PHASE_FLOW) == variant
         m.advance(25)
         m.advance(15)
         t, dt, n, _, rc = m.time()
@@ -70,8 +98,9 @@ def test_tma_variant_applies_only_where_it_can():
             setattr(p, k, v)
         m = Model(p)
         assert m.variant(XBG_PHASE_WAVE) == 0
-        with pytest.raises(XbgError):
-            m.set_variant(XBG_PHASE_WAVE, 1)
+        for v in (1, 2):
+            with pytest.raises(XbgError):
+                m.set_variant(XBG_PHASE_WAVE, v)
         m.close()
     p, zb, bnd = make_case("linear_beach", nx=64, ny=32, ntheta=6)
     m = Model(p)

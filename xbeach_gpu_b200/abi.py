@@ -26,6 +26,7 @@ XBG_FP32 = 0
 XBG_FP64 = 1
 
 XBG_PHASE_WAVE = 0   # xbg_set_kernel_variant phases
+XBG_PHASE_FLOW = 1
 
 XBG_FLAG_OUTPUT_DUE = 1
 XBG_FLAG_ENDED = 2

@@ -15,12 +15,22 @@
 #include "../../include/xbg.h"
 #include "../../include/xbg_io.h"
 
+// the wave rows variant a new handle or batch starts with (1: TMA tiles, one
+// cell per thread; 2: TMA tiles, two cells per thread)
+#ifndef XBG_WAVE_VARIANT_DEFAULT
+#define XBG_WAVE_VARIANT_DEFAULT 1
+#endif
+// the flow variant they start with (0: momentum steps in two passes, 1: one)
+#ifndef XBG_FLOW_VARIANT_DEFAULT
+#define XBG_FLOW_VARIANT_DEFAULT 1
+#endif
+
 namespace xbg {
-template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t, const WaveMaps*);
+template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t, const WaveMaps*, int);
 template <class R> int wave_maps_make(const Dev<R>&, const Konst<R>&, WaveMaps*);
 template <class R> int wave_parts(const Konst<R>&);
 template <class R> int wave_prepare(const Konst<R>&);
-template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool);
 template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
 template <class R> int step_begin_blocks(const Konst<R>&);
 template <class R> int launch_step_begin(const Dev<R>&, const Konst<R>&, const Series*, int, cudaStream_t, Prof*);
@@ -32,8 +42,8 @@ template <class R> int launch_wavebnd_batch(const BatchTab<R>&, const BatchLaunc
 template <class R> int launch_ubnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_means_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                         cudaEvent_t, const WaveMaps*);
-template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+                                         cudaEvent_t, const WaveMaps*, int);
+template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
 template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int ubnd_threads(const Konst<R>&);
 template <class R> void launch_output_done(const Dev<R>&, const Konst<R>&, cudaStream_t);
@@ -299,12 +309,16 @@ struct Handle : public xbg_handle {
     int nwave = 0;
     cudaError_t last_err = cudaSuccess;
     double* mass_buf = nullptr;
-    // wave rows pass: TMA tiles (variant 1, when its maps could be made and
-    // wave-current interaction is off) or thread-copied tiles (variant 0)
+    // wave rows pass: TMA tiles with one cell per thread (variant 1) or two
+    // (variant 2), when its maps could be made and wave-current interaction
+    // is off, or thread-copied tiles (variant 0)
     WaveMaps maps;
     bool maps_ok = false;
-    int wave_variant = 1;
-    const WaveMaps* wave_maps() const { return (maps_ok && wave_variant == 1) ? &maps : nullptr; }
+    int wave_variant = XBG_WAVE_VARIANT_DEFAULT;
+    const WaveMaps* wave_maps() const { return (maps_ok && wave_variant >= 1) ? &maps : nullptr; }
+    int wave_cpt() const { return wave_variant == 2 ? 2 : 1; }
+    // flow: momentum steps in one pass (variant 1) or two (variant 0)
+    int flow_variant = XBG_FLOW_VARIANT_DEFAULT;
 
     template <class T> int alloc(T** p, size_t n) {
         void* q = nullptr;
@@ -662,13 +676,13 @@ struct Handle : public xbg_handle {
             n += launch_wavebnd(S, K, ser, side, nullptr, 0);
             if (K.flow == 1) n += launch_ubnd(S, K, ser, side, nullptr);
             cudaEventRecord(ev_join, side);
-            n += launch_wave(S, K, st, nullptr, ev_join, wave_maps());
+            n += launch_wave(S, K, st, nullptr, ev_join, wave_maps(), wave_cpt());
         } else {
             if (K.swave == 1) n += launch_wavebnd(S, K, ser, st, pf, 0);
             if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
-            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps());
+            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps(), wave_cpt());
         }
-        if (K.flow == 1) n += launch_flow(S, K, st, pf);
+        if (K.flow == 1) n += launch_flow(S, K, st, pf, flow_variant == 1);
         if (P.sedtrans == 1) n += launch_sed(S, K, st, pf);
         if (K.means) n += launch_means(S, K, st, pf);
         return n;
@@ -713,8 +727,8 @@ struct Handle : public xbg_handle {
             case 0: n = launch_step_begin(S, K, ser, nwave, st, nullptr); break;
             case 1: if (K.swave == 1) n = launch_wavebnd(S, K, ser, st, nullptr, 1); break;
             case 2: if (K.flow == 1) n = launch_ubnd(S, K, ser, st, nullptr); break;
-            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps()); break;
-            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr); break;
+            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps(), wave_cpt()); break;
+            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr, flow_variant == 1); break;
             case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr); break;
             case 6: n = launch_means(S, K, st, nullptr); break;
             default: return XBG_ERR_ARG;
@@ -787,18 +801,28 @@ struct Handle : public xbg_handle {
         return XBG_OK;
     }
     int set_variant(int phase, int variant) override {
-        if (phase != XBG_PHASE_WAVE || variant < 0 || variant > 1) return XBG_ERR_ARG;
-        if (variant == 1 && !maps_ok) return XBG_ERR_ARG;
-        if (variant != wave_variant) {
+        int* slot = nullptr;
+        if (phase == XBG_PHASE_WAVE) {
+            if (variant < 0 || variant > 2 || (variant >= 1 && !maps_ok)) return XBG_ERR_ARG;
+            slot = &wave_variant;
+        } else if (phase == XBG_PHASE_FLOW) {
+            if (variant < 0 || variant > 1) return XBG_ERR_ARG;
+            slot = &flow_variant;
+        } else {
+            return XBG_ERR_ARG;
+        }
+        if (variant != *slot) {
             CK(cudaStreamSynchronize(st));
-            wave_variant = variant;
+            *slot = variant;
             drop_graph();
         }
         return XBG_OK;
     }
     int get_variant(int phase, int* variant) override {
-        if (phase != XBG_PHASE_WAVE || !variant) return XBG_ERR_ARG;
-        *variant = wave_maps() ? 1 : 0;
+        if (!variant) return XBG_ERR_ARG;
+        if (phase == XBG_PHASE_WAVE) *variant = wave_maps() ? wave_variant : 0;
+        else if (phase == XBG_PHASE_FLOW) *variant = flow_variant;
+        else return XBG_ERR_ARG;
         return XBG_OK;
     }
     int put_wave_records(int slot, int first, int n, const void* St, const void* q) override {
@@ -830,7 +854,7 @@ struct Handle : public xbg_handle {
                 k_set_forcing<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, ee_buf[0], ee_buf[1], rr_buf[0], rr_buf[1],
                                                                     a, b, (R)((double)j / k), j == k ? 1 : 0);
                 n++;
-                if (K.flow == 1) n += launch_flow(S, K, st, nullptr);
+                if (K.flow == 1) n += launch_flow(S, K, st, nullptr, flow_variant == 1);
                 if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr);
                 n += launch_means(S, K, st, nullptr);
             }
@@ -873,8 +897,10 @@ struct Batch : public xbg_batch {
     cudaError_t last_err = cudaSuccess;
     int nt = 0, swave = 0, flow = 0, sedtrans = 0, roller = 0, means = 0, wci = 0;   // wci: any scenario with wave-current interaction
     WaveMaps* dmaps = nullptr;            // the scenarios' tensor maps (TMA rows pass), if every scenario has them
-    int wave_variant = 1;                 // 1: TMA rows pass (when dmaps), 0: thread-copied tiles
-    const WaveMaps* wave_maps() const { return wave_variant == 1 ? dmaps : nullptr; }
+    int wave_variant = XBG_WAVE_VARIANT_DEFAULT;   // 1, 2: TMA rows pass (when dmaps), 0: thread-copied tiles
+    const WaveMaps* wave_maps() const { return wave_variant >= 1 ? dmaps : nullptr; }
+    int wave_cpt() const { return wave_variant == 2 ? 2 : 1; }
+    int flow_variant = XBG_FLOW_VARIANT_DEFAULT;   // 1: momentum steps in one pass, 0: two
     // surrogate-assisted stepping: forcing planes per scenario, graphs of
     // forced segments by length, judge accumulators
     std::vector<ForcingPair<R>> hfp;
@@ -999,18 +1025,18 @@ struct Batch : public xbg_batch {
             k += launch_wavebnd_batch(T, L, side, nullptr);
             if (flow == 1) k += launch_ubnd_batch(T, L, side, nullptr);
             cudaEventRecord(ev_join, side);
-            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join, wave_maps());
+            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join, wave_maps(), wave_cpt());
         } else {
             if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
             if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
-            if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr, wave_maps());
+            if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr, wave_maps(), wave_cpt());
         }
         return k;
     }
     // flow, sediment and means of one batched step
     int enqueue_rest(const BatchTab<R>& T, Prof* pf) {
         int k = 0;
-        if (flow == 1) k += launch_flow_batch(T, L, st, pf);
+        if (flow == 1) k += launch_flow_batch(T, L, st, pf, flow_variant == 1);
         if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf);
         if (means) k += launch_means_batch(T, L, st, pf);
         return k;
@@ -1083,10 +1109,19 @@ struct Batch : public xbg_batch {
     }
 
     int set_variant(int phase, int variant) override {
-        if (phase != XBG_PHASE_WAVE || variant < 0 || variant > 1 || (variant == 1 && !dmaps)) return XBG_ERR_ARG;
-        if (variant != wave_variant) {
+        int* slot = nullptr;
+        if (phase == XBG_PHASE_WAVE) {
+            if (variant < 0 || variant > 2 || (variant >= 1 && !dmaps)) return XBG_ERR_ARG;
+            slot = &wave_variant;
+        } else if (phase == XBG_PHASE_FLOW) {
+            if (variant < 0 || variant > 1) return XBG_ERR_ARG;
+            slot = &flow_variant;
+        } else {
+            return XBG_ERR_ARG;
+        }
+        if (variant != *slot) {
             CK(cudaStreamSynchronize(st));
-            wave_variant = variant;
+            *slot = variant;
             if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
             if (graph) { cudaGraphDestroy(graph); graph = nullptr; }
             drop_segments();
@@ -1094,8 +1129,10 @@ struct Batch : public xbg_batch {
         return XBG_OK;
     }
     int get_variant(int phase, int* variant) override {
-        if (phase != XBG_PHASE_WAVE || !variant) return XBG_ERR_ARG;
-        *variant = wave_maps() ? 1 : 0;
+        if (!variant) return XBG_ERR_ARG;
+        if (phase == XBG_PHASE_WAVE) *variant = wave_maps() ? wave_variant : 0;
+        else if (phase == XBG_PHASE_FLOW) *variant = flow_variant;
+        else return XBG_ERR_ARG;
         return XBG_OK;
     }
     int set_wave_mode(int s, int mode) override {

@@ -1,5 +1,6 @@
 // flow.cu -- shallow-water step on the staggered grid (flowstep,
-// Wave_gpu.cu:1106-1403; kernels of Flow_kernel.cu) in five fused passes.
+// Wave_gpu.cu:1106-1403; kernels of Flow_kernel.cu) in four fused passes
+// (k_flow_uv) or five (k_flow_u and k_flow_v apart).
 // Each pass cuts where the reference reads a field that an earlier launch of
 // the same step rewrote at a neighbouring cell; inside a pass, neighbour
 // values of per-cell intermediates are recomputed instead of stored.
@@ -9,6 +10,8 @@
 //                latbnd(uu)                           -> uu*
 //   k_flow_v     wlevslopes(y), vdvdy_adv, udvdx_adv, viscov1+2, eulervstep,
 //                vvlatbnd                             -> vv*
+//   k_flow_uv    k_flow_u and k_flow_v in one pass (uu* of the tile and its
+//                ring in shared memory)               -> uu* vv*
 //   k_flow_corr  wrkuu2Ocorr+uu2Ocorr, wrkvv2Ocorr+vv2Ocorr, then depthhu,
 //                depthhv, CalcQFlow, continuity      -> uu vv hu hv qx qy zs* dzsdt
 //   k_flow_final wrkzs2Ocorr+zs2Ocorr, latbnd(zs), hsbnd, calcuvvu, uvlatbnd
@@ -32,6 +35,10 @@ __device__ __forceinline__ R minmod(R d1, R d2) {   // Flow_kernel.cu:23-41
 }
 
 #define IDX(x, y) ((x) + (y) * nx)
+
+// the block tile of the staged passes (32 x 8 cells) and its one-cell ring
+constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT_TX * FT_TY;
+constexpr int FC_H = 3;   // tile halo of the momentum-correction pass
 
 // smago (Flow_kernel.cu:1282-1316) at cell (ix, iy)
 template <class R>
@@ -138,6 +145,17 @@ __device__ R euler_u(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
                         (R)1.25f * K.Cd * (R)sw * wu * wu / (rho * humi) - K.fc * ld(S.f[VU] + i));
 }
 
+// uu* (eulerustep, then latbnd(uu): rows 0 / ny-1 take the updated rows
+// 1 / ny-2) at cell (ix, iy)
+template <class R>
+__device__ __forceinline__ R ustar_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R wu) {
+    const int nx = K.nx, ny = K.ny;
+    int sy = iy;
+    if (iy == 0) sy = 1;
+    if (iy == ny - 1) sy = ny - 2;
+    return (ix > 0) ? euler_u(S, K, ix, sy, dtf, wu) : ld(S.f[UU] + IDX(ix, sy));
+}
+
 template <class R>
 __device__ __forceinline__ void b_flow_u(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
@@ -145,13 +163,7 @@ __device__ __forceinline__ void b_flow_u(const Dev<R>& S, const Konst<R>& K, con
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
-    R dtf = (R)clk->dt, wu = (R)clk->windu;
-    // latbnd(uu): rows 0 / ny-1 take the updated rows 1 / ny-2
-    int sy = iy;
-    if (iy == 0) sy = 1;
-    if (iy == ny - 1) sy = ny - 2;
-    R v = (ix > 0) ? euler_u(S, K, ix, sy, dtf, wu) : ld(S.f[UU] + IDX(ix, sy));
-    S.tmp[T_UU][IDX(ix, iy)] = v;
+    S.tmp[T_UU][IDX(ix, iy)] = ustar_cell(S, K, ix, iy, (R)clk->dt, (R)clk->windu);
 }
 XBG_KERNELS(flow_u)
 
@@ -182,11 +194,12 @@ __device__ __forceinline__ R vdvdy_cell(const Dev<R>& S, const Konst<R>& K, int 
 }
 
 // eulervstep (Flow_kernel.cu:1546-1599) at ix > 0, iy < ny-2, with udvdx_adv
-// (:1159, on the updated uu*), vdvdy_adv and viscov1 + viscov2.
-template <class R>
-__device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R wv) {
+// (:1159, on the updated uu*), vdvdy_adv and viscov1 + viscov2.  us(x, y)
+// gives uu* at cell (x, y).
+template <class R, class US>
+__device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R wv, const US& us) {
     const int nx = K.nx, ny = K.ny;
-    const R* uu = S.tmp[T_UU]; const R* vv = S.f[VV]; const R* hu = S.f[HU];
+    const R* vv = S.f[VV]; const R* hu = S.f[HU];
     const R* hum = S.f[HUM]; const R* hvm = S.f[HVM]; const R* nuhg = S.tmp[T_NUH];
     const R* hh = S.f[HH];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
@@ -197,7 +210,7 @@ __device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
     R dzsdy = (ld(S.f[ZS] + IDX(ix, yp)) - ld(S.f[ZS] + i)) * rdx;
     R vdvdy = vdvdy_cell(S, K, ix, iy);
     // udvdx_adv
-    R ul = ld(uu + IDX(xm, iy)), ultl = ld(uu + IDX(xm, yp)), ui = ld(uu + i), ur = ld(uu + IDX(xp, iy));
+    R ul = us(xm, iy), ultl = us(xm, yp), ui = us(ix, iy), ur = us(xp, iy);
     R vl = ld(vv + IDX(xm, iy)), vr = ld(vv + IDX(xp, iy));
     R udvdx = (R)0.0f;
     R qin = (R)(0.5 * (double)(ul * ld(hu + IDX(xm, iy)) + ultl * ld(hu + IDX(xm, yp))));
@@ -206,7 +219,7 @@ __device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
         if (du > (R)0.5f) udvdx = udvdx + (R)0.5f * (ul + ultl) * (vvi - vl) * rdx;
         else udvdx = udvdx + qin / hvmi * (vvi - vl) * rdx;
     }
-    qin = (R)(-0.5 * (double)(ui * ld(hu + i) + ld(uu + IDX(ix, yp)) * ld(hu + IDX(ix, yp))));
+    qin = (R)(-0.5 * (double)(ui * ld(hu + i) + us(ix, yp) * ld(hu + IDX(ix, yp))));
     du = ur - ui;
     if (qin > (R)0.0f) {
         if (du > (R)0.5f) udvdx = udvdx - (R)0.5f * (ui + ur) * (vvi - vr) * rdx;
@@ -244,12 +257,57 @@ __device__ __forceinline__ void b_flow_v(const Dev<R>& S, const Konst<R>& K, con
     int sy = iy;
     if (iy == 0) sy = 1;
     if (iy == ny - 2) sy = ny - 3;
+    const R* us = S.tmp[T_UU];
     R v;
-    if (sy < ny - 2 && ix > 0) v = euler_v(S, K, ix, sy, dtf, wv);
+    if (sy < ny - 2 && ix > 0) v = euler_v(S, K, ix, sy, dtf, wv, [&](int x, int y) { return ld(us + IDX(x, y)); });
     else v = ld(S.f[VV] + IDX(ix, sy));
     S.tmp[T_VV][IDX(ix, iy)] = v;
 }
 XBG_KERNELS(flow_v)
+
+// flow_u and flow_v in one pass.  eulervstep reads uu* at the cell, its left,
+// right and upper neighbours and the upper-left one, so the block first
+// evaluates uu* over its 32 x 8 tile plus the column on each side and the row
+// above (clamped like mm/pp) into shared memory, stores the tile's own
+// values, and then evaluates vv* from there.  The one row outside that range
+// (row ny-3 for the vvlatbnd copy into row ny-2, when ny-2 is the tile's
+// first row) evaluates its uu* directly.  Results are bit-identical to the
+// two passes.
+constexpr int UV_TX = FT_X + 2, UV_TY = FT_Y + 1;
+
+template <class R>
+__device__ __forceinline__ void b_flow_uv(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
+    const Clock* clk = S.clk;
+    if (halted(clk)) return;
+    __shared__ R sU[UV_TY * UV_TX];
+    const int nx = K.nx, ny = K.ny;
+    const int bx0 = bix * FT_X, by0 = biy * FT_Y;
+    const R dtf = (R)clk->dt, wu = (R)clk->windu, wv = (R)clk->windv;
+    for (int e = threadIdx.x + threadIdx.y * FT_X; e < UV_TX * UV_TY; e += FT_X * FT_Y) {
+        const int gx = min(max(bx0 - 1 + e % UV_TX, 0), nx - 1), gy = min(by0 + e / UV_TX, ny - 1);
+        sU[e] = ustar_cell(S, K, gx, gy, dtf, wu);
+    }
+    __syncthreads();
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    S.tmp[T_UU][IDX(ix, iy)] = sU[threadIdx.y * UV_TX + threadIdx.x + 1];
+    // vvlatbnd: row 0 <- row 1, row ny-2 <- row ny-3; row ny-1 keeps its value
+    int sy = iy;
+    if (iy == 0) sy = 1;
+    if (iy == ny - 2) sy = ny - 3;
+    R v;
+    if (sy < ny - 2 && ix > 0) {
+        // the accessed cells are clamped grid cells: x in [bx0-1, bx0+32], y in [sy, sy+1]
+        v = euler_v(S, K, ix, sy, dtf, wv, [&](int x, int y) {
+            const int ex = x - bx0 + 1, ey = y - by0;
+            return (ey >= 0 && ey < UV_TY) ? sU[ey * UV_TX + ex] : ustar_cell(S, K, x, y, dtf, wu);
+        });
+    } else {
+        v = ld(S.f[VV] + IDX(ix, sy));
+    }
+    S.tmp[T_VV][IDX(ix, iy)] = v;
+}
+XBG_KERNELS(flow_uv)
 
 // depthhu / depthhv (Flow_kernel.cu:653-750) at a u (v) point from the levels
 // and beds of the cell and its right (upper) neighbour and the velocity there
@@ -326,9 +384,8 @@ __device__ __forceinline__ void wrk_v(const A& a, const Konst<R>& K, int ix, int
 // wrk values of the tile cells and a one-cell ring (the left, right, lower and
 // upper neighbours the corrections read) are computed once from there.
 // Continuity needs the corrected velocities of the left and lower
-// neighbours, which each thread recomputes from the ring.
-constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT_TX * FT_TY;
-constexpr int FC_H = 3;
+// neighbours: the block evaluates them once, for its cells and for the
+// column to its left (u) and the row below it (v), in shared memory.
 
 template <class R>
 __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
@@ -353,9 +410,9 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
         sU1[e] = w1; sU2[e] = w2; sV1[e] = v1; sV2[e] = v2;
     }
     __syncthreads();
-    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    if (ix >= nx || iy >= ny) return;
-    int i = IDX(ix, iy);
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool inside = ix < nx && iy < ny;
+    const int i = IDX(ix, iy);
     R dtf = (R)clk->dt, rdx = K.rdx;
     const int kc = (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H;
     const int c = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
@@ -388,13 +445,34 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
         }
         return v;
     };
-    const R u = ucorr(kc, c, ix, iy, i);
-    const R v = vcorr(kc, c, ix, iy, i);
+    // corrected velocities once per cell: the tile's (u and v), the column to
+    // its left (u) and the row below it (v) into shared memory for the
+    // continuity of the neighbouring cells.  They take the tile planes of the
+    // previous step's velocities, which only the ring pass above reads.
+    static_assert(FT_Y * (FT_X + 1) <= G::N && (FT_Y + 1) * FT_X <= G::N, "corrected velocities fit a plane");
+    R* sUc = tile + C_UO * G::N;   // [FT_Y][FT_X + 1], x = bx0-1 .. bx0+31
+    R* sVc = tile + C_VO * G::N;   // [FT_Y + 1][FT_X], y = by0-1 .. by0+7
+    R u = (R)0, v = (R)0;
+    if (inside) {
+        u = ucorr(kc, c, ix, iy, i);
+        v = vcorr(kc, c, ix, iy, i);
+        sUc[threadIdx.y * (FT_X + 1) + threadIdx.x + 1] = u;
+        sVc[(threadIdx.y + 1) * FT_X + threadIdx.x] = v;
+    }
+    if (threadIdx.y == 0 && by0 > 0 && ix < nx)   // (ix, by0-1)
+        sVc[threadIdx.x] = vcorr(kc - G::TX, c - FT_TX, ix, by0 - 1, i - nx);
+    if (threadIdx.y == 1 && threadIdx.x < FT_Y && bx0 > 0 && by0 + (int)threadIdx.x < ny) {   // (bx0-1, by0+r)
+        const int r = threadIdx.x;
+        sUc[r * (FT_X + 1)] = ucorr((r + FC_H) * G::TX + FC_H - 1, (r + 1) * FT_TX, bx0 - 1, by0 + r,
+                                    IDX(bx0 - 1, by0 + r));
+    }
+    __syncthreads();
+    if (!inside) return;
     S.f[UU][i] = u;
     S.f[VV][i] = v;
     // depthhu, depthhv, CalcQFlow (Flow_kernel.cu:653-750, 1917) and continuity
-    // (:1626-1681) with the corrected velocities: the left (lower) neighbour's
-    // are recomputed from the ring; the tile is clamped like pp()
+    // (:1626-1681) with the corrected velocities of the cell and of its left
+    // (lower) neighbour; the tile is clamped like pp()
     TileAt<R, FC_H> a{tile, kc};
     const R eps = K.eps;
     const R hu = depth_face(a(C_ZS, 0, 0), a(C_ZS, 1, 0), a(C_ZB, 0, 0), a(C_ZB, 1, 0), u, eps);
@@ -403,11 +481,11 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
     R zs = a(C_ZS, 0, 0);
     R dzdt = (R)0;
     if (ix > 0) {
-        const R ul = ucorr(kc - 1, c - 1, ix - 1, iy, i - 1);
+        const R ul = sUc[threadIdx.y * (FT_X + 1) + threadIdx.x];
         const R qxl = ul * depth_face(a(C_ZS, -1, 0), a(C_ZS, 0, 0), a(C_ZB, -1, 0), a(C_ZB, 0, 0), ul, eps);
         R qyb = qyi;
         if (iy > 0) {
-            const R vb = vcorr(kc - G::TX, c - FT_TX, ix, iy - 1, i - nx);
+            const R vb = sVc[threadIdx.y * FT_X + threadIdx.x];
             qyb = vb * depth_face(a(C_ZS, 0, -1), a(C_ZS, 0, 0), a(C_ZB, 0, -1), a(C_ZB, 0, 0), vb, eps);
         }
         dzdt = (qxl - qxi + qyb - qyi) * rdx;
@@ -564,43 +642,55 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
 }
 XBG_KERNELS(flow_final)
 
+// fuse_uv: the momentum steps as one pass (k_flow_uv) instead of two
+// (k_flow_u, k_flow_v)
 template <class R>
-int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool fuse_uv) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
     k_flow_a<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_flow_a");
-    k_flow_u<R><<<g, b, 0, st>>>(S, K);
-    PMARK(pf, "k_flow_u");
-    k_flow_v<R><<<g, b, 0, st>>>(S, K);
-    PMARK(pf, "k_flow_v");
+    if (fuse_uv) {
+        k_flow_uv<R><<<g, b, 0, st>>>(S, K);
+        PMARK(pf, "k_flow_uv");
+    } else {
+        k_flow_u<R><<<g, b, 0, st>>>(S, K);
+        PMARK(pf, "k_flow_u");
+        k_flow_v<R><<<g, b, 0, st>>>(S, K);
+        PMARK(pf, "k_flow_v");
+    }
     k_flow_corr<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_flow_corr");
     k_flow_final<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_flow_final");
-    return 5;
+    return fuse_uv ? 4 : 5;
 }
-// the five flow kernels over every scenario of a batch
+// the flow kernels over every scenario of a batch
 template <class R>
-int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf, bool fuse_uv) {
     dim3 b(32, 8);
     const int2* it = L.items[BS_TILE];
     int n = L.n[BS_TILE], g = L.grid[BS_TILE];
     kb_flow_a<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_flow_a");
-    kb_flow_u<R><<<g, b, 0, st>>>(T, it, n);
-    PMARK(pf, "k_flow_u");
-    kb_flow_v<R><<<g, b, 0, st>>>(T, it, n);
-    PMARK(pf, "k_flow_v");
+    if (fuse_uv) {
+        kb_flow_uv<R><<<g, b, 0, st>>>(T, it, n);
+        PMARK(pf, "k_flow_uv");
+    } else {
+        kb_flow_u<R><<<g, b, 0, st>>>(T, it, n);
+        PMARK(pf, "k_flow_u");
+        kb_flow_v<R><<<g, b, 0, st>>>(T, it, n);
+        PMARK(pf, "k_flow_v");
+    }
     kb_flow_corr<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_flow_corr");
     kb_flow_final<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_flow_final");
-    return 5;
+    return fuse_uv ? 4 : 5;
 }
-template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*);
-template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*);
+template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
+template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
 
-template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
-template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
+template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool);
+template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool);
 
 }  // namespace xbg

@@ -168,6 +168,38 @@ __device__ __forceinline__ R flux2s(const R* q, int s, R qi, R cf, R cfmin) {
         return arrin - arrmin;
     }
 }
+// Without wave-current interaction every face speed of a bin is a cell
+// constant times cos(theta) (x) or sin(theta) (y).  The cell constants carry
+// dt / dx (kin, kmin: the face speeds 0.5 (cg_i + cg_j) dt / dx), so a bin's
+// x or y flux difference is cos (sin) times fk(), and its Euler update
+// A = e - (cos fk_x + sin fk_y + dt / dtheta (theta-face difference)).  The
+// upwind side is the one of cos (sin): pos.  Both rows-pass kernels use
+// these two (bit-identical results).
+template <class R, bool POS>
+__device__ __forceinline__ R flux2k(const R* q, int s, R qi, R kin, R kmin) {
+    R ain, amin;
+    if (POS) {
+        const R qm = q[-s];
+        ain = upw(qi, qm);
+        amin = upw(qm, q[-2 * s]);
+    } else {
+        const R qp = q[s];
+        ain = upw(qp, q[2 * s]);
+        amin = upw(qi, qp);
+    }
+    return DM<R>::fma(ain, kin, -(amin * kmin));
+}
+template <class R>
+__device__ __forceinline__ R flux2kv(R qm2, R qm, R qi, R qp, R qp2, bool pos, R kin, R kmin) {
+    const R ain = upw(pos ? qi : qp, pos ? qm : qp2);
+    const R amin = upw(pos ? qm : qi, pos ? qm2 : qp);
+    return DM<R>::fma(ain, kin, -(amin * kmin));
+}
+template <class R>
+__device__ __forceinline__ R euler_k(R e, R ct, R st, R fkx, R fky, R ft, R kth) {
+    return e - DM<R>::fma(ct, fkx, DM<R>::fma(st, fky, ft * kth));
+}
+
 // theta-face flux between bins t and t+1 (the arrint of bin t, which is the
 // arrmint of bin t+1): e(t-1), e(t), e(t+1), e(t+2), ctheta(t), ctheta(t+1)
 template <class R>
@@ -431,7 +463,9 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         const R* cgp = S.f[CG];
         const R* cp = S.f[CC_];
         cgi = ld(cgp + i); cci = ld(cp + i);
-        const R h = (R)0.5f;
+        // without wave-current interaction the face speeds carry dt / dx
+        // (flux2kv, euler_k: the arithmetic of the TMA rows pass)
+        const R h = WCI ? (R)0.5f : (R)0.5f * (dtf * rdx);
         axp = h * (cgi + ld(cgp + xp + iy * nx)); axm = h * (cgi + ld(cgp + xm + iy * nx));
         ayp = h * (cgi + ld(cgp + ix + yp * nx)); aym = h * (cgi + ld(cgp + ix + ym * nx));
         rxp = h * (cci + ld(cp + xp + iy * nx)); rxm = h * (cci + ld(cp + xm + iy * nx));
@@ -475,24 +509,39 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
             const R ct = d.c, st = d.s;
             const bool last = t == nt - 1;
             cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
-            R fx = flux2(qE[-2], qE[-1], we2, qE[1], qE[2], DM<R>::fma(ct, axp, bxp), DM<R>::fma(ct, axm, bxm));
-            R fy = flux2(qE[-2 * WT_TX], qE[-WT_TX], we2, qE[WT_TX], qE[2 * WT_TX], DM<R>::fma(st, ayp, byp),
-                         DM<R>::fma(st, aym, bym));
             // theta flux: upper face computed here, lower face carried from bin t-1
             R fup = last ? (R)0 : theta_face(we1, we2, we3, we4, c0, cpp);
             R ft = fup - fte;
             fte = fup;
-            R A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
+            R A;
+            const bool px = ct > (R)0, py = st > (R)0;
+            if (WCI) {
+                R fx = flux2(qE[-2], qE[-1], we2, qE[1], qE[2], DM<R>::fma(ct, axp, bxp), DM<R>::fma(ct, axm, bxm));
+                R fy = flux2(qE[-2 * WT_TX], qE[-WT_TX], we2, qE[WT_TX], qE[2 * WT_TX], DM<R>::fma(st, ayp, byp),
+                             DM<R>::fma(st, aym, bym));
+                A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
+            } else {
+                R fx = flux2kv(qE[-2], qE[-1], we2, qE[1], qE[2], px, axp, axm);
+                R fy = flux2kv(qE[-2 * WT_TX], qE[-WT_TX], we2, qE[WT_TX], qE[2 * WT_TX], py, ayp, aym);
+                A = euler_k(we2, ct, st, fx, fy, ft, dtf * rdth);
+            }
             R Ar;
             if (!ROLLER) Ar = ld(oldR + (size_t)t * C);
             if (ROLLER) {
-                R rx = flux2(qR[-2], qR[-1], wr2, qR[1], qR[2], DM<R>::fma(ct, rxp, bxp), DM<R>::fma(ct, rxm, bxm));
-                R ry = flux2(qR[-2 * WT_TX], qR[-WT_TX], wr2, qR[WT_TX], qR[2 * WT_TX], DM<R>::fma(st, ryp, byp),
-                             DM<R>::fma(st, rym, bym));
                 R rup = last ? (R)0 : theta_face(wr1, wr2, wr3, wr4, c0, cpp);
                 R rt = rup - ftr;
                 ftr = rup;
-                Ar = wr2 - dtf * ((rx + ry) * rdx + rt * rdth);
+                if (WCI) {
+                    R rx = flux2(qR[-2], qR[-1], wr2, qR[1], qR[2], DM<R>::fma(ct, rxp, bxp),
+                                 DM<R>::fma(ct, rxm, bxm));
+                    R ry = flux2(qR[-2 * WT_TX], qR[-WT_TX], wr2, qR[WT_TX], qR[2 * WT_TX],
+                                 DM<R>::fma(st, ryp, byp), DM<R>::fma(st, rym, bym));
+                    Ar = wr2 - dtf * ((rx + ry) * rdx + rt * rdth);
+                } else {
+                    R rx = flux2kv(qR[-2], qR[-1], wr2, qR[1], qR[2], px, rxp, rxm);
+                    R ry = flux2kv(qR[-2 * WT_TX], qR[-WT_TX], wr2, qR[WT_TX], qR[2 * WT_TX], py, ryp, rym);
+                    Ar = euler_k(wr2, ct, st, rx, ry, rt, dtf * rdth);
+                }
             }
             *oA = A;
             *oR = Ar;
@@ -690,9 +739,24 @@ size_t wave_tma_smem(int nt) {
     return 128 + ((size_t)2 * TM_NB * TM_N + (size_t)2 * nt * 256 + 6 * nt) * sizeof(R);
 }
 
-template <class R, bool ROLLER>
+// The state one thread keeps for one cell of the rows pass.
+template <class R>
+struct WCell {
+    int i, ctile, cid, ix, iy;
+    bool active;
+    R hh, axp, axm, ayp, aym, rxp, rxm, ryp, rym, cgi, cci, cthP, cthQ;
+    R we1, we2, we3, we4, wr1, wr2, wr3, wr4, c0, cpp, Etmp, cabs, fte, ftr;
+};
+
+// CPT cells per thread: the block is 32 x (8 / CPT) threads over the same
+// 32 x 8 cells (thread row r owns cell rows r, r + 8/CPT, ...); with two,
+// the per-bin work that does not depend on the cell (waits, barrier,
+// direction table, loop control) is shared by both cells and the two
+// cells' independent arithmetic interleaves.
+template <class R, bool ROLLER, int CPT>
 __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, const WaveMaps& M, const int bix,
                                            const int biy) {
+    constexpr int NTH = 256 / CPT, RPT = WT_Y / CPT;   // threads, thread rows
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long mbar[TM_NB];
     Clock* clk = S.clk;
@@ -712,8 +776,6 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         sMom[tid] = Dir4<R>{c * c, sn * sn, sn * c, K.theta[tid]};
     }
     const int bx0 = bix * WT_X, by0 = 1 + biy * WT_Y;
-    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    const bool active = ix < nx && iy <= ny - 2;
     const int par = clk->par;
     const CUtensorMap* mE = &M.ld_e[par ^ 1];
     const CUtensorMap* mR = &M.ld_r[par ^ 1];
@@ -723,6 +785,9 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
     const R dth = K.dtheta;
     const R rdth = (R)1 / dth;
     const R rdx = (R)1 / K.dx;
+    const R sg = (R)clk->sigm;
+    const R cmax_ = (R)(0.25f * sg), cmin_ = (R)(-0.25f * sg);   // propagtheta's clamp of ctheta
+    const R kxy = dtf * rdx, kth = dtf * rdth;
     constexpr unsigned TBYTES = (ROLLER ? 2u : 1u) * TM_N * sizeof(R);
     if (tid == 0) {
         for (int b = 0; b < TM_NB; b++) tm_mbar_init(su32(&mbar[b]));
@@ -750,7 +815,7 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
     auto fixup = [&](int p) {
         R* dE = tE + (p & (TM_NB - 1)) * TM_N;
         R* dR = tR + (p & (TM_NB - 1)) * TM_N;
-        for (int e = tid; e < TM_N; e += 256) {
+        for (int e = tid; e < TM_N; e += NTH) {
             const int gx = bx0 - 4 + e % TM_X, gy = by0 - 2 + e / TM_X;
             const int cx = min(max(gx, 0), nx - 1), cy = min(max(gy, 0), ny - 1);
             const bool in = cx == gx && cy == gy;
@@ -760,47 +825,51 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         }
         tm_fence_async();   // these writes before the buffer's next box copy
     };
-    const int ctile = (iy - by0 + 2) * TM_X + (ix - bx0 + 4);
-    int i = 0;
-    R hh = 0;
-    R axp = 0, axm = 0, ayp = 0, aym = 0, rxp = 0, rxm = 0, ryp = 0, rym = 0, cgi = 0, cci = 0;
-    CthCoef<R> cc{};
-    R we1 = 0, we2 = 0, we3 = 0, we4 = 0, wr1 = 0, wr2 = 0, wr3 = 0, wr4 = 0;
-    R c0 = 0, cpp = 0, Etmp = 0, cabs = 0, fte = 0, ftr = 0;
-    R cthP = 0, cthQ = 0;
-    auto cth = [&](R cx, R sx) -> R {
-        const R ctht = DM<R>::fma(cthP, sx, cthQ * cx);
-        return cmin(cmax(ctht, (R)(-0.25f * cc.sg)), (R)(0.25f * cc.sg));
+    auto cth = [&](const WCell<R>& w, R cx, R sx) -> R {
+        const R ctht = DM<R>::fma(w.cthP, sx, w.cthQ * cx);
+        return cmin(cmax(ctht, cmin_), cmax_);
     };
-    if (active) {
-        i = ix + iy * nx;
-        const int xm = mm(ix), xp = pp(ix, nx);
-        const int ym = mm(iy), yp = pp(iy, ny);
-        hh = ld(S.f[HH] + i);
-        cc = cth_coef(S, K, ix, iy, (R)clk->sigm);
-        const R* cgp = S.f[CG];
-        const R* cp = S.f[CC_];
-        cgi = ld(cgp + i); cci = ld(cp + i);
-        const R h = (R)0.5f;
-        // face speeds: without wave-current interaction the current terms of
-        // the face speed are exactly zero
-        axp = h * (cgi + ld(cgp + xp + iy * nx)); axm = h * (cgi + ld(cgp + xm + iy * nx));
-        ayp = h * (cgi + ld(cgp + ix + yp * nx)); aym = h * (cgi + ld(cgp + ix + ym * nx));
-        rxp = h * (cci + ld(cp + xp + iy * nx)); rxm = h * (cci + ld(cp + xm + iy * nx));
-        ryp = h * (cci + ld(cp + ix + yp * nx)); rym = h * (cci + ld(cp + ix + ym * nx));
-        cthP = cc.s * cc.dhdx; cthQ = -(cc.s * cc.dhdy);
-        c0 = cth(sCS2[0].c, sCS2[0].s);
-        const int t1 = nt > 1 ? 1 : 0;
-        cpp = cth(sCS2[t1].c, sCS2[t1].s);
+    WCell<R> cl[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        WCell<R>& w = cl[c];
+        w = WCell<R>{};
+        const int ty = threadIdx.y + c * RPT;
+        w.ix = bx0 + threadIdx.x;
+        w.iy = by0 + ty;
+        w.cid = threadIdx.x + ty * WT_X;
+        w.ctile = (ty + 2) * TM_X + (threadIdx.x + 4);
+        w.active = w.ix < nx && w.iy <= ny - 2;
+        w.i = 0;
+        if (w.active) {
+            const int ix = w.ix, iy = w.iy;
+            const int i = ix + iy * nx;
+            w.i = i;
+            const int xm = mm(ix), xp = pp(ix, nx);
+            const int ym = mm(iy), yp = pp(iy, ny);
+            w.hh = ld(S.f[HH] + i);
+            const CthCoef<R> cc = cth_coef(S, K, ix, iy, sg);
+            const R* cgp = S.f[CG];
+            const R* cp = S.f[CC_];
+            w.cgi = ld(cgp + i); w.cci = ld(cp + i);
+            // face speeds times dt / dx: without wave-current interaction the
+            // current terms of the face speed are exactly zero
+            const R h = (R)0.5f * kxy;
+            w.axp = h * (w.cgi + ld(cgp + xp + iy * nx)); w.axm = h * (w.cgi + ld(cgp + xm + iy * nx));
+            w.ayp = h * (w.cgi + ld(cgp + ix + yp * nx)); w.aym = h * (w.cgi + ld(cgp + ix + ym * nx));
+            w.rxp = h * (w.cci + ld(cp + xp + iy * nx)); w.rxm = h * (w.cci + ld(cp + xm + iy * nx));
+            w.ryp = h * (w.cci + ld(cp + ix + yp * nx)); w.rym = h * (w.cci + ld(cp + ix + ym * nx));
+            w.cthP = cc.s * cc.dhdx; w.cthQ = -(cc.s * cc.dhdy);
+            w.c0 = cth(w, sCS2[0].c, sCS2[0].s);
+            const int t1 = nt > 1 ? 1 : 0;
+            w.cpp = cth(w, sCS2[t1].c, sCS2[t1].s);
+        }
     }
     bool ok = wait_plane(0) && (nt < 2 || wait_plane(1));
     if (edge) {
         fixup(0);
         if (nt > 1) fixup(1);
     }
-    R* oA = sA + tid;
-    R* oR = sR + tid;
-    const R* oldR = rro + i;   // without the roller pass rr is carried unchanged
     bool failed = false;
 #pragma unroll 1
     for (int t = 0; t < nt; t++) {
@@ -811,31 +880,35 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         }
         if (__syncthreads_or(!ok)) { failed = true; break; }   // fixups visible; plane t-1 read by all
         if (tid == 0 && t >= 1 && t + 3 < nt) issue(t + 3);    // into plane t-1's buffer
-        if (active) {
-            const R* qE = tE + b * TM_N + ctile;
-            const R* qR = tR + b * TM_N + ctile;
+        const Dir2<R> d = sCS2[t];
+        const R ct = d.c, st = d.s;
+        const bool last = t == nt - 1;
+        const int b2 = (t + 2 < nt ? t + 2 : nt - 1) & (TM_NB - 1);
+        const Dir2<R> d2 = sCS2[t + 2 < nt ? t + 2 : nt - 1];
+#pragma unroll
+        for (int c = 0; c < CPT; c++) {
+            WCell<R>& w = cl[c];
+            if (!w.active) continue;
+            const R* qE = tE + b * TM_N + w.ctile;
+            const R* qR = tR + b * TM_N + w.ctile;
             if (t == 0) {
                 const int b1 = (nt > 1 ? 1 : 0);
-                we2 = qE[0]; we1 = we2; we3 = tE[b1 * TM_N + ctile];
-                if (ROLLER) { wr2 = qR[0]; wr1 = wr2; wr3 = tR[b1 * TM_N + ctile]; }
+                w.we2 = qE[0]; w.we1 = w.we2; w.we3 = tE[b1 * TM_N + w.ctile];
+                if (ROLLER) { w.wr2 = qR[0]; w.wr1 = w.wr2; w.wr3 = tR[b1 * TM_N + w.ctile]; }
             }
-            const int b2 = (t + 2 < nt ? t + 2 : nt - 1) & (TM_NB - 1);
-            we4 = tE[b2 * TM_N + ctile];
-            if (ROLLER) wr4 = tR[b2 * TM_N + ctile];
-            const Dir2<R> d = sCS2[t];
-            const R ct = d.c, st = d.s;
-            const bool last = t == nt - 1;
-            cabs = DM<R>::fmax(cabs, DM<R>::fabs(c0));
+            w.we4 = tE[b2 * TM_N + w.ctile];
+            if (ROLLER) w.wr4 = tR[b2 * TM_N + w.ctile];
+            w.cabs = DM<R>::fmax(w.cabs, DM<R>::fabs(w.c0));
             // x and y fluxes with the upwind side of the bin (the sign of
             // cos and sin is the same for every cell of the bin)
             R fx, fy, rx = 0, ry = 0;
             auto xy = [&](auto px, auto py) {
                 constexpr bool PX = decltype(px)::value, PY = decltype(py)::value;
-                fx = flux2s<R, PX>(qE, 1, we2, ct * axp, ct * axm);
-                fy = flux2s<R, PY>(qE, TM_X, we2, st * ayp, st * aym);
+                fx = flux2k<R, PX>(qE, 1, w.we2, w.axp, w.axm);
+                fy = flux2k<R, PY>(qE, TM_X, w.we2, w.ayp, w.aym);
                 if (ROLLER) {
-                    rx = flux2s<R, PX>(qR, 1, wr2, ct * rxp, ct * rxm);
-                    ry = flux2s<R, PY>(qR, TM_X, wr2, st * ryp, st * rym);
+                    rx = flux2k<R, PX>(qR, 1, w.wr2, w.rxp, w.rxm);
+                    ry = flux2k<R, PY>(qR, TM_X, w.wr2, w.ryp, w.rym);
                 }
             };
             using T_ = std::true_type;
@@ -845,27 +918,24 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
             } else {
                 if (st > (R)0) xy(F_{}, T_{}); else xy(F_{}, F_{});
             }
-            R fup = last ? (R)0 : theta_face(we1, we2, we3, we4, c0, cpp);
-            R ft = fup - fte;
-            fte = fup;
-            R A = we2 - dtf * ((fx + fy) * rdx + ft * rdth);
+            R fup = last ? (R)0 : theta_face(w.we1, w.we2, w.we3, w.we4, w.c0, w.cpp);
+            R ft = fup - w.fte;
+            w.fte = fup;
+            R A = euler_k(w.we2, ct, st, fx, fy, ft, kth);
             R Ar;
-            if (!ROLLER) Ar = ld(oldR + (size_t)t * C);
+            if (!ROLLER) Ar = ld(rro + w.i + (size_t)t * C);   // without the roller pass rr is carried unchanged
             if (ROLLER) {
-                R rup = last ? (R)0 : theta_face(wr1, wr2, wr3, wr4, c0, cpp);
-                R rt = rup - ftr;
-                ftr = rup;
-                Ar = wr2 - dtf * ((rx + ry) * rdx + rt * rdth);
+                R rup = last ? (R)0 : theta_face(w.wr1, w.wr2, w.wr3, w.wr4, w.c0, w.cpp);
+                R rt = rup - w.ftr;
+                w.ftr = rup;
+                Ar = euler_k(w.wr2, ct, st, rx, ry, rt, kth);
             }
-            *oA = A;
-            *oR = Ar;
-            oA += 256; oR += 256;
-            Etmp = Etmp + DM<R>::fmax(A, (R)0);
-            const int t2 = t + 2 < nt ? t + 2 : nt - 1;
-            we1 = we2; we2 = we3; we3 = we4;
-            wr1 = wr2; wr2 = wr3; wr3 = wr4;
-            const Dir2<R> d2 = sCS2[t2];
-            c0 = cpp; cpp = cth(d2.c, d2.s);
+            sA[t * 256 + w.cid] = A;
+            sR[t * 256 + w.cid] = Ar;
+            w.Etmp = w.Etmp + DM<R>::fmax(A, (R)0);
+            w.we1 = w.we2; w.we2 = w.we3; w.we3 = w.we4;
+            w.wr1 = w.wr2; w.wr2 = w.wr3; w.wr3 = w.wr4;
+            w.c0 = w.cpp; w.cpp = cth(w, d2.c, d2.s);
         }
     }
     if (failed) {   // a copy never completed: record, halt, let the copies in flight land (bounded), leave
@@ -879,35 +949,40 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         return;
     }
     R dtw = (R)3.0e38f;
-    if (active) {
-        dtw = DM<R>::fmin(K.cfl * dth / cabs, (R)9999999.9f);   // WAVEDT (Wave_kernel.cu:232-249)
-        R* een = S.ee[par];
-        R* rrn = S.rr[par];
-        const R Trep = (R)clk->Trep;
-        const R rho = K.rho, g = K.g;
+    R* een = S.ee[par];
+    R* rrn = S.rr[par];
+    const R Trep = (R)clk->Trep;
+    const R rho = K.rho, g = K.g;
+    const R twogb = (R)2.0f * g * K.beta;
+#pragma unroll
+    for (int c = 0; c < CPT; c++) {
+        const WCell<R>& w = cl[c];
+        if (!w.active) continue;
+        const int i = w.i, cid = w.cid;
+        dtw = DM<R>::fmin(dtw, DM<R>::fmin(K.cfl * dth / w.cabs, (R)9999999.9f));   // WAVEDT (Wave_kernel.cu:232-249)
         R ridiv, Dv, Dq;
-        wave_breaking(K, Etmp, hh, ld(S.f[WK] + i), ld(S.f[FWM] + i), Trep, ridiv, Dv, Dq);
-        const R cc_i = cci;
-        const R twogb = (R)2.0f * g * K.beta;
+        wave_breaking(K, w.Etmp, w.hh, ld(S.f[WK] + i), ld(S.f[FWM] + i), Trep, ridiv, Dv, Dq);
+        const R cc_i = w.cci;
         const R rcoef = twogb / cc_i;
-        const bool wet = hh > K.eps;
+        const bool wet = w.hh > K.eps;
         // the lateral rows 0 and ny-1 first, while sA / sR still hold the
         // advected bins; the source cell's new ee is formed as below
-        const R sg = (R)clk->sigm;
         auto fin = [&](int t) {
             R dd;
-            return wet ? diss_ee(sA[t * 256 + tid], ridiv, Dq, dtf, dd) : (R)0;
+            return wet ? diss_ee(sA[t * 256 + cid], ridiv, Dq, dtf, dd) : (R)0;
         };
-        if (iy == 1)
-            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, false>(S, K, ix, 0, sA, sR, sCS2, sMom, Etmp, sg, dtf,
+        if (w.iy == 1)
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, false>(S, K, w.ix, 0, sA + (cid - tid), sR + (cid - tid),
+                                                                   sCS2, sMom, w.Etmp, sg, dtf, Trep, rro, een, rrn,
+                                                                   fin));
+        if (w.iy == ny - 2)
+            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, false>(S, K, w.ix, ny - 1, sA + (cid - tid),
+                                                                   sR + (cid - tid), sCS2, sMom, w.Etmp, sg, dtf,
                                                                    Trep, rro, een, rrn, fin));
-        if (iy == ny - 2)
-            dtw = DM<R>::fmin(dtw, wave_edge_cell<R, ROLLER, false>(S, K, ix, ny - 1, sA, sR, sCS2, sMom, Etmp, sg,
-                                                                   dtf, Trep, rro, een, rrn, fin));
         R RR = (R)0.0f, drr = (R)0.0f, sume = (R)0, sumethet = (R)0;
         R ec = 0, es = 0, ecs = 0, rc = 0, rs = 0, rcs = 0;
-        R* pA = sA + tid;
-        R* pR = sR + tid;
+        R* pA = sA + cid;
+        R* pR = sR + cid;
         if (wet) {
 #pragma unroll 2
             for (int t = 0; t < nt; t++) {
@@ -944,7 +1019,7 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         S.f[D][i] = Dv;
         S.f[ROL][i] = RR * dth;
         S.f[DR][i] = drr * dth;
-        const R n = cgi / cc_i;
+        const R n = w.cgi / cc_i;
         S.tmp[T_SXX][i] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
         S.tmp[T_SYY][i] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
         S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
@@ -963,18 +1038,18 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
 // FP32: 64 registers, four blocks (32 warps) per SM, which hides the pass's
 // dependent-arithmetic latency better than three (-15 % at 2048 x 1024);
 // FP64 (the error-oracle build) keeps room for its wider registers.
-template <class R, bool ROLLER>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
+template <class R, bool ROLLER, int CPT>
+__global__ void __launch_bounds__(256 / CPT, sizeof(R) == 4 ? 4 : 2)
     k_wave_tma(Dev<R> S, Konst<R> K, const __grid_constant__ WaveMaps M) {
-    b_wave_tma<R, ROLLER>(S, K, M, blockIdx.x, blockIdx.y);
+    b_wave_tma<R, ROLLER, CPT>(S, K, M, blockIdx.x, blockIdx.y);
 }
 // every scenario of a batch: its tensor maps from a device array (written
 // by the host before the first launch), one per scenario
-template <class R, bool ROLLER>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 2)
+template <class R, bool ROLLER, int CPT>
+__global__ void __launch_bounds__(256 / CPT, sizeof(R) == 4 ? 4 : 2)
     kb_wave_tma(BatchTab<R> T, const WaveMaps* __restrict__ maps, const int2* items, int n) {
     batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux& A, int bx, int by) {
-        b_wave_tma<R, ROLLER>(S, K, maps[A.scen], bx, by);
+        b_wave_tma<R, ROLLER, CPT>(S, K, maps[A.scen], bx, by);
     });
 }
 
@@ -1096,7 +1171,7 @@ int wave_parts(const Konst<R>& K) {
 // tiles (b_wave_fast); the TMA pass has no wave-current interaction variant.
 template <class R>
 int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, cudaEvent_t join,
-                const WaveMaps* maps) {
+                const WaveMaps* maps, int cpt) {
     int n = 0;
     k_disp<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, K); n++;
     PMARK(pf, "k_disp");
@@ -1105,8 +1180,14 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, c
         dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny - 2 + 7) / 8);
         if (maps && K.wci == (R)0) {
             const size_t smem = wave_tma_smem<R>(K.nt);
-            if (K.roller == 1) k_wave_tma<R, true><<<g, b, smem, st>>>(S, K, *maps);
-            else k_wave_tma<R, false><<<g, b, smem, st>>>(S, K, *maps);
+            if (cpt == 2) {
+                const dim3 b2(32, 4);
+                if (K.roller == 1) k_wave_tma<R, true, 2><<<g, b2, smem, st>>>(S, K, *maps);
+                else k_wave_tma<R, false, 2><<<g, b2, smem, st>>>(S, K, *maps);
+            } else {
+                if (K.roller == 1) k_wave_tma<R, true, 1><<<g, b, smem, st>>>(S, K, *maps);
+                else k_wave_tma<R, false, 1><<<g, b, smem, st>>>(S, K, *maps);
+            }
             n++;
             PMARK(pf, "k_wave_tma");
         } else {
@@ -1126,7 +1207,7 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, c
 // null for the thread-copied tiles
 template <class R>
 int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
-                      Prof* pf, cudaEvent_t join, const WaveMaps* maps) {
+                      Prof* pf, cudaEvent_t join, const WaveMaps* maps, int cpt) {
     kb_disp<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
     PMARK(pf, "k_disp");
     if (join) cudaStreamWaitEvent(st, join, 0);
@@ -1134,8 +1215,13 @@ int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int ro
         const int g = L.grid[BS_WROWS], n = L.n[BS_WROWS];
         const int2* it = L.items[BS_WROWS];
         const size_t smem = wave_tma_smem<R>(nt);
-        if (roller == 1) kb_wave_tma<R, true><<<g, dim3(32, 8), smem, st>>>(T, maps, it, n);
-        else kb_wave_tma<R, false><<<g, dim3(32, 8), smem, st>>>(T, maps, it, n);
+        if (cpt == 2) {
+            if (roller == 1) kb_wave_tma<R, true, 2><<<g, dim3(32, 4), smem, st>>>(T, maps, it, n);
+            else kb_wave_tma<R, false, 2><<<g, dim3(32, 4), smem, st>>>(T, maps, it, n);
+        } else {
+            if (roller == 1) kb_wave_tma<R, true, 1><<<g, dim3(32, 8), smem, st>>>(T, maps, it, n);
+            else kb_wave_tma<R, false, 1><<<g, dim3(32, 8), smem, st>>>(T, maps, it, n);
+        }
         PMARK(pf, "k_wave_tma");
     } else {
         launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
@@ -1146,9 +1232,9 @@ int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int ro
     return 3;
 }
 template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                      cudaEvent_t, const WaveMaps*);
+                                      cudaEvent_t, const WaveMaps*, int);
 template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                       cudaEvent_t, const WaveMaps*);
+                                       cudaEvent_t, const WaveMaps*, int);
 
 // One-time kernel attributes (dynamic shared memory above 48 KB for wide
 // theta sets in FP64).
@@ -1157,10 +1243,14 @@ int wave_prepare(const Konst<R>& K) {
     const int smem = (int)wave_fast_smem<R>(K.nt);
     const int smem_tma = (int)wave_tma_smem<R>(K.nt);
     const cudaFuncAttribute a = cudaFuncAttributeMaxDynamicSharedMemorySize;
-    if (cudaFuncSetAttribute(k_wave_tma<R, true>, a, smem_tma) != cudaSuccess ||
-        cudaFuncSetAttribute(k_wave_tma<R, false>, a, smem_tma) != cudaSuccess ||
-        cudaFuncSetAttribute(kb_wave_tma<R, true>, a, smem_tma) != cudaSuccess ||
-        cudaFuncSetAttribute(kb_wave_tma<R, false>, a, smem_tma) != cudaSuccess)
+    if (cudaFuncSetAttribute(k_wave_tma<R, true, 1>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(k_wave_tma<R, false, 1>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(k_wave_tma<R, true, 2>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(k_wave_tma<R, false, 2>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(kb_wave_tma<R, true, 1>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(kb_wave_tma<R, false, 1>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(kb_wave_tma<R, true, 2>, a, smem_tma) != cudaSuccess ||
+        cudaFuncSetAttribute(kb_wave_tma<R, false, 2>, a, smem_tma) != cudaSuccess)
         return 1;
     cudaError_t e[8] = {
         cudaFuncSetAttribute(k_wave_fast<R, true, true>, a, smem), cudaFuncSetAttribute(k_wave_fast<R, true, false>, a, smem),
@@ -1175,9 +1265,9 @@ template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);
 
 template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, cudaEvent_t,
-                                const WaveMaps*);
+                                const WaveMaps*, int);
 template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, cudaEvent_t,
-                                 const WaveMaps*);
+                                 const WaveMaps*, int);
 template int wave_maps_make<float>(const Dev<float>&, const Konst<float>&, WaveMaps*);
 template int wave_maps_make<double>(const Dev<double>&, const Konst<double>&, WaveMaps*);
 template int wave_parts<float>(const Konst<float>&);

@@ -248,7 +248,9 @@ class Model:
         return [(names[k].decode(), float(ms[k])) for k in range(n.value)]
 
     def set_variant(self, phase, variant):
-        """Kernel variant of a phase (XBG_PHASE_WAVE: 1 TMA tiles, 0 thread-copied)."""
+        """Kernel variant of a phase (XBG_PHASE_WAVE: 1 / 2 TMA tiles with one /
+        two cells per thread, 0 thread-copied tiles; XBG_PHASE_FLOW: 1 fused
+        momentum pass, 0 two passes)."""
         _check(self.L.xbg_set_kernel_variant(self.h, phase, variant), "set_kernel_variant")
 
     def variant(self, phase):

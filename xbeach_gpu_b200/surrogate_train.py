@@ -71,13 +71,9 @@ def collect(nx=512, ny=256, seeds=(0, 1), Hs_list=(1.5, 2.5), warm=300, every=20
     return dict(x=np.stack(xs), y=np.stack(ys), hold=np.stack(hs))
 
 
-def collect_batch(scen, warm=200, every=20, count=6, k=10, crop=160, crops_per=4, seed=0):
-    """Snapshot pairs from a plain batched run of (params, zb, boundary)
-    scenarios (the storm ensemble: boundary["storm"] gives Hm0, Tp at model
-    time t): at each snapshot, crops_per windows of crop x crop cells per
-    scenario around its shoreline (x from 55 % to 85 % of the cross-shore
-    extent) of the inputs and held wave fields at t, and of the wave fields
-    at t + k in the same windows.  Returns dict(x, y, hold) as collect()."""
+def storm_batch(scen, warm):
+    """A plain FP32 Batch of (params, zb, boundary) scenarios, set up from
+    their boundaries and beds and advanced `warm` coupled steps."""
     from .model import Batch
     b = Batch([p for p, _, _ in scen])
     for s, (p, zb, bnd) in enumerate(scen):
@@ -87,6 +83,18 @@ def collect_batch(scen, warm=200, every=20, count=6, k=10, crop=160, crops_per=4
         m.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
         m.init_state(zb, 0.0, 0.0)
     b.advance(warm)
+    b.sync()
+    return b
+
+
+def collect_batch(scen, warm=200, every=20, count=6, k=10, crop=160, crops_per=4, seed=0):
+    """Snapshot pairs from a plain batched run of (params, zb, boundary)
+    scenarios (the storm ensemble: boundary["storm"] gives Hm0, Tp at model
+    time t): at each snapshot, crops_per windows of crop x crop cells per
+    scenario around its shoreline (x from 55 % to 85 % of the cross-shore
+    extent) of the inputs and held wave fields at t, and of the wave fields
+    at t + k in the same windows.  Returns dict(x, y, hold) as collect()."""
+    b = storm_batch(scen, warm)
     rng = np.random.default_rng(seed)
     xs, ys, hs = [], [], []
     for _ in range(count):
@@ -165,6 +173,26 @@ class CropRecorder:
 
     def data(self):
         return dict(x=np.stack(self.xs), y=np.stack(self.ys), hold=np.stack(self.hs))
+
+
+def pushforward_data(net, norm, scen, warm=150, steps=200, k=10, judge_every=20, crop=96, crops_per=4, seed=0):
+    """Training pairs against chained drift (push-forward data): the
+    scenarios step surrogate-assisted with `net` and no error bar, and at
+    every judge segment a CropRecorder keeps the inputs there -- whose held
+    wave fields, and wave energy, are the network's own earlier predictions
+    after judge_every - k forced steps -- with the plain solver's fields k
+    steps on as the targets.  Training on these as well teaches the network
+    to correct the drift its chained predictions leave in its inputs."""
+    from .surrogate_couple import BatchSurrogateRun
+    b = storm_batch(scen, warm)
+    rec = CropRecorder(b, scen, crop=crop, crops_per=crops_per, seed=seed)
+    run = BatchSurrogateRun(b, [p for p, _, _ in scen], net, norm, lambda s, t: scen[s][2]["storm"](t), k=k,
+                            judge_every=judge_every, threshold=float("inf"), recorder=rec)
+    run.advance(steps)
+    b.close()
+    d = rec.data()
+    d["judged"] = run.judged
+    return d
 
 
 def merge(*ds):
