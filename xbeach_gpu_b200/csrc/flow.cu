@@ -61,7 +61,7 @@ __device__ __forceinline__ R smago_cell(const Dev<R>& S, const Konst<R>& K, int 
 
 template <class R>
 __device__ __forceinline__ void b_flow_a(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
-    if (halted(S.clk)) return;
+    const bool off = halted(S.clk);   // tested before the first store (see halted())
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
@@ -69,12 +69,17 @@ __device__ __forceinline__ void b_flow_a(const Dev<R>& S, const Konst<R>& K, con
     R eps = K.eps;
     R hh = ld(S.f[HH] + i);
     R humi = (R)0.5f * (hh + ld(S.f[HH] + IDX(pp(ix, nx), iy)));
-    S.wetu[i] = (ld(S.f[HU] + i) > eps && humi > eps) ? 1 : 0;
-    S.f[HUM][i] = DM<R>::fmax(humi, eps);
+    const int wu = (ld(S.f[HU] + i) > eps && humi > eps) ? 1 : 0;
     R hvmi = (R)0.5f * (hh + ld(S.f[HH] + IDX(ix, pp(iy, ny))));
-    S.wetv[i] = (ld(S.f[HV] + i) > eps && hvmi > eps) ? 1 : 0;
+    const int wv = (ld(S.f[HV] + i) > eps && hvmi > eps) ? 1 : 0;
+    const R nuh = smago_cell(S, K, ix, iy);
+    loads_before_here();
+    if (off) return;
+    S.wetu[i] = wu;
+    S.f[HUM][i] = DM<R>::fmax(humi, eps);
+    S.wetv[i] = wv;
     S.f[HVM][i] = DM<R>::fmax(hvmi, eps);
-    S.tmp[T_NUH][i] = smago_cell(S, K, ix, iy);
+    S.tmp[T_NUH][i] = nuh;
 }
 XBG_KERNELS(flow_a)
 
@@ -159,11 +164,14 @@ __device__ __forceinline__ R ustar_cell(const Dev<R>& S, const Konst<R>& K, int 
 template <class R>
 __device__ __forceinline__ void b_flow_u(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    const bool off = halted(clk);
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
-    S.tmp[T_UU][IDX(ix, iy)] = ustar_cell(S, K, ix, iy, (R)clk->dt, (R)clk->windu);
+    const R u = ustar_cell(S, K, ix, iy, (R)clk->dt, (R)clk->windu);
+    loads_before_here();
+    if (off) return;
+    S.tmp[T_UU][IDX(ix, iy)] = u;
 }
 XBG_KERNELS(flow_u)
 
@@ -248,7 +256,7 @@ __device__ R euler_v(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, 
 template <class R>
 __device__ __forceinline__ void b_flow_v(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    const bool off = halted(clk);
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
@@ -261,6 +269,8 @@ __device__ __forceinline__ void b_flow_v(const Dev<R>& S, const Konst<R>& K, con
     R v;
     if (sy < ny - 2 && ix > 0) v = euler_v(S, K, ix, sy, dtf, wv, [&](int x, int y) { return ld(us + IDX(x, y)); });
     else v = ld(S.f[VV] + IDX(ix, sy));
+    loads_before_here();
+    if (off) return;
     S.tmp[T_VV][IDX(ix, iy)] = v;
 }
 XBG_KERNELS(flow_v)
@@ -278,7 +288,7 @@ constexpr int UV_TX = FT_X + 2, UV_TY = FT_Y + 1;
 template <class R>
 __device__ __forceinline__ void b_flow_uv(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    const bool off = halted(clk);
     __shared__ R sU[UV_TY * UV_TX];
     const int nx = K.nx, ny = K.ny;
     const int bx0 = bix * FT_X, by0 = biy * FT_Y;
@@ -289,7 +299,8 @@ __device__ __forceinline__ void b_flow_uv(const Dev<R>& S, const Konst<R>& K, co
     }
     __syncthreads();
     const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    if (ix >= nx || iy >= ny) return;
+    loads_before_here();
+    if (off || ix >= nx || iy >= ny) return;
     S.tmp[T_UU][IDX(ix, iy)] = sU[threadIdx.y * UV_TX + threadIdx.x + 1];
     // vvlatbnd: row 0 <- row 1, row ny-2 <- row ny-3; row ny-1 keeps its value
     int sy = iy;
@@ -390,7 +401,7 @@ __device__ __forceinline__ void wrk_v(const A& a, const Konst<R>& K, int ix, int
 template <class R>
 __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    const bool off = halted(clk);
     using G = TileG<FC_H>;
     __shared__ R tile[C_NF * G::N];
     __shared__ R sU1[FT_N], sU2[FT_N], sV1[FT_N], sV2[FT_N];
@@ -467,7 +478,8 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
                                     IDX(bx0 - 1, by0 + r));
     }
     __syncthreads();
-    if (!inside) return;
+    loads_before_here();
+    if (off || !inside) return;
     S.f[UU][i] = u;
     S.f[VV][i] = v;
     // depthhu, depthhv, CalcQFlow (Flow_kernel.cu:653-750, 1917) and continuity
@@ -578,7 +590,7 @@ __device__ __forceinline__ void uvvu_cell(const A& a, R wu, R wv, const R* sS, c
 template <class R>
 __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    if (halted(clk)) return;
+    const bool off = halted(clk);
     using G = TileG<FC_H>;
     __shared__ R tile[Z_NF * G::N];
     __shared__ R sW1[FT_N], sW2[FT_N], sS[FT_N], sC[FT_N];
@@ -630,6 +642,8 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
     R o6[6];
     uvvu_cell(as, wu, wv, sS, sC, ks, o6);   // calcuvvu + uvlatbnd
     // CalcQFlow's fluxes, with the zs2Ocorr update in the interior
+    loads_before_here();
+    if (off) return;
     S.f[QX][i] = (ix > 0 && iy > 0) ? qx + sW1[k] : qx;
     S.f[QY][i] = (ix > 0 && iy > 0) ? qy + sW2[k] : qy;
     S.f[ZS][i] = zf;

@@ -310,6 +310,56 @@ __device__ __forceinline__ void b_means(const Dev<R>& S, const Konst<R>& K, cons
 }
 XBG_KERNELS(means)
 
+// The single-domain running means with 16-byte loads and stores: four float
+// (two double) cells per thread, the clock's halt flag read with the loads
+// and tested before the stores; the last C mod 4 (2) cells by one more
+// thread.  Each field is its own allocation, so every vector is aligned.
+template <class R> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int N = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int N = 2; };
+
+template <class R>
+__global__ void __launch_bounds__(256) k_means_v(Dev<R> S, Konst<R> K) {
+    using VT = typename Vec16<R>::T;
+    constexpr int N = Vec16<R>::N;
+    union U { VT v; R a[N]; };
+    const bool off = halted(S.clk);
+    const int nv = S.C / N;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < nv) {
+        auto L = [&](int f) { U u; u.v = __ldg(reinterpret_cast<const VT*>(S.f[f]) + j); return u; };
+        auto M = [&](int f) { U u; u.v = reinterpret_cast<const VT*>(S.f[f])[j]; return u; };
+        const U zs = L(ZS), hr = L(H), u = L(UU), v = L(VV), h = L(HH), c = L(CSED);
+        U mH = M(HMEAN), mu = M(UUMEAN), mv = M(VVMEAN), mh = M(HHMEAN), mz = M(ZSMEAN), xz = M(ZSMAX),
+          mc = M(CMEAN);
+        loads_before_here();
+        if (off) return;
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            mH.a[k] = mH.a[k] + hr.a[k];
+            mu.a[k] = mu.a[k] + u.a[k];
+            mv.a[k] = mv.a[k] + v.a[k];
+            mh.a[k] = mh.a[k] + h.a[k];
+            mz.a[k] = mz.a[k] + zs.a[k];
+            xz.a[k] = DM<R>::fmax(xz.a[k], zs.a[k]);
+            mc.a[k] = mc.a[k] + c.a[k];
+        }
+        auto W = [&](int f, const U& x) { reinterpret_cast<VT*>(S.f[f])[j] = x.v; };
+        W(HMEAN, mH); W(UUMEAN, mu); W(VVMEAN, mv); W(HHMEAN, mh); W(ZSMEAN, mz); W(ZSMAX, xz); W(CMEAN, mc);
+    } else if (j == nv && !off) {
+        for (int i = nv * N; i < S.C; i++) {
+            const R zs = S.f[ZS][i];
+            S.f[HMEAN][i] += S.f[H][i];
+            S.f[UUMEAN][i] += S.f[UU][i];
+            S.f[VVMEAN][i] += S.f[VV][i];
+            S.f[HHMEAN][i] += S.f[HH][i];
+            S.f[ZSMEAN][i] += zs;
+            S.f[ZSMAX][i] = DM<R>::fmax(S.f[ZSMAX][i], zs);
+            S.f[CMEAN][i] += S.f[CSED][i];
+        }
+    }
+}
+
 template <class R>
 __global__ void k_output_done(Dev<R> S, Konst<R> K) {   // Wave_gpu.cu:786-824
     const Clock& c = *S.clk;
@@ -370,7 +420,9 @@ __global__ void k_mass(Dev<R> S, double dx2, double* out) {
 template <class R>
 int step_begin_blocks(const Konst<R>& K) {
     int nb = (K.nx * K.ny + 255) / 256;
-    return nb < 4 * 148 ? nb : 4 * 148;   // grid-stride: few partials to reduce
+    // grid-stride, eight blocks (2048 threads) per SM: enough loads in flight
+    // to cover the memory latency, and few partials to reduce
+    return nb < 8 * 148 ? nb : 8 * 148;
 }
 
 template <class R>
@@ -402,7 +454,8 @@ int launch_wavebnd(const Dev<R>& S, const Konst<R>& K, const Series* ser, cudaSt
 }
 template <class R>
 int launch_means(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
-    k_means<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, K);
+    const int nthr = S.C / Vec16<R>::N + 1;
+    k_means_v<R><<<(nthr + 255) / 256, 256, 0, st>>>(S, K);
     PMARK(pf, "k_means");
     return 1;
 }

@@ -58,12 +58,14 @@ __device__ void disp_cell(const Konst<R>& K, R sg, R h, R& k_, R& c_, R& cg_) {
 
 template <class R>
 __device__ __forceinline__ void b_disp(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
-    if (wave_off(S.clk)) return;
+    const bool off = wave_off(S.clk);   // tested once the cell's loads are issued (see halted())
     int i = bix * blockDim.x + threadIdx.x;
     if (i >= S.C) return;
-    R sg = (R)S.clk->sigm;
+    const R sg = (R)S.clk->sigm, h = ld(S.f[HH] + i);
+    loads_before_here();
+    if (off) return;
     R k_, c_, cg_;
-    disp_cell(K, sg, ld(S.f[HH] + i), k_, c_, cg_);
+    disp_cell(K, sg, h, k_, c_, cg_);
     S.f[WK][i] = k_;
     S.f[CC_][i] = c_;
     S.f[CG][i] = cg_;
@@ -207,7 +209,7 @@ __device__ __forceinline__ R theta_face(R em, R e0, R ep, R ep2, R c0, R cp) {
     const R cb = (R)0.5f * (c0 + cp);
     const bool p = cb > (R)0;
     const R a = p ? e0 : ep, b = p ? em : ep2;
-    R u = (R)1.5f * a - (R)0.5f * b;
+    R u = DM<R>::fma((R)1.5f, a, DM<R>::mul((R)-0.5f, b));
     u = u < (R)0 ? a : u;
     return cb * u;
 }
@@ -259,6 +261,19 @@ __device__ __forceinline__ R diss_ee(R a, R ridiv, R Dq, R dtf, R& dd) {
     const R eet = DM<R>::fmax(a, (R)0.0f) * ridiv;
     dd = eet * Dq;
     return DM<R>::fmax(eet - dtf * dd, (R)0.0f);
+}
+
+// radstress (wave_CPU.cpp:1123-1162) of one cell from its bin sums: sum2 =
+// sum ee, ec / es / ecs = sum (cos^2, sin^2, sin cos) ee, rc / rs / rcs the
+// same for rr, n = cg / c.  Every product and fused product is written out,
+// so the rounding is the same in every kernel that stores them.
+template <class R>
+__device__ __forceinline__ void radstress(R* sxx, R* sxy, R* syy, int i, R n, R sum2, R ec, R es, R ecs, R rc, R rs,
+                                          R rcs, R dth) {
+    const R half = DM<R>::mul((R)-0.5f, sum2);
+    sxx[i] = DM<R>::fma(DM<R>::fma(n, sum2 + ec, half), dth, DM<R>::mul(rc, dth));
+    syy[i] = DM<R>::fma(DM<R>::fma(n, sum2 + es, half), dth, DM<R>::mul(rs, dth));
+    sxy[i] = DM<R>::fma(DM<R>::mul(n, ecs), dth, DM<R>::mul(rcs, dth));
 }
 
 // Row 0 or ny-1 (iyE), the lateral copy of row iyS = 1 or ny-2
@@ -347,9 +362,7 @@ __device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, 
     S.f[ROL][ie] = RR * dth;
     S.f[DR][ie] = drr * dth;
     const R n = ld(S.f[CG] + ie) / cE;
-    S.tmp[T_SXX][ie] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
-    S.tmp[T_SYY][ie] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
-    S.tmp[T_SXY][ie] = n * ecs * dth + rcs * dth;
+    radstress(S.tmp[T_SXX], S.tmp[T_SXY], S.tmp[T_SYY], ie, n, sum2, ec, es, ecs, rc, rs, rcs, dth);
     return dtw;
 }
 
@@ -619,9 +632,7 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
         S.f[DR][i] = drr * dth;
         const R n = cgi / cc_i;
         // radstress: sum (1 + cos^2) e = sum e + sum cos^2 e, ...
-        S.tmp[T_SXX][i] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
-        S.tmp[T_SYY][i] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
-        S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
+        radstress(S.tmp[T_SXX], S.tmp[T_SXY], S.tmp[T_SYY], i, n, sum2, ec, es, ecs, rc, rs, rcs, dth);
         // the lateral rows 0 and ny-1, from rows 1 and ny-2
         const R sg = (R)clk->sigm;
         // the source cell's final bins: this thread's own stores, read back
@@ -1020,9 +1031,7 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         S.f[ROL][i] = RR * dth;
         S.f[DR][i] = drr * dth;
         const R n = w.cgi / cc_i;
-        S.tmp[T_SXX][i] = (n * (sum2 + ec) - (R)0.5f * sum2) * dth + rc * dth;
-        S.tmp[T_SYY][i] = (n * (sum2 + es) - (R)0.5f * sum2) * dth + rs * dth;
-        S.tmp[T_SXY][i] = n * ecs * dth + rcs * dth;
+        radstress(S.tmp[T_SXX], S.tmp[T_SXY], S.tmp[T_SYY], i, n, sum2, ec, es, ecs, rc, rs, rcs, dth);
     }
     // the block's new bins of rows 1..ny-2 in two box stores
     tm_fence_async();
@@ -1124,6 +1133,8 @@ __device__ __forceinline__ void breaker_raw(const Dev<R>& S, const Konst<R>& K, 
 template <class R>
 __device__ __forceinline__ void b_wave_force(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
+    // tested up front: under a surrogate forcing the pass is skipped, and its
+    // arithmetic is worth more than the flag's round trip
     if (wave_off(clk)) return;
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x;
@@ -1146,14 +1157,14 @@ __device__ __forceinline__ void b_wave_force(const Dev<R>& S, const Konst<R>& K,
     if (rowb) Fx = Fx * w;
     force_raw(S, K, fy_src_x, fy_src_y, tmp, Fy);
     if (anyb) Fy = Fy * w;
-    S.f[FX][i] = Fx;
-    S.f[FY][i] = Fy;
     R urms, ust, u2;
     breaker_raw(S, K, i, Trep, urms, ust);
     if (anyb) {
         breaker_raw(S, K, fy_src_x + fy_src_y * nx, Trep, u2, ust);
         ust = ust * w;
     }
+    S.f[FX][i] = Fx;
+    S.f[FY][i] = Fy;
     S.f[URMS][i] = urms;
     S.f[UST][i] = ust;
 }

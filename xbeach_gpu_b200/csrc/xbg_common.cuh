@@ -44,6 +44,9 @@ template <> struct DM<float> {
     static __device__ __forceinline__ float fmin(float a, float b) { return fminf(a, b); }
     static __device__ __forceinline__ float fmax(float a, float b) { return fmaxf(a, b); }
     static __device__ __forceinline__ float fma(float a, float b, float c) { return fmaf(a, b, c); }
+    // a product the compiler may not fuse into an fma (fixes the rounding of
+    // a*b +- c*d expressions whatever the surrounding code)
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
     static __device__ __forceinline__ float atan(float x) { return atanf(x); }
 };
 template <> struct DM<double> {
@@ -63,6 +66,7 @@ template <> struct DM<double> {
     static __device__ __forceinline__ double fmin(double a, double b) { return ::fmin(a, b); }
     static __device__ __forceinline__ double fmax(double a, double b) { return ::fmax(a, b); }
     static __device__ __forceinline__ double fma(double a, double b, double c) { return ::fma(a, b, c); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
     static __device__ __forceinline__ double atan(double x) { return ::atan(x); }
 };
 
@@ -335,7 +339,12 @@ __device__ __forceinline__ void batch_items(const BatchTab<R>& T, const int2* it
                                         int by) { b_##NAME<R>(S, K, bx, by); });                       \
     }
 
-// Early exit of a kernel in a step that the device clock has halted.
+// Early exit of a kernel in a step that the device clock has halted.  The
+// per-cell passes read the flag with their first loads and test it just
+// before their first store, behind a compiler barrier, so the flag's round
+// trip overlaps the field loads instead of preceding them (a halted step
+// computes and discards; nothing is stored).
+__device__ __forceinline__ void loads_before_here() { asm volatile("" ::: "memory"); }
 __device__ __forceinline__ bool halted(const Clock* c) {
     return *((volatile const int*)&c->halt) != 0;
 }

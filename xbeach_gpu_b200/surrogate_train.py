@@ -195,6 +195,75 @@ def pushforward_data(net, norm, scen, warm=150, steps=200, k=10, judge_every=20,
     return d
 
 
+def collect_chain(scen, warm=150, k=10, links=8, crop=96, crops_per=4, seed=0):
+    """Consecutive snapshots k steps apart of a plain batched run, in fixed
+    windows (crops_per per scenario, around the shoreline as in
+    collect_batch): x [links + 1, W, crop, crop, IN_CH] with the held wave
+    fields at each snapshot in its last channels.  Snapshot j + 1's held
+    fields are snapshot j's target, so a chain gives the plain pairs and,
+    with the network's own predictions in place of the held fields, the
+    push-forward pairs (pushforward_pairs)."""
+    b = storm_batch(scen, warm)
+    rng = np.random.default_rng(seed)
+    wins = []
+    for s, (p, _, _) in enumerate(scen):
+        for _c in range(crops_per):
+            lo = max(0, int(0.55 * p.nx) - crop // 2)
+            hi = max(lo, min(p.nx - crop, int(0.85 * p.nx) - crop // 2))
+            wins.append((s, int(rng.integers(0, p.ny - crop + 1)), int(rng.integers(lo, hi + 1))))
+    xs = []
+    for j in range(links + 1):
+        t = b.status()["t"]
+        cache = {}
+        snap = []
+        for s, y0, x0 in wins:
+            if s not in cache:
+                p, zb, bnd = scen[s]
+                m = b.scenario(s)
+                hs_, tp_ = bnd["storm"](float(t[s]))
+                fin = np.stack([m.get(f).reshape(p.ny, p.nx) for f in IN_FIELDS] +
+                               [np.full((p.ny, p.nx), hs_, np.float32), np.full((p.ny, p.nx), tp_, np.float32)], -1)
+                hold = np.stack([m.get(f).reshape(p.ny, p.nx) for f in OUT_FIELDS], -1)
+                z = np.zeros((p.ny, p.nx, IN_CH - len(IN_FIELDS) - 2 - OUT_CH), np.float32)
+                cache[s] = np.concatenate([fin, hold, z], -1).astype(np.float32)
+            snap.append(cache[s][y0:y0 + crop, x0:x0 + crop])
+        xs.append(np.stack(snap))
+        if j < links:
+            b.advance(k)
+    b.close()
+    return np.stack(xs)
+
+
+def pushforward_pairs(net, norm, chain):
+    """Training pairs whose held wave fields are the network's own
+    prediction (the push-forward trick against chained drift): for each link
+    j of a chain, the prediction from snapshot j replaces the held fields
+    (and the wave-energy input) of snapshot j + 1, whose target stays the
+    plain fields at snapshot j + 2."""
+    h0 = len(IN_FIELDS) + 2
+    ie = IN_FIELDS.index("E")
+    xs, ys, hs = [], [], []
+    for j in range(chain.shape[0] - 2):
+        x = chain[j]
+        pred = predict(net, norm, x, x[..., h0:h0 + OUT_CH])
+        xn = chain[j + 1].copy()
+        xn[..., h0:h0 + OUT_CH] = pred
+        xn[..., ie] = pred[..., OUT_FIELDS.index("E")]
+        xs.append(xn)
+        ys.append(chain[j + 2][..., h0:h0 + OUT_CH])
+        hs.append(pred.astype(np.float32))
+    return dict(x=np.concatenate(xs).astype(np.float32), y=np.concatenate(ys).astype(np.float32),
+                hold=np.concatenate(hs))
+
+
+def chain_pairs(chain):
+    """The plain pairs of a chain: snapshot j's inputs, snapshot j + 1's
+    held fields as the target."""
+    h0 = len(IN_FIELDS) + 2
+    return dict(x=np.concatenate(chain[:-1]), y=np.concatenate([c[..., h0:h0 + OUT_CH] for c in chain[1:]]),
+                hold=np.concatenate([c[..., h0:h0 + OUT_CH] for c in chain[:-1]]))
+
+
 def merge(*ds):
     """One training set from several of the same crop size."""
     return {k: np.concatenate([d[k] for d in ds]) for k in ("x", "y", "hold")}
