@@ -85,7 +85,7 @@ def test_batch_grid_choice_does_not_change_results(tmp_path):
     sc = _cases(4, 21)
     from xbeach_gpu_b200.abi import XBG_PHASE_FLOW, XBG_PHASE_WAVE
     runs = []
-    for variant in ("default", "tuned", "thread_tiles", "two_cells", "split_flow"):
+    for variant in ("default", "tuned", "thread_tiles", "two_cells", "other_flow_split"):
         b = Batch([p for p, _, _ in sc], XBG_FP32)
         for s, (p, zb, bnd) in enumerate(sc):
             _setup(b.scenario(s), p, zb, bnd)
@@ -99,9 +99,10 @@ def test_batch_grid_choice_does_not_change_results(tmp_path):
         if variant == "two_cells":
             b.set_variant(XBG_PHASE_WAVE, 2)
             assert b.variant(XBG_PHASE_WAVE) == 2
-        if variant == "split_flow":
-            b.set_variant(XBG_PHASE_FLOW, 0)
-            assert b.variant(XBG_PHASE_FLOW) == 0
+        if variant == "other_flow_split":
+            f = 1 - b.variant(XBG_PHASE_FLOW)
+            b.set_variant(XBG_PHASE_FLOW, f)
+            assert b.variant(XBG_PHASE_FLOW) == f
         b.advance(25)
         runs.append({s: {f: b.scenario(s).get(f).copy() for f in ("zs", "uu", "H", "ee")} for s in range(len(sc))})
         if variant == "tuned":
