@@ -343,19 +343,15 @@ __device__ __forceinline__ void wrk_u(const A& a, const Konst<R>& K, int ix, int
     const R eps2 = K.eps * (R)2.0f;
     w1 = (R)0.0f; w2 = (R)0.0f;
     if (ix > 0) {
-        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, -2, 0), a(C_ZS, -1, 0)), a(C_ZS, 0, 0)), a(C_ZS, 1, 0)), a(C_ZS, 2, 0));
-        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, -2, 0), a(C_ZB, -1, 0)), a(C_ZB, 0, 0)), a(C_ZB, 1, 0)), a(C_ZB, 2, 0));
-        if (minzs + minzb > eps2) {
+        const Pair2<R> m1 = zz_min<R>(a, -2, 2, 0, 0);   // zs, zb over x-2 .. x+2
+        if (m1.a + m1.b > eps2) {
             R qs = a(C_QX, 0, 0) + a(C_QX, -1, 0);
             if (qs > (R)0.0f) w1 = (R)0.5f * minmod(a(C_UU, 0, 0) - a(C_UO, -1, 0), a(C_UU, -1, 0) - a(C_UO, -2, 0));
             if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(a(C_UO, 0, 0) - a(C_UU, -1, 0), a(C_UO, 1, 0) - a(C_UU, 0, 0));
         }
         if (iy > 0) {
-            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, 0, 0), a(C_ZS, 0, -1)), a(C_ZS, 0, 1)), a(C_ZS, 0, 2));
-            mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, 1, 0), a(C_ZS, 1, -1)), a(C_ZS, 1, 1)), a(C_ZS, 1, 2)));
-            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, 0, 0), a(C_ZB, 0, -1)), a(C_ZB, 0, 1)), a(C_ZB, 0, 2));
-            mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, 1, 0), a(C_ZB, 1, -1)), a(C_ZB, 1, 1)), a(C_ZB, 1, 2)));
-            if (mzs + mzb > eps2) {
+            const Pair2<R> m2 = zz_min<R>(a, 0, 1, -1, 2);   // x, x+1 over y-1 .. y+2
+            if (m2.a + m2.b > eps2) {
                 R qs = a(C_QY, 1, 0) + a(C_QY, 0, 0);
                 if (qs > (R)0.0f) w2 = (R)0.5f * minmod(a(C_UU, 0, 1) - a(C_UO, 0, 0), a(C_UU, 0, 0) - a(C_UO, 0, -1));
                 if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(a(C_UO, 0, 1) - a(C_UU, 0, 0), a(C_UO, 0, 2) - a(C_UU, 0, 1));
@@ -370,18 +366,14 @@ __device__ __forceinline__ void wrk_v(const A& a, const Konst<R>& K, int ix, int
     const R eps2 = K.eps * (R)2.0f;
     w1 = (R)0.0f; w2 = (R)0.0f;
     if (ix > 0 && iy > 0 && iy < K.ny - 2) {
-        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, 0, -2), a(C_ZS, 0, -1)), a(C_ZS, 0, 0)), a(C_ZS, 0, 1)), a(C_ZS, 0, 2));
-        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, 0, -2), a(C_ZB, 0, -1)), a(C_ZB, 0, 0)), a(C_ZB, 0, 1)), a(C_ZB, 0, 2));
-        if (minzs + minzb > eps2) {
+        const Pair2<R> m1 = zz_min<R>(a, 0, 0, -2, 2);   // y-2 .. y+2
+        if (m1.a + m1.b > eps2) {
             R qs = a(C_QY, 0, 0) + a(C_QY, 0, -1);
             if (qs > (R)0.0f) w1 = (R)0.5f * minmod(a(C_VV, 0, 0) - a(C_VO, 0, -1), a(C_VV, 0, -1) - a(C_VO, 0, -2));
             if (qs < (R)0.0f) w1 = (R)-0.5f * minmod(a(C_VO, 0, 0) - a(C_VV, 0, -1), a(C_VO, 0, 1) - a(C_VV, 0, 0));
         }
-        R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, -1, 0), a(C_ZS, 0, 0)), a(C_ZS, 1, 0)), a(C_ZS, 2, 0));
-        mzs = DM<R>::fmin(mzs, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZS, -1, 1), a(C_ZS, 0, 1)), a(C_ZS, 1, 1)), a(C_ZS, 2, 1)));
-        R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, -1, 0), a(C_ZB, 0, 0)), a(C_ZB, 1, 0)), a(C_ZB, 2, 0));
-        mzb = DM<R>::fmin(mzb, DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(C_ZB, -1, 1), a(C_ZB, 0, 1)), a(C_ZB, 1, 1)), a(C_ZB, 2, 1)));
-        if (mzs + mzb > eps2) {
+        const Pair2<R> m2 = zz_min<R>(a, -1, 2, 0, 1);   // x-1 .. x+2 over y, y+1
+        if (m2.a + m2.b > eps2) {
             R qs = a(C_QX, 0, 1) + a(C_QX, 0, 0);
             if (qs > (R)0.0f) w2 = (R)0.5f * minmod(a(C_VV, 1, 0) - a(C_VO, 0, 0), a(C_VV, 0, 0) - a(C_VO, -1, 0));
             if (qs < (R)0.0f) w2 = (R)-0.5f * minmod(a(C_VO, 1, 0) - a(C_VV, 0, 0), a(C_VO, 2, 0) - a(C_VV, 1, 0));
@@ -403,7 +395,7 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
     const Clock* clk = S.clk;
     const bool off = halted(clk);
     using G = TileG<FC_H>;
-    __shared__ R tile[C_NF * G::N];
+    __shared__ __align__(16) R tile[C_NF * G::N];   // (level, bed) pairs, then planes
     __shared__ R sU1[FT_N], sU2[FT_N], sV1[FT_N], sV2[FT_N];
     const int nx = K.nx, ny = K.ny;
     const int bx0 = bix * FT_X, by0 = biy * FT_Y;
@@ -523,17 +515,15 @@ __device__ __forceinline__ void wrk_z(const A& a, const Konst<R>& K, int ix, int
     const R eps2 = K.eps * (R)2.0f;
     w1 = (R)0.0f; w2 = (R)0.0f;
     if (ix > 0) {
-        R minzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZS, -1, 0), a(Z_ZS, 0, 0)), a(Z_ZS, 1, 0)), a(Z_ZS, 2, 0));
-        R minzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZB, -1, 0), a(Z_ZB, 0, 0)), a(Z_ZB, 1, 0)), a(Z_ZB, 2, 0));
-        if (minzs + minzb > eps2) {
+        const Pair2<R> m1 = zz_min<R>(a, -1, 2, 0, 0);   // x-1 .. x+2
+        if (m1.a + m1.b > eps2) {
             R u = a(Z_UU, 0, 0);
             if (u > (R)0.0f) w1 = u * (R)0.5f * minmod(a(Z_ZS, 1, 0) - a(Z_ZO, 0, 0), a(Z_ZS, 0, 0) - a(Z_ZO, -1, 0));
             if (u < (R)0.0f) w1 = (R)-1.0f * u * (R)0.5f * minmod(a(Z_ZO, 2, 0) - a(Z_ZS, 1, 0), a(Z_ZO, 1, 0) - a(Z_ZS, 0, 0));
         }
         if (iy > 0) {
-            R mzs = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZS, 0, -1), a(Z_ZS, 0, 0)), a(Z_ZS, 0, 1)), a(Z_ZS, 0, 2));
-            R mzb = DM<R>::fmin(DM<R>::fmin(DM<R>::fmin(a(Z_ZB, 0, -1), a(Z_ZB, 0, 0)), a(Z_ZB, 0, 1)), a(Z_ZB, 0, 2));
-            if (mzs + mzb > eps2) {
+            const Pair2<R> m2 = zz_min<R>(a, 0, 0, -1, 2);   // y-1 .. y+2
+            if (m2.a + m2.b > eps2) {
                 R v = a(Z_VV, 0, 0);
                 if (v > (R)0.0f) w2 = v * (R)0.5f * minmod(a(Z_ZS, 0, 1) - a(Z_ZO, 0, 0), a(Z_ZS, 0, 0) - a(Z_ZO, 0, -1));
                 if (v < (R)0.0f) w2 = v * (R)0.5f * minmod(a(Z_ZO, 0, 2) - a(Z_ZS, 0, 1), a(Z_ZO, 0, 1) - a(Z_ZS, 0, 0));
@@ -592,7 +582,7 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
     const Clock* clk = S.clk;
     const bool off = halted(clk);
     using G = TileG<FC_H>;
-    __shared__ R tile[Z_NF * G::N];
+    __shared__ __align__(16) R tile[Z_NF * G::N];   // (level, bed) pairs, then planes
     __shared__ R sW1[FT_N], sW2[FT_N], sS[FT_N], sC[FT_N];
     const R* zsold_in = S.zsold[clk->par ^ 1];
     R* zsold_out = S.zsold[clk->par];

@@ -23,7 +23,7 @@ __device__ __forceinline__ bool sed_skip(const Clock* c) {
 template <class R>
 __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    const bool off = sed_skip(clk);   // tested before the first store (see halted())
+    if (sed_skip(clk)) return;
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
     if (ix >= nx || iy >= ny) return;
@@ -88,8 +88,6 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
         R exp_ero = K.morfac * dtf / ((R)1.0f - K.por) * hh * (ceqsg * (R)1.0f / Tsg + ceqbg * (R)1.0f / dtf);
         R facero = DM<R>::fmin((R)1.0f, ld(S.f[STDEP] + i) * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
         // all stores after all loads (the field pointers may alias as far as the compiler knows)
-        loads_before_here();
-        if (off) return;
         S.f[ROLTHICK][i] = rolth;
         S.f[KTURB][i] = (R)0.0f;
         S.f[CEQSG][i] = ceqsg;
@@ -180,6 +178,7 @@ constexpr int SB_X = 32, SB_Y = 8, SB_TX = SB_X + 1, SB_TY = SB_Y + 1;
 template <class R>
 __device__ __forceinline__ void b_sed_b(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
+    // tested once the block's loads are in flight (see halted())
     const bool off = sed_skip(clk);
     __shared__ R sSus[SB_TY * SB_TX], sSvs[SB_TY * SB_TX];
     const int nx = K.nx, ny = K.ny;
@@ -222,26 +221,24 @@ __device__ __forceinline__ void b_sed_b(const Dev<R>& S, const Konst<R>& K, cons
 XBG_KERNELS(sed_b)
 
 // zblatbnd source cell (Sediment_kernel.cu:970-1018, pre-kernel reads)
-__device__ __forceinline__ void zbl_src_xy(int ix, int iy, int nx, int ny, int& sx, int& sy) {
-    sx = ix; sy = iy;
+__device__ __forceinline__ int zbl_src(int ix, int iy, int nx, int ny) {
+    int sx = ix, sy = iy;
     if (iy == 0) sy = pp(iy, ny);
     if (iy == ny - 1) sy = mm(iy);
     if (ix == 0) { sx = pp(ix, nx); sy = iy; }
-}
-__device__ __forceinline__ int zbl_src(int ix, int iy, int nx, int ny) {
-    int sx, sy;
-    zbl_src_xy(ix, iy, nx, ny, sx, sy);
     return sx + sy * nx;
 }
 
-// avalanching (Sediment_kernel.cu:1020-1137) transfers (dzbx, dzby) of a cell
-// from its bed and sediment thickness (i: the cell, t: the one above, r: the
-// one to its right, all read at their zblatbnd sources) and its depth
+// avalanching (Sediment_kernel.cu:1020-1137) transfers (dzbx, dzby) of (ix, iy)
 template <class R>
-__device__ __forceinline__ void aval_from(const Konst<R>& K, R Zbi, R Zbt, R Zbr, R sti, R stt, R str, R hh, R dtf,
-                                          R& dzbx, R& dzby) {
+__device__ __forceinline__ void aval_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R& dzbx, R& dzby) {
+    const int nx = K.nx, ny = K.ny;
+    const R* zb = S.tmp[T_ZB]; const R* sd = S.tmp[T_STDEP];
+    int xp = pp(ix, nx), yp = pp(iy, ny);
+    R Zbi = ld(zb + zbl_src(ix, iy, nx, ny)), Zbt = ld(zb + zbl_src(ix, yp, nx, ny)), Zbr = ld(zb + zbl_src(xp, iy, nx, ny));
+    R sti = ld(sd + zbl_src(ix, iy, nx, ny)), stt = ld(sd + zbl_src(ix, yp, nx, ny)), str = ld(sd + zbl_src(xp, iy, nx, ny));
     R dx = K.dx, maxchg = K.maxslpchg;
-    R dzmax = hh > K.eps ? K.wetdzmax : K.drydzmax;
+    R dzmax = ld(S.tmp[T_HH] + IDX(ix, iy)) > K.eps ? K.wetdzmax : K.drydzmax;
     dzbx = (R)0.0f; dzby = (R)0.0f;
     R dzbdx = (Zbr - Zbi) / dx;
     if (DM<R>::fabs(dzbdx) > dzmax) {
@@ -269,17 +266,6 @@ __device__ __forceinline__ void aval_from(const Konst<R>& K, R Zbi, R Zbt, R Zbr
     }
 }
 
-// the transfers of (ix, iy) from global memory
-template <class R>
-__device__ __forceinline__ void aval_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy, R dtf, R& dzbx, R& dzby) {
-    const int nx = K.nx, ny = K.ny;
-    const R* zb = S.tmp[T_ZB]; const R* sd = S.tmp[T_STDEP];
-    int xp = pp(ix, nx), yp = pp(iy, ny);
-    const int ji = zbl_src(ix, iy, nx, ny), jt = zbl_src(ix, yp, nx, ny), jr = zbl_src(xp, iy, nx, ny);
-    aval_from(K, ld(zb + ji), ld(zb + jt), ld(zb + jr), ld(sd + ji), ld(sd + jt), ld(sd + jr),
-              ld(S.tmp[T_HH] + IDX(ix, iy)), dtf, dzbx, dzby);
-}
-
 // bed change of (ix, iy) gathered from its own and its neighbours' transfers,
 // in the order a serial launch adds them: ((-dzby[below] - dzbx[left]) + dzbx) + dzby
 template <class R>
@@ -293,62 +279,33 @@ __device__ __forceinline__ R ddzb_cell(const Dev<R>& S, const Konst<R>& K, int i
     return a;
 }
 
-// zblatbnd, avalanching, updatezb, zblatbnd, updatezom.  The block stages
-// the post-bedupdate bed and sediment thickness (each read at its zblatbnd
-// source) and depth over its 32 x 8 tile plus a one-cell ring (34 x 10) in
-// shared memory; the transfers (dzbx, dzby) of every cell of the tile, the
-// column to its left and the row below it follow from there, once each.  A
-// boundary cell whose zblatbnd source lies elsewhere evaluates that source's
-// bed change from global memory.  Every tile position is addressed by a
-// clamped grid cell, so positions outside the grid are never read.
-constexpr int SC_TX = SB_X + 2, SC_TY = SB_Y + 2;
-
+// zblatbnd, avalanching, updatezb, zblatbnd, updatezom.  The transfers
+// (dzbx, dzby) of every cell of the 32 x 8 tile, the column to its left and
+// the row below it go to shared memory once; a boundary cell whose zblatbnd
+// source lies elsewhere evaluates that source's bed change directly.
 template <class R>
 __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    const bool off = sed_skip(clk);
-    __shared__ R tZ[SC_TY * SC_TX], tS[SC_TY * SC_TX], tH[SC_TY * SC_TX];
+    if (sed_skip(clk)) return;
     __shared__ R sBx[SB_TY * SB_TX], sBy[SB_TY * SB_TX];
     const int nx = K.nx, ny = K.ny;
     const int bx0 = bix * SB_X, by0 = biy * SB_Y;
     const bool morph = K.morfac > (R)0.0f;
     const R dtf = (R)clk->dt;
-    const int tid = threadIdx.x + threadIdx.y * SB_X;
-    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    const bool inside = ix < nx && iy < ny;
-    const int i = IDX(ix, iy);
-    // the own cell's fields, loaded with the tile
-    R cnew = (R)0, dzb0 = (R)0, zs0 = (R)0;
-    if (inside) {
-        cnew = ld(S.tmp[T_UU] + i);
-        if (morph) { dzb0 = ld(S.f[DZB] + i); zs0 = ld(S.f[ZS] + i); }
-    }
-    auto pos = [&](int x, int y) { return (x - bx0 + 1) + (y - by0 + 1) * SC_TX; };
     if (morph) {
-        for (int e = tid; e < SC_TY * SC_TX; e += SB_X * SB_Y) {
-            const int x = bx0 - 1 + e % SC_TX, y = by0 - 1 + e / SC_TX;
-            if (x >= 0 && x < nx && y >= 0 && y < ny) {
-                const int j = zbl_src(x, y, nx, ny);
-                tZ[e] = ld(S.tmp[T_ZB] + j);
-                tS[e] = ld(S.tmp[T_STDEP] + j);
-                tH[e] = ld(S.tmp[T_HH] + IDX(x, y));
-            }
-        }
-        __syncthreads();
-        for (int e = tid; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
-            const int gx = min(max(bx0 - 1 + e % SB_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / SB_TX, 0), ny - 1);
-            const int xp = pp(gx, nx), yp = pp(gy, ny);
-            const int pi = pos(gx, gy), pt = pos(gx, yp), pr = pos(xp, gy);
+        for (int e = threadIdx.x + threadIdx.y * SB_X; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
+            int gx = min(max(bx0 - 1 + e % SB_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / SB_TX, 0), ny - 1);
             R a, b;
-            aval_from(K, tZ[pi], tZ[pt], tZ[pr], tS[pi], tS[pt], tS[pr], tH[pi], dtf, a, b);
+            aval_cell(S, K, gx, gy, dtf, a, b);
             sBx[e] = a;
             sBy[e] = b;
         }
     }
     __syncthreads();
-    loads_before_here();
-    if (off || !inside) return;
-    S.f[CSED][i] = cnew;
+    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy);
+    S.f[CSED][i] = ld(S.tmp[T_UU] + i);
     if (morph) {
         // bed change gathered in the serial launch order:
         // ((-dzby[below] - dzbx[left]) + dzbx) + dzby
@@ -359,17 +316,16 @@ __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, cons
         dd = dd + sBx[c];
         dd = dd + sBy[c];
         // updatezb (:1139-1160) at the own cell
-        S.f[DZB][i] = dzb0 - dd;
-        S.f[ZS][i] = zs0 - dd;
-        S.f[HH][i] = tH[pos(ix, iy)] - dd;
-        // zb, stdep: updatezb at the zblatbnd source, then the copy; the
-        // source's source is a neighbour, inside the staged tile
-        int sx, sy;
-        zbl_src_xy(ix, iy, nx, ny, sx, sy);
-        const R ds = (sx == ix && sy == iy) ? dd : ddzb_cell(S, K, sx, sy, dtf);
-        const int p1 = pos(sx, sy);
-        const R zbn = tZ[p1] + ds;
-        const R sdn = tS[p1] - ds;
+        S.f[DZB][i] = ld(S.f[DZB] + i) - dd;
+        S.f[ZS][i] = ld(S.f[ZS] + i) - dd;
+        S.f[HH][i] = ld(S.tmp[T_HH] + i) - dd;
+        // zb, stdep: updatezb at the zblatbnd source, then the copy
+        int s = zbl_src(ix, iy, nx, ny);
+        int sx = s % nx, sy = s / nx;
+        R ds = (s == i) ? dd : ddzb_cell(S, K, sx, sy, dtf);
+        int s1 = zbl_src(sx, sy, nx, ny);
+        R zbn = ld(S.tmp[T_ZB] + s1) + ds;
+        R sdn = ld(S.tmp[T_STDEP] + s1) - ds;
         S.f[ZB][i] = zbn;
         S.f[STDEP][i] = sdn;
         // updatezom (:1162-1190)

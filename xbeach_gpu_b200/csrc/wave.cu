@@ -1133,8 +1133,6 @@ __device__ __forceinline__ void breaker_raw(const Dev<R>& S, const Konst<R>& K, 
 template <class R>
 __device__ __forceinline__ void b_wave_force(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
     const Clock* clk = S.clk;
-    // tested up front: under a surrogate forcing the pass is skipped, and its
-    // arithmetic is worth more than the flag's round trip
     if (wave_off(clk)) return;
     const int nx = K.nx, ny = K.ny;
     int ix = bix * blockDim.x + threadIdx.x;
@@ -1157,14 +1155,14 @@ __device__ __forceinline__ void b_wave_force(const Dev<R>& S, const Konst<R>& K,
     if (rowb) Fx = Fx * w;
     force_raw(S, K, fy_src_x, fy_src_y, tmp, Fy);
     if (anyb) Fy = Fy * w;
+    S.f[FX][i] = Fx;
+    S.f[FY][i] = Fy;
     R urms, ust, u2;
     breaker_raw(S, K, i, Trep, urms, ust);
     if (anyb) {
         breaker_raw(S, K, fy_src_x + fy_src_y * nx, Trep, u2, ust);
         ust = ust * w;
     }
-    S.f[FX][i] = Fx;
-    S.f[FY][i] = Fy;
     S.f[URMS][i] = urms;
     S.f[UST][i] = ust;
 }

@@ -209,8 +209,11 @@ struct TileG {
     static constexpr int X = 32, Y = 8, TX = X + 2 * H, TY = Y + 2 * H, N = TX * TY;
 };
 
-// Copy NF fields over the tile into t[f * N + e] (cp.async), then wait and
-// synchronise the block.
+// Copy NF fields over the tile (cp.async), then wait and synchronise the
+// block.  Fields 0 and 1 (the water level and the bed in every staged pass,
+// read together by the wet tests) are interleaved, t[2 e + f], so a tile
+// cell's pair is one 8-byte (16-byte) shared-memory load; field f >= 2 is
+// the plane t[f * N + e].
 template <class R, int H, int NF>
 __device__ __forceinline__ void tile_load(R* t, const R* const (&src)[NF], int bx0, int by0, int nx, int ny) {
     using G = TileG<H>;
@@ -218,13 +221,47 @@ __device__ __forceinline__ void tile_load(R* t, const R* const (&src)[NF], int b
     for (int e = tid; e < G::N; e += G::X * G::Y) {
         int gx = min(max(bx0 - H + e % G::TX, 0), nx - 1), gy = min(max(by0 - H + e / G::TX, 0), ny - 1);
         size_t g = (size_t)gx + (size_t)gy * nx;
+        cp_async<sizeof(R)>(t + 2 * e, src[0] + g);
+        cp_async<sizeof(R)>(t + 2 * e + 1, src[1] + g);
 #pragma unroll
-        for (int f = 0; f < NF; f++) cp_async<sizeof(R)>(t + f * G::N + e, src[f] + g);
+        for (int f = 2; f < NF; f++) cp_async<sizeof(R)>(t + f * G::N + e, src[f] + g);
     }
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
 }
+// L2 prefetch, by the block's first warp, of the rows by0-1 .. by0+8 and
+// columns bx0-4 .. bx0+35 of the listed planes for the 32 x 8 tile `tile`
+// (row-major tile index over tiles_x tiles per row): one
+// cp.async.bulk.prefetch per plane and row.  A block issues it for the tile
+// that a block about one wave of the grid later will take, so that block's
+// loads find its fields in L2.  Needs 16-byte aligned rows (nx * sizeof(T) a
+// multiple of 16; otherwise nothing is issued); no effect on results.
+template <int NP>
+__device__ __forceinline__ void prefetch_tile_l2(const void* const (&planes)[NP], const int (&esize)[NP], int tile,
+                                                 int tiles_x, int tiles, int nx, int ny) {
+    if (threadIdx.y != 0 || tile >= tiles) return;
+    const int bx0 = (tile % tiles_x) * 32, by0 = (tile / tiles_x) * 8;
+    const int y0 = max(by0 - 1, 0), y1 = min(by0 + 9, ny);
+    const int rows = y1 - y0;
+    if ((int)threadIdx.x >= rows) return;
+    const int y = y0 + threadIdx.x;
+#pragma unroll
+    for (int p = 0; p < NP; p++) {   // unrolled: the plane lists stay in registers
+        const int es = esize[p];
+        if ((nx * es) % 16) continue;
+        const int al = 16 / es;
+        const int x0 = max(bx0 - 4, 0) / al * al, x1 = min((bx0 + 36 + al - 1) / al * al, nx);
+        const char* a = (const char*)planes[p] + ((size_t)y * nx + x0) * es;
+        const unsigned bytes = (unsigned)((x1 - x0) * es);
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"(bytes) : "memory");
+    }
+}
+// the tiles one wave of a 32 x 8 grid later: SMs x blocks per SM
+constexpr int PREFETCH_AHEAD = 148 * 6;
+
+template <class R> struct Pair2 { R a, b; };
+template <class R> struct alignas(2 * sizeof(R)) Pair2A { R a, b; };
 
 // Tile index of the cell that tile position (kx, ky) stands for (the grid
 // clamped), and that cell's grid coordinates.
@@ -239,12 +276,18 @@ __device__ __forceinline__ int tile_centre(int kx, int ky, int bx0, int by0, int
 
 // Field access around one cell: a(f, dx, dy) = field f at
 // (clamp(ix + dx), clamp(iy + dy)), from the shared-memory tile ...
+// zz(dx, dy): fields 0 and 1 there together.
 template <class R, int H>
 struct TileAt {
     const R* t;
     int k;
     __device__ __forceinline__ R operator()(int f, int dx, int dy) const {
-        return t[f * TileG<H>::N + k + dx + dy * TileG<H>::TX];
+        const int p = k + dx + dy * TileG<H>::TX;
+        return f < 2 ? t[2 * p + f] : t[f * TileG<H>::N + p];
+    }
+    __device__ __forceinline__ Pair2<R> zz(int dx, int dy) const {
+        const Pair2A<R> v = reinterpret_cast<const Pair2A<R>*>(t)[k + dx + dy * TileG<H>::TX];
+        return Pair2<R>{v.a, v.b};
     }
 };
 // ... or from global memory.
@@ -256,7 +299,23 @@ struct GlobalAt {
         int x = min(max(ix + dx, 0), nx - 1), y = min(max(iy + dy, 0), ny - 1);
         return __ldg(p[f] + x + (size_t)y * nx);
     }
+    __device__ __forceinline__ Pair2<R> zz(int dx, int dy) const {
+        return Pair2<R>{(*this)(0, dx, dy), (*this)(1, dx, dy)};
+    }
 };
+// Minima of fields 0 and 1 (level and bed) over the window x in [x0, x1],
+// y in [y0, y1] around a cell, one pair load per window cell.
+template <class R, class A>
+__device__ __forceinline__ Pair2<R> zz_min(const A& a, int x0, int x1, int y0, int y1) {
+    Pair2<R> m = a.zz(x0, y0);
+    for (int dy = y0; dy <= y1; dy++)
+        for (int dx = (dy == y0 ? x0 + 1 : x0); dx <= x1; dx++) {
+            const Pair2<R> v = a.zz(dx, dy);
+            m.a = DM<R>::fmin(m.a, v.a);
+            m.b = DM<R>::fmin(m.b, v.b);
+        }
+    return m;
+}
 
 // ---------------------------------------------------------------- batches
 // A batch advances many scenarios (each with its own grid, parameters, clock
@@ -328,22 +387,39 @@ __device__ __forceinline__ void batch_items(const BatchTab<R>& T, const int2* it
 }
 
 // Single-domain and batched kernels of a 256-thread body b_NAME(S, K, bx, by).
-#define XBG_KERNELS(NAME)                                                                              \
-    template <class R>                                                                                 \
-    __global__ void __launch_bounds__(256) k_##NAME(Dev<R> S, Konst<R> K) {                            \
-        b_##NAME<R>(S, K, blockIdx.x, blockIdx.y);                                                     \
-    }                                                                                                  \
+#define XBG_BATCH_KERNEL(NAME)                                                                         \
     template <class R>                                                                                 \
     __global__ void __launch_bounds__(256) kb_##NAME(BatchTab<R> T, const int2* items, int n) {        \
         batch_items<R>(T, items, n, [&](const Dev<R>& S, const Konst<R>& K, const BatchAux&, int bx,   \
                                         int by) { b_##NAME<R>(S, K, bx, by); });                       \
     }
+#define XBG_KERNELS(NAME)                                                                              \
+    template <class R>                                                                                 \
+    __global__ void __launch_bounds__(256) k_##NAME(Dev<R> S, Konst<R> K) {                            \
+        b_##NAME<R>(S, K, blockIdx.x, blockIdx.y);                                                     \
+    }                                                                                                  \
+    XBG_BATCH_KERNEL(NAME)
+// As XBG_KERNELS, the single-domain kernel also prefetching into L2 the
+// listed planes (P: an initializer list of plane pointers, E: their element
+// sizes) of the tile a block one wave later will take.
+#define XBG_KERNELS_PREFETCH(NAME, P, E)                                                               \
+    template <class R>                                                                                 \
+    __global__ void __launch_bounds__(256) k_##NAME(Dev<R> S, Konst<R> K) {                            \
+        const void* const pl[] = P;                                                                    \
+        const int es[] = E;                                                                            \
+        prefetch_tile_l2(pl, es, blockIdx.x + blockIdx.y * gridDim.x + PREFETCH_AHEAD, gridDim.x,      \
+                         gridDim.x * gridDim.y, K.nx, K.ny);                                           \
+        b_##NAME<R>(S, K, blockIdx.x, blockIdx.y);                                                     \
+    }                                                                                                  \
+    XBG_BATCH_KERNEL(NAME)
 
 // Early exit of a kernel in a step that the device clock has halted.  The
-// per-cell passes read the flag with their first loads and test it just
-// before their first store, behind a compiler barrier, so the flag's round
-// trip overlaps the field loads instead of preceding them (a halted step
-// computes and discards; nothing is stored).
+// flow passes, the second sediment pass and the dispersion pass read the
+// flag with their first loads and test it just before their first store,
+// behind a compiler barrier, so the flag's round trip overlaps the field
+// loads instead of preceding them (a halted step computes and discards;
+// nothing is stored).  Where a kernel timed faster testing it up front
+// (the other sediment passes, the wave force pass) it does that.
 __device__ __forceinline__ void loads_before_here() { asm volatile("" ::: "memory"); }
 __device__ __forceinline__ bool halted(const Clock* c) {
     return *((volatile const int*)&c->halt) != 0;
