@@ -703,24 +703,47 @@ def main():
         for name, t in m.profile_step():
             prof.setdefault(name, []).append(t)
     kern = {k: float(np.mean(v)) for k, v in prof.items()}
-    # end to end through the C ABI with host buffers: every step streams the
-    # boundary records it interpolates from pinned host memory and reads the
-    # step's clock (time, dt, status) back to the host
+    # end to end through the C ABI with host buffers: every step uploads the
+    # boundary records around its time (St and qbnd) from pinned host memory
+    # and copies its clock (time, dt, step count, status) back into pinned
+    # host memory (xbg_get_time_async); the host decodes step k's clock while
+    # step k+1 runs, and chooses step k+2's records from it (four records
+    # from the one at that time on bracket the two steps' times), so host and
+    # device work overlap instead of alternating
+    from xbeach_gpu_b200.abi import XBG_CLOCK_BYTES
     nyt = p.ny * p.ntheta
-    recs = torch.empty((2, nyt), dtype=torch.float32, pin_memory=True)
-    qrec = torch.empty((2, 4 * p.ny), dtype=torch.float32, pin_memory=True)
+    NR = 4
+    recs = [torch.empty((NR, nyt), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    qrec = [torch.empty((NR, 4 * p.ny), dtype=torch.float32, pin_memory=True) for _ in range(2)]
+    clkb = [torch.empty(XBG_CLOCK_BYTES, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    evs = [torch.cuda.Event() for _ in range(2)]
     Ke = max(10, K // 4)
+    t_known, _, n_e0, _, _ = m.time()
+    nrec = bnd["St"].shape[0]
+    rc = 0
     t0 = time.perf_counter()
     for k in range(Ke):
-        t_now = m.time()[0]
-        nb = int(t_now // p.dtbc)
-        recs.numpy()[:] = bnd["St"][nb:nb + 2].reshape(2, -1)
-        qrec.numpy()[:] = bnd["q"][nb:nb + 2].reshape(2, -1)
-        m.put_wave_records(0, nb, recs.numpy(), qrec.numpy())
+        b = k % 2
+        if k >= 2:   # step k-2 has finished: its clock is in clkb[b], its buffers are free
+            evs[b].synchronize()
+            t_known, _, _, _, rc = m.time_decode(clkb[b].data_ptr())
+            if rc != 0:
+                break
+        nb = min(int(t_known // p.dtbc), nrec - NR)
+        recs[b].numpy()[:] = bnd["St"][nb:nb + NR].reshape(NR, -1)
+        qrec[b].numpy()[:] = bnd["q"][nb:nb + NR].reshape(NR, -1)
+        m.put_wave_records(0, nb, recs[b].numpy(), qrec[b].numpy())
         m.step()
-    _, _, _, _, rc = m.time()
+        m.time_async(clkb[b].data_ptr())
+        evs[b].record(stream)
+    for k in range(max(0, Ke - 2), Ke):   # the last two steps' clocks
+        evs[k % 2].synchronize()
+        _, _, n_e, _, rck = m.time_decode(clkb[k % 2].data_ptr())
+        rc = rc or rck
     e2e_s = time.perf_counter() - t0
-    h2d = recs.numel() * 4 + qrec.numel() * 4
+    if rc != 0 or n_e != n_e0 + Ke:
+        raise RuntimeError(f"end-to-end steps: status {rc}, {n_e - n_e0} of {Ke} steps")
+    h2d = recs[0].numel() * 4 + qrec[0].numel() * 4
     # the clocks over a longer run of the same replays (>= 250 ms of device
     # work), so the clock record does not rest on the few samples a short
     # timed region allows; the timed region's own samples stay in "clocks"
@@ -734,7 +757,7 @@ def main():
     soak.mark_end()
     clocks_soak = soak.stop()
     clocks_soak["steps"] = n_soak
-    d2h = 240   # the device clock struct read by xbg_get_time (sizeof(Clock))
+    d2h = XBG_CLOCK_BYTES   # the device clock copied back by xbg_get_time_async
     # max over ranks
     if dist:
         (ms, e2e_s), _ = over_ranks(dist, [ms, e2e_s], [C], "cuda")

@@ -178,6 +178,14 @@ int  xbg_advance(xbg_handle* h, int nsteps);
 /* Synchronise and read time, dt, step count and the device status word.  */
 int  xbg_get_time(xbg_handle* h, double* totaltime, double* dt, int64_t* nstep,
                   int* flags);
+/* The same without waiting: copies the device clock (XBG_CLOCK_BYTES
+ * bytes) into dst (pinned host memory) in the handle's stream order; once
+ * the stream has passed the copy, xbg_clock_decode reads it (and returns
+ * the status word) as xbg_get_time would have at that point of the stream. */
+#define XBG_CLOCK_BYTES 240
+int  xbg_get_time_async(xbg_handle* h, void* dst);
+int  xbg_clock_decode(xbg_handle* h, const void* src, double* totaltime, double* dt,
+                      int64_t* nstep, int* flags);
 #define XBG_FLAG_OUTPUT_DUE   1   /* nextoutputtime reached               */
 #define XBG_FLAG_ENDED        2   /* totaltime >= endtime                 */
 #define XBG_FLAG_NEED_BOUNDARY 4  /* next wave-boundary chunk consumed    */

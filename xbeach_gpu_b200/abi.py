@@ -27,6 +27,7 @@ XBG_FP64 = 1
 
 XBG_PHASE_WAVE = 0   # xbg_set_kernel_variant phases
 XBG_PHASE_FLOW = 1
+XBG_CLOCK_BYTES = 240   # xbg_get_time_async copies this many bytes
 
 XBG_FLAG_OUTPUT_DUE = 1
 XBG_FLAG_ENDED = 2

@@ -247,6 +247,8 @@ struct xbg_handle {
     virtual int piece(int which) = 0;
     virtual int step(int nsteps) = 0;
     virtual int get_time(double* t, double* dt, int64_t* n, int* flags) = 0;
+    virtual int get_time_async(void* dst) = 0;
+    virtual int clock_decode(const void* src, double* t, double* dt, int64_t* n, int* flags) = 0;
     virtual int set_time(double t, double dt, double wdt) = 0;
     virtual int output_done() = 0;
     virtual int reset_means() = 0;
@@ -763,6 +765,24 @@ struct Handle : public xbg_handle {
         if (flags) *flags = c.flags;
         return c.status;
     }
+    // the clock copied to host memory in stream order, without waiting
+    int get_time_async(void* dst) override {
+        if (!dst) return XBG_ERR_ARG;
+        CK(cudaMemcpyAsync(dst, clk, sizeof(Clock), cudaMemcpyDeviceToHost, st));
+        return XBG_OK;
+    }
+    int clock_decode(const void* src, double* t, double* dt, int64_t* n, int* flags) override {
+        if (!src) return XBG_ERR_ARG;
+        Clock c;
+        std::memcpy(&c, src, sizeof(c));
+        host_cur_slot = c.cur_slot;   // as a synchronous read would
+        host_par = c.par;
+        if (t) *t = c.totaltime;
+        if (dt) *dt = c.dt;
+        if (n) *n = c.nstep_total;
+        if (flags) *flags = c.flags;
+        return c.status;
+    }
     int set_time(double t, double dt, double wdt) override {
         Clock c;
         int rc = read_clock(c);
@@ -1273,6 +1293,10 @@ int xbg_accumulate_means(xbg_handle* h) { return h ? h->piece(6) : XBG_ERR_ARG; 
 int xbg_step(xbg_handle* h) { return h ? h->step(1) : XBG_ERR_ARG; }
 int xbg_advance(xbg_handle* h, int n) { return h ? h->step(n) : XBG_ERR_ARG; }
 int xbg_get_time(xbg_handle* h, double* t, double* dt, int64_t* n, int* flags) { return h ? h->get_time(t, dt, n, flags) : XBG_ERR_ARG; }
+int xbg_get_time_async(xbg_handle* h, void* dst) { return h ? h->get_time_async(dst) : XBG_ERR_ARG; }
+int xbg_clock_decode(xbg_handle* h, const void* src, double* t, double* dt, int64_t* n, int* flags) {
+    return h ? h->clock_decode(src, t, dt, n, flags) : XBG_ERR_ARG;
+}
 int xbg_output_done(xbg_handle* h) { return h ? h->output_done() : XBG_ERR_ARG; }
 int xbg_reset_means(xbg_handle* h) { return h ? h->reset_means() : XBG_ERR_ARG; }
 int xbg_set_time(xbg_handle* h, double t, double dt, double wdt) { return h ? h->set_time(t, dt, wdt) : XBG_ERR_ARG; }

@@ -214,6 +214,42 @@ __device__ __forceinline__ R theta_face(R em, R e0, R ep, R ep2, R c0, R cp) {
     return cb * u;
 }
 
+// The same arithmetic on (wave energy, roller energy) pairs with the packed
+// FP32 instructions of sm_100 (fma / mul / add .f32x2): each lane rounds as
+// the scalar operation it replaces, so the results are the scalar path's bit
+// for bit, in half the floating-point instructions.  kminn is -kmin, and the
+// Euler update is written with negated factors (exact under round-to-nearest).
+__device__ __forceinline__ float2 upw2(float2 a, float2 b) {
+    float2 v = __ffma2_rn(make_float2(1.5f, 1.5f), a, __fmul2_rn(make_float2(-0.5f, -0.5f), b));
+    v.x = v.x < 0.f ? a.x : v.x;
+    v.y = v.y < 0.f ? a.y : v.y;
+    return v;
+}
+template <bool POS>
+__device__ __forceinline__ float2 flux2k2(const float* qE, const float* qR, int s, float2 qi, float2 kin,
+                                          float2 kminn) {
+    float2 ain, amin;
+    if (POS) {
+        const float2 qm = make_float2(qE[-s], qR[-s]);
+        ain = upw2(qi, qm);
+        amin = upw2(qm, make_float2(qE[-2 * s], qR[-2 * s]));
+    } else {
+        const float2 qp = make_float2(qE[s], qR[s]);
+        ain = upw2(qp, make_float2(qE[2 * s], qR[2 * s]));
+        amin = upw2(qi, qp);
+    }
+    return __ffma2_rn(ain, kin, __fmul2_rn(amin, kminn));
+}
+__device__ __forceinline__ float2 theta_face2(float2 em, float2 e0, float2 ep, float2 ep2, float c0, float cp) {
+    const float cb = 0.5f * (c0 + cp);
+    const bool p = cb > 0.f;
+    const float2 a = p ? e0 : ep, b = p ? em : ep2;
+    float2 u = __ffma2_rn(make_float2(1.5f, 1.5f), a, __fmul2_rn(make_float2(-0.5f, -0.5f), b));
+    u.x = u.x < 0.f ? a.x : u.x;
+    u.y = u.y < 0.f ? a.y : u.y;
+    return __fmul2_rn(make_float2(cb, cb), u);
+}
+
 // Direction tables of the bins in shared memory: (cos, sin) and
 // (cos^2, sin^2, sin cos, theta), one vector load each.
 template <class R> struct alignas(2 * sizeof(R)) Dir2 { R c, s; };
@@ -258,9 +294,15 @@ __device__ __forceinline__ void wave_breaking(const Konst<R>& K, R esum, R hh, R
 // that forms it, so they round alike.
 template <class R>
 __device__ __forceinline__ R diss_ee(R a, R ridiv, R Dq, R dtf, R& dd) {
-    const R eet = DM<R>::fmax(a, (R)0.0f) * ridiv;
-    dd = eet * Dq;
-    return DM<R>::fmax(eet - dtf * dd, (R)0.0f);
+    const R eet = DM<R>::mul(DM<R>::fmax(a, (R)0.0f), ridiv);
+    dd = DM<R>::mul(eet, Dq);
+    return DM<R>::fmax(DM<R>::fma(-dtf, dd, eet), (R)0.0f);
+}
+// the roller energy of one bin after the roller's dissipation (rrd, the
+// dissipation term) and the wave breaking dissipation dd it gains
+template <class R>
+__device__ __forceinline__ R diss_rr(R rrt, R rrd, R dd, R dtf) {
+    return DM<R>::fmax(DM<R>::fma(dtf, dd - rrd, rrt), (R)0.0f);
 }
 
 // radstress (wave_CPU.cpp:1123-1162) of one cell from its bin sums: sum2 =
@@ -330,9 +372,9 @@ __device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, 
             const R cx = cE * d.c + uE, cy = cE * d.s + vE;
             rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
         } else {
-            rrd = rrt * rcoef;
+            rrd = DM<R>::mul(rrt, rcoef);
         }
-        rrt = wet ? DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f) : (R)0;
+        rrt = wet ? diss_rr(rrt, rrd, dd, dtf) : (R)0;
         drr = wet ? drr + rrd : (R)0;
         RR = RR + rrt;
         rrn[ie + (size_t)t * C] = rrt;
@@ -348,7 +390,7 @@ __device__ __forceinline__ R wave_edge_cell(const Dev<R>& S, const Konst<R>& K, 
         een[ie + (size_t)t * C] = eet;
         const Dir4<R> m = sMom[t];
         sume = sume + eet;
-        sumethet = sumethet + eet * m.th;
+        sumethet = DM<R>::fma(eet, m.th, sumethet);
         ec = DM<R>::fma(m.c2, eet, ec);
         es = DM<R>::fma(m.s2, eet, es);
         ecs = DM<R>::fma(m.cs, eet, ecs);
@@ -599,16 +641,16 @@ __device__ __forceinline__ void b_wave_fast(const Dev<R>& S, const Konst<R>& K, 
                     const R cy = cc_i * d.s + vvi;
                     rrd = twogb * rrt / DM<R>::sqrt(cx * cx + cy * cy);
                 } else {
-                    rrd = rrt * rcoef;
+                    rrd = DM<R>::mul(rrt, rcoef);
                 }
-                rrt = DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                rrt = diss_rr(rrt, rrd, dd, dtf);
                 drr = drr + rrd;
                 RR = RR + rrt;
                 pe_n[(size_t)t * C] = eet;
                 pr_n[(size_t)t * C] = rrt;
                 const Dir4<R> m = sMom[t];
                 sume = sume + eet;
-                sumethet = sumethet + eet * m.th;
+                sumethet = DM<R>::fma(eet, m.th, sumethet);
                 ec = DM<R>::fma(m.c2, eet, ec);
                 es = DM<R>::fma(m.s2, eet, es);
                 ecs = DM<R>::fma(m.cs, eet, ecs);
@@ -757,6 +799,9 @@ struct WCell {
     bool active;
     R hh, axp, axm, ayp, aym, rxp, rxm, ryp, rym, cgi, cci, cthP, cthQ;
     R we1, we2, we3, we4, wr1, wr2, wr3, wr4, c0, cpp, Etmp, cabs, fte, ftr;
+    // the packed FP32 path: (ee, rr) window, face speeds (upper, lower negated),
+    // the negated θ flux of the face below
+    float2 p1, p2, p3, p4, kx, kxn, ky, kyn, ften;
 };
 
 // CPT cells per thread: the block is 32 x (8 / CPT) threads over the same
@@ -768,6 +813,7 @@ template <class R, bool ROLLER, int CPT>
 __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, const WaveMaps& M, const int bix,
                                            const int biy) {
     constexpr int NTH = 256 / CPT, RPT = WT_Y / CPT;   // threads, thread rows
+    constexpr bool PACKED = ROLLER && std::is_same<R, float>::value;   // (ee, rr) pairs in f32x2 instructions
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long mbar[TM_NB];
     Clock* clk = S.clk;
@@ -870,6 +916,11 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
             w.ayp = h * (w.cgi + ld(cgp + ix + yp * nx)); w.aym = h * (w.cgi + ld(cgp + ix + ym * nx));
             w.rxp = h * (w.cci + ld(cp + xp + iy * nx)); w.rxm = h * (w.cci + ld(cp + xm + iy * nx));
             w.ryp = h * (w.cci + ld(cp + ix + yp * nx)); w.rym = h * (w.cci + ld(cp + ix + ym * nx));
+            if constexpr (PACKED) {
+                w.kx = make_float2(w.axp, w.rxp); w.kxn = make_float2(-w.axm, -w.rxm);
+                w.ky = make_float2(w.ayp, w.ryp); w.kyn = make_float2(-w.aym, -w.rym);
+                w.ften = make_float2(0.f, 0.f);
+            }
             w.cthP = cc.s * cc.dhdx; w.cthQ = -(cc.s * cc.dhdy);
             w.c0 = cth(w, sCS2[0].c, sCS2[0].s);
             const int t1 = nt > 1 ? 1 : 0;
@@ -902,6 +953,39 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
             if (!w.active) continue;
             const R* qE = tE + b * TM_N + w.ctile;
             const R* qR = tR + b * TM_N + w.ctile;
+            if constexpr (PACKED) {
+                if (t == 0) {
+                    const int b1 = (nt > 1 ? 1 : 0);
+                    w.p2 = make_float2(qE[0], qR[0]);
+                    w.p1 = w.p2;
+                    w.p3 = make_float2(tE[b1 * TM_N + w.ctile], tR[b1 * TM_N + w.ctile]);
+                }
+                w.p4 = make_float2(tE[b2 * TM_N + w.ctile], tR[b2 * TM_N + w.ctile]);
+                w.cabs = DM<R>::fmax(w.cabs, DM<R>::fabs(w.c0));
+                float2 fx, fy;
+                auto xy2 = [&](auto px, auto py) {
+                    constexpr bool PX = decltype(px)::value, PY = decltype(py)::value;
+                    fx = flux2k2<PX>(qE, qR, 1, w.p2, w.kx, w.kxn);
+                    fy = flux2k2<PY>(qE, qR, TM_X, w.p2, w.ky, w.kyn);
+                };
+                if (ct > (R)0) {
+                    if (st > (R)0) xy2(std::true_type{}, std::true_type{}); else xy2(std::true_type{}, std::false_type{});
+                } else {
+                    if (st > (R)0) xy2(std::false_type{}, std::true_type{}); else xy2(std::false_type{}, std::false_type{});
+                }
+                const float2 fup = last ? make_float2(0.f, 0.f) : theta_face2(w.p1, w.p2, w.p3, w.p4, w.c0, w.cpp);
+                const float2 ft = __fadd2_rn(fup, w.ften);
+                w.ften = __fmul2_rn(fup, make_float2(-1.f, -1.f));
+                const float2 A2 = __fadd2_rn(
+                    w.p2, __ffma2_rn(make_float2(-ct, -ct), fx,
+                                     __ffma2_rn(make_float2(-st, -st), fy, __fmul2_rn(ft, make_float2(-kth, -kth)))));
+                sA[t * 256 + w.cid] = A2.x;
+                sR[t * 256 + w.cid] = A2.y;
+                w.Etmp = w.Etmp + DM<R>::fmax(A2.x, (R)0);
+                w.p1 = w.p2; w.p2 = w.p3; w.p3 = w.p4;
+                w.c0 = w.cpp; w.cpp = cth(w, d2.c, d2.s);
+                continue;
+            }
             if (t == 0) {
                 const int b1 = (nt > 1 ? 1 : 0);
                 w.we2 = qE[0]; w.we1 = w.we2; w.we3 = tE[b1 * TM_N + w.ctile];
@@ -994,21 +1078,43 @@ __device__ __forceinline__ void b_wave_tma(const Dev<R>& S, const Konst<R>& K, c
         R ec = 0, es = 0, ecs = 0, rc = 0, rs = 0, rcs = 0;
         R* pA = sA + cid;
         R* pR = sR + cid;
-        if (wet) {
+        if (wet && PACKED) {   // the (ee, rr) sums in f32x2 instructions, rounding as the scalar loop
+            float2 sr = make_float2(0.f, 0.f), cc2 = sr, ss2 = sr, cs2 = sr;
+#pragma unroll 2
+            for (int t = 0; t < nt; t++) {
+                float dd;
+                const float eet = diss_ee((float)pA[t * 256], (float)ridiv, (float)Dq, (float)dtf, dd);
+                float rrt = pR[t * 256];
+                const float rrd = __fmul_rn(rrt, (float)rcoef);
+                rrt = diss_rr(rrt, rrd, dd, (float)dtf);
+                drr = drr + rrd;
+                pA[t * 256] = eet;
+                pR[t * 256] = rrt;
+                const Dir4<R> m = sMom[t];
+                const float2 er = make_float2(eet, rrt);
+                sr = __fadd2_rn(sr, er);
+                sumethet = DM<R>::fma(eet, m.th, sumethet);
+                cc2 = __ffma2_rn(make_float2(m.c2, m.c2), er, cc2);
+                ss2 = __ffma2_rn(make_float2(m.s2, m.s2), er, ss2);
+                cs2 = __ffma2_rn(make_float2(m.cs, m.cs), er, cs2);
+            }
+            sume = sr.x; RR = sr.y;
+            ec = cc2.x; rc = cc2.y; es = ss2.x; rs = ss2.y; ecs = cs2.x; rcs = cs2.y;
+        } else if (wet) {
 #pragma unroll 2
             for (int t = 0; t < nt; t++) {
                 R dd;
                 const R eet = diss_ee(pA[t * 256], ridiv, Dq, dtf, dd);
                 R rrt = pR[t * 256];
-                const R rrd = rrt * rcoef;
-                rrt = DM<R>::fmax(rrt + dtf * (dd - rrd), (R)0.0f);
+                const R rrd = DM<R>::mul(rrt, rcoef);
+                rrt = diss_rr(rrt, rrd, dd, dtf);
                 drr = drr + rrd;
                 RR = RR + rrt;
                 pA[t * 256] = eet;
                 pR[t * 256] = rrt;
                 const Dir4<R> m = sMom[t];
                 sume = sume + eet;
-                sumethet = sumethet + eet * m.th;
+                sumethet = DM<R>::fma(eet, m.th, sumethet);
                 ec = DM<R>::fma(m.c2, eet, ec);
                 es = DM<R>::fma(m.s2, eet, es);
                 ecs = DM<R>::fma(m.cs, eet, ecs);

@@ -145,6 +145,7 @@ struct Clock {
 };
 static_assert(offsetof(Clock, forced) == offsetof(Clock, halt) + sizeof(int) && offsetof(Clock, halt) % 8 == 0,
               "halt and forced form one aligned 8-byte word (read together by wave_off)");
+static_assert(sizeof(Clock) == 240, "XBG_CLOCK_BYTES in xbg.h is the clock's size");
 #define XBG_MAX_SERIES 4096
 struct Series {
     double slt[XBG_MAX_SERIES], sla[XBG_MAX_SERIES], slb[XBG_MAX_SERIES];
@@ -230,36 +231,6 @@ __device__ __forceinline__ void tile_load(R* t, const R* const (&src)[NF], int b
     cp_async_wait_all();
     __syncthreads();
 }
-// L2 prefetch, by the block's first warp, of the rows by0-1 .. by0+8 and
-// columns bx0-4 .. bx0+35 of the listed planes for the 32 x 8 tile `tile`
-// (row-major tile index over tiles_x tiles per row): one
-// cp.async.bulk.prefetch per plane and row.  A block issues it for the tile
-// that a block about one wave of the grid later will take, so that block's
-// loads find its fields in L2.  Needs 16-byte aligned rows (nx * sizeof(T) a
-// multiple of 16; otherwise nothing is issued); no effect on results.
-template <int NP>
-__device__ __forceinline__ void prefetch_tile_l2(const void* const (&planes)[NP], const int (&esize)[NP], int tile,
-                                                 int tiles_x, int tiles, int nx, int ny) {
-    if (threadIdx.y != 0 || tile >= tiles) return;
-    const int bx0 = (tile % tiles_x) * 32, by0 = (tile / tiles_x) * 8;
-    const int y0 = max(by0 - 1, 0), y1 = min(by0 + 9, ny);
-    const int rows = y1 - y0;
-    if ((int)threadIdx.x >= rows) return;
-    const int y = y0 + threadIdx.x;
-#pragma unroll
-    for (int p = 0; p < NP; p++) {   // unrolled: the plane lists stay in registers
-        const int es = esize[p];
-        if ((nx * es) % 16) continue;
-        const int al = 16 / es;
-        const int x0 = max(bx0 - 4, 0) / al * al, x1 = min((bx0 + 36 + al - 1) / al * al, nx);
-        const char* a = (const char*)planes[p] + ((size_t)y * nx + x0) * es;
-        const unsigned bytes = (unsigned)((x1 - x0) * es);
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(a), "r"(bytes) : "memory");
-    }
-}
-// the tiles one wave of a 32 x 8 grid later: SMs x blocks per SM
-constexpr int PREFETCH_AHEAD = 148 * 6;
-
 template <class R> struct Pair2 { R a, b; };
 template <class R> struct alignas(2 * sizeof(R)) Pair2A { R a, b; };
 
@@ -396,19 +367,6 @@ __device__ __forceinline__ void batch_items(const BatchTab<R>& T, const int2* it
 #define XBG_KERNELS(NAME)                                                                              \
     template <class R>                                                                                 \
     __global__ void __launch_bounds__(256) k_##NAME(Dev<R> S, Konst<R> K) {                            \
-        b_##NAME<R>(S, K, blockIdx.x, blockIdx.y);                                                     \
-    }                                                                                                  \
-    XBG_BATCH_KERNEL(NAME)
-// As XBG_KERNELS, the single-domain kernel also prefetching into L2 the
-// listed planes (P: an initializer list of plane pointers, E: their element
-// sizes) of the tile a block one wave later will take.
-#define XBG_KERNELS_PREFETCH(NAME, P, E)                                                               \
-    template <class R>                                                                                 \
-    __global__ void __launch_bounds__(256) k_##NAME(Dev<R> S, Konst<R> K) {                            \
-        const void* const pl[] = P;                                                                    \
-        const int es[] = E;                                                                            \
-        prefetch_tile_l2(pl, es, blockIdx.x + blockIdx.y * gridDim.x + PREFETCH_AHEAD, gridDim.x,      \
-                         gridDim.x * gridDim.y, K.nx, K.ny);                                           \
         b_##NAME<R>(S, K, blockIdx.x, blockIdx.y);                                                     \
     }                                                                                                  \
     XBG_BATCH_KERNEL(NAME)

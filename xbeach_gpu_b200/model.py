@@ -26,6 +26,7 @@ EXPORTS = [
     "xbg_set_wave_boundary", "xbg_set_sealevel", "xbg_set_wind", "xbg_compute_dt",
     "xbg_wave_boundary", "xbg_flow_boundary", "xbg_wave_step", "xbg_flow_step",
     "xbg_sediment_step", "xbg_accumulate_means", "xbg_step", "xbg_advance", "xbg_get_time",
+    "xbg_get_time_async", "xbg_clock_decode",
     "xbg_output_done", "xbg_reset_means", "xbg_set_time", "xbg_sync", "xbg_launch_count",
     "xbg_mass", "xbg_put_wave_records", "xbg_get_stream", "xbg_profile_step",
     "xbg_flow_dt_noalloc", "xbg_set_kernel_variant", "xbg_get_kernel_variant",
@@ -69,6 +70,8 @@ def load():
     L.xbg_set_wind.argtypes = [vp, vp, vp, vp, ip]
     L.xbg_advance.argtypes = [vp, ip]
     L.xbg_get_time.argtypes = [vp, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
+    L.xbg_get_time_async.argtypes = [vp, vp]
+    L.xbg_clock_decode.argtypes = [vp, vp, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
     L.xbg_set_time.argtypes = [vp, C.c_double, C.c_double, C.c_double]
     L.xbg_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
     L.xbg_mass.argtypes = [vp, dp, dp, dp]
@@ -202,6 +205,19 @@ class Model:
     def time(self):
         t, dt, n, fl = C.c_double(), C.c_double(), C.c_int64(), C.c_int()
         rc = self.L.xbg_get_time(self.h, C.byref(t), C.byref(dt), C.byref(n), C.byref(fl))
+        return t.value, dt.value, n.value, fl.value, rc
+
+    def time_async(self, buf):
+        """Enqueue a copy of the device clock into buf (XBG_CLOCK_BYTES of
+        pinned host memory, e.g. a pinned uint8 torch tensor's data_ptr()) in
+        the model's stream order; read it with time_decode once the stream
+        has passed it."""
+        _check(self.L.xbg_get_time_async(self.h, C.c_void_p(buf)), "get_time_async")
+
+    def time_decode(self, buf):
+        """(t, dt, nstep, flags, status) from a clock copied by time_async."""
+        t, dt, n, fl = C.c_double(), C.c_double(), C.c_int64(), C.c_int()
+        rc = self.L.xbg_clock_decode(self.h, C.c_void_p(buf), C.byref(t), C.byref(dt), C.byref(n), C.byref(fl))
         return t.value, dt.value, n.value, fl.value, rc
 
     def set_time(self, t, dt, wdt):
