@@ -33,7 +33,7 @@ B_ALGO = lambda nt: 4 * (77 + 4 * nt)   # algorithmic bytes per coupled cell-upd
 # (kernel, nx, ny, ntheta); other workloads report traffic null.
 NCU_TRAFFIC = {
     ("k_wave_fast", 2048, 1024, 18): 361049088 + 335545344,
-    ("k_wave_tma", 2048, 1024, 18): 344964352 + 332152576,
+    ("k_wave_tma", 2048, 1024, 18): 345307392 + 328110592,
 }
 
 
@@ -264,24 +264,27 @@ def _ref_worker(job):
     import pyoracle
     from xbeach_gpu_b200.abi import FIELD_NAMES
     from xbeach_gpu_b200.scenarios import make_case
-    nx, ny, seed, steps, warmup, limit = job
+    nx, ny, seed, steps, warmup, limit, presteps = job
     p, zb, bnd = make_case("barred_beach", nx=nx, ny=ny, seed=seed)
     o = pyoracle.Oracle(p)   # a physically consistent starting state
     o.set_wave_boundary(0, bnd["St"], bnd["q"], t0=0.0, tend=p.rtlength, Trep=bnd["Trep"])
     o.set_sealevel([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
     o.set_wind([0.0, 1e6], [0.0, 0.0], [0.0, 0.0])
     o.init_state(zb, 0.0, 0.0)
-    o.advance(3)
+    o.advance(presteps)
     r = pyoracle.RefEmu(p)
     for n in FIELD_NAMES:
         r.set(n, o.get(n))
     t, dt, _, _, _ = o.time()
+    del o
     nb = int(t // p.dtbc)
     St = bnd["St"][nb].astype(np.float32)
     q0, q1 = bnd["q"][nb].astype(np.float32), bnd["q"][nb + 1].astype(np.float32)
+    trep = np.float32(bnd["Trep"])
+    del bnd
     per = []
     for k in range(warmup + steps):
-        r.step_inputs(dt, t + k * dt, np.float32(bnd["Trep"]), St, q0, q1, 0.5, 1.0, 0.0, 0.0, 0.0, 0.0)
+        r.step_inputs(dt, t + k * dt, trep, St, q0, q1, 0.5, 1.0, 0.0, 0.0, 0.0, 0.0)
         t0 = time.perf_counter()
         for call in ("wave_step", "flow_boundary", "flow_step", "sediment_step"):
             r.call(call)
@@ -294,10 +297,12 @@ def _ref_worker(job):
 
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU code (wave_CPU.cpp and its flow
-    and sediment kernels run on the CPU, oracle/_ref) on every host core: the
-    reference code is serial, so each core runs an independent replica on its
-    own 256 x 128 crop of the barred beach, and the value is their summed
-    cell-updates/s."""
+    and sediment kernels run on the CPU, oracle/_ref) on the host cores: the
+    reference code is serial, so each core runs an independent replica of the
+    whole benchmarked domain (the barred beach at --nx x --ny, 18 bins; as
+    many replicas as cores, at most 16 and bounded by the host memory at about
+    6 GB each), each timing whole steps (at least one) until a 60 s cap, and
+    the value is their summed cell-updates/s."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -309,20 +314,32 @@ def run_reference(args, rank, world):
         cores = len(os.sched_getaffinity(0))
     except Exception:
         cores = os.cpu_count() or 1
-    nx, ny = 256, 128
-    jobs = [(nx, ny, k, args.steps, args.warmup, 45.0) for k in range(cores)]
+    nx, ny = args.nx, args.ny
+    try:   # each replica holds the boundary series and two model states of the whole domain
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+        cores = max(1, min(cores, int(avail // (6e9 * max(1.0, nx * ny / 2.1e6)))))
+    except (ValueError, OSError):
+        pass
+    # at most 16 replicas: a whole-domain step of the serial code takes tens of
+    # seconds and the replicas share the host's memory bandwidth, so more would
+    # only stretch the run past a few minutes
+    cores = min(cores, 16)
+    jobs = [(nx, ny, k, max(1, args.steps), 0, 60.0, 1) for k in range(cores)]
     with mp.get_context("spawn").Pool(cores) as pool:
         res = pool.map(_ref_worker, jobs)
     v = float(sum(n * c / max(s, 1e-9) for n, s, c in res))
     steps = int(min(n for n, _, _ in res))
     ms = 1e3 * float(np.mean([s / max(n, 1) for n, s, _ in res]))
-    sample = (f"reference wave_CPU.cpp + reference flow/sediment kernels on the CPU, one serial replica per core "
-              f"({cores} cores), barred beach crop {nx}x{ny} ntheta=18, >= {steps} timed steps each")
+    sample = (f"reference wave_CPU.cpp + reference flow/sediment kernels on the CPU, one serial replica of the "
+              f"whole {nx}x{ny} ntheta=18 barred beach per core ({cores} cores), >= {steps} timed steps each "
+              f"(60 s cap per replica)")
     return {"metric": "coupled cell-updates/s", "value": v, "unit": "cell-updates/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded barred beach)",
-            "config": {"workload": f"barred_beach {args.nx}x{args.ny} ntheta=18 (sample {nx}x{ny} per core)"},
+            "config": {"workload": f"barred_beach {args.nx}x{args.ny} ntheta=18 (large single domain)",
+                       "nx": nx, "ny": ny, "ntheta": 18, "cells": nx * ny,
+                       "parallelism": f"{cores} serial replicas, one per core"},
             "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": cores, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
