@@ -183,6 +183,20 @@ int  xbg_get_time(xbg_handle* h, double* totaltime, double* dt, int64_t* nstep,
  * the stream has passed the copy, xbg_clock_decode reads it (and returns
  * the status word) as xbg_get_time would have at that point of the stream. */
 #define XBG_CLOCK_BYTES 240
+/* Checkpoint / resume (the reference has none: its hot start is commented
+ * out, Wave_gpu.cu:2973-2984).  One host buffer holds every buffer that
+ * carries state from step to step -- the persistent fields, both plane sets
+ * of ee and rr, the previous level, the running means, the WAVEDT partials,
+ * the boundary slots and series, and the device clock (time, dt, step
+ * counters, boundary cursors, status) -- behind a header naming the grid and
+ * precision.  Loading it into a handle created with the same parameters
+ * continues the run bit for bit; a buffer of another grid or precision is
+ * XBG_ERR_ARG.  A scenario of a batch takes only a snapshot whose boundary
+ * slots have its own capacity (else XBG_ERR_STATE).  Both synchronise the
+ * handle's stream.                                                        */
+int  xbg_state_bytes(xbg_handle* h, size_t* bytes);
+int  xbg_save_state(xbg_handle* h, void* dst, size_t bytes);
+int  xbg_load_state(xbg_handle* h, const void* src, size_t bytes);
 int  xbg_get_time_async(xbg_handle* h, void* dst);
 int  xbg_clock_decode(xbg_handle* h, const void* src, double* totaltime, double* dt,
                       int64_t* nstep, int* flags);

@@ -248,6 +248,9 @@ struct xbg_handle {
     virtual int step(int nsteps) = 0;
     virtual int get_time(double* t, double* dt, int64_t* n, int* flags) = 0;
     virtual int get_time_async(void* dst) = 0;
+    virtual int state_bytes(size_t* n) = 0;
+    virtual int save_state(void* dst, size_t n) = 0;
+    virtual int load_state(const void* src, size_t n) = 0;
     virtual int clock_decode(const void* src, double* t, double* dt, int64_t* n, int* flags) = 0;
     virtual int set_time(double t, double dt, double wdt) = 0;
     virtual int output_done() = 0;
@@ -331,6 +334,14 @@ struct Handle : public xbg_handle {
         allocs.push_back(q);
         *p = (T*)q;
         return XBG_OK;
+    }
+    // free one allocation made by alloc() before the handle's end
+    void release(void* p) {
+        auto it = std::find(allocs.begin(), allocs.end(), p);
+        if (it != allocs.end()) {
+            allocs.erase(it);
+            cudaFree(p);
+        }
     }
 
     int setup(const xbg_params* p, int prec) {
@@ -765,6 +776,99 @@ struct Handle : public xbg_handle {
         if (flags) *flags = c.flags;
         return c.status;
     }
+    // ---- checkpoint / resume: every buffer that carries state from one step
+    // to the next, in one host buffer behind a header that names the grid
+    struct StateHeader {
+        uint64_t magic, version;
+        int32_t precision, nx, ny, nt;
+        uint64_t slot_cap, nwave, nflow, total;
+    };
+    static constexpr uint64_t STATE_MAGIC = 0x5854535447425858ull;   // "XXBGTSTX"
+    template <class F> void state_regions(F&& f) {
+        const size_t C = (size_t)S.C, nt = (size_t)K.nt, ny = (size_t)K.ny;
+        for (int k = 0; k < NF2D; k++) f((void*)S.f[k], C * sizeof(R));
+        f((void*)S.wetu, C * sizeof(int));
+        f((void*)S.wetv, C * sizeof(int));
+        f((void*)S.umeanbnd, ny * sizeof(R));
+        for (int k = 0; k < 2; k++) {
+            f((void*)ee_buf[k], C * nt * sizeof(R));
+            f((void*)rr_buf[k], C * nt * sizeof(R));
+            f((void*)zsold_buf[k], C * sizeof(R));
+        }
+        f((void*)S.St, ny * nt * sizeof(R));
+        f((void*)S.part_wave, (size_t)nwave * sizeof(R));
+        f((void*)S.part_flow, (size_t)2 * step_begin_blocks(K) * sizeof(R));
+        f((void*)clk, sizeof(Clock));
+        f((void*)ser, sizeof(Series));
+        for (int k = 0; k < 2; k++) {
+            f((void*)S.stfile[k], slot_cap * sizeof(R));
+            f((void*)S.qfile[k], slot_cap / nt * 4 * sizeof(R));
+        }
+    }
+    int state_bytes(size_t* n) override {
+        if (!n) return XBG_ERR_ARG;
+        size_t t = sizeof(StateHeader);
+        state_regions([&](void*, size_t b) { t += b; });
+        *n = t;
+        return XBG_OK;
+    }
+    int save_state(void* dst, size_t n) override {
+        size_t need = 0;
+        state_bytes(&need);
+        if (!dst || n < need) return XBG_ERR_ARG;
+        if (ext) CK(cudaStreamSynchronize(ext));
+        CK(cudaStreamSynchronize(st));
+        StateHeader h{STATE_MAGIC, 1, precision, K.nx, K.ny, K.nt, slot_cap, (uint64_t)nwave,
+                      (uint64_t)step_begin_blocks(K), need};
+        std::memcpy(dst, &h, sizeof(h));
+        unsigned char* p = (unsigned char*)dst + sizeof(h);
+        int rc = XBG_OK;
+        state_regions([&](void* d, size_t b) {
+            if (b && !rc && cudaMemcpy(p, d, b, cudaMemcpyDeviceToHost) != cudaSuccess) rc = XBG_ERR_CUDA;
+            p += b;
+        });
+        return rc;
+    }
+    int load_state(const void* src, size_t n) override {
+        if (!src || n < sizeof(StateHeader)) return XBG_ERR_ARG;
+        StateHeader h;
+        std::memcpy(&h, src, sizeof(h));
+        if (h.magic != STATE_MAGIC || h.version != 1 || h.precision != precision || h.nx != K.nx ||
+            h.ny != K.ny || h.nt != K.nt || h.nwave != (uint64_t)nwave ||
+            h.nflow != (uint64_t)step_begin_blocks(K) || h.total != n)
+            return XBG_ERR_ARG;
+        if (ext) CK(cudaStreamSynchronize(ext));
+        CK(cudaStreamSynchronize(st));
+        // a batch's tables hold this handle's slot pointers: a batch scenario
+        // takes only snapshots whose boundary slots fit its own
+        if (ext && h.slot_cap != slot_cap) return XBG_ERR_STATE;
+        if (h.slot_cap != slot_cap) {   // the boundary slots of the saved run
+            for (int k = 0; k < 2; k++) {
+                if (S.stfile[k]) { release(S.stfile[k]); S.stfile[k] = nullptr; }
+                if (S.qfile[k]) { release(S.qfile[k]); S.qfile[k] = nullptr; }
+                if (h.slot_cap) {
+                    int rc;
+                    if ((rc = alloc(&S.stfile[k], h.slot_cap)) || (rc = alloc(&S.qfile[k], h.slot_cap / K.nt * 4)))
+                        return rc;
+                }
+            }
+            slot_cap = h.slot_cap;
+        }
+        drop_graph();   // re-captured with the buffers as they are now
+        const unsigned char* p = (const unsigned char*)src + sizeof(h);
+        int rc = XBG_OK;
+        state_regions([&](void* d, size_t b) {
+            if (b && !rc && cudaMemcpy(d, p, b, cudaMemcpyHostToDevice) != cudaSuccess) rc = XBG_ERR_CUDA;
+            p += b;
+        });
+        clock_stale = true;
+        if (!rc) {
+            Clock c;
+            rc = read_clock(c);
+        }
+        return rc;
+    }
+
     // the clock copied to host memory in stream order, without waiting
     int get_time_async(void* dst) override {
         if (!dst) return XBG_ERR_ARG;
@@ -1294,6 +1398,11 @@ int xbg_step(xbg_handle* h) { return h ? h->step(1) : XBG_ERR_ARG; }
 int xbg_advance(xbg_handle* h, int n) { return h ? h->step(n) : XBG_ERR_ARG; }
 int xbg_get_time(xbg_handle* h, double* t, double* dt, int64_t* n, int* flags) { return h ? h->get_time(t, dt, n, flags) : XBG_ERR_ARG; }
 int xbg_get_time_async(xbg_handle* h, void* dst) { return h ? h->get_time_async(dst) : XBG_ERR_ARG; }
+int xbg_state_bytes(xbg_handle* h, size_t* bytes) { return h ? h->state_bytes(bytes) : XBG_ERR_ARG; }
+int xbg_save_state(xbg_handle* h, void* dst, size_t bytes) { return h ? h->save_state(dst, bytes) : XBG_ERR_ARG; }
+int xbg_load_state(xbg_handle* h, const void* src, size_t bytes) {
+    return h ? h->load_state(src, bytes) : XBG_ERR_ARG;
+}
 int xbg_clock_decode(xbg_handle* h, const void* src, double* t, double* dt, int64_t* n, int* flags) {
     return h ? h->clock_decode(src, t, dt, n, flags) : XBG_ERR_ARG;
 }

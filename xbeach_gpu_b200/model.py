@@ -26,7 +26,7 @@ EXPORTS = [
     "xbg_set_wave_boundary", "xbg_set_sealevel", "xbg_set_wind", "xbg_compute_dt",
     "xbg_wave_boundary", "xbg_flow_boundary", "xbg_wave_step", "xbg_flow_step",
     "xbg_sediment_step", "xbg_accumulate_means", "xbg_step", "xbg_advance", "xbg_get_time",
-    "xbg_get_time_async", "xbg_clock_decode",
+    "xbg_get_time_async", "xbg_clock_decode", "xbg_state_bytes", "xbg_save_state", "xbg_load_state",
     "xbg_output_done", "xbg_reset_means", "xbg_set_time", "xbg_sync", "xbg_launch_count",
     "xbg_mass", "xbg_put_wave_records", "xbg_get_stream", "xbg_profile_step",
     "xbg_flow_dt_noalloc", "xbg_set_kernel_variant", "xbg_get_kernel_variant",
@@ -72,6 +72,9 @@ def load():
     L.xbg_get_time.argtypes = [vp, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
     L.xbg_get_time_async.argtypes = [vp, vp]
     L.xbg_clock_decode.argtypes = [vp, vp, dp, dp, C.POINTER(C.c_int64), C.POINTER(C.c_int)]
+    L.xbg_state_bytes.argtypes = [vp, C.POINTER(C.c_size_t)]
+    L.xbg_save_state.argtypes = [vp, vp, C.c_size_t]
+    L.xbg_load_state.argtypes = [vp, vp, C.c_size_t]
     L.xbg_set_time.argtypes = [vp, C.c_double, C.c_double, C.c_double]
     L.xbg_launch_count.argtypes = [vp, C.POINTER(C.c_int64)]
     L.xbg_mass.argtypes = [vp, dp, dp, dp]
@@ -219,6 +222,21 @@ class Model:
         t, dt, n, fl = C.c_double(), C.c_double(), C.c_int64(), C.c_int()
         rc = self.L.xbg_clock_decode(self.h, C.c_void_p(buf), C.byref(t), C.byref(dt), C.byref(n), C.byref(fl))
         return t.value, dt.value, n.value, fl.value, rc
+
+    def save_state(self):
+        """A snapshot of the whole device state (numpy uint8 array); see
+        load_state."""
+        n = C.c_size_t()
+        _check(self.L.xbg_state_bytes(self.h, C.byref(n)), "state_bytes")
+        buf = np.empty(n.value, np.uint8)
+        _check(self.L.xbg_save_state(self.h, buf.ctypes.data_as(C.c_void_p), n.value), "save_state")
+        return buf
+
+    def load_state(self, buf):
+        """Restore a snapshot taken by save_state on a handle with the same
+        parameters: the run continues from it bit for bit."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        _check(self.L.xbg_load_state(self.h, buf.ctypes.data_as(C.c_void_p), buf.size), "load_state")
 
     def set_time(self, t, dt, wdt):
         _check(self.L.xbg_set_time(self.h, t, dt, wdt), "set_time")
