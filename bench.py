@@ -295,6 +295,19 @@ def _ref_worker(job):
     return len(timed), float(np.sum(timed)), nx * ny
 
 
+def reference_replicas(cores, avail_bytes, nx, ny):
+    """How many whole-domain replicas of the reference's serial CPU code to
+    run: one per core, as many as the host memory holds at about 6 GB per
+    2048 x 1024 replica (the boundary series and two model states), and at
+    most 16 -- a whole-domain step takes tens of seconds and the replicas
+    share the host's memory bandwidth, so more would only stretch the run
+    past a few minutes."""
+    n = max(1, cores)
+    if avail_bytes is not None:
+        n = min(n, int(avail_bytes // (6e9 * max(1.0, nx * ny / 2.1e6))))
+    return max(1, min(n, 16))
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's own CPU code (wave_CPU.cpp and its flow
     and sediment kernels run on the CPU, oracle/_ref) on the host cores: the
@@ -315,15 +328,11 @@ def run_reference(args, rank, world):
     except Exception:
         cores = os.cpu_count() or 1
     nx, ny = args.nx, args.ny
-    try:   # each replica holds the boundary series and two model states of the whole domain
+    try:
         avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
-        cores = max(1, min(cores, int(avail // (6e9 * max(1.0, nx * ny / 2.1e6)))))
     except (ValueError, OSError):
-        pass
-    # at most 16 replicas: a whole-domain step of the serial code takes tens of
-    # seconds and the replicas share the host's memory bandwidth, so more would
-    # only stretch the run past a few minutes
-    cores = min(cores, 16)
+        avail = None
+    cores = reference_replicas(cores, avail, nx, ny)
     jobs = [(nx, ny, k, max(1, args.steps), 0, 60.0, 1) for k in range(cores)]
     with mp.get_context("spawn").Pool(cores) as pool:
         res = pool.map(_ref_worker, jobs)

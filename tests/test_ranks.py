@@ -1,6 +1,7 @@
-"""The multi-GPU bench path's rank logic on CPU: two gloo ranks (the replicas
-of bench.py --gpus 2) reduce their timings with a max and their work with a
-sum, the way the NCCL run does."""
+"""The bench's host logic on CPU: two gloo ranks (the replicas of bench.py
+--gpus 2) reduce their timings with a max and their work with a sum, the way
+the NCCL run does; the reference arm's replica count follows the host's
+cores and memory."""
 import os
 import socket
 
@@ -48,3 +49,15 @@ def test_over_ranks_gloo_two_ranks():
 def test_over_ranks_single_process():
     import bench
     assert bench.over_ranks(None, [1.5, 2.0], [3.0], "cpu") == ([1.5, 2.0], [3.0])
+
+
+def test_reference_arm_replica_count():
+    """The reference arm runs one whole-domain replica per core, bounded by
+    host memory (about 6 GB per 2048 x 1024 replica) and by 16."""
+    import bench
+    assert bench.reference_replicas(16, 196e9, 2048, 1024) == 16
+    assert bench.reference_replicas(64, 196e9, 2048, 1024) == 16
+    assert bench.reference_replicas(64, 30e9, 2048, 1024) == 5
+    assert bench.reference_replicas(8, None, 2048, 1024) == 8
+    assert bench.reference_replicas(8, 1e9, 2048, 1024) == 1
+    assert bench.reference_replicas(0, None, 256, 128) == 1
