@@ -536,7 +536,8 @@ def run_storm(args, local):
     """The surrogate-assisted storm ensemble: n scenarios (nx 256..1024, ny
     128..512, 12 bins, morfac 10, the 6 h storm from storm time 2 h) stepped
     plain and surrogate-assisted (network trained here on snapshots of other
-    storm scenarios; judge every 50 steps; 2 % bar, and without a bar) from
+    storm scenarios, then two push-forward rounds; judge every 50 steps; 2 %
+    bar, and without a bar) from
     the same state; cell-updates/s of each, final H and zb against the plain
     run, fallback rate, inference tensor throughput and the Amdahl bound of
     replacing the wave sub-step (the wave kernels' share of a plain step)."""
@@ -553,6 +554,16 @@ def run_storm(args, local):
     net = UNet(seed=0, base=32)
     t0 = time.perf_counter()
     st.train(net, data, norm, steps=2000, batch=16, crop=96, lr=5e-4, log_every=500)
+    # push-forward rounds against chained drift: pairs whose held wave fields
+    # are the network's own prediction one link earlier on plain chains of
+    # the training scenarios, trained with the plain pairs
+    chain = st.collect_chain(train_sc, warm=160, k=10, links=8, crop=96, crops_per=4, seed=3)
+    plain_pairs = st.chain_pairs(chain)
+    pf_rounds = 2
+    for r in range(pf_rounds):
+        pf = st.pushforward_pairs(net, norm, chain)
+        st.train(net, st.merge(data, plain_pairs, pf), norm, steps=1500, batch=16, crop=96, lr=2.5e-4, seed=r + 1,
+                 log_every=500)
     t_train = time.perf_counter() - t0
     sc = list(iter_storm_ensemble(args.storm_scenarios, seed=7, rtlength=600.0))
     params = [p for p, _, _ in sc]
@@ -561,7 +572,8 @@ def run_storm(args, local):
     storm = lambda s, t: sc[s][2]["storm"](t)   # noqa: E731
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out = {"scenarios": len(sc), "cells": cells, "steps": K, "k": 10, "judge_every": 50, "train_s": t_train,
-           "train_crops": int(data["x"].shape[0])}
+           "train_crops": int(data["x"].shape[0]), "pushforward_rounds": pf_rounds,
+           "pushforward_pairs": int(pf["x"].shape[0])}
     finals = {}
     for mode in ("plain", "2pct", "nobar"):
         b = st.storm_batch(sc, warm)
