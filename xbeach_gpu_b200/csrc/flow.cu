@@ -399,6 +399,18 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
     __shared__ R sU1[FT_N], sU2[FT_N], sV1[FT_N], sV2[FT_N];
     const int nx = K.nx, ny = K.ny;
     const int bx0 = bix * FT_X, by0 = biy * FT_Y;
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool inside = ix < nx && iy < ny;
+    const int i = IDX(ix, iy);
+    // the face depths the corrections divide by (the cell's, and those of the
+    // extra column / row cells this thread corrects) are loaded first, so
+    // their round trip overlaps the tile's
+    const bool xrow = threadIdx.y == 0 && by0 > 0 && ix < nx;   // corrects v at (ix, by0-1)
+    const bool xcol = threadIdx.y == 1 && threadIdx.x < FT_Y && bx0 > 0 && by0 + (int)threadIdx.x < ny;   // u at (bx0-1, by0+r)
+    R hum_c = (R)1, hvm_c = (R)1, hvm_x = (R)1, hum_x = (R)1;
+    if (inside) { hum_c = ld(S.f[HUM] + i); hvm_c = ld(S.f[HVM] + i); }
+    if (xrow) hvm_x = ld(S.f[HVM] + i - nx);
+    if (xcol) hum_x = ld(S.f[HUM] + IDX(bx0 - 1, by0 + (int)threadIdx.x));
     {
         const R* src[C_NF] = {S.f[ZS], S.f[ZB], S.tmp[T_UU], S.tmp[T_VV], S.f[UUOLD], S.f[VVOLD], S.f[QX], S.f[QY]};
         tile_load<R, FC_H, C_NF>(tile, src, bx0, by0, nx, ny);
@@ -413,15 +425,12 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
         sU1[e] = w1; sU2[e] = w2; sV1[e] = v1; sV2[e] = v2;
     }
     __syncthreads();
-    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    const bool inside = ix < nx && iy < ny;
-    const int i = IDX(ix, iy);
     R dtf = (R)clk->dt, rdx = K.rdx;
     const int kc = (threadIdx.y + FC_H) * G::TX + threadIdx.x + FC_H;
     const int c = (threadIdx.y + 1) * FT_TX + threadIdx.x + 1;
-    // uu2Ocorr at the cell r (ring index) of tile slot k, grid cell (x, y), index j:
-    // wrk at the cell, its right and lower neighbours
-    auto ucorr = [&](int k, int r, int x, int y, int j) -> R {
+    // uu2Ocorr at the cell r (ring index) of tile slot k, grid cell (x, y) with
+    // face depth hm: wrk at the cell, its right and lower neighbours
+    auto ucorr = [&](int k, int r, int x, int y, R hm) -> R {
         TileAt<R, FC_H> a{tile, k};
         R u = a(C_UU, 0, 0);
         if (x > 0 && y > 0) {
@@ -430,12 +439,12 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
             R qw = (R)0.5f * (a(C_QX, 0, 0) + a(C_QX, -1, 0));
             R qn = (R)0.5f * (a(C_QY, 0, -1) + a(C_QY, 1, -1));
             R qs = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, -1, 0));
-            u = u - dtf / ld(S.f[HUM] + j) * ((qe * w1r - qw * w1i) * rdx + (qs * w2i - qn * w2b) * rdx);
+            u = u - dtf / hm * ((qe * w1r - qw * w1i) * rdx + (qs * w2i - qn * w2b) * rdx);
         }
         return u;
     };
     // vv2Ocorr: wrk at the cell, its left and upper neighbours
-    auto vcorr = [&](int k, int r, int x, int y, int j) -> R {
+    auto vcorr = [&](int k, int r, int x, int y, R hm) -> R {
         TileAt<R, FC_H> a{tile, k};
         R v = a(C_VV, 0, 0);
         if (x > 0 && y > 0) {
@@ -444,7 +453,7 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
             R qw = (R)0.5f * (a(C_QX, -1, 0) + a(C_QX, -1, 1));
             R qn = (R)0.5f * (a(C_QY, 0, 0) + a(C_QY, 0, -1));
             R qs = (R)0.5f * (a(C_QY, 0, 1) + a(C_QY, 0, 0));
-            v = v - dtf / ld(S.f[HVM] + j) * ((qe * v2i - qw * v2l) * rdx + (qs * v1t - qn * v1i) * rdx);
+            v = v - dtf / hm * ((qe * v2i - qw * v2l) * rdx + (qs * v1t - qn * v1i) * rdx);
         }
         return v;
     };
@@ -457,17 +466,16 @@ __device__ __forceinline__ void b_flow_corr(const Dev<R>& S, const Konst<R>& K, 
     R* sVc = tile + C_VO * G::N;   // [FT_Y + 1][FT_X], y = by0-1 .. by0+7
     R u = (R)0, v = (R)0;
     if (inside) {
-        u = ucorr(kc, c, ix, iy, i);
-        v = vcorr(kc, c, ix, iy, i);
+        u = ucorr(kc, c, ix, iy, hum_c);
+        v = vcorr(kc, c, ix, iy, hvm_c);
         sUc[threadIdx.y * (FT_X + 1) + threadIdx.x + 1] = u;
         sVc[(threadIdx.y + 1) * FT_X + threadIdx.x] = v;
     }
-    if (threadIdx.y == 0 && by0 > 0 && ix < nx)   // (ix, by0-1)
-        sVc[threadIdx.x] = vcorr(kc - G::TX, c - FT_TX, ix, by0 - 1, i - nx);
-    if (threadIdx.y == 1 && threadIdx.x < FT_Y && bx0 > 0 && by0 + (int)threadIdx.x < ny) {   // (bx0-1, by0+r)
+    if (xrow)   // (ix, by0-1)
+        sVc[threadIdx.x] = vcorr(kc - G::TX, c - FT_TX, ix, by0 - 1, hvm_x);
+    if (xcol) {   // (bx0-1, by0+r)
         const int r = threadIdx.x;
-        sUc[r * (FT_X + 1)] = ucorr((r + FC_H) * G::TX + FC_H - 1, (r + 1) * FT_TX, bx0 - 1, by0 + r,
-                                    IDX(bx0 - 1, by0 + r));
+        sUc[r * (FT_X + 1)] = ucorr((r + FC_H) * G::TX + FC_H - 1, (r + 1) * FT_TX, bx0 - 1, by0 + r, hum_x);
     }
     __syncthreads();
     loads_before_here();
