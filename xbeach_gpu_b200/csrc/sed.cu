@@ -31,6 +31,10 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
     R dtf = (R)clk->dt, Trep = (R)clk->Trep;
     R rho = K.rho, g = K.g, eps = K.eps;
     R c = ld(S.f[CC_] + i);
+    // every input is loaded here, ahead of the branches below, so that the
+    // loads make one round trip to memory
+    const R Hi = ld(S.f[H] + i), stdep = ld(S.f[STDEP] + i), cfm = ld(S.f[CFM] + i), rol = ld(S.f[ROL] + i);
+    const R dri = ld(S.f[DR] + i), urms = ld(S.f[URMS] + i);
     // longturb (Sediment_kernel.cu:27-164)
     R rolth = ld(S.f[ROLTHICK] + i) + dtf * (DM<R>::fabs(ld(S.f[DZSDT] + i)) - K.beta * c);
     rolth = DM<R>::fmax(rolth, (R)0.0f);
@@ -43,11 +47,10 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
     R ue = (R)(0.5 * (double)(ld(S.f[UEU] + IDX(xm, iy)) + ld(S.f[UEU] + i)));
     R ve = (R)(0.5 * (double)(ld(S.f[VEV] + IDX(ix, ym)) + ld(S.f[VEV] + i)));
     R vmags = ue * ue + ve * ve;
-    R ML = DM<R>::fmax(DM<R>::fmin(DM<R>::sqrt((R)2.0f * ld(S.f[ROL] + i) * Trep / (rho * c)), hhi), (R)0.01f);
+    R ML = DM<R>::fmax(DM<R>::fmin(DM<R>::sqrt((R)2.0f * rol * Trep / (rho * c)), hhi), (R)0.01f);
     R dcfin = DM<R>::exp(DM<R>::fmin(hhi, (R)100.0f) / ML);
     R dcf = DM<R>::fmin((R)1 / (dcfin - (R)1), (R)1.0f);
-    R kb = K.nuhfac * DM<R>::pow23(ld(S.f[DR] + i) / rho) * dcf;
-    R urms = ld(S.f[URMS] + i);
+    R kb = K.nuhfac * DM<R>::pow23(dri / rho) * dcf;
     R Urms2 = urms * urms + (R)1.45f * (kb + (R)0.0f);
     R Tsg = DM<R>::fmax((R)0.1f * hhi / K.wws, (R)0.5f);
     R Ucr;
@@ -58,7 +61,7 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
     R Asb = (R)0.005f * hhi * DM<R>::pow((R)1 / hhi / drhog, (R)1.2f);
     R Ass = K.sed_Ass;
     R T1 = vmags + (R)0.018f / Cd * Urms2;
-    T1 = DM<R>::fmin(T1, (R)100000.0f * g / ld(S.f[CFM] + i) * D50 * K.sed_drho);
+    T1 = DM<R>::fmin(T1, (R)100000.0f * g / cfm * D50 * K.sed_drho);
     T1 = DM<R>::sqrt(T1);
     R wetz = hhi > eps ? (R)1 : (R)0;
     R T2 = (R)0.0f;
@@ -75,7 +78,7 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
         R alpha = K.rvr_alpha;
         R beta = K.rvr_beta;
         R k = (R)(2 * XBG_PI / (double)(c * Trep));
-        R Ur = (R)3.0f / (R)8.0f * DM<R>::sqrt((R)2.0f) * ld(S.f[H] + i) * k / ((k * hh) * (k * hh) * (k * hh));
+        R Ur = (R)3.0f / (R)8.0f * DM<R>::sqrt((R)2.0f) * Hi * k / ((k * hh) * (k * hh) * (k * hh));
         Ur = DM<R>::fmax(Ur, (R)0.00001f);
         R Bm = m1 + (m2 - m1) / ((R)1.0f + beta * DM<R>::pow(Ur, alpha));
         R B1 = (R)((double)((R)-90.0f + (R)90.0f * DM<R>::tanh(m5 / DM<R>::pow(Ur, m6))) * XBG_PI / 180.0f);
@@ -86,7 +89,7 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
     // Erosus (:512-531)
     {
         R exp_ero = K.morfac * dtf / ((R)1.0f - K.por) * hh * (ceqsg * (R)1.0f / Tsg + ceqbg * (R)1.0f / dtf);
-        R facero = DM<R>::fmin((R)1.0f, ld(S.f[STDEP] + i) * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
+        R facero = DM<R>::fmin((R)1.0f, stdep * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
         // all stores after all loads (the field pointers may alias as far as the compiler knows)
         S.f[ROLTHICK][i] = rolth;
         S.f[KTURB][i] = (R)0.0f;
@@ -109,6 +112,7 @@ __device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, in
     R hhi = ld(S.f[HH] + i), zbi = ld(S.f[ZB] + i), zbr = ld(S.f[ZB] + IDX(xp, iy)), zbt = ld(S.f[ZB] + IDX(ix, yp));
     R cci = ld(S.f[CSED] + i), ccr = ld(S.f[CSED] + IDX(xp, iy)), cct = ld(S.f[CSED] + IDX(ix, yp));
     R uui = ld(S.f[UU] + i), vvi = ld(S.f[VV] + i), tm = ld(S.f[THM] + i);
+    const R hu = ld(S.f[HU] + i), hv = ld(S.f[HV] + i), dri = ld(S.f[DR] + i);   // ahead of the branches
     R uai = ld(ua + i), uar = ld(ua + IDX(xp, iy)), uat = ld(ua + IDX(ix, yp));
     double ctm = (double)DM<R>::cos(tm), stm = (double)DM<R>::sin(tm);
     R uau = (R)(0.5 * ctm * (double)(uai + uar));
@@ -122,7 +126,6 @@ __device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, in
     R vmagv = DM<R>::sqrt((uv + uau) * (uv + uau) + (vvi + uav) * (vvi + uav));
     R dzbdx = (R)-1.0f * (zbr - zbi) / dx;
     R dzbdy = (R)-1.0f * (zbt - zbi) / dx;
-    R hu = ld(S.f[HU] + i), hv = ld(S.f[HV] + i);
     R wu = hu > eps ? (R)1.0f : (R)0.0f;
     R wv = hv > eps ? (R)1.0f : (R)0.0f;
     R cu, cv;
@@ -134,7 +137,7 @@ __device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, in
     else if (vrep < (R)0.0f) cv = cct;
     else cv = (R)0.50f * (cci + cct);
     R dcsdy = (cct - cci) / dx;
-    R Dc = K.nuh + K.nuhfac * hhi * DM<R>::pow13(ld(S.f[DR] + i) / K.rho);
+    R Dc = K.nuh + K.nuhfac * hhi * DM<R>::pow13(dri / K.rho);
     Sus = K.sus * (cu * urep * hu - Dc * hu * dcsdx - facsl * cu * vmagu * hu * dzbdx) * wu;
     Svs = K.sus * (cv * vrep * hv - Dc * hv * dcsdy - facsl * cv * vmagv * hv * dzbdy) * wv;
 }
@@ -143,19 +146,30 @@ __device__ __forceinline__ void susp_cell(const Dev<R>& S, const Konst<R>& K, in
 // the cell (Susi, Svsi), its left face neighbour (Susl) and the one below
 // (Svsb): new C, ero, depo.
 template <class R>
-__device__ __forceinline__ R conc_from(const Dev<R>& S, const Konst<R>& K, int i, R dtf, R Susi, R Svsi, R Susl,
-                                       R Svsb, R& ero, R& depo) {
-    R hhi = ld(S.f[HH] + i);
+struct ConcIn { R hhi, Tsg, facero, ceqsg, csed; };
+template <class R>
+__device__ __forceinline__ ConcIn<R> conc_in(const Dev<R>& S, int i) {
+    return ConcIn<R>{ld(S.f[HH] + i), ld(S.tmp[T_TSG] + i), ld(S.tmp[T_FACERO] + i), ld(S.f[CEQSG] + i),
+                     ld(S.f[CSED] + i)};
+}
+template <class R>
+__device__ __forceinline__ R conc_of(const Konst<R>& K, const ConcIn<R>& c, R dtf, R Susi, R Svsi, R Susl, R Svsb,
+                                     R& ero, R& depo) {
+    const R hhi = c.hhi, Tsg = c.Tsg;
     R wetz = hhi > K.eps ? (R)1.0f : (R)0.0f;
-    R Tsg = ld(S.tmp[T_TSG] + i);
-    ero = ld(S.tmp[T_FACERO] + i) * hhi * ld(S.f[CEQSG] + i) * (R)1.0f / Tsg;
+    ero = c.facero * hhi * c.ceqsg * (R)1.0f / Tsg;
     R dsusdx = (Susi - Susl) / K.dx;
     R dsvsdy = (Svsi - Svsb) / K.dx;
-    R cs = (dtf * Tsg) / (dtf + Tsg) * (hhi * ld(S.f[CSED] + i) / dtf - (dsusdx + dsvsdy - ero)) * wetz;
+    R cs = (dtf * Tsg) / (dtf + Tsg) * (hhi * c.csed / dtf - (dsusdx + dsvsdy - ero)) * wetz;
     cs = DM<R>::fmax(cs, (R)0.0f);
     cs = DM<R>::fmin(cs, (R)0.1f * hhi);
     depo = cs / Tsg;
     return cs / hhi;
+}
+template <class R>
+__device__ __forceinline__ R conc_from(const Dev<R>& S, const Konst<R>& K, int i, R dtf, R Susi, R Svsi, R Susl,
+                                       R Svsb, R& ero, R& depo) {
+    return conc_of(K, conc_in(S, i), dtf, Susi, Svsi, Susl, Svsb, ero, depo);
 }
 
 // Conc at (ix, iy) evaluating the three Susp it needs (lateral rows only).
@@ -184,6 +198,17 @@ __device__ __forceinline__ void b_sed_b(const Dev<R>& S, const Konst<R>& K, cons
     const int nx = K.nx, ny = K.ny;
     const int bx0 = bix * SB_X, by0 = biy * SB_Y;
     const int tid = threadIdx.x + threadIdx.y * SB_X;
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool cell = ix < nx && iy < ny;
+    const int i = IDX(ix, iy);
+    const bool morph = K.morfac > (R)0.0f;
+    // the cell's own inputs first, so that their round trip overlaps the tile's
+    ConcIn<R> ci{};
+    R zb0 = (R)0, sd0 = (R)0;
+    if (cell) {
+        ci = conc_in(S, i);
+        if (morph) { zb0 = ld(S.f[ZB] + i); sd0 = ld(S.f[STDEP] + i); }
+    }
     for (int e = tid; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
         int kx = e % SB_TX, ky = e / SB_TX;
         int gx = min(max(bx0 - 1 + kx, 0), nx - 1), gy = min(max(by0 - 1 + ky, 0), ny - 1);
@@ -193,13 +218,11 @@ __device__ __forceinline__ void b_sed_b(const Dev<R>& S, const Konst<R>& K, cons
         sSvs[e] = b;
     }
     __syncthreads();
-    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    if (ix >= nx || iy >= ny) return;
-    int i = IDX(ix, iy);
+    if (!cell) return;
     R dtf = (R)clk->dt;
     R ero, depo, cnew;
     const int c = (threadIdx.y + 1) * SB_TX + threadIdx.x + 1;
-    cnew = conc_from(S, K, i, dtf, sSus[c], sSvs[c], sSus[c - 1], sSvs[c - SB_TX], ero, depo);
+    cnew = conc_of(K, ci, dtf, sSus[c], sSvs[c], sSus[c - 1], sSvs[c - SB_TX], ero, depo);
     // CClatbnd (Sediment_kernel.cu:782-821)
     if (iy == 0 || iy == ny - 1) {
         R e2, d2;
@@ -209,13 +232,13 @@ __device__ __forceinline__ void b_sed_b(const Dev<R>& S, const Konst<R>& K, cons
     loads_before_here();
     if (off) return;
     S.tmp[T_UU][i] = cnew;   // per-step buffer reused for the new C
-    if (K.morfac > (R)0.0f) {
+    if (morph) {
         // bedupdate (:881-968), bed-load divergence commented out there
         R dzg = K.morfac * dtf / ((R)1.0f - K.por) * (ero - depo);
-        S.tmp[T_ZB][i] = ld(S.f[ZB] + i) + dzg;
-        S.tmp[T_HH][i] = ld(S.f[HH] + i) + dzg;
+        S.tmp[T_ZB][i] = zb0 + dzg;
+        S.tmp[T_HH][i] = ci.hhi + dzg;
         S.f[DZB][i] = (R)-1 * dzg;
-        S.tmp[T_STDEP][i] = ld(S.f[STDEP] + i) - dzg;
+        S.tmp[T_STDEP][i] = sd0 - dzg;
     }
 }
 XBG_KERNELS(sed_b)
@@ -227,6 +250,14 @@ __device__ __forceinline__ int zbl_src(int ix, int iy, int nx, int ny) {
     if (iy == ny - 1) sy = mm(iy);
     if (ix == 0) { sx = pp(ix, nx); sy = iy; }
     return sx + sy * nx;
+}
+
+// the same source as a column and row
+__device__ __forceinline__ void zbl_xy(int ix, int iy, int nx, int ny, int& sx, int& sy) {
+    sx = ix; sy = iy;
+    if (iy == 0) sy = pp(iy, ny);
+    if (iy == ny - 1) sy = mm(iy);
+    if (ix == 0) { sx = pp(ix, nx); sy = iy; }
 }
 
 // avalanching (Sediment_kernel.cu:1020-1137) transfers (dzbx, dzby) of (ix, iy)
@@ -292,6 +323,25 @@ __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, cons
     const int bx0 = bix * SB_X, by0 = biy * SB_Y;
     const bool morph = K.morfac > (R)0.0f;
     const R dtf = (R)clk->dt;
+    const int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
+    const bool cell = ix < nx && iy < ny;
+    const int i = IDX(ix, iy);
+    // the cell's own inputs first, so that their round trip overlaps the tile's
+    R cnew = (R)0, dzb0 = (R)0, zs0 = (R)0, hh0 = (R)0, zb1 = (R)0, sd1 = (R)0;
+    int sx = ix, sy = iy;
+    if (cell) {
+        cnew = ld(S.tmp[T_UU] + i);
+        if (morph) {
+            dzb0 = ld(S.f[DZB] + i);
+            zs0 = ld(S.f[ZS] + i);
+            hh0 = ld(S.tmp[T_HH] + i);
+            zbl_xy(ix, iy, nx, ny, sx, sy);
+            int s1x, s1y;
+            zbl_xy(sx, sy, nx, ny, s1x, s1y);
+            zb1 = ld(S.tmp[T_ZB] + IDX(s1x, s1y));
+            sd1 = ld(S.tmp[T_STDEP] + IDX(s1x, s1y));
+        }
+    }
     if (morph) {
         for (int e = threadIdx.x + threadIdx.y * SB_X; e < SB_TY * SB_TX; e += SB_X * SB_Y) {
             int gx = min(max(bx0 - 1 + e % SB_TX, 0), nx - 1), gy = min(max(by0 - 1 + e / SB_TX, 0), ny - 1);
@@ -302,10 +352,8 @@ __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, cons
         }
     }
     __syncthreads();
-    int ix = bx0 + threadIdx.x, iy = by0 + threadIdx.y;
-    if (ix >= nx || iy >= ny) return;
-    int i = IDX(ix, iy);
-    S.f[CSED][i] = ld(S.tmp[T_UU] + i);
+    if (!cell) return;
+    S.f[CSED][i] = cnew;
     if (morph) {
         // bed change gathered in the serial launch order:
         // ((-dzby[below] - dzbx[left]) + dzbx) + dzby
@@ -316,16 +364,14 @@ __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, cons
         dd = dd + sBx[c];
         dd = dd + sBy[c];
         // updatezb (:1139-1160) at the own cell
-        S.f[DZB][i] = ld(S.f[DZB] + i) - dd;
-        S.f[ZS][i] = ld(S.f[ZS] + i) - dd;
-        S.f[HH][i] = ld(S.tmp[T_HH] + i) - dd;
+        S.f[DZB][i] = dzb0 - dd;
+        S.f[ZS][i] = zs0 - dd;
+        S.f[HH][i] = hh0 - dd;
         // zb, stdep: updatezb at the zblatbnd source, then the copy
-        int s = zbl_src(ix, iy, nx, ny);
-        int sx = s % nx, sy = s / nx;
+        const int s = IDX(sx, sy);
         R ds = (s == i) ? dd : ddzb_cell(S, K, sx, sy, dtf);
-        int s1 = zbl_src(sx, sy, nx, ny);
-        R zbn = ld(S.tmp[T_ZB] + s1) + ds;
-        R sdn = ld(S.tmp[T_STDEP] + s1) - ds;
+        R zbn = zb1 + ds;
+        R sdn = sd1 - ds;
         S.f[ZB][i] = zbn;
         S.f[STDEP][i] = sdn;
         // updatezom (:1162-1190)

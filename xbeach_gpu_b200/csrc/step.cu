@@ -71,6 +71,11 @@ __device__ void finalize_scalar(const Dev<R>& S, const Konst<R>& K, const Series
     if (K.swave == 1) wavebnd_cursor(c, K, ser);   // wavebnd follows the clock
 }
 
+// 16-byte vectors of the state's fields (their bases are 16-byte aligned)
+template <class R> struct Vec16;
+template <> struct Vec16<float> { using T = float4; static constexpr int N = 4; };
+template <> struct Vec16<double> { using T = double2; static constexpr int N = 2; };
+
 template <class R>
 __device__ __forceinline__ void b_step_begin(const Dev<R>& S, const Konst<R>& K, const Series* ser, int nflow,
                                              int nwave, const int bi, const int nb) {
@@ -78,22 +83,44 @@ __device__ __forceinline__ void b_step_begin(const Dev<R>& S, const Konst<R>& K,
     __shared__ int last;
     int tid = threadIdx.x;
     R m = (R)3.0e38f;
-    {   // FLOWDT: min of hh first (4 loads in flight per thread), one sqrt per thread
+    {   // FLOWDT: max of hh first (16-byte loads, two of each field in flight
+        // per thread), one sqrt per thread
+        using VT = typename Vec16<R>::T;
+        constexpr int N = Vec16<R>::N;
+        union U { VT v; R a[N]; };
         const R* hh = S.f[HH];
         const R* zs = S.f[ZS];
+        const VT* hv = reinterpret_cast<const VT*>(hh);
+        const VT* zv = reinterpret_cast<const VT*>(zs);
+        const int nv = S.C / N;
         const int stride = nb * blockDim.x;
         R hmax = (R)0;
         // health check of the state: a NaN or infinite depth or water level
-        // anywhere (the sum of every value read is finite only if each is)
+        // anywhere (the sum of every value read times 0 is 0 only if each is finite)
         R probe = (R)0;
-        int i = bi * blockDim.x + tid;
-        for (; i + 3 * stride < S.C; i += 4 * stride) {
-            R a = ld(hh + i), b = ld(hh + i + stride), c = ld(hh + i + 2 * stride), d = ld(hh + i + 3 * stride);
-            R za = ld(zs + i), zb = ld(zs + i + stride), zc = ld(zs + i + 2 * stride), zd = ld(zs + i + 3 * stride);
-            hmax = DM<R>::fmax(hmax, DM<R>::fmax(DM<R>::fmax(a, b), DM<R>::fmax(c, d)));
-            probe = probe + (((a + b) + (c + d)) * (R)0 + ((za + zb) + (zc + zd)) * (R)0);
+        auto take = [&](const U& h, const U& z) {
+#pragma unroll
+            for (int k = 0; k < N; k++) {
+                hmax = DM<R>::fmax(hmax, h.a[k]);
+                probe = probe + (h.a[k] * (R)0 + z.a[k] * (R)0);
+            }
+        };
+        int j = bi * blockDim.x + tid;
+        for (; j + stride < nv; j += 2 * stride) {
+            U h0, h1, z0, z1;
+            h0.v = __ldg(hv + j); h1.v = __ldg(hv + j + stride);
+            z0.v = __ldg(zv + j); z1.v = __ldg(zv + j + stride);
+            take(h0, z0);
+            take(h1, z1);
         }
-        for (; i < S.C; i += stride) {
+        if (j < nv) {
+            U h0, z0;
+            h0.v = __ldg(hv + j); z0.v = __ldg(zv + j);
+            take(h0, z0);
+        }
+        // the cells past the last whole vector
+        if (bi == 0 && tid < S.C - nv * N) {
+            const int i = nv * N + tid;
             hmax = DM<R>::fmax(hmax, ld(hh + i));
             probe = probe + (ld(hh + i) * (R)0 + ld(zs + i) * (R)0);
         }
@@ -314,9 +341,6 @@ XBG_KERNELS(means)
 // (two double) cells per thread, the clock's halt flag read with the loads
 // and tested before the stores; the last C mod 4 (2) cells by one more
 // thread.  Each field is its own allocation, so every vector is aligned.
-template <class R> struct Vec16;
-template <> struct Vec16<float> { using T = float4; static constexpr int N = 4; };
-template <> struct Vec16<double> { using T = double2; static constexpr int N = 2; };
 
 template <class R>
 __global__ void __launch_bounds__(256) k_means_v(Dev<R> S, Konst<R> K) {
