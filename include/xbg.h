@@ -232,9 +232,13 @@ int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
  * eulerustep and eulervstep as one pass (uu* of the block's tile and its
  * ring in shared memory), variant 0 as two.  All variants of a phase give
  * the same results bit for bit.  Setting a variant that does not apply is
- * XBG_ERR_ARG; get reports the one in use.                                */
+ * XBG_ERR_ARG; get reports the one in use.  Phase XBG_PHASE_TILE: the tile
+ * shape of the passes that read only a cell and its nearest neighbours
+ * (wavforce, the depth/viscosity and momentum passes, the first sediment
+ * pass): variant 0 blocks of 32 x 8 cells, variant 1 blocks of 64 x 4.   */
 #define XBG_PHASE_WAVE 0
 #define XBG_PHASE_FLOW 1
+#define XBG_PHASE_TILE 2
 int  xbg_set_kernel_variant(xbg_handle* h, int phase, int variant);
 int  xbg_get_kernel_variant(xbg_handle* h, int phase, int* variant);
 /* Device-side water and sediment ledgers (sum zs*dx^2, sum (C*h) dx^2,
@@ -295,7 +299,7 @@ int  xbg_batch_profile_step(xbg_batch* b, float* ms, const char** names,
                             int* n);
 /* Persistent blocks of the launches of one tile shape (0: 32x8 tiles,
  * 1: wave rows, 2: 256-cell runs, 3: one block per scenario, 4: boundary
- * values, 5: dt reduction); used by the autotuner. */
+ * values, 5: dt reduction, 6: 64x4 tiles); used by the autotuner. */
 int  xbg_batch_set_grid(xbg_batch* b, int shape, int blocks);
 int  xbg_batch_launch_count(xbg_batch* b, int64_t* count);
 /* As xbg_set_kernel_variant, for every scenario of a batch (the TMA rows

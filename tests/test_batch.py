@@ -83,9 +83,9 @@ def test_batch_grid_choice_does_not_change_results(tmp_path):
     block counts and any of the variants end bit for bit the same."""
     from xbeach_gpu_b200.autotune import tune
     sc = _cases(4, 21)
-    from xbeach_gpu_b200.abi import XBG_PHASE_FLOW, XBG_PHASE_WAVE
+    from xbeach_gpu_b200.abi import XBG_PHASE_FLOW, XBG_PHASE_TILE, XBG_PHASE_WAVE
     runs = []
-    for variant in ("default", "tuned", "thread_tiles", "two_cells", "other_flow_split"):
+    for variant in ("default", "tuned", "thread_tiles", "two_cells", "other_flow_split", "wide_tiles"):
         b = Batch([p for p, _, _ in sc], XBG_FP32)
         for s, (p, zb, bnd) in enumerate(sc):
             _setup(b.scenario(s), p, zb, bnd)
@@ -103,11 +103,16 @@ def test_batch_grid_choice_does_not_change_results(tmp_path):
             f = 1 - b.variant(XBG_PHASE_FLOW)
             b.set_variant(XBG_PHASE_FLOW, f)
             assert b.variant(XBG_PHASE_FLOW) == f
+        if variant == "wide_tiles":
+            b.set_variant(XBG_PHASE_TILE, 1)
+            assert b.variant(XBG_PHASE_TILE) == 1
+            b.set_grid(6, 5)
         b.advance(25)
         runs.append({s: {f: b.scenario(s).get(f).copy() for f in ("zs", "uu", "H", "ee")} for s in range(len(sc))})
         if variant == "tuned":
             choice = tune(b, cache=str(tmp_path / "tune.json"), reps=1)
             assert {0, 1, 2, 5} <= set(choice) and all(choice[k] >= 1 for k in (0, 1, 2, 5))
+            assert choice["tile_variant"] in (0, 1) and b.variant(XBG_PHASE_TILE) == choice["tile_variant"]
             assert choice["wave_variant"] in (0, 1, 2) and b.variant(XBG_PHASE_WAVE) == choice["wave_variant"]
             assert choice["flow_variant"] in (0, 1) and b.variant(XBG_PHASE_FLOW) == choice["flow_variant"]
             again = tune(b, cache=str(tmp_path / "tune.json"), reps=1)   # from the cache

@@ -3,14 +3,15 @@ plane tiles moved by the tensor memory accelerator (one box copy per bin,
 issued by one thread; the default where it applies) with one or with two
 cells per thread, and plane tiles copied by every thread (cp.async).  The
 flow step's momentum updates run as one pass (uu* of the tile and its ring
-in shared memory) or as two.  Each must give the same state bit for bit over
-whole coupled steps, on grids whose tiles are partial in x and in y, at the
+in shared memory) or as two.  The passes that read only a cell and its
+nearest neighbours run in 32 x 8 or 64 x 4 blocks.  Each must give the same
+state bit for bit over whole coupled steps, on grids whose tiles are partial in x and in y, at the
 offshore and lateral edges, for few bins (fewer than the four tile buffers),
 with and without the roller, in FP32 and FP64."""
 import numpy as np
 import pytest
 
-from xbeach_gpu_b200.abi import XBG_FP32, XBG_FP64, XBG_PHASE_FLOW, XBG_PHASE_WAVE
+from xbeach_gpu_b200.abi import XBG_FP32, XBG_FP64, XBG_PHASE_FLOW, XBG_PHASE_TILE, XBG_PHASE_WAVE
 from xbeach_gpu_b200.model import Model, XbgError
 from xbeach_gpu_b200.scenarios import make_case
 
@@ -86,6 +87,61 @@ def test_fused_momentum_pass_equals_two_passes(name, precision):
     assert runs[0][:2] == runs[1][:2]
     for f in FIELDS:
         assert np.array_equal(runs[0][2][f], runs[1][2][f]), f
+
+
+# grids that leave partial 64 x 4 tiles in x and in y, and a sediment case
+TILE_CASES = dict(FLOW_CASES, linear_130x45_n5=dict(case="linear_beach", nx=130, ny=45, nt=5, kw={}),
+                  sediment_96x38=dict(case="linear_beach", nx=96, ny=38, nt=6,
+                                      kw=dict(sedtrans=1, morfac=10.0, sedstart=0.0)))
+
+
+@pytest.mark.parametrize("precision", [XBG_FP32, XBG_FP64])
+@pytest.mark.parametrize("name", sorted(TILE_CASES))
+def test_wide_tiles_equal_narrow_tiles(name, precision):
+    c = TILE_CASES[name]
+    runs = []
+    for variant in (0, 1):
+        m = _model(c, precision, variant, XBG_PHASE_TILE)
+        assert m.variant(XBG_PHASE_TILE) == variant
+        m.advance(25)
+        m.advance(15)
+        t, dt, n, _, rc = m.time()
+        assert rc == 0 and n == 40
+        runs.append((t, dt, {f: m.get(f).copy() for f in FIELDS}))
+        m.close()
+    assert runs[0][:2] == runs[1][:2]
+    for f in FIELDS:
+        assert np.array_equal(runs[0][2][f], runs[1][2][f]), f
+
+
+def test_single_domain_autotune(tmp_path):
+    """The single-domain autotuner measures each phase's variants, applies the
+    fastest and caches it; a second call reuses the cache.  The results do
+    not depend on the choice."""
+    from xbeach_gpu_b200.autotune import tune
+    c = CASES["barred_256x128_n18"]
+    ref = _model(c, XBG_FP32, 1)
+    ref.advance(12)
+    want = {f: ref.get(f).copy() for f in FIELDS}
+    ref.close()
+    m = _model(c, XBG_FP32, 1)
+    cache = str(tmp_path / "tune.json")
+    choice = tune(m, cache=cache, reps=1)
+    assert set(choice) == {"wave_variant", "flow_variant", "tile_variant"}
+    assert m.variant(XBG_PHASE_WAVE) == choice["wave_variant"]
+    assert m.variant(XBG_PHASE_FLOW) == choice["flow_variant"]
+    assert m.variant(XBG_PHASE_TILE) == choice["tile_variant"]
+    _, _, n, _, rc = m.time()
+    assert rc == 0 and 0 < n < 12
+    m.advance(12 - n)
+    for f in FIELDS:
+        assert np.array_equal(m.get(f), want[f]), f
+    m2 = _model(c, XBG_FP32, 1)
+    assert tune(m2, cache=cache, reps=1) == choice
+    _, _, n2, _, _ = m2.time()
+    assert n2 == 0   # from the cache: nothing profiled
+    m.close()
+    m2.close()
 
 
 def test_tma_variant_applies_only_where_it_can():

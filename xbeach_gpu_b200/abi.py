@@ -27,6 +27,7 @@ XBG_FP64 = 1
 
 XBG_PHASE_WAVE = 0   # xbg_set_kernel_variant phases
 XBG_PHASE_FLOW = 1
+XBG_PHASE_TILE = 2   # the pointwise passes' block shape: 0 32 x 8 cells, 1 64 x 4
 XBG_CLOCK_BYTES = 240   # xbg_get_time_async copies this many bytes
 
 XBG_FLAG_OUTPUT_DUE = 1

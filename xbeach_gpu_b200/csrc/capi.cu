@@ -27,12 +27,13 @@
 #endif
 
 namespace xbg {
-template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t, const WaveMaps*, int);
+template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, cudaEvent_t, const WaveMaps*, int,
+                                   bool);
 template <class R> int wave_maps_make(const Dev<R>&, const Konst<R>&, WaveMaps*);
 template <class R> int wave_parts(const Konst<R>&);
 template <class R> int wave_prepare(const Konst<R>&);
-template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool);
-template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*);
+template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool, bool);
+template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool);
 template <class R> int step_begin_blocks(const Konst<R>&);
 template <class R> int launch_step_begin(const Dev<R>&, const Konst<R>&, const Series*, int, cudaStream_t, Prof*);
 template <class R> int launch_ubnd(const Dev<R>&, const Konst<R>&, const Series*, cudaStream_t, Prof*);
@@ -43,9 +44,9 @@ template <class R> int launch_wavebnd_batch(const BatchTab<R>&, const BatchLaunc
 template <class R> int launch_ubnd_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_means_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
 template <class R> int launch_wave_batch(const BatchTab<R>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                         cudaEvent_t, const WaveMaps*, int);
-template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
-template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*);
+                                         cudaEvent_t, const WaveMaps*, int, bool);
+template <class R> int launch_flow_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*, bool, bool);
+template <class R> int launch_sed_batch(const BatchTab<R>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
 template <class R> int ubnd_threads(const Konst<R>&);
 template <class R> void launch_output_done(const Dev<R>&, const Konst<R>&, cudaStream_t);
 template <class R> void launch_reset_means(const Dev<R>&, cudaStream_t);
@@ -325,6 +326,9 @@ struct Handle : public xbg_handle {
     int wave_cpt() const { return wave_variant == 2 ? 2 : 1; }
     // flow: momentum steps in one pass (variant 1) or two (variant 0)
     int flow_variant = XBG_FLOW_VARIANT_DEFAULT;
+    // the pointwise passes in 32 x 8 (variant 0) or 64 x 4 (variant 1) blocks
+    int tile_variant = 0;
+    bool wide() const { return tile_variant == 1; }
 
     template <class T> int alloc(T** p, size_t n) {
         void* q = nullptr;
@@ -690,14 +694,14 @@ struct Handle : public xbg_handle {
             n += launch_wavebnd(S, K, ser, side, nullptr, 0);
             if (K.flow == 1) n += launch_ubnd(S, K, ser, side, nullptr);
             cudaEventRecord(ev_join, side);
-            n += launch_wave(S, K, st, nullptr, ev_join, wave_maps(), wave_cpt());
+            n += launch_wave(S, K, st, nullptr, ev_join, wave_maps(), wave_cpt(), wide());
         } else {
             if (K.swave == 1) n += launch_wavebnd(S, K, ser, st, pf, 0);
             if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
-            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps(), wave_cpt());
+            if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps(), wave_cpt(), wide());
         }
-        if (K.flow == 1) n += launch_flow(S, K, st, pf, flow_variant == 1);
-        if (P.sedtrans == 1) n += launch_sed(S, K, st, pf);
+        if (K.flow == 1) n += launch_flow(S, K, st, pf, flow_variant == 1, wide());
+        if (P.sedtrans == 1) n += launch_sed(S, K, st, pf, wide());
         if (K.means) n += launch_means(S, K, st, pf);
         return n;
     }
@@ -741,9 +745,11 @@ struct Handle : public xbg_handle {
             case 0: n = launch_step_begin(S, K, ser, nwave, st, nullptr); break;
             case 1: if (K.swave == 1) n = launch_wavebnd(S, K, ser, st, nullptr, 1); break;
             case 2: if (K.flow == 1) n = launch_ubnd(S, K, ser, st, nullptr); break;
-            case 3: if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps(), wave_cpt()); break;
-            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr, flow_variant == 1); break;
-            case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr); break;
+            case 3:
+                if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps(), wave_cpt(), wide());
+                break;
+            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr, flow_variant == 1, wide()); break;
+            case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr, wide()); break;
             case 6: n = launch_means(S, K, st, nullptr); break;
             default: return XBG_ERR_ARG;
         }
@@ -933,6 +939,9 @@ struct Handle : public xbg_handle {
         } else if (phase == XBG_PHASE_FLOW) {
             if (variant < 0 || variant > 1) return XBG_ERR_ARG;
             slot = &flow_variant;
+        } else if (phase == XBG_PHASE_TILE) {
+            if (variant < 0 || variant > 1) return XBG_ERR_ARG;
+            slot = &tile_variant;
         } else {
             return XBG_ERR_ARG;
         }
@@ -947,6 +956,7 @@ struct Handle : public xbg_handle {
         if (!variant) return XBG_ERR_ARG;
         if (phase == XBG_PHASE_WAVE) *variant = wave_maps() ? wave_variant : 0;
         else if (phase == XBG_PHASE_FLOW) *variant = flow_variant;
+        else if (phase == XBG_PHASE_TILE) *variant = tile_variant;
         else return XBG_ERR_ARG;
         return XBG_OK;
     }
@@ -979,8 +989,8 @@ struct Handle : public xbg_handle {
                 k_set_forcing<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, ee_buf[0], ee_buf[1], rr_buf[0], rr_buf[1],
                                                                     a, b, (R)((double)j / k), j == k ? 1 : 0);
                 n++;
-                if (K.flow == 1) n += launch_flow(S, K, st, nullptr, flow_variant == 1);
-                if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr);
+                if (K.flow == 1) n += launch_flow(S, K, st, nullptr, flow_variant == 1, wide());
+                if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr, wide());
                 n += launch_means(S, K, st, nullptr);
             }
             cudaError_t e = cudaStreamEndCapture(st, &seg_graph);
@@ -1025,6 +1035,8 @@ struct Batch : public xbg_batch {
     int wave_variant = XBG_WAVE_VARIANT_DEFAULT;   // 1, 2: TMA rows pass (when dmaps), 0: thread-copied tiles
     const WaveMaps* wave_maps() const { return wave_variant >= 1 ? dmaps : nullptr; }
     int wave_cpt() const { return wave_variant == 2 ? 2 : 1; }
+    int tile_variant = 0;   // the pointwise passes over 32 x 8 (0) or 64 x 4 (1) tiles
+    bool wide() const { return tile_variant == 1; }
     int flow_variant = XBG_FLOW_VARIANT_DEFAULT;   // 1: momentum steps in one pass, 0: two
     // surrogate-assisted stepping: forcing planes per scenario, graphs of
     // forced segments by length, judge accumulators
@@ -1093,6 +1105,8 @@ struct Batch : public xbg_batch {
             auto add = [&](int sh, int bx, int by) { it[sh].push_back(make_int2(s, bx | (by << 16))); };
             for (int by = 0; by < (ny + 7) / 8; by++)
                 for (int bx = 0; bx < (nx + 31) / 32; bx++) add(BS_TILE, bx, by);
+            for (int by = 0; by < (ny + 3) / 4; by++)
+                for (int bx = 0; bx < (nx + 63) / 64; bx++) add(BS_WIDE, bx, by);
             for (int by = 0; by < (ny - 2 + 7) / 8; by++)
                 for (int bx = 0; bx < (nx + 31) / 32; bx++) add(BS_WROWS, bx, by);
             for (int b = 0; b < (C + 255) / 256; b++) add(BS_LIN, b, 0);
@@ -1118,7 +1132,7 @@ struct Batch : public xbg_batch {
         int dev = 0, sms = 148;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        const int per_sm[BS_N] = {8, dmaps ? 4 : 3, 8, 2, 8, 8};   // resident-block targets per SM
+        const int per_sm[BS_N] = {8, dmaps ? 4 : 3, 8, 2, 8, 8, 8};   // resident-block targets per SM
         for (int k = 0; k < BS_N; k++) {
             CK(cudaMalloc(&ditems[k], std::max<size_t>(1, it[k].size()) * sizeof(int2)));
             CK(cudaMemcpy(ditems[k], it[k].data(), it[k].size() * sizeof(int2), cudaMemcpyHostToDevice));
@@ -1150,19 +1164,20 @@ struct Batch : public xbg_batch {
             k += launch_wavebnd_batch(T, L, side, nullptr);
             if (flow == 1) k += launch_ubnd_batch(T, L, side, nullptr);
             cudaEventRecord(ev_join, side);
-            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join, wave_maps(), wave_cpt());
+            k += launch_wave_batch(T, L, nt, roller, wci, st, nullptr, ev_join, wave_maps(), wave_cpt(), wide());
         } else {
             if (swave == 1) k += launch_wavebnd_batch(T, L, st, pf);
             if (flow == 1) k += launch_ubnd_batch(T, L, st, pf);
-            if (swave == 1) k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr, wave_maps(), wave_cpt());
+            if (swave == 1)
+                k += launch_wave_batch(T, L, nt, roller, wci, st, pf, nullptr, wave_maps(), wave_cpt(), wide());
         }
         return k;
     }
     // flow, sediment and means of one batched step
     int enqueue_rest(const BatchTab<R>& T, Prof* pf) {
         int k = 0;
-        if (flow == 1) k += launch_flow_batch(T, L, st, pf, flow_variant == 1);
-        if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf);
+        if (flow == 1) k += launch_flow_batch(T, L, st, pf, flow_variant == 1, wide());
+        if (sedtrans == 1) k += launch_sed_batch(T, L, st, pf, wide());
         if (means) k += launch_means_batch(T, L, st, pf);
         return k;
     }
@@ -1241,6 +1256,9 @@ struct Batch : public xbg_batch {
         } else if (phase == XBG_PHASE_FLOW) {
             if (variant < 0 || variant > 1) return XBG_ERR_ARG;
             slot = &flow_variant;
+        } else if (phase == XBG_PHASE_TILE) {
+            if (variant < 0 || variant > 1) return XBG_ERR_ARG;
+            slot = &tile_variant;
         } else {
             return XBG_ERR_ARG;
         }
@@ -1257,6 +1275,7 @@ struct Batch : public xbg_batch {
         if (!variant) return XBG_ERR_ARG;
         if (phase == XBG_PHASE_WAVE) *variant = wave_maps() ? wave_variant : 0;
         else if (phase == XBG_PHASE_FLOW) *variant = flow_variant;
+        else if (phase == XBG_PHASE_TILE) *variant = tile_variant;
         else return XBG_ERR_ARG;
         return XBG_OK;
     }

@@ -655,19 +655,22 @@ __device__ __forceinline__ void b_flow_final(const Dev<R>& S, const Konst<R>& K,
 XBG_KERNELS(flow_final)
 
 // fuse_uv: the momentum steps as one pass (k_flow_uv) instead of two
-// (k_flow_u, k_flow_v)
+// (k_flow_u, k_flow_v); wide: the pointwise passes (k_flow_a, k_flow_u,
+// k_flow_v) in 64 x 4 blocks instead of 32 x 8 (their bodies index cells by
+// the block's shape; the staged passes keep their 32 x 8 tiles)
 template <class R>
-int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool fuse_uv) {
+int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool fuse_uv, bool wide) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
-    k_flow_a<R><<<g, b, 0, st>>>(S, K);
+    dim3 bp = wide ? dim3(64, 4) : b, gp = wide ? dim3((K.nx + 63) / 64, (K.ny + 3) / 4) : g;
+    k_flow_a<R><<<gp, bp, 0, st>>>(S, K);
     PMARK(pf, "k_flow_a");
     if (fuse_uv) {
         k_flow_uv<R><<<g, b, 0, st>>>(S, K);
         PMARK(pf, "k_flow_uv");
     } else {
-        k_flow_u<R><<<g, b, 0, st>>>(S, K);
+        k_flow_u<R><<<gp, bp, 0, st>>>(S, K);
         PMARK(pf, "k_flow_u");
-        k_flow_v<R><<<g, b, 0, st>>>(S, K);
+        k_flow_v<R><<<gp, bp, 0, st>>>(S, K);
         PMARK(pf, "k_flow_v");
     }
     k_flow_corr<R><<<g, b, 0, st>>>(S, K);
@@ -678,19 +681,24 @@ int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, b
 }
 // the flow kernels over every scenario of a batch
 template <class R>
-int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf, bool fuse_uv) {
+int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf, bool fuse_uv,
+                      bool wide) {
     dim3 b(32, 8);
     const int2* it = L.items[BS_TILE];
     int n = L.n[BS_TILE], g = L.grid[BS_TILE];
-    kb_flow_a<R><<<g, b, 0, st>>>(T, it, n);
+    const int sp = wide ? BS_WIDE : BS_TILE;
+    const dim3 bp = wide ? dim3(64, 4) : b;
+    const int2* itp = L.items[sp];
+    const int np = L.n[sp], gp = L.grid[sp];
+    kb_flow_a<R><<<gp, bp, 0, st>>>(T, itp, np);
     PMARK(pf, "k_flow_a");
     if (fuse_uv) {
         kb_flow_uv<R><<<g, b, 0, st>>>(T, it, n);
         PMARK(pf, "k_flow_uv");
     } else {
-        kb_flow_u<R><<<g, b, 0, st>>>(T, it, n);
+        kb_flow_u<R><<<gp, bp, 0, st>>>(T, itp, np);
         PMARK(pf, "k_flow_u");
-        kb_flow_v<R><<<g, b, 0, st>>>(T, it, n);
+        kb_flow_v<R><<<gp, bp, 0, st>>>(T, itp, np);
         PMARK(pf, "k_flow_v");
     }
     kb_flow_corr<R><<<g, b, 0, st>>>(T, it, n);
@@ -699,10 +707,10 @@ int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t s
     PMARK(pf, "k_flow_final");
     return fuse_uv ? 4 : 5;
 }
-template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
-template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
+template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*, bool, bool);
+template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*, bool, bool);
 
-template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool);
-template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool);
+template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool, bool);
+template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool, bool);
 
 }  // namespace xbg

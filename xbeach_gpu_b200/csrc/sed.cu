@@ -381,10 +381,12 @@ __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, cons
 }
 XBG_KERNELS(sed_c)
 
+// wide: the pointwise first pass in 64 x 4 blocks instead of 32 x 8
 template <class R>
-int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
+int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool wide) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
-    k_sed_a<R><<<g, b, 0, st>>>(S, K);
+    if (wide) k_sed_a<R><<<dim3((K.nx + 63) / 64, (K.ny + 3) / 4), dim3(64, 4), 0, st>>>(S, K);
+    else k_sed_a<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_sed_a");
     k_sed_b<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_sed_b");
@@ -394,11 +396,12 @@ int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf) {
 }
 // the three sediment kernels over every scenario of a batch
 template <class R>
-int launch_sed_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf) {
+int launch_sed_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st, Prof* pf, bool wide) {
     dim3 b(32, 8);
     const int2* it = L.items[BS_TILE];
     int n = L.n[BS_TILE], g = L.grid[BS_TILE];
-    kb_sed_a<R><<<g, b, 0, st>>>(T, it, n);
+    if (wide) kb_sed_a<R><<<L.grid[BS_WIDE], dim3(64, 4), 0, st>>>(T, L.items[BS_WIDE], L.n[BS_WIDE]);
+    else kb_sed_a<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_sed_a");
     kb_sed_b<R><<<g, b, 0, st>>>(T, it, n);
     PMARK(pf, "k_sed_b");
@@ -406,10 +409,10 @@ int launch_sed_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st
     PMARK(pf, "k_sed_c");
     return 3;
 }
-template int launch_sed_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*);
-template int launch_sed_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*);
+template int launch_sed_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
+template int launch_sed_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
 
-template int launch_sed<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*);
-template int launch_sed<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*);
+template int launch_sed<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool);
+template int launch_sed<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool);
 
 }  // namespace xbg

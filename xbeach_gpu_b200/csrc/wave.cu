@@ -1286,7 +1286,7 @@ int wave_parts(const Konst<R>& K) {
 // tiles (b_wave_fast); the TMA pass has no wave-current interaction variant.
 template <class R>
 int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, cudaEvent_t join,
-                const WaveMaps* maps, int cpt) {
+                const WaveMaps* maps, int cpt, bool wide) {
     int n = 0;
     k_disp<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, K); n++;
     PMARK(pf, "k_disp");
@@ -1310,8 +1310,10 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, c
             PMARK(pf, "k_wave_fast");
         }
     }
-    dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
-    k_wave_force<R><<<g, b, 0, st>>>(S, K); n++;
+    // the force pass is pointwise: 32 x 8 or (wide) 64 x 4 blocks
+    if (wide) k_wave_force<R><<<dim3((K.nx + 63) / 64, (K.ny + 3) / 4), dim3(64, 4), 0, st>>>(S, K);
+    else k_wave_force<R><<<dim3((K.nx + 31) / 32, (K.ny + 7) / 8), dim3(32, 8), 0, st>>>(S, K);
+    n++;
     PMARK(pf, "k_wave_force");
     return n;
 }
@@ -1322,7 +1324,7 @@ int launch_wave(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, c
 // null for the thread-copied tiles
 template <class R>
 int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int roller, int wci, cudaStream_t st,
-                      Prof* pf, cudaEvent_t join, const WaveMaps* maps, int cpt) {
+                      Prof* pf, cudaEvent_t join, const WaveMaps* maps, int cpt, bool wide) {
     kb_disp<R><<<L.grid[BS_LIN], 256, 0, st>>>(T, L.items[BS_LIN], L.n[BS_LIN]);
     PMARK(pf, "k_disp");
     if (join) cudaStreamWaitEvent(st, join, 0);
@@ -1342,14 +1344,15 @@ int launch_wave_batch(const BatchTab<R>& T, const BatchLaunch& L, int nt, int ro
         launch_wave_fast_batch(T, L, roller, wci, wave_fast_smem<R>(nt), st);
         PMARK(pf, "k_wave_fast");
     }
-    kb_wave_force<R><<<L.grid[BS_TILE], dim3(32, 8), 0, st>>>(T, L.items[BS_TILE], L.n[BS_TILE]);
+    const int sf = wide ? BS_WIDE : BS_TILE;
+    kb_wave_force<R><<<L.grid[sf], wide ? dim3(64, 4) : dim3(32, 8), 0, st>>>(T, L.items[sf], L.n[sf]);
     PMARK(pf, "k_wave_force");
     return 3;
 }
 template int launch_wave_batch<float>(const BatchTab<float>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                      cudaEvent_t, const WaveMaps*, int);
+                                      cudaEvent_t, const WaveMaps*, int, bool);
 template int launch_wave_batch<double>(const BatchTab<double>&, const BatchLaunch&, int, int, int, cudaStream_t, Prof*,
-                                       cudaEvent_t, const WaveMaps*, int);
+                                       cudaEvent_t, const WaveMaps*, int, bool);
 
 // One-time kernel attributes (dynamic shared memory above 48 KB for wide
 // theta sets in FP64).
@@ -1380,9 +1383,9 @@ template int wave_prepare<float>(const Konst<float>&);
 template int wave_prepare<double>(const Konst<double>&);
 
 template int launch_wave<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, cudaEvent_t,
-                                const WaveMaps*, int);
+                                const WaveMaps*, int, bool);
 template int launch_wave<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, cudaEvent_t,
-                                 const WaveMaps*, int);
+                                 const WaveMaps*, int, bool);
 template int wave_maps_make<float>(const Dev<float>&, const Konst<float>&, WaveMaps*);
 template int wave_maps_make<double>(const Dev<double>&, const Konst<double>&, WaveMaps*);
 template int wave_parts<float>(const Konst<float>&);

@@ -320,6 +320,7 @@ enum BatchShape {
     BS_ONE,     // one block per scenario
     BS_BND,     // 256-value runs of the ny*ntheta boundary values
     BS_DT,      // the blocks of the dt reduction
+    BS_WIDE,    // 64 x 4 tiles over nx x ny (the pointwise passes' other shape)
     BS_N
 };
 struct BatchLaunch {

@@ -284,7 +284,8 @@ class Model:
     def set_variant(self, phase, variant):
         """Kernel variant of a phase (XBG_PHASE_WAVE: 1 / 2 TMA tiles with one /
         two cells per thread, 0 thread-copied tiles; XBG_PHASE_FLOW: 1 fused
-        momentum pass, 0 two passes)."""
+        momentum pass, 0 two passes; XBG_PHASE_TILE: the pointwise passes in
+        0 32 x 8 or 1 64 x 4 blocks)."""
         _check(self.L.xbg_set_kernel_variant(self.h, phase, variant), "set_kernel_variant")
 
     def variant(self, phase):
