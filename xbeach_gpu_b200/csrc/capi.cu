@@ -32,7 +32,7 @@ template <class R> int launch_wave(const Dev<R>&, const Konst<R>&, cudaStream_t,
 template <class R> int wave_maps_make(const Dev<R>&, const Konst<R>&, WaveMaps*);
 template <class R> int wave_parts(const Konst<R>&);
 template <class R> int wave_prepare(const Konst<R>&);
-template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool, bool);
+template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool, bool, bool);
 template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool);
 template <class R> int step_begin_blocks(const Konst<R>&);
 template <class R> int launch_step_begin(const Dev<R>&, const Konst<R>&, const Series*, int, cudaStream_t, Prof*);
@@ -326,9 +326,11 @@ struct Handle : public xbg_handle {
     int wave_cpt() const { return wave_variant == 2 ? 2 : 1; }
     // flow: momentum steps in one pass (variant 1) or two (variant 0)
     int flow_variant = XBG_FLOW_VARIANT_DEFAULT;
-    // the pointwise passes in 32 x 8 (variant 0) or 64 x 4 (variant 1) blocks
+    // the pointwise passes in 32 x 8 (variant 0) or 64 x 4 (variant 1) blocks,
+    // or (variant 2) row segments of 16-byte loads where a pass has that form
     int tile_variant = 0;
     bool wide() const { return tile_variant == 1; }
+    bool vec() const { return tile_variant == 2; }
 
     template <class T> int alloc(T** p, size_t n) {
         void* q = nullptr;
@@ -700,7 +702,7 @@ struct Handle : public xbg_handle {
             if (K.flow == 1) n += launch_ubnd(S, K, ser, st, pf);
             if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps(), wave_cpt(), wide());
         }
-        if (K.flow == 1) n += launch_flow(S, K, st, pf, flow_variant == 1, wide());
+        if (K.flow == 1) n += launch_flow(S, K, st, pf, flow_variant == 1, wide(), vec());
         if (P.sedtrans == 1) n += launch_sed(S, K, st, pf, wide());
         if (K.means) n += launch_means(S, K, st, pf);
         return n;
@@ -748,7 +750,7 @@ struct Handle : public xbg_handle {
             case 3:
                 if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps(), wave_cpt(), wide());
                 break;
-            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr, flow_variant == 1, wide()); break;
+            case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr, flow_variant == 1, wide(), vec()); break;
             case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr, wide()); break;
             case 6: n = launch_means(S, K, st, nullptr); break;
             default: return XBG_ERR_ARG;
@@ -940,7 +942,8 @@ struct Handle : public xbg_handle {
             if (variant < 0 || variant > 1) return XBG_ERR_ARG;
             slot = &flow_variant;
         } else if (phase == XBG_PHASE_TILE) {
-            if (variant < 0 || variant > 1) return XBG_ERR_ARG;
+            const int vw = sizeof(R) == 4 ? 4 : 2;   // cells per 16-byte segment
+            if (variant < 0 || variant > 2 || (variant == 2 && K.nx % vw != 0)) return XBG_ERR_ARG;
             slot = &tile_variant;
         } else {
             return XBG_ERR_ARG;
@@ -989,7 +992,7 @@ struct Handle : public xbg_handle {
                 k_set_forcing<R><<<(S.C + 255) / 256, 256, 0, st>>>(S, ee_buf[0], ee_buf[1], rr_buf[0], rr_buf[1],
                                                                     a, b, (R)((double)j / k), j == k ? 1 : 0);
                 n++;
-                if (K.flow == 1) n += launch_flow(S, K, st, nullptr, flow_variant == 1, wide());
+                if (K.flow == 1) n += launch_flow(S, K, st, nullptr, flow_variant == 1, wide(), vec());
                 if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr, wide());
                 n += launch_means(S, K, st, nullptr);
             }

@@ -40,23 +40,57 @@ __device__ __forceinline__ R minmod(R d1, R d2) {   // Flow_kernel.cu:23-41
 constexpr int FT_X = 32, FT_Y = 8, FT_TX = FT_X + 2, FT_TY = FT_Y + 2, FT_N = FT_TX * FT_TY;
 constexpr int FC_H = 3;   // tile halo of the momentum-correction pass
 
-// smago (Flow_kernel.cu:1282-1316) at cell (ix, iy)
+// smago (Flow_kernel.cu:1282-1316) from its inputs: depth and DR of the
+// cell; uu at the cell and its left (xm), upper (yp), lower (ym), upper-left
+// and lower-left neighbours; vv at the cell and its lower, right, left,
+// lower-right and lower-left neighbours (mm/pp-clamped at the grid edges)
+template <class R>
+struct SmagoIn { R h, dr, u, uxm, uyp, uym, uxmyp, uxmym, v, vym, vxp, vxm, vxpym, vxmym; };
+template <class R>
+__device__ __forceinline__ R smago_of(const Konst<R>& K, const SmagoIn<R>& a) {
+    R dx = K.dx, rdx = K.rdx, nuh = K.nuh, nuhfac = K.nuhfac, rho = K.rho;
+    R b = nuhfac * a.h * DM<R>::pow13(a.dr / rho);
+    if (K.usesmago == 1) {
+        R dudx = (a.u - a.uxm) * rdx;
+        R dudy = (R)0.50f * (a.uyp - a.uym + a.uxmyp - a.uxmym) * rdx;
+        R dvdy = (a.v - a.vym) * rdx;
+        R dvdx = (R)0.50f * (a.vxp - a.vxm + a.vxpym - a.vxmym) * rdx;
+        R tau = DM<R>::sqrt((R)2.0f * dudx * dudx + (R)2.0f * dvdy * dvdy + (dudy + dvdx) * (dudy + dvdx));
+        return DM<R>::fmax(nuh * nuh * dx * dx * tau, b);
+    }
+    return DM<R>::fmax(nuh, b);
+}
+// smago at cell (ix, iy)
 template <class R>
 __device__ __forceinline__ R smago_cell(const Dev<R>& S, const Konst<R>& K, int ix, int iy) {
     const int nx = K.nx, ny = K.ny;
     const R* uu = S.f[UU]; const R* vv = S.f[VV];
     int i = IDX(ix, iy), xm = mm(ix), xp = pp(ix, nx), ym = mm(iy), yp = pp(iy, ny);
-    R dx = K.dx, rdx = K.rdx, nuh = K.nuh, nuhfac = K.nuhfac, rho = K.rho;
-    R b = nuhfac * ld(S.f[HH] + i) * DM<R>::pow13(ld(S.f[DR] + i) / rho);
+    SmagoIn<R> a{};
+    a.h = ld(S.f[HH] + i);
+    a.dr = ld(S.f[DR] + i);
     if (K.usesmago == 1) {
-        R dudx = (ld(uu + i) - ld(uu + IDX(xm, iy))) * rdx;
-        R dudy = (R)0.50f * (ld(uu + IDX(ix, yp)) - ld(uu + IDX(ix, ym)) + ld(uu + IDX(xm, yp)) - ld(uu + IDX(xm, ym))) * rdx;
-        R dvdy = (ld(vv + i) - ld(vv + IDX(ix, ym))) * rdx;
-        R dvdx = (R)0.50f * (ld(vv + IDX(xp, iy)) - ld(vv + IDX(xm, iy)) + ld(vv + IDX(xp, ym)) - ld(vv + IDX(xm, ym))) * rdx;
-        R tau = DM<R>::sqrt((R)2.0f * dudx * dudx + (R)2.0f * dvdy * dvdy + (dudy + dvdx) * (dudy + dvdx));
-        return DM<R>::fmax(nuh * nuh * dx * dx * tau, b);
+        a.u = ld(uu + i); a.uxm = ld(uu + IDX(xm, iy)); a.uyp = ld(uu + IDX(ix, yp)); a.uym = ld(uu + IDX(ix, ym));
+        a.uxmyp = ld(uu + IDX(xm, yp)); a.uxmym = ld(uu + IDX(xm, ym));
+        a.v = ld(vv + i); a.vym = ld(vv + IDX(ix, ym)); a.vxp = ld(vv + IDX(xp, iy)); a.vxm = ld(vv + IDX(xm, iy));
+        a.vxpym = ld(vv + IDX(xp, ym)); a.vxmym = ld(vv + IDX(xm, ym));
     }
-    return DM<R>::fmax(nuh, b);
+    return smago_of(K, a);
+}
+
+// udepthmomcont / vdepthmomcont (Flow_kernel.cu:653-750) from the cell's
+// depth, its right and upper neighbours' and the cell's hu, hv
+template <class R>
+struct DepthMom { R humi, hvmi; int wu, wv; };
+template <class R>
+__device__ __forceinline__ DepthMom<R> depthmom_of(const Konst<R>& K, R hh, R hhxp, R hhyp, R hu, R hv) {
+    const R eps = K.eps;
+    DepthMom<R> o;
+    o.humi = (R)0.5f * (hh + hhxp);
+    o.wu = (hu > eps && o.humi > eps) ? 1 : 0;
+    o.hvmi = (R)0.5f * (hh + hhyp);
+    o.wv = (hv > eps && o.hvmi > eps) ? 1 : 0;
+    return o;
 }
 
 template <class R>
@@ -68,20 +102,105 @@ __device__ __forceinline__ void b_flow_a(const Dev<R>& S, const Konst<R>& K, con
     int i = IDX(ix, iy);
     R eps = K.eps;
     R hh = ld(S.f[HH] + i);
-    R humi = (R)0.5f * (hh + ld(S.f[HH] + IDX(pp(ix, nx), iy)));
-    const int wu = (ld(S.f[HU] + i) > eps && humi > eps) ? 1 : 0;
-    R hvmi = (R)0.5f * (hh + ld(S.f[HH] + IDX(ix, pp(iy, ny))));
-    const int wv = (ld(S.f[HV] + i) > eps && hvmi > eps) ? 1 : 0;
+    const DepthMom<R> d = depthmom_of(K, hh, ld(S.f[HH] + IDX(pp(ix, nx), iy)), ld(S.f[HH] + IDX(ix, pp(iy, ny))),
+                                      ld(S.f[HU] + i), ld(S.f[HV] + i));
     const R nuh = smago_cell(S, K, ix, iy);
     loads_before_here();
     if (off) return;
-    S.wetu[i] = wu;
-    S.f[HUM][i] = DM<R>::fmax(humi, eps);
-    S.wetv[i] = wv;
-    S.f[HVM][i] = DM<R>::fmax(hvmi, eps);
+    S.wetu[i] = d.wu;
+    S.f[HUM][i] = DM<R>::fmax(d.humi, eps);
+    S.wetv[i] = d.wv;
+    S.f[HVM][i] = DM<R>::fmax(d.hvmi, eps);
     S.tmp[T_NUH][i] = nuh;
 }
 XBG_KERNELS(flow_a)
+
+// The same pass over row segments: each thread takes V consecutive cells of
+// one row (V = 4 in FP32, 2 in FP64) with one 16-byte load per field and row;
+// a warp is one row of 32 V cells, and the neighbours left and right of a
+// thread's segment come from the adjacent lanes (the first and last lane of
+// a warp load theirs).  The arithmetic is the scalar pass's (the same
+// functions), so the results are bit-identical.  Needs nx a multiple of V.
+template <class R> struct FlowVec;
+template <> struct FlowVec<float> { using T = float4; using I = int4; static constexpr int V = 4; };
+template <> struct FlowVec<double> { using T = double2; using I = int2; static constexpr int V = 2; };
+
+template <class R>
+__global__ void __launch_bounds__(256) k_flow_a_v(Dev<R> S, Konst<R> K) {
+    using VT = typename FlowVec<R>::T;
+    using VI = typename FlowVec<R>::I;
+    constexpr int V = FlowVec<R>::V;
+    union U { VT v; R a[V]; };
+    union W { VI v; int a[V]; };
+    const bool off = halted(S.clk);
+    const int nx = K.nx, ny = K.ny;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (iy >= ny) return;   // the whole warp: a warp is one row
+    const int lane = threadIdx.x;
+    const int x0 = (blockIdx.x * blockDim.x + lane) * V;
+    const bool act = x0 < nx;
+    const int ym = mm(iy), yp = pp(iy, ny);
+    auto row = [&](const R* f, int y) {
+        U u;
+        if (act) u.v = __ldg(reinterpret_cast<const VT*>(f + (size_t)y * nx + x0));
+        else
+            for (int k = 0; k < V; k++) u.a[k] = (R)0;
+        return u;
+    };
+    // the value left of the segment (mm: the cell itself at column 0) and
+    // right of it (pp: the cell itself at the last column)
+    auto left = [&](const U& u, const R* f, int y) -> R {
+        R w = __shfl_up_sync(0xffffffffu, u.a[V - 1], 1);
+        if (lane == 0 && act && x0 > 0) w = ld(f + (size_t)y * nx + x0 - 1);
+        return x0 > 0 ? w : u.a[0];
+    };
+    auto right = [&](const U& u, const R* f, int y) -> R {
+        R w = __shfl_down_sync(0xffffffffu, u.a[0], 1);
+        if (lane == 31 && act && x0 + V < nx) w = ld(f + (size_t)y * nx + x0 + V);
+        return x0 + V < nx ? w : u.a[V - 1];
+    };
+    const U h = row(S.f[HH], iy), hyp = row(S.f[HH], yp), hu = row(S.f[HU], iy), hv = row(S.f[HV], iy);
+    const U dr = row(S.f[DR], iy);
+    const R hr = right(h, S.f[HH], iy);
+    U u{}, uyp{}, uym{}, v{}, vym{};
+    R ul = 0, ulyp = 0, ulym = 0, vl = 0, vr = 0, vlym = 0, vrym = 0;
+    const bool smago = K.usesmago == 1;   // uniform
+    if (smago) {
+        const R* uu = S.f[UU]; const R* vv = S.f[VV];
+        u = row(uu, iy); uyp = row(uu, yp); uym = row(uu, ym); v = row(vv, iy); vym = row(vv, ym);
+        ul = left(u, uu, iy); ulyp = left(uyp, uu, yp); ulym = left(uym, uu, ym);
+        vl = left(v, vv, iy); vr = right(v, vv, iy); vlym = left(vym, vv, ym); vrym = right(vym, vv, ym);
+    }
+    const R eps = K.eps;
+    U hum, hvm, nuh;
+    W wu, wv;
+#pragma unroll
+    for (int k = 0; k < V; k++) {
+        const DepthMom<R> d = depthmom_of(K, h.a[k], k < V - 1 ? h.a[k + 1] : hr, hyp.a[k], hu.a[k], hv.a[k]);
+        SmagoIn<R> a{};
+        a.h = h.a[k];
+        a.dr = dr.a[k];
+        if (smago) {
+            a.u = u.a[k]; a.uxm = k > 0 ? u.a[k - 1] : ul; a.uyp = uyp.a[k]; a.uym = uym.a[k];
+            a.uxmyp = k > 0 ? uyp.a[k - 1] : ulyp; a.uxmym = k > 0 ? uym.a[k - 1] : ulym;
+            a.v = v.a[k]; a.vym = vym.a[k]; a.vxp = k < V - 1 ? v.a[k + 1] : vr; a.vxm = k > 0 ? v.a[k - 1] : vl;
+            a.vxpym = k < V - 1 ? vym.a[k + 1] : vrym; a.vxmym = k > 0 ? vym.a[k - 1] : vlym;
+        }
+        nuh.a[k] = smago_of(K, a);
+        hum.a[k] = DM<R>::fmax(d.humi, eps);
+        hvm.a[k] = DM<R>::fmax(d.hvmi, eps);
+        wu.a[k] = d.wu;
+        wv.a[k] = d.wv;
+    }
+    loads_before_here();
+    if (off || !act) return;
+    const size_t i = (size_t)iy * nx + x0;
+    *reinterpret_cast<VI*>(S.wetu + i) = wu.v;
+    *reinterpret_cast<VT*>(S.f[HUM] + i) = hum.v;
+    *reinterpret_cast<VI*>(S.wetv + i) = wv.v;
+    *reinterpret_cast<VT*>(S.f[HVM] + i) = hvm.v;
+    *reinterpret_cast<VT*>(S.tmp[T_NUH] + i) = nuh.v;
+}
 
 // eulerustep (Flow_kernel.cu:1487-1544) at an interior-x cell, with the
 // advection (ududx_adv :752, vdudy_adv :887) and viscosity (viscou1 :1319,
@@ -659,10 +778,16 @@ XBG_KERNELS(flow_final)
 // k_flow_v) in 64 x 4 blocks instead of 32 x 8 (their bodies index cells by
 // the block's shape; the staged passes keep their 32 x 8 tiles)
 template <class R>
-int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool fuse_uv, bool wide) {
+int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool fuse_uv, bool wide,
+                bool vec) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
     dim3 bp = wide ? dim3(64, 4) : b, gp = wide ? dim3((K.nx + 63) / 64, (K.ny + 3) / 4) : g;
-    k_flow_a<R><<<gp, bp, 0, st>>>(S, K);
+    if (vec && K.nx % FlowVec<R>::V == 0) {
+        const int V = FlowVec<R>::V;
+        k_flow_a_v<R><<<dim3((K.nx / V + 31) / 32, (K.ny + 7) / 8), dim3(32, 8), 0, st>>>(S, K);
+    } else {
+        k_flow_a<R><<<gp, bp, 0, st>>>(S, K);
+    }
     PMARK(pf, "k_flow_a");
     if (fuse_uv) {
         k_flow_uv<R><<<g, b, 0, st>>>(S, K);
@@ -710,7 +835,7 @@ int launch_flow_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t s
 template int launch_flow_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*, bool, bool);
 template int launch_flow_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*, bool, bool);
 
-template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool, bool);
-template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool, bool);
+template int launch_flow<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool, bool, bool);
+template int launch_flow<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool, bool, bool);
 
 }  // namespace xbg
