@@ -235,7 +235,11 @@ int  xbg_profile_step(xbg_handle* h, float* ms, const char** names, int* n);
  * XBG_ERR_ARG; get reports the one in use.  Phase XBG_PHASE_TILE: the tile
  * shape of the passes that read only a cell and its nearest neighbours
  * (wavforce, the depth/viscosity and momentum passes, the first sediment
- * pass): variant 0 blocks of 32 x 8 cells, variant 1 blocks of 64 x 4.   */
+ * pass): variant 0 blocks of 32 x 8 cells, variant 1 blocks of 64 x 4;
+ * variant 2 (single domain, nx a multiple of 4 in FP32 or 2 in FP64; the
+ * default there) runs the depth/viscosity pass and the first sediment pass
+ * over row segments, 4 (2) cells per thread with 16-byte loads, and the
+ * others in 32 x 8 blocks.                                                 */
 #define XBG_PHASE_WAVE 0
 #define XBG_PHASE_FLOW 1
 #define XBG_PHASE_TILE 2

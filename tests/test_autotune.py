@@ -56,6 +56,7 @@ class FakeBatch(FakeModel):
     are fastest at `best_blocks` on the shape they run on."""
 
     def __init__(self, best_blocks=148 * 4, **kw):
+        kw.setdefault("refuse", {(XBG_PHASE_TILE, 2)})   # row segments are a single-domain form
         super().__init__(**kw)
         self.models = [FakeModel(nx, ny) for nx, ny in ((256, 128), (512, 256))]
         self.n = len(self.models)
@@ -96,7 +97,8 @@ def test_batch_search_applies_and_caches(tmp_path):
 
 
 def test_refused_variant_is_skipped(tmp_path):
-    b = FakeBatch(refuse={(XBG_PHASE_WAVE, 2)}, best={XBG_PHASE_WAVE: 2, XBG_PHASE_FLOW: 0, XBG_PHASE_TILE: 0})
+    b = FakeBatch(refuse={(XBG_PHASE_WAVE, 2), (XBG_PHASE_TILE, 2)},
+                  best={XBG_PHASE_WAVE: 2, XBG_PHASE_FLOW: 0, XBG_PHASE_TILE: 0})
     choice = at.tune(b, cache=str(tmp_path / "t.json"), reps=1)
     assert choice["wave_variant"] in (0, 1) and choice["flow_variant"] == 0 and choice["tile_variant"] == 0
     assert b.var[XBG_PHASE_TILE] == 0 and b.grid[at.SHAPE_TILE] == 148 * 4
@@ -117,10 +119,12 @@ def test_single_domain_search(tmp_path):
     m = FakeModel()
     choice = at.tune(m, cache=cache, reps=1)
     assert choice == {"wave_variant": 2, "flow_variant": 1, "tile_variant": 1}
-    assert m.steps == 4 + 3   # four tile-phase settings and three wave variants, one step each
+    assert m.steps == 6 + 3   # six tile-phase settings and three wave variants, one step each
     m2 = FakeModel()
     assert at.tune(m2, cache=cache, reps=1) == choice and m2.steps == 0
+    m4 = FakeModel(best={XBG_PHASE_WAVE: 1, XBG_PHASE_FLOW: 0, XBG_PHASE_TILE: 2})
+    assert at.tune(m4, cache=str(tmp_path / "t4.json"), reps=1)["tile_variant"] == 2
     # another grid is another cache key
     m3 = FakeModel(nx=512)
     at.tune(m3, cache=cache, reps=1)
-    assert m3.steps == 7
+    assert m3.steps == 9

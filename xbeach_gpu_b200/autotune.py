@@ -9,7 +9,8 @@ runs: the wave rows pass has TMA plane tiles with one or two cells per thread
 momentum updates run fused into one pass or split in two (a fusion split);
 and the passes that read only a cell and its nearest neighbours (wavforce,
 the depth/viscosity and momentum passes, the first sediment pass) run in
-tiles of 32 x 8 or 64 x 4 cells (two tile shapes, both compiled).  They
+tiles of 32 x 8 or 64 x 4 cells (two tile shapes, both compiled) or, for one
+domain, over row segments of four cells per thread.  They
 trade per-item latency, occupancy, per-cell instructions and memory traffic
 differently, so all are measured: for each phase, every (kernel variants,
 block count) candidate is timed with CUDA events around each kernel of a
@@ -37,12 +38,14 @@ SHAPE_TILE, SHAPE_WROWS, SHAPE_LIN, SHAPE_DT, SHAPE_WIDE = 0, 1, 2, 5, 6
 # (xbg_set_kernel_variant phase, variant) pairs (empty: the phase has one
 # form).  The "tile" phase searches the momentum fusion split with the
 # pointwise passes' tile shape; with 64 x 4 tiles those passes take the
-# 64 x 4 work list, given the same number of persistent blocks.
+# 64 x 4 work list, given the same number of persistent blocks; the row
+# segments (tile variant 2) are a single-domain form, which a batch refuses.
 _T, _F = XBG_PHASE_TILE, XBG_PHASE_FLOW
 PHASES = {
     "tile": (SHAPE_TILE, {"k_wave_force", "k_flow_a", "k_flow_u", "k_flow_v", "k_flow_uv", "k_flow_corr",
                           "k_flow_final", "k_sed_a", "k_sed_b", "k_sed_c"},
-             (((_F, 1), (_T, 0)), ((_F, 0), (_T, 0)), ((_F, 1), (_T, 1)), ((_F, 0), (_T, 1)))),
+             (((_F, 1), (_T, 0)), ((_F, 0), (_T, 0)), ((_F, 1), (_T, 1)), ((_F, 0), (_T, 1)),
+              ((_F, 1), (_T, 2)), ((_F, 0), (_T, 2)))),
     "wave_rows": (SHAPE_WROWS, {"k_wave_fast", "k_wave_tma"}, (((XBG_PHASE_WAVE, 1),), ((XBG_PHASE_WAVE, 2),),
                                                                ((XBG_PHASE_WAVE, 0),))),
     "lin": (SHAPE_LIN, {"k_disp", "k_means"}, ((),)),

@@ -33,7 +33,7 @@ template <class R> int wave_maps_make(const Dev<R>&, const Konst<R>&, WaveMaps*)
 template <class R> int wave_parts(const Konst<R>&);
 template <class R> int wave_prepare(const Konst<R>&);
 template <class R> int launch_flow(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool, bool, bool);
-template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool);
+template <class R> int launch_sed(const Dev<R>&, const Konst<R>&, cudaStream_t, Prof*, bool, bool);
 template <class R> int step_begin_blocks(const Konst<R>&);
 template <class R> int launch_step_begin(const Dev<R>&, const Konst<R>&, const Series*, int, cudaStream_t, Prof*);
 template <class R> int launch_ubnd(const Dev<R>&, const Konst<R>&, const Series*, cudaStream_t, Prof*);
@@ -327,7 +327,9 @@ struct Handle : public xbg_handle {
     // flow: momentum steps in one pass (variant 1) or two (variant 0)
     int flow_variant = XBG_FLOW_VARIANT_DEFAULT;
     // the pointwise passes in 32 x 8 (variant 0) or 64 x 4 (variant 1) blocks,
-    // or (variant 2) row segments of 16-byte loads where a pass has that form
+    // or (variant 2, the default where nx is a multiple of the segment width)
+    // row segments of 16-byte loads where a pass has that form (the first
+    // flow and sediment passes; the others take 32 x 8 blocks)
     int tile_variant = 0;
     bool wide() const { return tile_variant == 1; }
     bool vec() const { return tile_variant == 2; }
@@ -410,6 +412,8 @@ struct Handle : public xbg_handle {
         }
         if (wave_prepare(K)) return XBG_ERR_CUDA;
         maps_ok = K.wci == (R)0 && wave_maps_make(S, K, &maps) == 0;
+        // the row-segment passes where the rows split into whole segments
+        tile_variant = K.nx % (sizeof(R) == 4 ? 4 : 2) == 0 ? 2 : 0;
         // reductions and clock
         int nflow = step_begin_blocks(K);
         nwave = wave_parts(K);
@@ -703,7 +707,7 @@ struct Handle : public xbg_handle {
             if (K.swave == 1) n += launch_wave(S, K, st, pf, nullptr, wave_maps(), wave_cpt(), wide());
         }
         if (K.flow == 1) n += launch_flow(S, K, st, pf, flow_variant == 1, wide(), vec());
-        if (P.sedtrans == 1) n += launch_sed(S, K, st, pf, wide());
+        if (P.sedtrans == 1) n += launch_sed(S, K, st, pf, wide(), vec());
         if (K.means) n += launch_means(S, K, st, pf);
         return n;
     }
@@ -751,7 +755,7 @@ struct Handle : public xbg_handle {
                 if (K.swave == 1) n = launch_wave(S, K, st, nullptr, nullptr, wave_maps(), wave_cpt(), wide());
                 break;
             case 4: if (K.flow == 1) n = launch_flow(S, K, st, nullptr, flow_variant == 1, wide(), vec()); break;
-            case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr, wide()); break;
+            case 5: if (P.sedtrans == 1) n = launch_sed(S, K, st, nullptr, wide(), vec()); break;
             case 6: n = launch_means(S, K, st, nullptr); break;
             default: return XBG_ERR_ARG;
         }
@@ -993,7 +997,7 @@ struct Handle : public xbg_handle {
                                                                     a, b, (R)((double)j / k), j == k ? 1 : 0);
                 n++;
                 if (K.flow == 1) n += launch_flow(S, K, st, nullptr, flow_variant == 1, wide(), vec());
-                if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr, wide());
+                if (P.sedtrans == 1) n += launch_sed(S, K, st, nullptr, wide(), vec());
                 n += launch_means(S, K, st, nullptr);
             }
             cudaError_t e = cudaStreamEndCapture(st, &seg_graph);

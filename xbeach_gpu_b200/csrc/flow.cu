@@ -115,65 +115,34 @@ __device__ __forceinline__ void b_flow_a(const Dev<R>& S, const Konst<R>& K, con
 }
 XBG_KERNELS(flow_a)
 
-// The same pass over row segments: each thread takes V consecutive cells of
-// one row (V = 4 in FP32, 2 in FP64) with one 16-byte load per field and row;
-// a warp is one row of 32 V cells, and the neighbours left and right of a
-// thread's segment come from the adjacent lanes (the first and last lane of
-// a warp load theirs).  The arithmetic is the scalar pass's (the same
-// functions), so the results are bit-identical.  Needs nx a multiple of V.
-template <class R> struct FlowVec;
-template <> struct FlowVec<float> { using T = float4; using I = int4; static constexpr int V = 4; };
-template <> struct FlowVec<double> { using T = double2; using I = int2; static constexpr int V = 2; };
-
+// The same pass over row segments (Seg: V cells of a row per thread, 16-byte
+// loads, neighbours by lane shuffles), with the scalar pass's arithmetic
+// (the same functions), so the results are bit-identical.
 template <class R>
-__global__ void __launch_bounds__(256) k_flow_a_v(Dev<R> S, Konst<R> K) {
-    using VT = typename FlowVec<R>::T;
-    using VI = typename FlowVec<R>::I;
-    constexpr int V = FlowVec<R>::V;
-    union U { VT v; R a[V]; };
-    union W { VI v; int a[V]; };
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 4 : 1) k_flow_a_v(Dev<R> S, Konst<R> K) {
+    using G = Seg<R>;
+    constexpr int V = G::V;
     const bool off = halted(S.clk);
     const int nx = K.nx, ny = K.ny;
     const int iy = blockIdx.y * blockDim.y + threadIdx.y;
     if (iy >= ny) return;   // the whole warp: a warp is one row
-    const int lane = threadIdx.x;
-    const int x0 = (blockIdx.x * blockDim.x + lane) * V;
-    const bool act = x0 < nx;
+    const G g(nx, blockIdx.x);
     const int ym = mm(iy), yp = pp(iy, ny);
-    auto row = [&](const R* f, int y) {
-        U u;
-        if (act) u.v = __ldg(reinterpret_cast<const VT*>(f + (size_t)y * nx + x0));
-        else
-            for (int k = 0; k < V; k++) u.a[k] = (R)0;
-        return u;
-    };
-    // the value left of the segment (mm: the cell itself at column 0) and
-    // right of it (pp: the cell itself at the last column)
-    auto left = [&](const U& u, const R* f, int y) -> R {
-        R w = __shfl_up_sync(0xffffffffu, u.a[V - 1], 1);
-        if (lane == 0 && act && x0 > 0) w = ld(f + (size_t)y * nx + x0 - 1);
-        return x0 > 0 ? w : u.a[0];
-    };
-    auto right = [&](const U& u, const R* f, int y) -> R {
-        R w = __shfl_down_sync(0xffffffffu, u.a[0], 1);
-        if (lane == 31 && act && x0 + V < nx) w = ld(f + (size_t)y * nx + x0 + V);
-        return x0 + V < nx ? w : u.a[V - 1];
-    };
-    const U h = row(S.f[HH], iy), hyp = row(S.f[HH], yp), hu = row(S.f[HU], iy), hv = row(S.f[HV], iy);
-    const U dr = row(S.f[DR], iy);
-    const R hr = right(h, S.f[HH], iy);
-    U u{}, uyp{}, uym{}, v{}, vym{};
+    const typename G::U h = g.row(S.f[HH], iy), hyp = g.row(S.f[HH], yp), hu = g.row(S.f[HU], iy),
+                        hv = g.row(S.f[HV], iy), dr = g.row(S.f[DR], iy);
+    const R hr = g.right(h, S.f[HH], iy);
+    typename G::U u{}, uyp{}, uym{}, v{}, vym{};
     R ul = 0, ulyp = 0, ulym = 0, vl = 0, vr = 0, vlym = 0, vrym = 0;
     const bool smago = K.usesmago == 1;   // uniform
     if (smago) {
         const R* uu = S.f[UU]; const R* vv = S.f[VV];
-        u = row(uu, iy); uyp = row(uu, yp); uym = row(uu, ym); v = row(vv, iy); vym = row(vv, ym);
-        ul = left(u, uu, iy); ulyp = left(uyp, uu, yp); ulym = left(uym, uu, ym);
-        vl = left(v, vv, iy); vr = right(v, vv, iy); vlym = left(vym, vv, ym); vrym = right(vym, vv, ym);
+        u = g.row(uu, iy); uyp = g.row(uu, yp); uym = g.row(uu, ym); v = g.row(vv, iy); vym = g.row(vv, ym);
+        ul = g.left(u, uu, iy); ulyp = g.left(uyp, uu, yp); ulym = g.left(uym, uu, ym);
+        vl = g.left(v, vv, iy); vr = g.right(v, vv, iy); vlym = g.left(vym, vv, ym); vrym = g.right(vym, vv, ym);
     }
     const R eps = K.eps;
-    U hum, hvm, nuh;
-    W wu, wv;
+    typename G::U hum, hvm, nuh;
+    typename G::W wu, wv;
 #pragma unroll
     for (int k = 0; k < V; k++) {
         const DepthMom<R> d = depthmom_of(K, h.a[k], k < V - 1 ? h.a[k + 1] : hr, hyp.a[k], hu.a[k], hv.a[k]);
@@ -193,13 +162,12 @@ __global__ void __launch_bounds__(256) k_flow_a_v(Dev<R> S, Konst<R> K) {
         wv.a[k] = d.wv;
     }
     loads_before_here();
-    if (off || !act) return;
-    const size_t i = (size_t)iy * nx + x0;
-    *reinterpret_cast<VI*>(S.wetu + i) = wu.v;
-    *reinterpret_cast<VT*>(S.f[HUM] + i) = hum.v;
-    *reinterpret_cast<VI*>(S.wetv + i) = wv.v;
-    *reinterpret_cast<VT*>(S.f[HVM] + i) = hvm.v;
-    *reinterpret_cast<VT*>(S.tmp[T_NUH] + i) = nuh.v;
+    if (off || !g.act) return;
+    g.put(S.wetu, iy, wu);
+    g.put(S.f[HUM], iy, hum);
+    g.put(S.wetv, iy, wv);
+    g.put(S.f[HVM], iy, hvm);
+    g.put(S.tmp[T_NUH], iy, nuh);
 }
 
 // eulerustep (Flow_kernel.cu:1487-1544) at an interior-x cell, with the
@@ -782,8 +750,8 @@ int launch_flow(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, b
                 bool vec) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
     dim3 bp = wide ? dim3(64, 4) : b, gp = wide ? dim3((K.nx + 63) / 64, (K.ny + 3) / 4) : g;
-    if (vec && K.nx % FlowVec<R>::V == 0) {
-        const int V = FlowVec<R>::V;
+    if (vec && K.nx % SegVec<R>::V == 0) {
+        const int V = SegVec<R>::V;
         k_flow_a_v<R><<<dim3((K.nx / V + 31) / 32, (K.ny + 7) / 8), dim3(32, 8), 0, st>>>(S, K);
     } else {
         k_flow_a<R><<<gp, bp, 0, st>>>(S, K);

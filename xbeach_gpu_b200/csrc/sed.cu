@@ -20,32 +20,28 @@ __device__ __forceinline__ bool sed_skip(const Clock* c) {
     return halted(c) || *((volatile const int*)&c->do_sed) == 0;
 }
 
+// longturb, Sbvr, Rvr, Erosus (Sediment_kernel.cu:27-531) of one cell from
+// its inputs: ueu_l is ueu of the left neighbour (mm), vev_b vev of the one
+// below (mm)
 template <class R>
-__device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
-    const Clock* clk = S.clk;
-    if (sed_skip(clk)) return;
-    const int nx = K.nx, ny = K.ny;
-    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
-    if (ix >= nx || iy >= ny) return;
-    int i = IDX(ix, iy), xm = mm(ix), ym = mm(iy);
-    R dtf = (R)clk->dt, Trep = (R)clk->Trep;
+struct SedAIn { R c, H, stdep, cfm, rol, dr, urms, rolth, dzsdt, hh, ueu_l, ueu, vev_b, vev; };
+template <class R>
+struct SedAOut { R rolth, ceqsg, ceqbg, Tsg, ua, facero; };
+template <class R>
+__device__ __forceinline__ SedAOut<R> sed_a_of(const Konst<R>& K, R dtf, R Trep, const SedAIn<R>& in) {
     R rho = K.rho, g = K.g, eps = K.eps;
-    R c = ld(S.f[CC_] + i);
-    // every input is loaded here, ahead of the branches below, so that the
-    // loads make one round trip to memory
-    const R Hi = ld(S.f[H] + i), stdep = ld(S.f[STDEP] + i), cfm = ld(S.f[CFM] + i), rol = ld(S.f[ROL] + i);
-    const R dri = ld(S.f[DR] + i), urms = ld(S.f[URMS] + i);
+    const R c = in.c, Hi = in.H, stdep = in.stdep, cfm = in.cfm, rol = in.rol, dri = in.dr, urms = in.urms;
     // longturb (Sediment_kernel.cu:27-164)
-    R rolth = ld(S.f[ROLTHICK] + i) + dtf * (DM<R>::fabs(ld(S.f[DZSDT] + i)) - K.beta * c);
+    R rolth = in.rolth + dtf * (DM<R>::fabs(in.dzsdt) - K.beta * c);
     rolth = DM<R>::fmax(rolth, (R)0.0f);
     // Sbvr (:167-326); kturb is 0 after longturb
     R zo = (R)0.006f, sedcal = (R)1.0f, bulk = (R)1.0f;
     R D50 = K.D50, D90 = K.D90;
     const R drhog = K.sed_drhog;
-    R hh = ld(S.f[HH] + i);
+    R hh = in.hh;
     R hhi = DM<R>::fmax(hh, (R)0.01f);
-    R ue = (R)(0.5 * (double)(ld(S.f[UEU] + IDX(xm, iy)) + ld(S.f[UEU] + i)));
-    R ve = (R)(0.5 * (double)(ld(S.f[VEV] + IDX(ix, ym)) + ld(S.f[VEV] + i)));
+    R ue = (R)(0.5 * (double)(in.ueu_l + in.ueu));
+    R ve = (R)(0.5 * (double)(in.vev_b + in.vev));
     R vmags = ue * ue + ve * ve;
     R ML = DM<R>::fmax(DM<R>::fmin(DM<R>::sqrt((R)2.0f * rol * Trep / (rho * c)), hhi), (R)0.01f);
     R dcfin = DM<R>::exp(DM<R>::fmin(hhi, (R)100.0f) / ML);
@@ -90,17 +86,73 @@ __device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, cons
     {
         R exp_ero = K.morfac * dtf / ((R)1.0f - K.por) * hh * (ceqsg * (R)1.0f / Tsg + ceqbg * (R)1.0f / dtf);
         R facero = DM<R>::fmin((R)1.0f, stdep * (R)1.0f / DM<R>::fmax((R)0.000001f, exp_ero));
-        // all stores after all loads (the field pointers may alias as far as the compiler knows)
-        S.f[ROLTHICK][i] = rolth;
-        S.f[KTURB][i] = (R)0.0f;
-        S.f[CEQSG][i] = ceqsg;
-        S.tmp[T_CEQBG][i] = ceqbg;
-        S.tmp[T_TSG][i] = Tsg;
-        S.tmp[T_UA][i] = ua;
-        S.tmp[T_FACERO][i] = facero;
+        return SedAOut<R>{rolth, ceqsg, ceqbg, Tsg, ua, facero};
     }
 }
+
+template <class R>
+__device__ __forceinline__ void b_sed_a(const Dev<R>& S, const Konst<R>& K, const int bix, const int biy) {
+    const Clock* clk = S.clk;
+    if (sed_skip(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    int ix = bix * blockDim.x + threadIdx.x, iy = biy * blockDim.y + threadIdx.y;
+    if (ix >= nx || iy >= ny) return;
+    int i = IDX(ix, iy), xm = mm(ix), ym = mm(iy);
+    const R dtf = (R)clk->dt, Trep = (R)clk->Trep;
+    // every input is loaded here, ahead of the arithmetic's branches, so that
+    // the loads make one round trip to memory
+    const SedAIn<R> in{ld(S.f[CC_] + i), ld(S.f[H] + i), ld(S.f[STDEP] + i), ld(S.f[CFM] + i), ld(S.f[ROL] + i),
+                       ld(S.f[DR] + i), ld(S.f[URMS] + i), ld(S.f[ROLTHICK] + i), ld(S.f[DZSDT] + i),
+                       ld(S.f[HH] + i), ld(S.f[UEU] + IDX(xm, iy)), ld(S.f[UEU] + i), ld(S.f[VEV] + IDX(ix, ym)),
+                       ld(S.f[VEV] + i)};
+    const SedAOut<R> o = sed_a_of(K, dtf, Trep, in);
+    S.f[ROLTHICK][i] = o.rolth;
+    S.f[KTURB][i] = (R)0.0f;
+    S.f[CEQSG][i] = o.ceqsg;
+    S.tmp[T_CEQBG][i] = o.ceqbg;
+    S.tmp[T_TSG][i] = o.Tsg;
+    S.tmp[T_UA][i] = o.ua;
+    S.tmp[T_FACERO][i] = o.facero;
+}
 XBG_KERNELS(sed_a)
+
+// The same pass over row segments (Seg), with the same arithmetic.
+template <class R>
+__global__ void __launch_bounds__(256) k_sed_a_v(Dev<R> S, Konst<R> K) {
+    using G = Seg<R>;
+    constexpr int V = G::V;
+    const Clock* clk = S.clk;
+    if (sed_skip(clk)) return;
+    const int nx = K.nx, ny = K.ny;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    if (iy >= ny) return;   // the whole warp: a warp is one row
+    const G g(nx, blockIdx.x);
+    const int ym = mm(iy);
+    const R dtf = (R)clk->dt, Trep = (R)clk->Trep;
+    const typename G::U c = g.row(S.f[CC_], iy), Hs = g.row(S.f[H], iy), sd = g.row(S.f[STDEP], iy),
+                        cf = g.row(S.f[CFM], iy), ro = g.row(S.f[ROL], iy), dr = g.row(S.f[DR], iy),
+                        ur = g.row(S.f[URMS], iy), rt = g.row(S.f[ROLTHICK], iy), dz = g.row(S.f[DZSDT], iy),
+                        hh = g.row(S.f[HH], iy), ue = g.row(S.f[UEU], iy), vb = g.row(S.f[VEV], ym),
+                        ve = g.row(S.f[VEV], iy);
+    const R uel = g.left(ue, S.f[UEU], iy);
+    typename G::U o_rt, o_cs, o_cb, o_ts, o_ua, o_fe, zero;
+#pragma unroll
+    for (int k = 0; k < V; k++) {
+        const SedAIn<R> in{c.a[k], Hs.a[k], sd.a[k], cf.a[k], ro.a[k], dr.a[k], ur.a[k], rt.a[k], dz.a[k], hh.a[k],
+                           k > 0 ? ue.a[k - 1] : uel, ue.a[k], vb.a[k], ve.a[k]};
+        const SedAOut<R> o = sed_a_of(K, dtf, Trep, in);
+        o_rt.a[k] = o.rolth; o_cs.a[k] = o.ceqsg; o_cb.a[k] = o.ceqbg; o_ts.a[k] = o.Tsg; o_ua.a[k] = o.ua;
+        o_fe.a[k] = o.facero; zero.a[k] = (R)0.0f;
+    }
+    if (!g.act) return;
+    g.put(S.f[ROLTHICK], iy, o_rt);
+    g.put(S.f[KTURB], iy, zero);
+    g.put(S.f[CEQSG], iy, o_cs);
+    g.put(S.tmp[T_CEQBG], iy, o_cb);
+    g.put(S.tmp[T_TSG], iy, o_ts);
+    g.put(S.tmp[T_UA], iy, o_ua);
+    g.put(S.tmp[T_FACERO], iy, o_fe);
+}
 
 // Susp (Sediment_kernel.cu:534-719): suspended fluxes Sus, Svs at (ix, iy)
 template <class R>
@@ -381,11 +433,14 @@ __device__ __forceinline__ void b_sed_c(const Dev<R>& S, const Konst<R>& K, cons
 }
 XBG_KERNELS(sed_c)
 
-// wide: the pointwise first pass in 64 x 4 blocks instead of 32 x 8
+// wide: the pointwise first pass in 64 x 4 blocks instead of 32 x 8; vec: over
+// row segments (where nx is a multiple of the segment width)
 template <class R>
-int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool wide) {
+int launch_sed(const Dev<R>& S, const Konst<R>& K, cudaStream_t st, Prof* pf, bool wide, bool vec) {
     dim3 b(32, 8), g((K.nx + 31) / 32, (K.ny + 7) / 8);
-    if (wide) k_sed_a<R><<<dim3((K.nx + 63) / 64, (K.ny + 3) / 4), dim3(64, 4), 0, st>>>(S, K);
+    constexpr int V = SegVec<R>::V;
+    if (vec && K.nx % V == 0) k_sed_a_v<R><<<dim3((K.nx / V + 31) / 32, (K.ny + 7) / 8), b, 0, st>>>(S, K);
+    else if (wide) k_sed_a<R><<<dim3((K.nx + 63) / 64, (K.ny + 3) / 4), dim3(64, 4), 0, st>>>(S, K);
     else k_sed_a<R><<<g, b, 0, st>>>(S, K);
     PMARK(pf, "k_sed_a");
     k_sed_b<R><<<g, b, 0, st>>>(S, K);
@@ -412,7 +467,7 @@ int launch_sed_batch(const BatchTab<R>& T, const BatchLaunch& L, cudaStream_t st
 template int launch_sed_batch<float>(const BatchTab<float>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
 template int launch_sed_batch<double>(const BatchTab<double>&, const BatchLaunch&, cudaStream_t, Prof*, bool);
 
-template int launch_sed<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool);
-template int launch_sed<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool);
+template int launch_sed<float>(const Dev<float>&, const Konst<float>&, cudaStream_t, Prof*, bool, bool);
+template int launch_sed<double>(const Dev<double>&, const Konst<double>&, cudaStream_t, Prof*, bool, bool);
 
 }  // namespace xbg

@@ -288,6 +288,53 @@ __device__ __forceinline__ Pair2<R> zz_min(const A& a, int x0, int x1, int y0, i
     return m;
 }
 
+// Row segments: a thread takes V consecutive cells of one row (V = 4 in
+// FP32, 2 in FP64) with one 16-byte load per field and row, and a warp one
+// row of 32 V cells; the cells left and right of a thread's segment come from
+// the adjacent lanes (the first and last lane of a warp load theirs), and
+// mm()/pp() clamping at the grid's edges gives the segment's own end cell.
+// Needs nx a multiple of V (row starts 16-byte aligned).  Every lane of a
+// warp takes part in the shuffles, including lanes past the row's end.
+template <class R> struct SegVec;
+template <> struct SegVec<float> { using T = float4; using I = int4; static constexpr int V = 4; };
+template <> struct SegVec<double> { using T = double2; using I = int2; static constexpr int V = 2; };
+template <class R>
+struct Seg {
+    using VT = typename SegVec<R>::T;
+    using VI = typename SegVec<R>::I;
+    static constexpr int V = SegVec<R>::V;
+    union U { VT v; R a[V]; };
+    union W { VI v; int a[V]; };
+    int nx, x0, lane;
+    bool act;   // the segment lies in the row
+    __device__ __forceinline__ Seg(int nx_, int bx) : nx(nx_), lane((int)threadIdx.x) {
+        x0 = (bx * (int)blockDim.x + lane) * V;
+        act = x0 < nx;
+    }
+    __device__ __forceinline__ size_t at(int y) const { return (size_t)y * nx + x0; }
+    __device__ __forceinline__ U row(const R* f, int y) const {
+        U u;
+        if (act) u.v = __ldg(reinterpret_cast<const VT*>(f + at(y)));
+        else
+            for (int k = 0; k < V; k++) u.a[k] = (R)0;
+        return u;
+    }
+    // the cell left of the segment (mm: the segment's first cell at column 0)
+    __device__ __forceinline__ R left(const U& u, const R* f, int y) const {
+        R w = __shfl_up_sync(0xffffffffu, u.a[V - 1], 1);
+        if (lane == 0 && act && x0 > 0) w = __ldg(f + at(y) - 1);
+        return x0 > 0 ? w : u.a[0];
+    }
+    // the cell right of the segment (pp: the segment's last cell at column nx-1)
+    __device__ __forceinline__ R right(const U& u, const R* f, int y) const {
+        R w = __shfl_down_sync(0xffffffffu, u.a[0], 1);
+        if (lane == 31 && act && x0 + V < nx) w = __ldg(f + at(y) + V);
+        return x0 + V < nx ? w : u.a[V - 1];
+    }
+    __device__ __forceinline__ void put(R* f, int y, const U& u) const { *reinterpret_cast<VT*>(f + at(y)) = u.v; }
+    __device__ __forceinline__ void put(int* f, int y, const W& w) const { *reinterpret_cast<VI*>(f + at(y)) = w.v; }
+};
+
 // ---------------------------------------------------------------- batches
 // A batch advances many scenarios (each with its own grid, parameters, clock
 // and dt) with one launch per kernel of the step.  Each kernel is a body
